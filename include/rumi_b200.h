@@ -1,0 +1,199 @@
+/* rumi_b200.h -- C-ABI of the B200 rendering path for Rumi-Renderer scenes.
+ *
+ * The reference renders with Scene::Rendering (src/Scene/scene.cpp:206-258), which calls
+ * Integrator::Trace(w, h, camera, film) (src/Integrator/integrator.h:15-28) once per pixel
+ * sample and sums the results into Film's float buffer (src/Camera/film.cpp:83-97).  This
+ * library replaces that loop and the integrators beneath it with GPU kernels:
+ *
+ *   rumi_scene_create   <- Scene::Build's objects + BVHAccel::BuildBVH
+ *                          (src/Scene/scene.cpp:135-204, src/Acceleration/bvh.cpp:129-148)
+ *   rumi_render         <- Scene::Rendering + PathTracer::Trace / BidirectionalPathTracer::Trace
+ *                          (src/Integrator/pathtracer.cpp:117-354,
+ *                           src/Integrator/bidirectionalpathtracer.cpp:121-394)
+ *   rumi_trace_rays     <- BVHAccel::Travel (src/Acceleration/bvh.cpp:150-213), closest-hit
+ *                          (isect != NULL) and shadow (isect == NULL) forms
+ *
+ * Conventions
+ *   - Every entry point returns rumi_status; nothing throws across the ABI.  The text of
+ *     the last error of the calling thread is available from rumi_last_error_string().
+ *   - Colours are given as (r, g, b) like the reference's Color(r, g, b) constructor.
+ *     Film buffers are H*W*3 floats in the reference's B,G,R storage order
+ *     (src/Kernel/color.h:7-9), row h, column w at ((h * W) + w) * 3 -- the same layout as
+ *     Film::_pixel_buffer -- and hold the SUM of the samples of each pixel.
+ *   - rumi_scene_create copies everything it is given; the caller's arrays may be freed
+ *     on return.  Output buffers belong to the caller.
+ *   - A rumi_scene may be used by one host thread at a time.  Calls are synchronous
+ *     unless noted: they return once results are in the caller's buffer.
+ *   - The library allocates device memory with cudaMalloc on the current CUDA device.
+ */
+#ifndef RUMI_B200_H
+#define RUMI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    RUMI_OK = 0,
+    RUMI_ERR_INVALID_ARG = 1,
+    RUMI_ERR_OOM = 2,
+    RUMI_ERR_CUDA = 3,
+    RUMI_ERR_QUEUE_OVERFLOW = 4,
+    RUMI_ERR_TIMEOUT = 5,
+    RUMI_ERR_INTERNAL = 6
+} rumi_status;
+
+/* material kinds (the reference's Material subclasses, src/Material/) */
+enum {
+    RUMI_MAT_MATTE = 0,      /* Matte(kd, rgb)                                 matte.cpp:27-31   */
+    RUMI_MAT_GLOSSY = 1,     /* Glossy(kd, ks, e, rgb)                         glossy.cpp:19-25  */
+    RUMI_MAT_SPECULAR = 2,   /* Specular(kr, rgb)                              specular.cpp:18-23 */
+    RUMI_MAT_EMISSIVE = 3,   /* Emissive(ls, rgb)                              emissive.cpp:17-23 */
+    RUMI_MAT_DIELECTRIC = 4, /* Dielectric(eta_in, eta_out, absorption)        dielectric.cpp:18-23 */
+    RUMI_MAT_SUBSURFACE = 5  /* Subsurface(eta_in, eta_out, sigma_s, sigma_a, density) subsurface.cpp:21-40 */
+};
+
+typedef struct {
+    int32_t type;
+    float kd;        /* Matte kd, Glossy kd, Specular kr, Emissive ls */
+    float ks;        /* Glossy ks */
+    float exponent;  /* Glossy Phong exponent e */
+    float rgb[3];    /* colour; Dielectric absorption; Subsurface sigma_s */
+    float eta_in, eta_out;
+    float rgb2[3];   /* Subsurface sigma_a */
+    float density;   /* Subsurface density (1 = none) */
+} rumi_material;
+
+enum { RUMI_SHAPE_TRIANGLE = 0, RUMI_SHAPE_RECT = 1, RUMI_SHAPE_SPHERE = 2 };
+enum { RUMI_LIGHT_AREA = 0, RUMI_LIGHT_SPOT = 1 };
+
+typedef struct {
+    int32_t type;         /* RUMI_LIGHT_AREA: AreaLight(shape) (src/Light/arealight.cpp);
+                             RUMI_LIGHT_SPOT: point emitter with a cone (no reference
+                             counterpart) */
+    int32_t shape_type;   /* area light: RUMI_SHAPE_RECT or RUMI_SHAPE_SPHERE */
+    int32_t shape_index;  /* area light: index within that shape array */
+    float position[3];    /* spot */
+    float direction[3];   /* spot, unit */
+    float cone_deg;       /* spot half-angle */
+    float intensity[3];   /* spot */
+} rumi_light;
+
+typedef struct {
+    int32_t present;
+    float pmin[3], pmax[3];   /* HomogeneousVolume(BBox(pmin, pmax), sigma_s, sigma_a) */
+    float sigma_s[3], sigma_a[3];
+    float g;                  /* Henyey-Greenstein asymmetry; 0 = the reference's Isotropic */
+} rumi_volume;
+
+typedef struct {
+    float position[3];
+    float basis[16];      /* Pinhole::_basis_transform, row-major */
+    float y_ratio;        /* Pinhole y_ratio (1 / Film aspect in the reference presets) */
+    float fov_deg;        /* Pinhole::_fov (the reference constructor fixes 20) */
+} rumi_camera;
+
+typedef struct {
+    int32_t width, height;
+
+    int32_t n_triangles;
+    const float *tri_vertices;    /* n*9: v0, v1, v2 */
+    const float *tri_normals;     /* n*9: n0, n1, n2 (Triangle::Normal); NULL = face normal */
+    const int32_t *tri_material;  /* n material indices */
+    const float *tri_albedo;      /* n*3 per-triangle colour overriding the material's rgb; may be NULL */
+
+    int32_t n_rects;
+    const float *rects;           /* n*9: p, l, w  (Rect(p, l, w)) */
+    const int32_t *rect_material;
+
+    int32_t n_spheres;
+    const float *spheres;         /* n*4: centre, radius */
+    const int32_t *sphere_material;
+
+    int32_t n_materials;
+    const rumi_material *materials;
+
+    int32_t n_lights;
+    const rumi_light *lights;
+
+    rumi_volume volume;
+    rumi_camera camera;
+} rumi_scene_desc;
+
+typedef struct rumi_scene rumi_scene;
+
+enum { RUMI_PATH_TRACER = 0, RUMI_BDPT = 1 };
+enum { RUMI_FLAG_TIMING = 1 };
+
+typedef struct {
+    int32_t integrator;    /* RUMI_PATH_TRACER (PathTracer(scene, max_depth)) or RUMI_BDPT */
+    int32_t max_depth;     /* path tracer: vertices per path */
+    int32_t n_light;       /* BDPT nL (light subpath vertices) */
+    int32_t n_eye;         /* BDPT nE (eye subpath vertices) */
+    int32_t spp;           /* samples per pixel, rendered exactly */
+    uint64_t seed;         /* Philox key: same seed -> same image */
+    int32_t wave_paths;    /* paths in flight per wave; 0 = library default */
+    int32_t flags;         /* RUMI_FLAG_TIMING: per-kernel CUDA-event timing into stats */
+    void *stream;          /* cudaStream_t, NULL = the library's own stream */
+} rumi_render_params;
+
+typedef struct {
+    int64_t paths;               /* camera paths traced */
+    int64_t nan_samples;         /* samples dropped for NaN (counted, as the reference does) */
+    int64_t extend_launches;     /* closest-hit launches */
+    double extend_ms;            /* summed device time of closest-hit launches (TIMING) */
+    int64_t shade_launches;
+    double shade_ms;
+    int64_t shadow_launches;
+    double shadow_ms;
+    double total_ms;             /* device time of the whole render (TIMING) */
+    int64_t rays_extend;         /* closest-hit rays traced (TIMING) */
+    int64_t rays_shadow;         /* shadow rays traced (TIMING) */
+} rumi_render_stats;
+
+typedef struct {
+    int32_t large_levels;
+    int32_t small_tasks;
+    int32_t n_nodes;             /* node slots reserved */
+    double build_ms;
+} rumi_bvh_info;
+
+/* Creates a scene on the current device: copies the description, builds the BVH on the
+ * GPU.  *out receives the scene or NULL on error. */
+rumi_status rumi_scene_create(const rumi_scene_desc *desc, rumi_scene **out);
+
+/* Releases every device allocation of the scene. */
+rumi_status rumi_scene_destroy(rumi_scene *scene);
+
+/* Information about the scene's BVH build. */
+rumi_status rumi_scene_bvh_info(const rumi_scene *scene, rumi_bvh_info *info);
+
+/* Renders one frame: film receives H*W*3 floats (B,G,R sums of `spp` samples per pixel).
+ * film_on_device != 0: film is a device pointer (no host copy).  stats may be NULL. */
+rumi_status rumi_render(rumi_scene *scene, const rumi_render_params *params, float *film, int32_t film_on_device,
+                        rumi_render_stats *stats);
+
+/* Ray queries against the scene's BVH.  rays: n*8 floats (o.xyz, in_object flag as
+ * 0/1, d.xyz, tmax).  anyhit = 0: closest hit -> t (0 = miss, the reference's
+ * Ray::_tmin after Travel) and prim (canonical primitive id, -1 = miss).  anyhit = 1:
+ * occlusion -> prim 1 when something lies in [1e-4, tmax - 1e-4], else 0.
+ * on_device != 0: all pointers are device pointers.  node_visits / prim_tests (may be
+ * NULL): summed 32-byte node fetches and primitive tests over the batch. */
+rumi_status rumi_trace_rays(rumi_scene *scene, int64_t n, const float *rays, int32_t anyhit, float *t,
+                            int32_t *prim, int32_t on_device, int64_t *node_visits, int64_t *prim_tests,
+                            void *stream);
+
+/* Text of the calling thread's last error ("" if none). */
+const char *rumi_last_error_string(void);
+
+/* Library version string. */
+const char *rumi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RUMI_B200_H */

@@ -1,0 +1,440 @@
+// C-ABI entry points (include/rumi_b200.h): scene upload + BVH build, render, ray
+// queries, errors.  Derived constants are computed the way the reference's constructors
+// compute them, in float (double where the reference mixes in its double PI):
+//   Rect          src/Shape/rect.cpp:12-38          Sphere  src/Shape/sphere.cpp:18-38
+//   Glossy        src/Material/glossy.cpp:19-25      Subsurface src/Material/subsurface.cpp:21-40
+//   HomogeneousVolume src/Volume/homogeneousvolume.cpp:24-44
+//   Pinhole       src/Camera/pinhole.cpp:30-51
+#include "renderer.h"
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <chrono>
+
+static thread_local std::string g_last_error;
+
+namespace rumi {
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+rumi_status cuda_status(cudaError_t e, const char *what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? RUMI_ERR_OOM : RUMI_ERR_CUDA;
+}
+
+rumi_status ensure_workspace(rumi_scene *sc, size_t bytes) {
+    if (sc->ws_bytes >= bytes) return RUMI_OK;
+    if (sc->ws) {
+        cudaStreamSynchronize(sc->stream);
+        cudaFree(sc->ws);
+        sc->ws = nullptr;
+        sc->ws_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&sc->ws, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_status(e, "workspace allocation");
+    }
+    sc->ws_bytes = bytes;
+    return RUMI_OK;
+}
+
+}  // namespace rumi
+
+using namespace rumi;
+
+namespace {
+
+template <typename T>
+rumi_status upload(T **dst, const void *src, size_t bytes, cudaStream_t s) {
+    *dst = nullptr;
+    if (bytes == 0) return RUMI_OK;
+    cudaError_t e = cudaMalloc((void **)dst, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_status(e, "cudaMalloc");
+    }
+    e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMemcpyAsync");
+    return RUMI_OK;
+}
+
+float f_len(const float *v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+void free_scene(rumi_scene *sc) {
+    if (!sc) return;
+    if (sc->stream) cudaStreamSynchronize(sc->stream);
+    cudaFree(sc->nodes);
+    cudaFree(sc->leaf_prims);
+    cudaFree(sc->tri_shade);
+    cudaFree(sc->tri_albedo);
+    cudaFree(sc->rects);
+    cudaFree(sc->spheres);
+    cudaFree(sc->sphere_mat);
+    cudaFree(sc->materials);
+    cudaFree(sc->lights);
+    cudaFree(sc->ws);
+    if (sc->stream) cudaStreamDestroy(sc->stream);
+    delete sc;
+}
+
+rumi_status validate(const rumi_scene_desc *d) {
+    if (!d) return set_error("desc is NULL"), RUMI_ERR_INVALID_ARG;
+    if (d->width <= 0 || d->height <= 0) return set_error("film size must be positive"), RUMI_ERR_INVALID_ARG;
+    if (d->n_triangles < 0 || d->n_rects < 0 || d->n_spheres < 0 || d->n_materials < 0 || d->n_lights < 0)
+        return set_error("negative count"), RUMI_ERR_INVALID_ARG;
+    if ((long long)d->n_triangles + d->n_rects + d->n_spheres > 0x3fffffffLL)
+        return set_error("too many primitives"), RUMI_ERR_INVALID_ARG;
+    if (d->n_triangles > 0 && (!d->tri_vertices || !d->tri_material))
+        return set_error("triangle arrays missing"), RUMI_ERR_INVALID_ARG;
+    if (d->n_rects > 0 && (!d->rects || !d->rect_material)) return set_error("rect arrays missing"), RUMI_ERR_INVALID_ARG;
+    if (d->n_spheres > 0 && (!d->spheres || !d->sphere_material))
+        return set_error("sphere arrays missing"), RUMI_ERR_INVALID_ARG;
+    if (d->n_materials > 0 && !d->materials) return set_error("materials missing"), RUMI_ERR_INVALID_ARG;
+    if (d->n_lights > 0 && !d->lights) return set_error("lights missing"), RUMI_ERR_INVALID_ARG;
+    auto check_mat = [&](const int32_t *m, int n) -> bool {
+        for (int i = 0; i < n; ++i)
+            if (m[i] < 0 || m[i] >= d->n_materials) return false;
+        return true;
+    };
+    if (!check_mat(d->tri_material, d->n_triangles) || !check_mat(d->rect_material, d->n_rects) ||
+        !check_mat(d->sphere_material, d->n_spheres))
+        return set_error("material index out of range"), RUMI_ERR_INVALID_ARG;
+    for (int i = 0; i < d->n_materials; ++i)
+        if (d->materials[i].type < RUMI_MAT_MATTE || d->materials[i].type > RUMI_MAT_SUBSURFACE)
+            return set_error("unknown material type"), RUMI_ERR_INVALID_ARG;
+    for (int i = 0; i < d->n_lights; ++i) {
+        const rumi_light &L = d->lights[i];
+        if (L.type == RUMI_LIGHT_AREA) {
+            if (L.shape_type == RUMI_SHAPE_RECT && (L.shape_index < 0 || L.shape_index >= d->n_rects))
+                return set_error("light rect index out of range"), RUMI_ERR_INVALID_ARG;
+            if (L.shape_type == RUMI_SHAPE_SPHERE && (L.shape_index < 0 || L.shape_index >= d->n_spheres))
+                return set_error("light sphere index out of range"), RUMI_ERR_INVALID_ARG;
+            if (L.shape_type != RUMI_SHAPE_RECT && L.shape_type != RUMI_SHAPE_SPHERE)
+                return set_error("area lights must be rects or spheres"), RUMI_ERR_INVALID_ARG;
+        } else if (L.type != RUMI_LIGHT_SPOT) {
+            return set_error("unknown light type"), RUMI_ERR_INVALID_ARG;
+        }
+    }
+    return RUMI_OK;
+}
+
+DevMaterial make_material(const rumi_material &m) {
+    DevMaterial d;
+    memset(&d, 0, sizeof(d));
+    d.type = m.type;
+    d.kd = m.kd;
+    d.ks = m.ks;
+    d.e = m.exponent;
+    d.rgb = make_float3(m.rgb[0], m.rgb[1], m.rgb[2]);
+    d.eta_in = m.eta_in;
+    d.eta_out = m.eta_out;
+    d.rgb2 = make_float3(m.rgb2[0], m.rgb2[1], m.rgb2[2]);
+    if (m.type == RUMI_MAT_GLOSSY) {
+        d.kd_pdf = m.kd / (m.kd + m.ks);
+        d.phong_norm = (float)((m.exponent + 1.0f) / (2.0f * 3.14159265358979323846));
+    }
+    if (m.type == RUMI_MAT_SUBSURFACE) {
+        const float st[3] = {m.rgb[0] + m.rgb2[0], m.rgb[1] + m.rgb2[1], m.rgb[2] + m.rgb2[2]};
+        d.sigma_t = make_float3(st[0], st[1], st[2]);
+        const float density = m.density > 0.0f ? m.density : 1.0f;
+        d.avg_sigma_t = (st[2] + st[1] + st[0]) / 3.0f * density;
+        d.absorb = ((m.rgb2[2] / st[2]) + (m.rgb2[1] / st[1]) + (m.rgb2[0] / st[0])) / 3.0f;
+    }
+    if (m.type == RUMI_MAT_EMISSIVE) d.le = make_float3(m.rgb[0] * m.kd, m.rgb[1] * m.kd, m.rgb[2] * m.kd);
+    return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *rumi_last_error_string(void) { return g_last_error.c_str(); }
+
+const char *rumi_version(void) { return "rumi_b200 0.1 (sm_100a)"; }
+
+rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
+    if (!out) return set_error("out is NULL"), RUMI_ERR_INVALID_ARG;
+    *out = nullptr;
+    rumi_status st = validate(d);
+    if (st != RUMI_OK) return st;
+    rumi_scene *sc = new rumi_scene();
+    cudaGetDevice(&sc->device);
+    cudaDeviceGetAttribute(&sc->num_sms, cudaDevAttrMultiProcessorCount, sc->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete sc;
+        return cuda_status(e, "cudaStreamCreate");
+    }
+    cudaStream_t s = sc->stream;
+    const int nT = d->n_triangles, nR = d->n_rects, nS = d->n_spheres;
+    const int N = nT + nR + nS;
+    // ---- shading data (canonical order)
+    std::vector<float4> tri_shade((size_t)nT * 3);
+    for (int i = 0; i < nT; ++i) {
+        const float *v = d->tri_vertices + 9 * (size_t)i;
+        float n[9];
+        if (d->tri_normals) {
+            memcpy(n, d->tri_normals + 9 * (size_t)i, sizeof(n));
+        } else {  // Normalize(Cross(v1 - v0, v2 - v0))
+            const float e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+            const float e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+            const float c[3] = {e1[1] * e2[2] - e2[1] * e1[2], e1[2] * e2[0] - e2[2] * e1[0],
+                                e1[0] * e2[1] - e2[0] * e1[1]};
+            const float inv = 1.0f / std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+            for (int k = 0; k < 3; ++k) n[3 * k] = c[0] * inv, n[3 * k + 1] = c[1] * inv, n[3 * k + 2] = c[2] * inv;
+        }
+        int mi = d->tri_material[i];
+        float mif;
+        memcpy(&mif, &mi, 4);
+        tri_shade[3 * (size_t)i + 0] = make_float4(n[0], n[1], n[2], mif);
+        tri_shade[3 * (size_t)i + 1] = make_float4(n[3], n[4], n[5], 0.0f);
+        tri_shade[3 * (size_t)i + 2] = make_float4(n[6], n[7], n[8], 0.0f);
+    }
+    std::vector<float4> tri_albedo;
+    if (d->tri_albedo) {
+        tri_albedo.resize(nT);
+        for (int i = 0; i < nT; ++i)
+            tri_albedo[i] = make_float4(d->tri_albedo[3 * i], d->tri_albedo[3 * i + 1], d->tri_albedo[3 * i + 2], 0.0f);
+    }
+    std::vector<float4> rects((size_t)nR * 3);
+    std::vector<int> rect_emissive(nR);
+    std::vector<DevMaterial> mats(d->n_materials);
+    for (int i = 0; i < d->n_materials; ++i) mats[i] = make_material(d->materials[i]);
+    for (int i = 0; i < nR; ++i) {
+        const float *r = d->rects + 9 * (size_t)i;
+        int mi = d->rect_material[i];
+        float mif;
+        memcpy(&mif, &mi, 4);
+        rects[3 * i + 0] = make_float4(r[0], r[1], r[2], mif);
+        rects[3 * i + 1] = make_float4(r[3], r[4], r[5], 0.0f);
+        rects[3 * i + 2] = make_float4(r[6], r[7], r[8], 0.0f);
+        const DevMaterial &m = mats[mi];
+        // Rect::Intersect's one-sided test keys on Le() != Color() (rect.cpp:80-81)
+        rect_emissive[i] = m.type == RUMI_MAT_EMISSIVE && (m.le.x != 0.0f || m.le.y != 0.0f || m.le.z != 0.0f);
+    }
+    std::vector<float4> spheres(nS);
+    for (int i = 0; i < nS; ++i)
+        spheres[i] = make_float4(d->spheres[4 * i], d->spheres[4 * i + 1], d->spheres[4 * i + 2], d->spheres[4 * i + 3]);
+    std::vector<DevLight> lights(d->n_lights);
+    for (int i = 0; i < d->n_lights; ++i) {
+        const rumi_light &L = d->lights[i];
+        DevLight &dl = lights[i];
+        memset(&dl, 0, sizeof(dl));
+        dl.type = L.type;
+        dl.shape_type = L.shape_type;
+        dl.shape_index = L.shape_index;
+        if (L.type == RUMI_LIGHT_AREA) {
+            int mi;
+            if (L.shape_type == RUMI_SHAPE_RECT) {
+                const float *r = d->rects + 9 * (size_t)L.shape_index;
+                const float len = f_len(r + 3), wid = f_len(r + 6);
+                dl.inv_area = 1.0f / (len * wid);
+                mi = d->rect_material[L.shape_index];
+            } else {
+                const float rad = d->spheres[4 * L.shape_index + 3];
+                dl.inv_area = (float)(1.0f / (4.0f * 3.14159265358979323846 * rad * rad));
+                mi = d->sphere_material[L.shape_index];
+            }
+            dl.le = mats[mi].le;
+        } else {
+            dl.position = make_float3(L.position[0], L.position[1], L.position[2]);
+            dl.direction = make_float3(L.direction[0], L.direction[1], L.direction[2]);
+            dl.cos_cone = (float)std::cos(L.cone_deg * 3.14159265358979323846 / 180.0);
+            dl.intensity = make_float3(L.intensity[0], L.intensity[1], L.intensity[2]);
+            dl.inv_area = 1.0f;
+        }
+    }
+    DevScene &ds = sc->dev;
+    memset(&ds, 0, sizeof(ds));
+    ds.width = d->width;
+    ds.height = d->height;
+    ds.n_tris = nT;
+    ds.n_rects = nR;
+    ds.n_spheres = nS;
+    ds.n_prims = N;
+    ds.n_materials = d->n_materials;
+    ds.n_lights = d->n_lights;
+    // volume
+    if (d->volume.present) {
+        const rumi_volume &v = d->volume;
+        DevVolume &dv = ds.volume;
+        dv.present = 1;
+        dv.bmin = make_float3(v.pmin[0], v.pmin[1], v.pmin[2]);
+        dv.bmax = make_float3(v.pmax[0], v.pmax[1], v.pmax[2]);
+        dv.sigma_s = make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]);
+        dv.sigma_a = make_float3(v.sigma_a[0], v.sigma_a[1], v.sigma_a[2]);
+        dv.sigma_t = make_float3(v.sigma_a[0] + v.sigma_s[0], v.sigma_a[1] + v.sigma_s[1], v.sigma_a[2] + v.sigma_s[2]);
+        dv.avg_sigma_t = (dv.sigma_t.z + dv.sigma_t.y + dv.sigma_t.x) * 0.33333333333f;
+        const float3 r = make_float3(dv.sigma_a.x / dv.sigma_t.x, dv.sigma_a.y / dv.sigma_t.y, dv.sigma_a.z / dv.sigma_t.z);
+        dv.absorb = (r.z + r.y + r.x) * 0.33333333333f;
+        dv.g = v.g;
+    }
+    // camera
+    {
+        const rumi_camera &c = d->camera;
+        DevCamera &dc = ds.camera;
+        dc.p = make_float3(c.position[0], c.position[1], c.position[2]);
+        for (int k = 0; k < 12; ++k) dc.m[k] = c.basis[k];
+        const float fov = c.fov_deg > 0.0f ? c.fov_deg : 20.0f;
+        dc.tanfov = (float)std::tan(3.14159265358979323846 / 180.f * fov * 0.5f);
+        dc.plane_dist = 1.0f;
+        dc.y_ratio = c.y_ratio;
+        dc.film_area = (2.0f * dc.tanfov) * (2.0f * dc.tanfov * c.y_ratio);
+        dc.dir = make_float3(c.basis[2] + c.basis[3], c.basis[6] + c.basis[7], c.basis[10] + c.basis[11]);
+    }
+    // ---- uploads
+    float *d_tri_v = nullptr;
+    int *d_rect_em = nullptr;
+    void *scratch = nullptr;
+    auto fail = [&](rumi_status code) {
+        cudaFree(d_tri_v);
+        cudaFree(d_rect_em);
+        cudaFree(scratch);
+        free_scene(sc);
+        return code;
+    };
+    if ((st = upload(&d_tri_v, d->tri_vertices, sizeof(float) * 9 * (size_t)nT, s)) != RUMI_OK) return fail(st);
+    if ((st = upload(&sc->tri_shade, tri_shade.data(), sizeof(float4) * tri_shade.size(), s)) != RUMI_OK)
+        return fail(st);
+    if (!tri_albedo.empty() &&
+        (st = upload(&sc->tri_albedo, tri_albedo.data(), sizeof(float4) * tri_albedo.size(), s)) != RUMI_OK)
+        return fail(st);
+    if ((st = upload(&sc->rects, rects.data(), sizeof(float4) * rects.size(), s)) != RUMI_OK) return fail(st);
+    if ((st = upload(&d_rect_em, rect_emissive.data(), sizeof(int) * rect_emissive.size(), s)) != RUMI_OK)
+        return fail(st);
+    if ((st = upload(&sc->spheres, spheres.data(), sizeof(float4) * spheres.size(), s)) != RUMI_OK) return fail(st);
+    if ((st = upload(&sc->sphere_mat, d->sphere_material, sizeof(int) * (size_t)nS, s)) != RUMI_OK) return fail(st);
+    if ((st = upload(&sc->materials, mats.data(), sizeof(DevMaterial) * mats.size(), s)) != RUMI_OK) return fail(st);
+    if ((st = upload(&sc->lights, lights.data(), sizeof(DevLight) * lights.size(), s)) != RUMI_OK) return fail(st);
+    // ---- BVH
+    sc->n_nodes = bvh_node_capacity(N);
+    e = cudaMalloc(&sc->nodes, sizeof(BvhNode) * (size_t)sc->n_nodes);
+    if (e != cudaSuccess) return fail(cuda_status(e, "cudaMalloc nodes"));
+    e = cudaMalloc(&sc->leaf_prims, sizeof(float4) * 3 * (size_t)(N > 0 ? N : 1));
+    if (e != cudaSuccess) return fail(cuda_status(e, "cudaMalloc prims"));
+    e = cudaMalloc(&scratch, bvh_scratch_bytes(N));
+    if (e != cudaSuccess) return fail(cuda_status(e, "cudaMalloc BVH scratch"));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    int rc = bvh_build(d_tri_v, nT, sc->rects, d_rect_em, nR, sc->spheres, nS, sc->nodes, sc->leaf_prims, scratch, s,
+                       &sc->info);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    sc->build_ms = ms;
+    if (rc != 0) {
+        if (rc > 0) return fail(cuda_status((cudaError_t)rc, "bvh_build"));
+        set_error("bvh_build: internal limit reached");
+        return fail(RUMI_ERR_INTERNAL);
+    }
+    cudaFree(d_tri_v);
+    d_tri_v = nullptr;
+    cudaFree(d_rect_em);
+    d_rect_em = nullptr;
+    cudaFree(scratch);
+    scratch = nullptr;
+    ds.nodes = sc->nodes;
+    ds.leaf_prims = sc->leaf_prims;
+    ds.tri_shade = sc->tri_shade;
+    ds.tri_albedo = sc->tri_albedo;
+    ds.rects = sc->rects;
+    ds.spheres = sc->spheres;
+    ds.sphere_mat = sc->sphere_mat;
+    ds.materials = sc->materials;
+    ds.lights = sc->lights;
+    ds.n_nodes = sc->n_nodes;
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(cuda_status(e, "scene upload"));
+    *out = sc;
+    return RUMI_OK;
+}
+
+rumi_status rumi_scene_destroy(rumi_scene *scene) {
+    free_scene(scene);
+    return RUMI_OK;
+}
+
+rumi_status rumi_scene_bvh_info(const rumi_scene *sc, rumi_bvh_info *info) {
+    if (!sc || !info) return set_error("NULL argument"), RUMI_ERR_INVALID_ARG;
+    info->large_levels = sc->info.large_levels;
+    info->small_tasks = sc->info.small_tasks;
+    info->n_nodes = sc->n_nodes;
+    info->build_ms = sc->build_ms;
+    return RUMI_OK;
+}
+
+rumi_status rumi_render(rumi_scene *sc, const rumi_render_params *p, float *film, int32_t film_on_device,
+                        rumi_render_stats *stats) {
+    if (!sc || !p || !film) return set_error("NULL argument"), RUMI_ERR_INVALID_ARG;
+    if (p->spp <= 0) return set_error("spp must be positive"), RUMI_ERR_INVALID_ARG;
+    cudaStream_t s = p->stream ? (cudaStream_t)p->stream : sc->stream;
+    const size_t film_bytes = sizeof(float) * 3 * (size_t)sc->dev.width * sc->dev.height;
+    float *film_dev = film;
+    float *tmp = nullptr;
+    if (!film_on_device) {
+        cudaError_t e = cudaMalloc(&tmp, film_bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return cuda_status(e, "cudaMalloc film");
+        }
+        film_dev = tmp;
+    }
+    rumi_status st;
+    if (p->integrator == RUMI_PATH_TRACER) {
+        if (p->max_depth <= 0) {
+            cudaFree(tmp);
+            return set_error("max_depth must be positive"), RUMI_ERR_INVALID_ARG;
+        }
+        st = pt_render(sc, p, film_dev, stats, s);
+    } else {
+        cudaFree(tmp);
+        return set_error("integrator not available"), RUMI_ERR_INVALID_ARG;
+    }
+    if (st == RUMI_OK && !film_on_device) {
+        cudaError_t e = cudaMemcpyAsync(film, film_dev, film_bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_status(e, "film copy");
+    }
+    cudaFree(tmp);
+    return st;
+}
+
+rumi_status rumi_trace_rays(rumi_scene *sc, int64_t n, const float *rays, int32_t anyhit, float *t, int32_t *prim,
+                            int32_t on_device, int64_t *node_visits, int64_t *prim_tests, void *stream) {
+    if (!sc || n < 0 || (n > 0 && (!rays || !t || !prim))) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    cudaStream_t s = stream ? (cudaStream_t)stream : sc->stream;
+    if (on_device) return trace_rays(sc, n, rays, anyhit, t, prim, node_visits, prim_tests, s);
+    float *dr = nullptr, *dt = nullptr;
+    int32_t *dp = nullptr;
+    rumi_status st = RUMI_OK;
+    cudaError_t e = cudaMalloc(&dr, sizeof(float) * 8 * (size_t)(n > 0 ? n : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&dt, sizeof(float) * (size_t)(n > 0 ? n : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&dp, sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        st = cuda_status(e, "cudaMalloc rays");
+    }
+    if (st == RUMI_OK) {
+        cudaMemcpyAsync(dr, rays, sizeof(float) * 8 * (size_t)n, cudaMemcpyHostToDevice, s);
+        st = trace_rays(sc, n, dr, anyhit, dt, dp, node_visits, prim_tests, s);
+    }
+    if (st == RUMI_OK) {
+        cudaMemcpyAsync(t, dt, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(prim, dp, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, s);
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_status(e, "trace copy");
+    }
+    cudaFree(dr);
+    cudaFree(dt);
+    cudaFree(dp);
+    return st;
+}
+
+}  // extern "C"

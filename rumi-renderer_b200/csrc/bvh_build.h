@@ -1,0 +1,22 @@
+// On-device SAH BVH builder (bvh_build.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include "scene.cuh"
+
+namespace rumi {
+
+struct BvhBuildInfo {
+    int large_levels;      // breadth-first levels of the large-task phase
+    int small_tasks;       // subtrees built by the warp-per-task phase
+    int node_capacity;     // entries reserved in the node array
+    int node_high_water;   // first unused index of the large-phase region
+};
+
+int bvh_node_capacity(int n_prims);
+size_t bvh_scratch_bytes(int n_prims);
+int bvh_build(const float *d_tri_v, int n_tris, const float4 *d_rects, const int *d_rect_emissive, int n_rects,
+              const float4 *d_spheres, int n_spheres, BvhNode *nodes, float4 *leaf_prims, void *scratch,
+              cudaStream_t stream, BvhBuildInfo *info);
+
+}  // namespace rumi

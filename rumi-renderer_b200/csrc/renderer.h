@@ -1,0 +1,43 @@
+// Host-side owner of a scene's device allocations and the render entry points.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include "../../include/rumi_b200.h"
+#include "scene.cuh"
+#include "bvh_build.h"
+
+struct rumi_scene {
+    DevScene dev;
+    // owned device allocations
+    BvhNode *nodes = nullptr;
+    float4 *leaf_prims = nullptr;
+    float4 *tri_shade = nullptr;
+    float4 *tri_albedo = nullptr;
+    float4 *rects = nullptr;
+    float4 *spheres = nullptr;
+    int *sphere_mat = nullptr;
+    DevMaterial *materials = nullptr;
+    DevLight *lights = nullptr;
+    int n_nodes = 0;
+    rumi::BvhBuildInfo info{};
+    double build_ms = 0.0;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int num_sms = 148;
+    // render workspace, grown on demand
+    void *ws = nullptr;
+    size_t ws_bytes = 0;
+};
+
+namespace rumi {
+
+void set_error(const std::string &msg);
+rumi_status cuda_status(cudaError_t e, const char *what);
+
+rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
+                      cudaStream_t stream);
+rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, float *t_dev, int32_t *prim_dev,
+                       int64_t *node_visits, int64_t *prim_tests, cudaStream_t stream);
+rumi_status ensure_workspace(rumi_scene *sc, size_t bytes);
+
+}  // namespace rumi

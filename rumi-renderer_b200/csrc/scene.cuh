@@ -1,0 +1,101 @@
+// Device-resident scene layout (one struct of pointers, passed by value to kernels).
+//
+// HBM layout (all arrays cudaMalloc'd by rumi_scene_create, 256-byte aligned):
+//   nodes      : BvhNode[n_nodes]        32 B each; siblings adjacent, pairs 64-B aligned
+//   leaf_prims : float4[3 * n_prims]     48 B per primitive, in BVH leaf order
+//   tri_shade  : float4[3 * n_tris]      shading normals n0,n1,n2 (canonical order);
+//                                        .w of the first holds the material index
+//   tri_albedo : float4[n_tris]          optional per-triangle Matte colour (rgb)
+//   rects      : float4[3 * n_rects]     p, l, w (.w of p = material index)
+//   spheres    : float4[n_spheres]       centre xyz, radius
+//   sphere_mat : int[n_spheres]
+//   materials  : DevMaterial[n_materials]
+//   lights     : DevLight[n_lights]
+#pragma once
+#include "common.cuh"
+
+// Primitive kinds stored in leaf_prims[3i+1].w (as int bits).
+enum { PRIM_TRI = 0, PRIM_RECT = 1, PRIM_SPHERE = 2 };
+#define PRIM_FLAG_EMISSIVE 0x100
+
+enum { MAT_MATTE = 0, MAT_GLOSSY = 1, MAT_SPECULAR = 2, MAT_EMISSIVE = 3, MAT_DIELECTRIC = 4, MAT_SUBSURFACE = 5 };
+enum { LIGHT_AREA = 0, LIGHT_SPOT = 1 };
+enum { SHAPE_TRI = 0, SHAPE_RECT = 1, SHAPE_SPHERE = 2 };
+
+// 32-byte BVH node.  count > 0: leaf over leaf_prims[first .. first+count).
+// count == 0: interior; its two children are nodes[first] and nodes[first + 1].
+struct __align__(16) BvhNode {
+    float lo_x, lo_y, lo_z, hi_x;
+    float hi_y, hi_z;
+    int first;
+    int count;
+};
+
+struct DevMaterial {
+    int type;
+    float kd, ks, e;          // Matte kd; Glossy kd, ks, Phong exponent; Specular kr; Emissive ls
+    float3 rgb;               // albedo / emission colour / Dielectric absorption / Subsurface sigma_s
+    float eta_in, eta_out;
+    float3 rgb2;              // Subsurface sigma_a
+    float3 sigma_t;           // Subsurface sigma_s + sigma_a
+    float avg_sigma_t;        // Subsurface mean sigma_t * density
+    float absorb;             // Subsurface mean sigma_a / sigma_t
+    float kd_pdf;             // Glossy kd / (kd + ks)
+    float phong_norm;         // Glossy (e + 1) / (2 pi)
+    float3 le;                // Emissive rgb * ls
+};
+
+struct DevLight {
+    int type;                 // LIGHT_AREA / LIGHT_SPOT
+    int shape_type;           // SHAPE_RECT / SHAPE_SPHERE / SHAPE_TRI
+    int shape_index;          // index within its shape array
+    float inv_area;           // Shape::Pdf()
+    float3 le;                // Emissive::Le()
+    // spot light
+    float3 position, direction;
+    float cos_cone;
+    float3 intensity;
+};
+
+struct DevVolume {
+    int present;
+    float3 bmin, bmax;
+    float3 sigma_s, sigma_a, sigma_t;
+    float avg_sigma_t;        // Average(sigma_t)
+    float absorb;             // Average(sigma_a / sigma_t)
+    float g;                  // Henyey-Greenstein asymmetry (0 = isotropic)
+};
+
+struct DevCamera {
+    float3 p;
+    float m[12];              // first three rows of Pinhole::_basis_transform
+    float tanfov, y_ratio, film_area, plane_dist;
+    float3 dir;               // _basis_transform * (0,0,1)
+};
+
+struct DevScene {
+    const BvhNode *nodes;
+    const float4 *leaf_prims;
+    const float4 *tri_shade;
+    const float4 *tri_albedo;   // may be null
+    const float4 *rects;
+    const float4 *spheres;
+    const int *sphere_mat;
+    const DevMaterial *materials;
+    const DevLight *lights;
+    int n_tris, n_rects, n_spheres, n_prims;
+    int n_materials, n_lights;
+    int n_nodes;
+    DevVolume volume;
+    DevCamera camera;
+    int width, height;
+};
+
+// Canonical primitive id -> material index.
+RUMI_D int prim_material(const DevScene &s, int id) {
+    if (id < s.n_tris) return __float_as_int(__ldg(&s.tri_shade[3 * id].w));
+    id -= s.n_tris;
+    if (id < s.n_rects) return __float_as_int(__ldg(&s.rects[3 * id].w));
+    id -= s.n_rects;
+    return __ldg(&s.sphere_mat[id]);
+}

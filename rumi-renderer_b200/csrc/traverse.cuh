@@ -1,0 +1,253 @@
+// Closest-hit and any-hit traversal over the 32-byte-node BVH.
+//
+// Primitive tests restate the reference's Shape::Intersect routines operation by
+// operation with correctly rounded intrinsics (no FMA contraction), so accept/reject
+// decisions and hit distances equal the reference's x86 float arithmetic:
+//   Triangle::Intersect  src/Shape/triangle.cpp:41-118
+//   Rect::Intersect      src/Shape/rect.cpp:51-122
+//   Sphere::Intersect    src/Shape/sphere.cpp:51-132 (+ SolveQuadratic src/Kernel/clibrary.h:62-87)
+// The running closest distance plays the role of Ray::_tmin (0 = nothing hit yet), with
+// the same tie rule: an equal t replaces the previous hit.
+//
+// Traversal: both children of an interior node are adjacent (one 64-byte pair, four
+// float4 loads); leaf children are intersected at once, interior children are visited
+// near-first with the far one pushed.  The stack keeps its top STACK_SMEM entries in
+// shared memory (one column per thread) and spills deeper entries to a local array.
+#pragma once
+#include "scene.cuh"
+
+#define RUMI_MAX_BVH_DEPTH 64
+
+struct HitRec {
+    float t;      // 0 = miss
+    int id;       // canonical primitive id, -1 = miss
+    float u, v;   // triangle barycentrics (reference naming)
+    int back;     // triangle determinant < 0
+};
+
+// ---------------------------------------------------------------- primitive tests
+RUMI_D bool isect_triangle(float3 o, float3 d, float tmax, float tbest, float4 A, float4 B, float4 C, float &t_out,
+                           float &u_out, float &v_out, int &back) {
+    const float3 v0 = f4xyz(A), e1 = f4xyz(B), e2 = f4xyz(C);
+    const float3 P = rn_cross(d, e2);
+    const float det = rn_dot(P, e1);
+    if (-1e-8f < det && det < 1e-8f) return false;
+    const float inv_det = __frcp_rn(det);
+    const float3 T = rn_sub(o, v0);
+    const float u = __fmul_rn(rn_dot(P, T), inv_det);
+    if (u < 0.0f || u > 1.0f) return false;
+    const float3 Q = rn_cross(T, e1);
+    const float v = __fmul_rn(rn_dot(Q, d), inv_det);
+    if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
+    const float t = __fmul_rn(rn_dot(Q, e2), inv_det);
+    if (t < RUMI_EPS) return false;
+    if (tbest > RUMI_EPS && t > tbest) return false;
+    if (__fsub_rn(tmax, t) < RUMI_EPS) return false;
+    t_out = t;
+    u_out = u;
+    v_out = v;
+    back = det < 0.0f;
+    return true;
+}
+
+// Rect geometry derived exactly as the Rect constructor does (src/Shape/rect.cpp:12-20).
+struct RectGeom {
+    float3 n;
+    float length, width, inv_area;
+};
+RUMI_D RectGeom rect_geom(float3 l, float3 w) {
+    RectGeom g;
+    g.n = normalize_ref(rn_cross(l, w));
+    g.length = __fsqrt_rn(rn_dot(l, l));
+    g.width = __fsqrt_rn(rn_dot(w, w));
+    g.inv_area = __frcp_rn(__fmul_rn(g.length, g.width));
+    return g;
+}
+
+RUMI_D bool isect_rect(float3 o, float3 d, float tmax, float tbest, float4 A, float4 B, float4 C, bool emissive,
+                       float &t_out) {
+    const float3 p = f4xyz(A), l = f4xyz(B), w = f4xyz(C);
+    const RectGeom g = rect_geom(l, w);
+    const float cost = rn_dot(d, g.n);
+    if (cost == 0.0f) return false;
+    const float t = __fdiv_rn(-rn_dot(rn_sub(o, p), g.n), cost);
+    if (t < 0.0f) return false;
+    if (t < RUMI_EPS) return false;
+    if (__fsub_rn(tmax, t) < RUMI_EPS) return false;
+    if (!emissive && (0.0f < cost && cost < 1.0f)) return false;  // one-sided unless emissive
+    if (t > tbest && tbest > 0.0f) return false;
+    const float3 ip = rn_madd(o, d, t);
+    const float3 on = rn_sub(ip, p);
+    const float il = __fmul_rn(rn_dot(on, l), __fmul_rn(g.inv_area, g.width));
+    if (il < 0.0f || il > g.length) return false;
+    const float iw = __fmul_rn(rn_dot(on, w), __fmul_rn(g.inv_area, g.length));
+    if (iw < 0.0f || iw > g.width) return false;
+    t_out = t;
+    return true;
+}
+
+RUMI_D bool isect_sphere(float3 o, float3 d, float tmax, float tbest, float4 A, float4 B, bool in_object,
+                         float &t_out) {
+    const float3 c = f4xyz(A);
+    const float r = B.x;
+    const float3 roc = rn_sub(o, c);
+    const float Bq = __fmul_rn(2.0f, rn_dot(d, roc));
+    const float Cq = __fsub_rn(rn_dot(roc, roc), __fmul_rn(r, r));
+    const float disc = __fsub_rn(__fmul_rn(Bq, Bq), __fmul_rn(4.0f, Cq));
+    if (disc < 0.0f) return false;
+    float t0, t1;
+    if (disc == 0.0f) {
+        t0 = t1 = __fmul_rn(-Bq, 0.5f);
+    } else {
+        const float sq = __fsqrt_rn(disc);
+        t0 = __fmul_rn(__fsub_rn(-Bq, sq), 0.5f);
+        t1 = __fmul_rn(__fadd_rn(-Bq, sq), 0.5f);
+    }
+    if (t0 < 0.0f && t1 < 0.0f) return false;
+    if (in_object) {
+        float tmp = t0; t0 = t1; t1 = tmp;
+    }
+    if (t0 < RUMI_EPS) return false;
+    if (__fsub_rn(tmax, t0) < RUMI_EPS) return false;
+    if (t0 > tbest && tbest > 0.0f) return false;
+    t_out = t0;
+    return true;
+}
+
+// ---------------------------------------------------------------------- node test
+RUMI_D bool slab(float4 a, float4 b, float3 inv, float3 oinv, float tlimit, float &tnear) {
+    // t = lo * inv - o * inv; conservative for zero direction components (NaN lanes are
+    // dropped by fminf/fmaxf).
+    const float tx0 = fmaf(a.x, inv.x, -oinv.x), tx1 = fmaf(a.w, inv.x, -oinv.x);
+    const float ty0 = fmaf(a.y, inv.y, -oinv.y), ty1 = fmaf(b.x, inv.y, -oinv.y);
+    const float tz0 = fmaf(a.z, inv.z, -oinv.z), tz1 = fmaf(b.y, inv.z, -oinv.z);
+    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
+    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+    tnear = tn;
+    return tn <= tf && tf >= 0.0f && tn <= tlimit;
+}
+
+struct TraceStats {
+    int nodes;   // 32-byte nodes fetched
+    int prims;   // primitives tested
+};
+
+// Intersects every primitive of one leaf.  Returns true when ANYHIT and a hit was found.
+template <bool ANYHIT, bool STATS>
+RUMI_D bool leaf_isect(const DevScene &s, int first, int count, float3 o, float3 d, float tmax, bool in_object,
+                       HitRec &h, TraceStats &st) {
+    if (first < 0 || count > s.n_prims - first) return false;  // malformed leaf guard
+    for (int i = first; i < first + count; ++i) {
+        const float4 A = __ldg(&s.leaf_prims[3 * i + 0]);
+        const float4 B = __ldg(&s.leaf_prims[3 * i + 1]);
+        const float4 C = __ldg(&s.leaf_prims[3 * i + 2]);
+        if (STATS) st.prims++;
+        const int tag = __float_as_int(B.w);
+        const int kind = tag & 0xff;
+        float t, u = 0.0f, v = 0.0f;
+        int back = 0;
+        bool ok;
+        if (kind == PRIM_TRI)
+            ok = isect_triangle(o, d, tmax, h.t, A, B, C, t, u, v, back);
+        else if (kind == PRIM_RECT)
+            ok = isect_rect(o, d, tmax, h.t, A, B, C, (tag & PRIM_FLAG_EMISSIVE) != 0, t);
+        else
+            ok = isect_sphere(o, d, tmax, h.t, A, B, in_object && !ANYHIT, t);
+        if (ok) {
+            h.t = t;
+            h.id = __float_as_int(A.w);
+            h.u = u;
+            h.v = v;
+            h.back = back;
+        }
+    }
+    return ANYHIT && h.t > 0.0f;
+}
+
+// Closest-hit (ANYHIT=false) or occlusion (ANYHIT=true) query.
+// smem_stack: this thread's first shared-memory stack slot; consecutive slots are
+// `stride` ints apart.
+template <bool ANYHIT, int STACK_SMEM, bool STATS>
+RUMI_D HitRec trace_ray(const DevScene &s, float3 o, float3 d, float tmax, bool in_object, int *smem_stack,
+                        int stride, TraceStats &st) {
+    HitRec h;
+    h.t = 0.0f;
+    h.id = -1;
+    h.u = h.v = 0.0f;
+    h.back = 0;
+    if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) return h;  // bvh.cpp:161-162
+    const float3 inv = mk3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const float3 oinv = mk3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+    int spill[RUMI_MAX_BVH_DEPTH - STACK_SMEM > 0 ? RUMI_MAX_BVH_DEPTH - STACK_SMEM : 1];
+    int sp = 0;
+
+    // root
+    {
+        const float4 *rp = reinterpret_cast<const float4 *>(s.nodes);
+        const float4 a = __ldg(rp), b = __ldg(rp + 1);
+        if (STATS) st.nodes++;
+        float tn;
+        if (!slab(a, b, inv, oinv, tmax, tn)) return h;
+        const int first = __float_as_int(b.z), count = __float_as_int(b.w);
+        if (count > 0) {
+            leaf_isect<ANYHIT, STATS>(s, first, count, o, d, tmax, in_object, h, st);
+            return h;
+        }
+        // fall through with the root's children pair
+        int cur = first;
+        if ((unsigned)cur >= (unsigned)(s.n_nodes - 1)) return h;
+        // every node pair is visited at most once per ray, so the bound is never reached
+        // by a well-formed tree; it keeps a malformed one from looping
+        for (int guard = 0; guard < s.n_nodes; ++guard) {
+            const float4 *np = reinterpret_cast<const float4 *>(s.nodes + cur);
+            const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
+            if (STATS) st.nodes += 2;
+            const float lim = h.t > 0.0f ? fminf(h.t, tmax) : tmax;
+            float tn0, tn1;
+            bool h0 = slab(a0, b0, inv, oinv, lim, tn0);
+            bool h1 = slab(a1, b1, inv, oinv, lim, tn1);
+            const int f0 = __float_as_int(b0.z), c0 = __float_as_int(b0.w);
+            const int f1 = __float_as_int(b1.z), c1 = __float_as_int(b1.w);
+            // leaves: nearest first
+            const bool l0 = h0 && c0 > 0, l1 = h1 && c1 > 0;
+            if (l0 || l1) {
+                int fa = f0, ca = c0, fb = f1, cb = c1;
+                float tnb = tn1;
+                bool la = l0, lb = l1;
+                if (l0 && l1 && tn1 < tn0) {
+                    fa = f1; ca = c1; fb = f0; cb = c0; tnb = tn0;
+                }
+                if (!la) {  // only child 1 is a leaf
+                    fa = f1; ca = c1; la = true; lb = false;
+                }
+                if (leaf_isect<ANYHIT, STATS>(s, fa, ca, o, d, tmax, in_object, h, st)) return h;
+                if (lb && (h.t <= 0.0f || tnb <= h.t))
+                    if (leaf_isect<ANYHIT, STATS>(s, fb, cb, o, d, tmax, in_object, h, st)) return h;
+            }
+            const bool i0 = h0 && c0 == 0 && (h.t <= 0.0f || tn0 <= h.t);
+            const bool i1 = h1 && c1 == 0 && (h.t <= 0.0f || tn1 <= h.t);
+            int next;
+            if (i0 && i1) {
+                const bool swap01 = tn1 < tn0;
+                const int near_ = swap01 ? f1 : f0, far_ = swap01 ? f0 : f1;
+                if (sp < STACK_SMEM)
+                    smem_stack[sp * stride] = far_;
+                else if (sp < RUMI_MAX_BVH_DEPTH)
+                    spill[sp - STACK_SMEM] = far_;
+                if (sp < RUMI_MAX_BVH_DEPTH) ++sp;  // the build caps depth at 63, so this always holds
+                next = near_;
+            } else if (i0) {
+                next = f0;
+            } else if (i1) {
+                next = f1;
+            } else {
+                if (sp == 0) break;
+                --sp;
+                next = sp < STACK_SMEM ? smem_stack[sp * stride] : spill[sp - STACK_SMEM];
+            }
+            if ((unsigned)next >= (unsigned)(s.n_nodes - 1)) break;  // malformed tree guard
+            cur = next;
+        }
+    }
+    return h;
+}

@@ -1,0 +1,177 @@
+"""B200 rendering path for Rumi-Renderer scenes.
+
+``GpuScene(scene)`` uploads a ``scene.Scene`` (the reference-shaped scene API) through
+``rumi_scene_create`` and renders it with ``rumi_render``; ``trace`` queries the BVH
+like the reference's ``BVHAccel::Travel``.  Everything runs in lib/librumi_b200.so."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from .scene import (Scene, FlatScene, PathTracer, BidirectionalPathTracer, PATH_TRACER, BDPT, LIGHT_AREA, LIGHT_SPOT)
+
+__all__ = ["GpuScene", "render", "Scene"]
+
+
+def _fp(a):
+    return a.ctypes.data_as(_capi.FP) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(_capi.IP) if a is not None else None
+
+
+def build_desc(fs: FlatScene):
+    """rumi_scene_desc for a flattened scene; returns (desc, keep-alive list)."""
+    keep = []
+
+    def arr(a, dt):
+        if a is None:
+            return None
+        b = np.ascontiguousarray(a, dtype=dt)
+        keep.append(b)
+        return b
+
+    d = _capi.rumi_scene_desc()
+    d.width, d.height = fs.image.width, fs.image.height
+    tv = arr(fs.tri_vertices.reshape(-1, 9), np.float32)
+    tn = arr(fs.tri_normals.reshape(-1, 9), np.float32)
+    tm = arr(fs.tri_material, np.int32)
+    ta = arr(fs.tri_albedo, np.float32)
+    d.n_triangles = tv.shape[0]
+    d.tri_vertices, d.tri_normals, d.tri_material, d.tri_albedo = _fp(tv), _fp(tn), _ip(tm), _fp(ta)
+    r = arr(fs.rects, np.float32)
+    rm = arr(fs.rect_material, np.int32)
+    d.n_rects, d.rects, d.rect_material = r.shape[0], _fp(r), _ip(rm)
+    s = arr(fs.spheres, np.float32)
+    sm = arr(fs.sphere_material, np.int32)
+    d.n_spheres, d.spheres, d.sphere_material = s.shape[0], _fp(s), _ip(sm)
+    mats = (_capi.rumi_material * max(1, len(fs.materials)))()
+    for i, m in enumerate(fs.materials):
+        mats[i].type = m.type
+        mats[i].kd, mats[i].ks, mats[i].exponent = m.kd, m.ks, m.exponent
+        mats[i].rgb = _capi.f3(*m.rgb)
+        mats[i].eta_in, mats[i].eta_out = m.eta_in, m.eta_out
+        mats[i].rgb2 = _capi.f3(*m.rgb2)
+        mats[i].density = m.density
+    keep.append(mats)
+    d.n_materials, d.materials = len(fs.materials), C.cast(mats, C.POINTER(_capi.rumi_material))
+    lights = (_capi.rumi_light * max(1, len(fs.lights)))()
+    for i, L in enumerate(fs.lights):
+        lights[i].type = L["type"]
+        if L["type"] == LIGHT_AREA:
+            lights[i].shape_type, lights[i].shape_index = L["shape_type"], L["shape_index"]
+        else:
+            lights[i].position = _capi.f3(*L["position"])
+            lights[i].direction = _capi.f3(*L["direction"])
+            lights[i].cone_deg = L["cone_deg"]
+            lights[i].intensity = _capi.f3(*L["intensity"])
+    keep.append(lights)
+    d.n_lights, d.lights = len(fs.lights), C.cast(lights, C.POINTER(_capi.rumi_light))
+    if fs.volume is not None:
+        v = fs.volume
+        d.volume.present = 1
+        d.volume.pmin, d.volume.pmax = _capi.f3(*v.pmin), _capi.f3(*v.pmax)
+        d.volume.sigma_s, d.volume.sigma_a = _capi.f3(*v.sigma_s), _capi.f3(*v.sigma_a)
+        d.volume.g = v.g
+    cam = fs.camera
+    d.camera.position = _capi.f3(*cam.position)
+    d.camera.basis = _capi.f16(*np.asarray(cam.basis, np.float32).reshape(16))
+    d.camera.y_ratio = cam.y_ratio
+    d.camera.fov_deg = cam.fov
+    return d, keep
+
+
+class GpuScene:
+    """A scene resident on the GPU (rumi_scene)."""
+
+    def __init__(self, scene: Scene):
+        self.lib = _capi.load()
+        self.flat = scene.flatten() if isinstance(scene, Scene) else scene
+        self.width, self.height = self.flat.image.width, self.flat.image.height
+        desc, keep = build_desc(self.flat)
+        h = C.c_void_p()
+        _capi.check(self.lib.rumi_scene_create(C.byref(desc), C.byref(h)), "rumi_scene_create")
+        self.h = h
+
+    def bvh_info(self) -> dict:
+        info = _capi.rumi_bvh_info()
+        _capi.check(self.lib.rumi_scene_bvh_info(self.h, C.byref(info)), "rumi_scene_bvh_info")
+        return {k: getattr(info, k) for k, _ in info._fields_}
+
+    def render(self, spp: int = None, seed: int = 1, tracer=None, wave_paths: int = 0, timing: bool = False,
+               film_device_ptr: int = None, stream: int = None):
+        """Renders one frame.  Returns (film (H, W, 3) B,G,R sums, stats dict); with
+        film_device_ptr the film stays on the device and the first value is None."""
+        tr = tracer or self.flat.tracer
+        p = _capi.rumi_render_params()
+        if isinstance(tr, BidirectionalPathTracer):
+            p.integrator, p.n_light, p.n_eye = BDPT, tr.nL, tr.nE
+            p.max_depth = tr.nL + tr.nE
+        else:
+            p.integrator, p.max_depth = PATH_TRACER, tr.max_depth
+        p.spp = int(spp if spp is not None else self.flat.image.n_samples)
+        p.seed = int(seed)
+        p.wave_paths = int(wave_paths)
+        p.flags = 1 if timing else 0
+        p.stream = stream
+        st = _capi.rumi_render_stats()
+        if film_device_ptr is not None:
+            _capi.check(self.lib.rumi_render(self.h, C.byref(p), C.c_void_p(film_device_ptr), 1, C.byref(st)),
+                        "rumi_render")
+            return None, st.as_dict()
+        film = np.zeros((self.height, self.width, 3), np.float32)
+        _capi.check(self.lib.rumi_render(self.h, C.byref(p), film.ctypes.data_as(C.c_void_p), 0, C.byref(st)),
+                    "rumi_render")
+        return film, st.as_dict()
+
+    def trace(self, rays: np.ndarray, anyhit: bool = False, in_object=None):
+        """rays (n, 7) o, d, tmax (or (n, 8) in the C-ABI layout).  Returns (t, prim,
+        node_visits, prim_tests)."""
+        r = np.asarray(rays, np.float32)
+        if r.shape[-1] == 7:
+            r8 = np.zeros((r.shape[0], 8), np.float32)
+            r8[:, 0:3] = r[:, 0:3]
+            r8[:, 4:7] = r[:, 3:6]
+            r8[:, 7] = r[:, 6]
+            if in_object is not None:
+                r8[:, 3] = np.asarray(in_object, np.float32)
+            r = r8
+        r = np.ascontiguousarray(r)
+        n = r.shape[0]
+        t = np.zeros(n, np.float32)
+        prim = np.zeros(n, np.int32)
+        nv, pt = C.c_int64(), C.c_int64()
+        _capi.check(self.lib.rumi_trace_rays(self.h, n, r.ctypes.data_as(C.c_void_p), 1 if anyhit else 0,
+                                             t.ctypes.data_as(C.c_void_p), prim.ctypes.data_as(C.c_void_p), 0,
+                                             C.byref(nv), C.byref(pt), None), "rumi_trace_rays")
+        return t, prim, nv.value, pt.value
+
+    def trace_device(self, n: int, rays_ptr: int, t_ptr: int, prim_ptr: int, anyhit: bool = False, stream=None):
+        nv, pt = C.c_int64(), C.c_int64()
+        _capi.check(self.lib.rumi_trace_rays(self.h, n, C.c_void_p(rays_ptr), 1 if anyhit else 0, C.c_void_p(t_ptr),
+                                             C.c_void_p(prim_ptr), 1, C.byref(nv), C.byref(pt), stream),
+                    "rumi_trace_rays")
+        return nv.value, pt.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rumi_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def render(scene: Scene, seed: int = 1, **kw):
+    """One-shot: upload, render, release."""
+    g = GpuScene(scene)
+    try:
+        return g.render(seed=seed, **kw)
+    finally:
+        g.close()

@@ -1,0 +1,114 @@
+"""ctypes declarations of include/rumi_b200.h and the loader of lib/librumi_b200.so.
+
+The library is the only implementation: there is no CPU fallback, and loading fails
+loudly when the CUDA build is missing."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "librumi_b200.so")
+
+f3 = C.c_float * 3
+f16 = C.c_float * 16
+
+
+class rumi_material(C.Structure):
+    _fields_ = [("type", C.c_int32), ("kd", C.c_float), ("ks", C.c_float), ("exponent", C.c_float),
+                ("rgb", f3), ("eta_in", C.c_float), ("eta_out", C.c_float), ("rgb2", f3), ("density", C.c_float)]
+
+
+class rumi_light(C.Structure):
+    _fields_ = [("type", C.c_int32), ("shape_type", C.c_int32), ("shape_index", C.c_int32),
+                ("position", f3), ("direction", f3), ("cone_deg", C.c_float), ("intensity", f3)]
+
+
+class rumi_volume(C.Structure):
+    _fields_ = [("present", C.c_int32), ("pmin", f3), ("pmax", f3), ("sigma_s", f3), ("sigma_a", f3),
+                ("g", C.c_float)]
+
+
+class rumi_camera(C.Structure):
+    _fields_ = [("position", f3), ("basis", f16), ("y_ratio", C.c_float), ("fov_deg", C.c_float)]
+
+
+FP = C.POINTER(C.c_float)
+IP = C.POINTER(C.c_int32)
+
+
+class rumi_scene_desc(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32),
+                ("n_triangles", C.c_int32), ("tri_vertices", FP), ("tri_normals", FP), ("tri_material", IP),
+                ("tri_albedo", FP),
+                ("n_rects", C.c_int32), ("rects", FP), ("rect_material", IP),
+                ("n_spheres", C.c_int32), ("spheres", FP), ("sphere_material", IP),
+                ("n_materials", C.c_int32), ("materials", C.POINTER(rumi_material)),
+                ("n_lights", C.c_int32), ("lights", C.POINTER(rumi_light)),
+                ("volume", rumi_volume), ("camera", rumi_camera)]
+
+
+class rumi_render_params(C.Structure):
+    _fields_ = [("integrator", C.c_int32), ("max_depth", C.c_int32), ("n_light", C.c_int32), ("n_eye", C.c_int32),
+                ("spp", C.c_int32), ("seed", C.c_uint64), ("wave_paths", C.c_int32), ("flags", C.c_int32),
+                ("stream", C.c_void_p)]
+
+
+class rumi_render_stats(C.Structure):
+    _fields_ = [("paths", C.c_int64), ("nan_samples", C.c_int64), ("extend_launches", C.c_int64),
+                ("extend_ms", C.c_double), ("shade_launches", C.c_int64), ("shade_ms", C.c_double),
+                ("shadow_launches", C.c_int64), ("shadow_ms", C.c_double), ("total_ms", C.c_double),
+                ("rays_extend", C.c_int64), ("rays_shadow", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class rumi_bvh_info(C.Structure):
+    _fields_ = [("large_levels", C.c_int32), ("small_tasks", C.c_int32), ("n_nodes", C.c_int32),
+                ("build_ms", C.c_double)]
+
+
+# every symbol the header declares
+EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "rumi_render", "rumi_trace_rays",
+           "rumi_last_error_string", "rumi_version"]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built: run `python rumi-renderer_b200/build.py`")
+    L = C.CDLL(path)
+    L.rumi_scene_create.restype = C.c_int
+    L.rumi_scene_create.argtypes = [C.POINTER(rumi_scene_desc), C.POINTER(C.c_void_p)]
+    L.rumi_scene_destroy.restype = C.c_int
+    L.rumi_scene_destroy.argtypes = [C.c_void_p]
+    L.rumi_scene_bvh_info.restype = C.c_int
+    L.rumi_scene_bvh_info.argtypes = [C.c_void_p, C.POINTER(rumi_bvh_info)]
+    L.rumi_render.restype = C.c_int
+    L.rumi_render.argtypes = [C.c_void_p, C.POINTER(rumi_render_params), C.c_void_p, C.c_int32,
+                              C.POINTER(rumi_render_stats)]
+    L.rumi_trace_rays.restype = C.c_int
+    L.rumi_trace_rays.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                  C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_void_p]
+    L.rumi_last_error_string.restype = C.c_char_p
+    L.rumi_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+class RumiError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = load().rumi_last_error_string().decode(errors="replace")
+        super().__init__(f"{where} failed with status {status}: {msg}")
+        self.status = status
+
+
+def check(status: int, where: str):
+    if status != 0:
+        raise RumiError(status, where)

@@ -1,0 +1,179 @@
+"""Seeded synthetic workloads (the reference ships no benchmark scenes).
+
+Every builder returns a ``scene.Scene`` assembled with the reference-shaped API, so the
+same object graph drives the GPU path and the reference oracle.
+
+Geometry generation uses float32 numpy arithmetic restricted to + - * / sqrt and integer
+hashing, all correctly rounded in IEEE-754, so a mesh is bit-identical on every x86-64
+host (no libm transcendental functions are involved).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .scene import (Scene, Rect, Sphere, Model, Matte, Specular, Emissive, Dielectric, AreaLight,
+                    SpotLight, HomogeneousVolume, Pinhole, Film, PathTracer, BidirectionalPathTracer,
+                    identity16)
+
+F32 = np.float32
+
+# Cornell-box palette of the plain path-tracer workload.
+RED = (0.63, 0.065, 0.05)
+GREEN = (0.14, 0.45, 0.09)
+WHITE = (0.73, 0.73, 0.73)
+LIGHT_RADIANCE = (17.0, 12.0, 4.0)
+
+
+def cornell_walls() -> list:
+    """Five walls of [0,1]^3 (front z=0 open) as 10 triangles with face normals.
+    Returns a list of (vertices (2,3,3), albedo)."""
+    P = np.array
+    quads = [
+        (P([[0, 0, 0], [1, 0, 0], [1, 0, 1], [0, 0, 1]], F32), WHITE),  # floor y=0
+        (P([[0, 1, 0], [0, 1, 1], [1, 1, 1], [1, 1, 0]], F32), WHITE),  # ceiling y=1
+        (P([[0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], F32), WHITE),  # back z=1
+        (P([[0, 0, 0], [0, 0, 1], [0, 1, 1], [0, 1, 0]], F32), RED),    # left x=0
+        (P([[1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], F32), GREEN),  # right x=1
+    ]
+    out = []
+    for q, alb in quads:
+        tris = np.stack([np.stack([q[0], q[1], q[2]]), np.stack([q[0], q[2], q[3]])]).astype(F32)
+        out.append((tris, alb))
+    return out
+
+
+def add_cornell_box(sc: Scene, light_samples: int = 256) -> Rect:
+    for tris, alb in cornell_walls():
+        sc.add(Model(tris), Matte(1.0, alb))
+    light = Rect((0.375, 0.999, 0.375), (0.25, 0.0, 0.0), (0.0, 0.0, 0.25), light_samples)
+    sc.add(light, Emissive(1.0, LIGHT_RADIANCE))
+    sc.lights.append(AreaLight(light))
+    return light
+
+
+def cornell_camera() -> Pinhole:
+    return Pinhole((0.5, 0.5, -1.4), identity16(), 1.0, fov=40.0)
+
+
+def cornell_pt(width: int = 256, height: int = 256, spp: int = 16, max_depth: int = 8) -> Scene:
+    """Plain path tracer, Cornell box: 10 wall triangles, 0.25 x 0.25 quad light at y=0.999
+    with radiance (17,12,4), a white Lambertian sphere r=0.15 at (0.3,0.15,0.6), a mirror
+    sphere r=0.1 at (0.7,0.1,0.4), pinhole at (0.5,0.5,-1.4) with 40 degree fov."""
+    sc = Scene()
+    add_cornell_box(sc)
+    sc.add(Sphere((0.3, 0.15, 0.6), 0.15), Matte(1.0, WHITE))
+    sc.add(Sphere((0.7, 0.1, 0.4), 0.1), Specular(1.0, (0.9, 0.9, 0.9)))
+    sc.camera = cornell_camera()
+    sc.image = Film(width, height, spp)
+    sc.tracer = PathTracer(max_depth)
+    return sc
+
+
+# ----------------------------------------------------------------------------- meshes
+def _hash3(ix, iy, iz, seed):
+    """32-bit integer hash of lattice coordinates -> float32 in [-1, 1)."""
+    h = (ix.astype(np.uint32) * np.uint32(0x8DA6B343)) ^ (iy.astype(np.uint32) * np.uint32(0xD8163841)) \
+        ^ (iz.astype(np.uint32) * np.uint32(0xCB1AB31F)) ^ np.uint32(seed * 0x9E3779B9 & 0xFFFFFFFF)
+    h ^= h >> np.uint32(16)
+    h *= np.uint32(0x7FEB352D)
+    h ^= h >> np.uint32(15)
+    h *= np.uint32(0x846CA68B)
+    h ^= h >> np.uint32(16)
+    return (h >> np.uint32(8)).astype(F32) * F32(2.0 / 16777216.0) - F32(1.0)
+
+
+def _value_noise(p: np.ndarray, seed: int) -> np.ndarray:
+    """Trilinear value noise with smoothstep weights; p (n,3) float32."""
+    fl = np.floor(p).astype(F32)
+    f = (p - fl).astype(F32)
+    w = (f * f * (F32(3.0) - F32(2.0) * f)).astype(F32)
+    i = fl.astype(np.int64) + 4096  # keep lattice coordinates positive before hashing
+    acc = np.zeros(p.shape[0], F32)
+    for dz in (0, 1):
+        wz = w[:, 2] if dz else (F32(1.0) - w[:, 2])
+        for dy in (0, 1):
+            wy = w[:, 1] if dy else (F32(1.0) - w[:, 1])
+            for dx in (0, 1):
+                wx = w[:, 0] if dx else (F32(1.0) - w[:, 0])
+                v = _hash3(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz, seed)
+                acc = (acc + ((wx * wy).astype(F32) * wz).astype(F32) * v).astype(F32)
+    return acc
+
+
+def fbm(p: np.ndarray, seed: int, octaves: int = 6) -> np.ndarray:
+    """Fractal sum of value noise, lacunarity 2, gain 0.5, normalised to about [-1, 1]."""
+    total = np.zeros(p.shape[0], F32)
+    amp = F32(0.5)
+    norm = F32(0.0)
+    q = p.astype(F32)
+    for o in range(octaves):
+        total = (total + amp * _value_noise(q, seed + 101 * o)).astype(F32)
+        norm = F32(norm + amp)
+        amp = F32(amp * F32(0.5))
+        q = (q * F32(2.0)).astype(F32)
+    return (total / norm).astype(F32)
+
+
+def subdivided_tetrahedron(levels: int):
+    """Regular tetrahedron subdivided ``levels`` times (4 * 4**levels faces), vertices
+    projected to the unit sphere.  Returns (vertices (V,3) float32, faces (F,3) int64)."""
+    s = F32(1.0) / np.sqrt(F32(3.0))
+    verts = np.array([[1, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], F32) * s
+    faces = np.array([[0, 1, 2], [0, 3, 1], [0, 2, 3], [1, 3, 2]], np.int64)
+    for _ in range(levels):
+        e = np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]])
+        e.sort(axis=1)
+        uniq, inv = np.unique(e, axis=0, return_inverse=True)
+        inv = inv.reshape(-1)
+        mid = (verts[uniq[:, 0]] + verts[uniq[:, 1]]).astype(F32)
+        nrm = np.sqrt((mid * mid).sum(axis=1, dtype=F32)).astype(F32)
+        mid = (mid / nrm[:, None]).astype(F32)
+        base = verts.shape[0]
+        verts = np.concatenate([verts, mid]).astype(F32)
+        nf = faces.shape[0]
+        m01 = base + inv[0:nf]
+        m12 = base + inv[nf:2 * nf]
+        m20 = base + inv[2 * nf:3 * nf]
+        a, b, c = faces[:, 0], faces[:, 1], faces[:, 2]
+        faces = np.concatenate([
+            np.stack([a, m01, m20], 1), np.stack([m01, b, m12], 1),
+            np.stack([m20, m12, c], 1), np.stack([m01, m12, m20], 1)])
+    return verts, faces
+
+
+def displaced_sphere(levels: int, center, radius: float, amplitude: float, seed: int, freq: float = 4.0):
+    """Seeded displaced sphere: subdivided tetrahedron, each vertex moved along its
+    direction by ``amplitude * fbm(freq * dir)`` (6 octaves).  Returns (F,3,3) float32."""
+    verts, faces = subdivided_tetrahedron(levels)
+    disp = fbm((verts * F32(freq)).astype(F32), seed)
+    r = (F32(radius) + F32(amplitude) * disp).astype(F32)
+    pos = (verts * r[:, None] + np.asarray(center, F32)[None, :]).astype(F32)
+    return np.ascontiguousarray(pos[faces], dtype=F32)
+
+
+def random_albedo(n: int, seed: int, lo: float = 0.2, hi: float = 0.8) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return (F32(lo) + rng.random((n, 3), dtype=F32) * F32(hi - lo)).astype(F32)
+
+
+def mesh_checksum(tris: np.ndarray) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(tris, np.float32).tobytes()).hexdigest()[:16]
+
+
+def bvh_bound_pt(width: int = 1024, height: int = 1024, spp: int = 64, max_depth: int = 10,
+                 levels: int = 9, seed: int = 7) -> Scene:
+    """BVH-bound path tracing: the Cornell box (walls + light) holding a displaced sphere of
+    4 * 4**levels triangles (levels=9: 1,048,576) centred at (0.5,0.35,0.5), radius 0.25,
+    displaced by 0.05 * fBm, with uniform random per-triangle albedo in [0.2,0.8]^3."""
+    sc = Scene()
+    add_cornell_box(sc)
+    tris = displaced_sphere(levels, (0.5, 0.35, 0.5), 0.25, 0.05, seed)
+    alb = random_albedo(tris.shape[0], seed + 1)
+    sc.add(Model(tris, albedo=alb), Matte(1.0, WHITE))
+    sc.camera = cornell_camera()
+    sc.image = Film(width, height, spp)
+    sc.tracer = PathTracer(max_depth)
+    return sc

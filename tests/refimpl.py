@@ -1,0 +1,199 @@
+"""ctypes driver for oracle/_ref/librumi_ref.so: the reference renderer's own classes,
+compiled from its sources by oracle/build_ref.py.  Test infrastructure only -- used as
+the parity checker and never as the thing measured."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(ROOT, "oracle", "_ref", "librumi_ref.so")
+
+_lib = None
+fp = C.POINTER(C.c_float)
+ip = C.POINTER(C.c_int)
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} missing: run `python oracle/build_ref.py`")
+        L = C.CDLL(LIB_PATH)
+        L.ref_scene_new.restype = C.c_void_p
+        L.ref_scene_new.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float]
+        L.ref_add_triangles.argtypes = [C.c_void_p, C.c_int, fp, fp, C.c_int, fp, C.c_int]
+        L.ref_add_model.argtypes = [C.c_void_p, C.c_int, fp, fp, C.c_int, fp]
+        L.ref_add_rect.argtypes = [C.c_void_p, fp, fp, fp, C.c_int, C.c_int, fp]
+        L.ref_add_sphere.argtypes = [C.c_void_p, fp, C.c_float, C.c_int, C.c_int, fp]
+        L.ref_add_area_light.argtypes = [C.c_void_p, C.c_int]
+        L.ref_set_volume.argtypes = [C.c_void_p, fp, fp, fp, fp]
+        L.ref_set_camera.argtypes = [C.c_void_p, fp, fp, C.c_float, C.c_float]
+        L.ref_finalize.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_ulonglong]
+        L.ref_render_rows.restype = C.c_longlong
+        L.ref_render_rows.argtypes = [C.c_void_p, C.c_ulonglong, C.c_int, C.c_int, fp, fp]
+        L.ref_sample_count.argtypes = [C.c_void_p]
+        L.ref_trace.argtypes = [C.c_void_p, C.c_int, fp, C.c_int, fp, ip, fp]
+        L.ref_scene_free.argtypes = [C.c_void_p]
+        L.ref_seed.argtypes = [C.c_ulonglong]
+        L.ref_inject.argtypes = [fp, C.c_int]
+        L.ref_material_sample.argtypes = [C.c_int, fp, fp, fp, fp]
+        L.ref_material_fr.argtypes = [C.c_int, fp, fp, fp, fp, C.c_int, C.c_float, C.c_float, C.c_float,
+                                      fp, fp, fp]
+        L.ref_material_pdfw.restype = C.c_float
+        L.ref_material_pdfw.argtypes = [C.c_int, fp, fp, fp, fp, C.c_float]
+        L.ref_fresnel.restype = C.c_float
+        L.ref_fresnel.argtypes = [fp, fp, C.c_float, C.c_float]
+        L.ref_isotropic_sample.argtypes = [fp, fp]
+        L.ref_onb.argtypes = [fp, fp]
+        L.ref_volume_distance_sampling.argtypes = [fp, fp, C.c_float, fp]
+        L.ref_volume_segment.argtypes = [fp, fp, fp, fp, C.c_float, fp]
+        L.ref_volume_shadow_tr.argtypes = [fp, fp, fp, fp, fp, fp, C.c_float, fp]
+        L.ref_subsurface_distance_sampling.argtypes = [fp, C.c_float, fp]
+        L.ref_camera_cast.argtypes = [fp, fp, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      C.c_float, C.c_float, fp]
+        L.ref_camera_params.argtypes = [C.c_void_p, fp]
+        _lib = L
+    return _lib
+
+
+def f32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def P(a):
+    """float* into a contiguous float32 array (caller keeps the array alive)."""
+    return a.ctypes.data_as(fp) if a is not None else None
+
+
+class RefScene:
+    """A reference Scene built from a ``rumi_b200.scene.Scene``.
+
+    Triangles of ``Model`` shapes with a per-triangle albedo become standalone Triangle
+    shapes (each with its own Matte), since the reference's Model shares one material;
+    other Models keep the reference's two-level Model BVH."""
+
+    def __init__(self, scene, seed: int = 1, integrator=None):
+        from rumi_b200.scene import (Triangle, Model, Rect, Sphere, AreaLight, PathTracer,
+                                     BidirectionalPathTracer, MATTE)
+        L = lib()
+        self._keep = []
+        img = scene.image
+        self.width, self.height = img.width, img.height
+        self.h = L.ref_scene_new(img.width, img.height, img.n_samples, img.gamma)
+        # primitive ids follow the canonical order: triangles, rects, spheres.  The
+        # harness numbers shapes in insertion order, so insert in that order.
+        order = ([s for s in scene.objects if isinstance(s, (Triangle, Model))] +
+                 [s for s in scene.objects if isinstance(s, Rect)] +
+                 [s for s in scene.objects if isinstance(s, Sphere)])
+        obj_index = {}
+        for s in order:
+            mp = f32(s.material.ref_params())
+            self._keep.append(mp)
+            if isinstance(s, Triangle):
+                v = f32(s.v.reshape(1, 9))
+                n = f32(s.n.reshape(1, 9)) if s.n is not None else None
+                self._keep += [v, n]
+                obj_index[id(s)] = L.ref_add_triangles(self.h, 1, P(v), P(n), s.material.type, P(mp), 0)
+            elif isinstance(s, Model):
+                from rumi_b200.scene import _face_normal
+                v = f32(s.vertices.reshape(-1, 9))
+                if s.normals is not None:
+                    n = f32(s.normals.reshape(-1, 9))
+                else:
+                    n = f32(np.repeat(_face_normal(s.vertices)[:, None, :], 3, axis=1).reshape(-1, 9))
+                self._keep += [v, n]
+                k = v.shape[0]
+                if s.albedo is not None:
+                    assert s.material.type == MATTE
+                    per = np.tile(mp, (k, 1))
+                    per[:, 3:6] = s.albedo
+                    per = f32(per)
+                    self._keep.append(per)
+                    obj_index[id(s)] = L.ref_add_triangles(self.h, k, P(v), P(n), s.material.type, P(per),
+                                                           per.shape[1])
+                else:
+                    obj_index[id(s)] = L.ref_add_model(self.h, k, P(v), P(n), s.material.type, P(mp))
+            elif isinstance(s, Rect):
+                a, b, c = f32(s.p), f32(s.l), f32(s.w)
+                self._keep += [a, b, c]
+                obj_index[id(s)] = L.ref_add_rect(self.h, P(a), P(b), P(c), s.n_samples, s.material.type, P(mp))
+            elif isinstance(s, Sphere):
+                c = f32(s.c)
+                self._keep.append(c)
+                obj_index[id(s)] = L.ref_add_sphere(self.h, P(c), s.r, s.n_samples, s.material.type, P(mp))
+        for light in scene.lights:
+            if not isinstance(light, AreaLight):
+                raise NotImplementedError("the reference has area lights only")
+            L.ref_add_area_light(self.h, obj_index[id(light.shape)])
+        if scene.volume is not None:
+            v = scene.volume
+            if v.g != 0.0:
+                raise NotImplementedError("the reference's medium is isotropic (g = 0)")
+            arrs = [f32(v.pmin), f32(v.pmax), f32(v.sigma_s), f32(v.sigma_a)]
+            self._keep += arrs
+            L.ref_set_volume(self.h, *[P(a) for a in arrs])
+        cam = scene.camera
+        pos, basis = f32(cam.position), f32(cam.basis)
+        self._keep += [pos, basis]
+        L.ref_set_camera(self.h, P(pos), P(basis), cam.y_ratio, cam.fov)
+        tr = integrator or scene.tracer
+        if isinstance(tr, PathTracer):
+            L.ref_finalize(self.h, 0, tr.max_depth, 0, seed)
+        elif isinstance(tr, BidirectionalPathTracer):
+            L.ref_finalize(self.h, 1, tr.nL, tr.nE, seed)
+        else:
+            L.ref_finalize(self.h, 0, 1, 0, seed)
+
+    def render_rows(self, seed: int, row0: int, row1: int):
+        """Film pixel sums (H, W, 3) in B,G,R order for rows [row0, row1), the light
+        buffer, and the NaN sample count."""
+        L = lib()
+        film = np.zeros((self.height, self.width, 3), np.float32)
+        light = np.zeros((self.height, self.width, 3), np.float32)
+        nans = L.ref_render_rows(self.h, seed, row0, row1, P(film), P(light))
+        return film, light, int(nans)
+
+    def render(self, seed: int):
+        film, light, nans = self.render_rows(seed, 0, self.height)
+        return film + light, nans
+
+    @property
+    def spp(self) -> int:
+        return lib().ref_sample_count(self.h)
+
+    def trace(self, rays: np.ndarray, anyhit: bool = False, want_normals: bool = False):
+        """rays (n, 7): o, d, tmax.  Returns t (0 = miss), id (-1 = miss; any-hit: 0/1) and
+        optionally the shading normal."""
+        L = lib()
+        r = f32(rays).reshape(-1, 7)
+        n = r.shape[0]
+        t = np.zeros(n, np.float32)
+        ids = np.zeros(n, np.int32)
+        nn = np.zeros((n, 3), np.float32) if want_normals else None
+        L.ref_trace(self.h, n, P(r), 1 if anyhit else 0, P(t), ids.ctypes.data_as(ip), P(nn))
+        return (t, ids, nn) if want_normals else (t, ids)
+
+    def close(self):
+        if self.h:
+            lib().ref_scene_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def inject(u: np.ndarray):
+    """Make the reference's rand() return exactly the uniforms u (each m * 2^-24)."""
+    u = f32(u)
+    lib().ref_inject(P(u), u.shape[0])
+    return u
