@@ -1,0 +1,407 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 rendering path on the BVH-bound path-tracing workload:
+the Cornell box holding a seeded 1,048,576-triangle displaced sphere, 1024x1024 pixels,
+64 samples per pixel, max depth 10, next-event estimation (67,108,864 paths per frame).
+
+One step = one path-traced frame of that workload.  Our arm times the frames on the
+device (scene and BVH resident in HBM), measures the closest-hit kernel's launches with
+CUDA events for the roofline, repeats the frame end to end through the C-ABI from pinned
+host buffers (scene upload + GPU BVH build + render + film read-back), and times the
+reference renderer itself (oracle/_ref) on a bounded sample of the same workload on the
+host cores.  ``--impl reference`` times only the reference, with every host core.
+
+Multi-GPU (torchrun): one process per GPU renders its own frame (an independent spp
+shard with its own seed); no data exchange on the path; value = all ranks' paths / the
+slowest rank's time.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rumi-renderer_b200"))
+
+WORKLOAD = dict(width=1024, height=1024, spp=64, max_depth=10, levels=9, seed=7)
+METRIC = "path samples/sec"
+UNIT = "paths/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--wave-paths", type=int, default=0)
+    ap.add_argument("--small", action="store_true", help="256x256 at 16 spp (profiling runs)")
+    return ap.parse_args()
+
+
+def workload(args):
+    w = dict(WORKLOAD)
+    if args.small:
+        w.update(width=256, height=256, spp=16)
+    return w
+
+
+def build_scene(w):
+    from rumi_b200 import scenes
+    return scenes.bvh_bound_pt(w["width"], w["height"], w["spp"], w["max_depth"], levels=w["levels"], seed=w["seed"])
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="rumi_clocks_", suffix=".csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() in ("active", "1"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------ reference (CPU) arm
+def _ref_worker(conn, w):
+    """One host process: builds the reference scene once, then renders the rows it is sent."""
+    sys.path.insert(0, os.path.join(ROOT, "rumi-renderer_b200"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refimpl
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)  # the reference prints progress to stdout
+    sc = build_scene(w)
+    rs = refimpl.RefScene(sc, seed=1)
+    conn.send(("ready", rs.spp))
+    while True:
+        msg = conn.recv()
+        if msg is None:
+            break
+        seed, rows = msg
+        t0 = time.perf_counter()
+        paths = 0
+        for r in rows:
+            rs.render_rows(seed, r, r + 1)
+            paths += w["width"] * rs.spp
+        conn.send((paths, time.perf_counter() - t0))
+    rs.close()
+
+
+class RefPool:
+    def __init__(self, w, n_procs):
+        ctx = mp.get_context("spawn")
+        self.w = w
+        self.conns, self.procs = [], []
+        for _ in range(n_procs):
+            a, b = ctx.Pipe()
+            p = ctx.Process(target=_ref_worker, args=(b, w), daemon=True)
+            p.start()
+            self.conns.append(a)
+            self.procs.append(p)
+        self.spp = None
+        for c in self.conns:
+            tag, spp = c.recv()
+            self.spp = spp
+
+    def step(self, seed, rows_per_proc, offset):
+        """Every process renders rows_per_proc rows spread over the image; returns
+        (paths, seconds) with seconds = wall time of the slowest process."""
+        H = self.w["height"]
+        n = len(self.conns)
+        total = n * rows_per_proc
+        t0 = time.perf_counter()
+        for i, c in enumerate(self.conns):
+            rows = [((i * rows_per_proc + k) * H // total + offset) % H for k in range(rows_per_proc)]
+            c.send((seed, rows))
+        paths = 0
+        for c in self.conns:
+            p, _ = c.recv()
+            paths += p
+        return paths, time.perf_counter() - t0
+
+    def close(self):
+        for c in self.conns:
+            c.send(None)
+        for p in self.procs:
+            p.join(timeout=30)
+
+
+def ref_procs(limit=None):
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        n = min(n, max(1, int(psutil.virtual_memory().available / (1.2 * 1024 ** 3))))
+    except Exception:
+        pass
+    return max(1, min(n, limit or n))
+
+
+def cpu_baseline_sample(w, procs, rows_per_proc=1):
+    pool = RefPool(w, procs)
+    paths, secs = pool.step(seed=3, rows_per_proc=rows_per_proc, offset=0)
+    pool.close()
+    return dict(value=paths / secs, unit=UNIT, cores=procs, kind="reference",
+                sample=f"{paths} paths = {procs} processes x {rows_per_proc} row(s) of 1024 px x {pool.spp} spp "
+                       f"of the same workload, reference renderer built from its sources (oracle/_ref), "
+                       f"one thread per process, CPU {cpu_model()}",
+                seconds=secs)
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = workload(args)
+    procs = ref_procs()
+    pool = RefPool(w, procs)
+    for s in range(args.warmup):
+        pool.step(100 + s, 1, offset=s)
+    total_paths, total_s = 0, 0.0
+    for s in range(args.steps):
+        p, sec = pool.step(200 + s, 1, offset=args.warmup + s)
+        total_paths += p
+        total_s += sec
+    pool.close()
+    value = total_paths / total_s
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                ms_per_step=1000.0 * total_s / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32", data="synthetic (seeded displaced-sphere mesh)", impl="reference",
+                config=dict(workload="bvh_bound_pt", width=w["width"], height=w["height"], spp=w["spp"],
+                            max_depth=w["max_depth"], triangles=4 * 4 ** w["levels"]),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=procs, kind="reference",
+                                  sample=f"each step: {procs} processes x 1 row of {w['width']} px x {pool.spp} spp, "
+                                         f"CPU {cpu_model()}"),
+                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- our arm
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def extend_traffic():
+    """DRAM bytes per closest-hit launch from the committed ncu summary, if any."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "extend_traffic.json")))
+    except Exception:
+        return None
+
+
+def our_arm(args):
+    import numpy as np
+    import torch
+    import rumi_b200
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = workload(args)
+    sc = build_scene(w)
+    gs = rumi_b200.GpuScene(sc)
+    bvh = gs.bvh_info()
+    paths_per_frame = w["width"] * w["height"] * w["spp"]
+    film = torch.empty((w["height"], w["width"], 3), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    seed0 = 1000 * rank
+
+    # algorithmic bytes per closest-hit ray, from an instrumented (untimed) frame
+    _, st0 = gs.render(seed=seed0 + 999, film_device_ptr=film.data_ptr(), stream=stream, count_stats=True,
+                       wave_paths=args.wave_paths)
+    nodes_per_ray = st0["extend_node_fetches"] / st0["rays_extend"]
+    prims_per_ray = st0["extend_prim_tests"] / st0["rays_extend"]
+    bytes_per_ray = 32.0 * nodes_per_ray + 48.0 * prims_per_ray + 32.0 + 16.0
+
+    for s in range(args.warmup):
+        gs.render(seed=seed0 + s, film_device_ptr=film.data_ptr(), stream=stream, wave_paths=args.wave_paths)
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ext_ms, ext_launches, rays_ext, rays_sh, launches = 0.0, 0, 0, 0, 0
+    barrier()
+    ev0.record()
+    for s in range(args.steps):
+        _, st = gs.render(seed=seed0 + 100 + s, film_device_ptr=film.data_ptr(), stream=stream, timing=True,
+                          wave_paths=args.wave_paths)
+        ext_ms += st["extend_ms"]
+        ext_launches += st["extend_launches"]
+        rays_ext += st["rays_extend"]
+        rays_sh += st["rays_shadow"]
+        waves = st["extend_launches"] // w["max_depth"]
+        launches += waves * (3 + 4 * w["max_depth"])
+    ev1.record()
+    barrier()
+    clocks_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms)
+    value = world * paths_per_frame * args.steps / (ms / 1000.0)
+    rays_per_s = world * (rays_ext + rays_sh) / (ms / 1000.0)
+
+    avg_launch_ms = ext_ms / ext_launches
+    rays_per_launch = rays_ext / ext_launches
+    achieved = bytes_per_ray * rays_per_launch / (avg_launch_ms / 1000.0) / 1e9
+    pk, pk_kind = peaks()
+    traffic = extend_traffic()
+    roofline = dict(bound="hbm", achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s", frac=achieved / pk["hbm_gbs"],
+                    traffic=(traffic or {}).get("bytes_per_launch_full_workload"),
+                    kernel="pt_extend (closest-hit)", peak_kind=pk_kind,
+                    algorithmic_bytes_per_ray=bytes_per_ray, nodes_per_ray=nodes_per_ray, prims_per_ray=prims_per_ray,
+                    rays_per_launch=rays_per_launch, avg_launch_ms=avg_launch_ms,
+                    closest_hit_rays_per_s=rays_ext / (ext_ms / 1000.0))
+
+    # ---- end to end through the C-ABI: pinned host scene -> device, BVH build, render, film -> host
+    e2e = None
+    if not args.no_e2e:
+        from rumi_b200 import _capi, build_desc
+        import ctypes as C
+        fs = sc.flatten()
+        pinned = {}
+        for name in ("tri_vertices", "tri_normals", "tri_material", "tri_albedo", "rects", "rect_material",
+                     "spheres", "sphere_material"):
+            a = getattr(fs, name)
+            if a is None:
+                continue
+            t = torch.empty(a.shape, dtype=torch.from_numpy(np.ascontiguousarray(a)).dtype, pin_memory=True)
+            t.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+            pinned[name] = t
+            setattr(fs, name, t.numpy())
+        desc, keep = build_desc(fs)
+        h2d = sum(t.numel() * t.element_size() for t in pinned.values())
+        film_host = torch.empty((w["height"], w["width"], 3), dtype=torch.float32, pin_memory=True)
+        d2h = film_host.numel() * 4
+        lib = _capi.load()
+        params = _capi.rumi_render_params()
+        params.integrator, params.max_depth, params.spp = 0, w["max_depth"], w["spp"]
+        params.wave_paths = args.wave_paths
+
+        def e2e_step(seed):
+            hnd = C.c_void_p()
+            _capi.check(lib.rumi_scene_create(C.byref(desc), C.byref(hnd)), "rumi_scene_create")
+            params.seed = seed
+            _capi.check(lib.rumi_render(hnd, C.byref(params), C.c_void_p(film_host.data_ptr()), 0, None), "rumi_render")
+            lib.rumi_scene_destroy(hnd)
+
+        e2e_step(seed0 + 500)
+        barrier()
+        t0 = time.perf_counter()
+        for s in range(args.steps):
+            e2e_step(seed0 + 600 + s)
+        barrier()
+        sec = max_over_ranks(time.perf_counter() - t0)
+        e2e = dict(value=world * paths_per_frame * args.steps / sec, unit=UNIT, h2d_bytes_per_step=h2d,
+                   d2h_bytes_per_step=d2h, ms_per_step=1000.0 * sec / args.steps)
+        film_np = film_host.numpy()
+        assert np.isfinite(film_np).all()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(w, ref_procs(limit=16))
+
+    gs.close()
+    if rank == 0:
+        line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=ms / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                    data="synthetic (seeded 1,048,576-triangle displaced sphere, random per-triangle albedo)",
+                    config=dict(workload="bvh_bound_pt: Cornell box + displaced sphere", width=w["width"],
+                                height=w["height"], spp=w["spp"], max_depth=w["max_depth"],
+                                triangles=4 * 4 ** w["levels"], parallelism=f"replicas x{world} (spp shards)",
+                                l2="inputs larger than L2 (scene ~170 MB + wave queues ~330 MB per GPU)",
+                                bvh_build_ms=bvh["build_ms"]),
+                    rays_per_sec=rays_per_s, roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=launches,
+                    clocks=clocks_info)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

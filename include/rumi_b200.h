@@ -126,7 +126,10 @@ typedef struct {
 typedef struct rumi_scene rumi_scene;
 
 enum { RUMI_PATH_TRACER = 0, RUMI_BDPT = 1 };
-enum { RUMI_FLAG_TIMING = 1 };
+enum {
+    RUMI_FLAG_TIMING = 1,  /* per-kernel CUDA-event timing into rumi_render_stats */
+    RUMI_FLAG_STATS = 2    /* count BVH node fetches and primitive tests of closest-hit rays */
+};
 
 typedef struct {
     int32_t integrator;    /* RUMI_PATH_TRACER (PathTracer(scene, max_depth)) or RUMI_BDPT */
@@ -136,7 +139,7 @@ typedef struct {
     int32_t spp;           /* samples per pixel, rendered exactly */
     uint64_t seed;         /* Philox key: same seed -> same image */
     int32_t wave_paths;    /* paths in flight per wave; 0 = library default */
-    int32_t flags;         /* RUMI_FLAG_TIMING: per-kernel CUDA-event timing into stats */
+    int32_t flags;         /* RUMI_FLAG_* */
     void *stream;          /* cudaStream_t, NULL = the library's own stream */
 } rumi_render_params;
 
@@ -150,8 +153,10 @@ typedef struct {
     int64_t shadow_launches;
     double shadow_ms;
     double total_ms;             /* device time of the whole render (TIMING) */
-    int64_t rays_extend;         /* closest-hit rays traced (TIMING) */
-    int64_t rays_shadow;         /* shadow rays traced (TIMING) */
+    int64_t rays_extend;         /* closest-hit rays traced */
+    int64_t rays_shadow;         /* shadow rays traced */
+    int64_t extend_node_fetches; /* 32-byte nodes fetched by closest-hit rays (STATS) */
+    int64_t extend_prim_tests;   /* primitives tested by closest-hit rays (STATS) */
 } rumi_render_stats;
 
 typedef struct {

@@ -21,6 +21,7 @@
 #include "renderer.h"
 #include "traverse.cuh"
 #include "shading.cuh"
+#include "camera.cuh"
 #include <vector>
 
 namespace rumi {
@@ -50,82 +51,6 @@ struct PtLaunch {
     unsigned long long *stats;
     float *film;
 };
-
-// ------------------------------------------------------------- pixel samples
-// Keyed bijection on [0, n): balanced Feistel network on the next even bit width with
-// cycle walking.
-RUMI_D uint32_t mix32(uint32_t x) {
-    x ^= x >> 16;
-    x *= 0x7FEB352Du;
-    x ^= x >> 15;
-    x *= 0x846CA68Bu;
-    x ^= x >> 16;
-    return x;
-}
-
-RUMI_HD int perm_index(int i, int n, uint32_t key) {
-    if (n <= 1) return 0;
-    int bits = 0;
-    while ((1 << bits) < n) ++bits;
-    if (bits & 1) ++bits;
-    if (bits < 2) bits = 2;
-    const int half = bits >> 1;
-    const uint32_t mask = (1u << half) - 1u;
-    uint32_t x = (uint32_t)i;
-    for (int walk = 0; walk < 4096; ++walk) {
-        uint32_t Lh = x >> half, R = x & mask;
-        for (int r = 0; r < 4; ++r) {
-#ifdef __CUDA_ARCH__
-            const uint32_t F = mix32(R ^ (key + 0x9E3779B9u * (uint32_t)(r + 1))) & mask;
-#else
-            uint32_t y = R ^ (key + 0x9E3779B9u * (uint32_t)(r + 1));
-            y ^= y >> 16; y *= 0x7FEB352Du; y ^= y >> 15; y *= 0x846CA68Bu; y ^= y >> 16;
-            const uint32_t F = y & mask;
-#endif
-            const uint32_t nl = R;
-            R = Lh ^ F;
-            Lh = nl;
-        }
-        x = (Lh << half) | R;
-        if ((int)x < n) return (int)x;
-    }
-    return i;  // unreachable for a permutation; keeps the loop bounded
-}
-
-// The reference's pixel sampler (src/Sample/uniformsample.cpp:32-58, sampler.cpp:17-38):
-// one jittered sqrt(n) x sqrt(n) grid per frame shared by all pixels; each pixel draws
-// its n samples' x and y coordinates independently without replacement.  Here the two
-// draws are keyed permutations of the grid per pixel.  Non-square counts use n strata
-// per axis.
-RUMI_D float2 pixel_sample(int s, int spp, int grid_d, bool square, long long pixel, uint32_t k0, uint32_t k1) {
-    const uint32_t pk = (uint32_t)pixel * 0x9E3779B1u ^ (uint32_t)(pixel >> 32);
-    const int kx = perm_index(s, spp, mix32(pk ^ k0) ^ 0x68E31DA4u);
-    const int ky = perm_index(s, spp, mix32(pk ^ k1) ^ 0xB5297A4Du);
-    const Philox4 jx = philox4x32_10((uint32_t)kx, 0u, 0xFFFFFFFFu, 0u, k0, k1);
-    const Philox4 jy = philox4x32_10((uint32_t)ky, 0u, 0xFFFFFFFFu, 0u, k0, k1);
-    float2 r;
-    if (square) {
-        const float normalize = 1.0f / (float)grid_d;
-        r.x = ((float)(kx % grid_d) + u01(jx.v[0])) * normalize;
-        r.y = ((float)(ky / grid_d) + u01(jy.v[1])) * normalize;
-    } else {
-        const float normalize = 1.0f / (float)spp;
-        r.x = ((float)kx + u01(jx.v[0])) * normalize;
-        r.y = ((float)ky + u01(jy.v[1])) * normalize;
-    }
-    return r;
-}
-
-// Pinhole::CastViewRay (src/Camera/pinhole.cpp:97-136) without depth of field.
-RUMI_D void camera_ray(const DevCamera &c, int W, int H, int w, int h, float sx, float sy, float3 &o, float3 &d) {
-    const float half_w = W * 0.5f, half_h = H * 0.5f;
-    const float x = -(((float)w - half_w) + sx) / half_w * c.tanfov;
-    const float y = -(((float)h - half_h) + sy) / half_h * c.tanfov * c.y_ratio;
-    const float3 l = normalize_ref(mk3(x, y, c.plane_dist));
-    d = mk3(c.m[0] * l.x + c.m[1] * l.y + c.m[2] * l.z + c.m[3], c.m[4] * l.x + c.m[5] * l.y + c.m[6] * l.z + c.m[7],
-            c.m[8] * l.x + c.m[9] * l.y + c.m[10] * l.z + c.m[11]);
-    o = c.p;
-}
 
 __global__ void pt_generate(PtLaunch P) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -539,6 +464,7 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
     const int shadow_grid = sc->num_sms * occ_sh;
 
     const bool timing = (p->flags & RUMI_FLAG_TIMING) != 0;
+    const bool count_stats = (p->flags & RUMI_FLAG_STATS) != 0;
     std::vector<cudaEvent_t> evs;
     auto mark = [&]() {
         cudaEvent_t e;
@@ -561,7 +487,10 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
             pt_reset<<<1, 1, 0, stream>>>(L, b);
             int e0 = 0;
             if (timing) { e0 = (int)evs.size(); mark(); }
-            pt_extend<false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
+            if (count_stats)
+                pt_extend<true><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
+            else
+                pt_extend<false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
             if (timing) { mark(); ext_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
             pt_shade<<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
@@ -590,6 +519,8 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
         stats->nan_samples = (int64_t)h_stats[S_NAN];
         stats->rays_extend = (int64_t)h_stats[S_RAYS_EXT];
         stats->rays_shadow = (int64_t)h_stats[S_RAYS_SH];
+        stats->extend_node_fetches = (int64_t)h_stats[S_NODES];
+        stats->extend_prim_tests = (int64_t)h_stats[S_PRIMS];
         stats->extend_launches = (int64_t)waves * p->max_depth;
         stats->shade_launches = stats->extend_launches;
         stats->shadow_launches = stats->extend_launches;

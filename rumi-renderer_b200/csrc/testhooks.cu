@@ -1,0 +1,223 @@
+// Verification entry points (include/rumi_b200_test.h): one device routine of the
+// renderer per call, evaluated over a batch of caller-supplied inputs.
+#include "renderer.h"
+#include "shading.cuh"
+#include "camera.cuh"
+#include "../../include/rumi_b200_test.h"
+#include <vector>
+
+using namespace rumi;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { cudaFree(p); }
+};
+
+template <typename T>
+rumi_status to_dev(DevBuf &b, const T *src, size_t count) {
+    if (cudaMalloc(&b.p, sizeof(T) * (count > 0 ? count : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaMalloc");
+        return RUMI_ERR_OOM;
+    }
+    if (src && count) cudaMemcpy(b.p, src, sizeof(T) * count, cudaMemcpyHostToDevice);
+    return RUMI_OK;
+}
+
+template <typename T>
+rumi_status from_dev(T *dst, const DevBuf &b, size_t count) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && count) e = cudaMemcpy(dst, b.p, sizeof(T) * count, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "test hook");
+    return RUMI_OK;
+}
+
+DevMaterial dev_material(const rumi_material &m) {
+    DevMaterial d;
+    memset(&d, 0, sizeof(d));
+    d.type = m.type;
+    d.kd = m.kd;
+    d.ks = m.ks;
+    d.e = m.exponent;
+    d.rgb = make_float3(m.rgb[0], m.rgb[1], m.rgb[2]);
+    d.eta_in = m.eta_in;
+    d.eta_out = m.eta_out;
+    d.rgb2 = make_float3(m.rgb2[0], m.rgb2[1], m.rgb2[2]);
+    if (m.type == RUMI_MAT_GLOSSY) {
+        d.kd_pdf = m.kd / (m.kd + m.ks);
+        d.phong_norm = (float)((m.exponent + 1.0f) / (2.0f * 3.14159265358979323846));
+    }
+    if (m.type == RUMI_MAT_EMISSIVE) d.le = make_float3(m.rgb[0] * m.kd, m.rgb[1] * m.kd, m.rgb[2] * m.kd);
+    return d;
+}
+
+inline int blocks(int64_t n) { return (int)((n + 255) / 256); }
+
+__global__ void k_philox(int64_t n, const uint32_t *ctr, uint32_t k0, uint32_t k1, uint32_t *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Philox4 r = philox4x32_10(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3], k0, k1);
+    for (int k = 0; k < 4; ++k) out[4 * i + k] = r.v[k];
+}
+
+__global__ void k_mat_sample(DevMaterial m, int64_t n, const float *wo, const float *nrm, const float *u,
+                             float *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BsdfSample b = material_sample(m, mk3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]),
+                                         mk3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]), u[3 * i], u[3 * i + 1],
+                                         u[3 * i + 2]);
+    float *o = out + 9 * i;
+    o[0] = b.w.x; o[1] = b.w.y; o[2] = b.w.z;
+    o[3] = b.le; o[4] = b.go_in; o[5] = b.xi; o[6] = b.pdf_path; o[7] = b.cost; o[8] = b.pdfw;
+}
+
+__global__ void k_mat_fr(DevMaterial m, int64_t n, const float *nrm, const float *wi, const float *wo, const int32_t *inobj,
+                         const float *xi, const float *pdf_path, const float *t_in, const float *vr, float *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float3 f = material_fr(m, m.rgb, mk3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]),
+                                 mk3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), mk3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]),
+                                 inobj[i] != 0, xi[i], pdf_path[i], t_in[i], mk3(vr[3 * i], vr[3 * i + 1], vr[3 * i + 2]));
+    out[3 * i] = f.x; out[3 * i + 1] = f.y; out[3 * i + 2] = f.z;
+}
+
+__global__ void k_dist(float3 ss, float3 sa, int64_t n, const float *smax, const float *xi, const float *xa, float *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float3 st = ss + sa;
+    const float avg = avg3(st);
+    const float ab = avg3(sa / st);
+    const DistSample d = distance_sample(st, avg, ab, smax[i], xi[i], xa[i]);
+    float *o = out + 9 * i;
+    o[0] = (float)d.outcome; o[1] = d.s;
+    o[2] = d.tau.x; o[3] = d.tau.y; o[4] = d.tau.z; o[5] = d.pdf.x; o[6] = d.pdf.y; o[7] = d.pdf.z; o[8] = 0.0f;
+}
+
+__global__ void k_phase(int64_t n, const float *d, float g, const float *u, float *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float3 dd = mk3(d[3 * i], d[3 * i + 1], d[3 * i + 2]);
+    float pdf = 1.0f / (4.0f * RUMI_PI_F);
+    const float3 w = g == 0.0f ? isotropic_dir(dd, u[2 * i], u[2 * i + 1]) : hg_sample(dd, g, u[2 * i], u[2 * i + 1], pdf);
+    out[4 * i] = w.x; out[4 * i + 1] = w.y; out[4 * i + 2] = w.z; out[4 * i + 3] = pdf;
+}
+
+__global__ void k_camera(DevCamera c, int W, int H, int64_t n, const int32_t *pix, const float *smp, float *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 o, d;
+    camera_ray(c, W, H, pix[2 * i], pix[2 * i + 1], smp[2 * i], smp[2 * i + 1], o, d);
+    float *q = out + 6 * i;
+    q[0] = o.x; q[1] = o.y; q[2] = o.z; q[3] = d.x; q[4] = d.y; q[5] = d.z;
+}
+
+__global__ void k_pixel_samples(int64_t n, const int32_t *s, int spp, int grid_d, int square, const int64_t *pixel,
+                                uint32_t k0, uint32_t k1, float *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float2 r = pixel_sample(s[i], spp, grid_d, square != 0, pixel[i], k0, k1);
+    out[2 * i] = r.x;
+    out[2 * i + 1] = r.y;
+}
+
+}  // namespace
+
+extern "C" {
+
+rumi_status rumi_test_philox(int64_t n, const uint32_t *ctr, const uint32_t *key, uint32_t *out) {
+    if (n < 0 || (n > 0 && (!ctr || !key || !out))) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    DevBuf c, o;
+    rumi_status st;
+    if ((st = to_dev(c, ctr, 4 * n)) != RUMI_OK || (st = to_dev<uint32_t>(o, nullptr, 4 * n)) != RUMI_OK) return st;
+    if (n) k_philox<<<blocks(n), 256>>>(n, (const uint32_t *)c.p, key[0], key[1], (uint32_t *)o.p);
+    return from_dev(out, o, 4 * n);
+}
+
+rumi_status rumi_test_material_sample(const rumi_material *m, int64_t n, const float *wo, const float *nrm,
+                                      const float *u, float *out) {
+    if (!m || n < 0) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    DevBuf a, b, c, o;
+    rumi_status st;
+    if ((st = to_dev(a, wo, 3 * n)) || (st = to_dev(b, nrm, 3 * n)) || (st = to_dev(c, u, 3 * n)) ||
+        (st = to_dev<float>(o, nullptr, 9 * n)))
+        return st;
+    if (n) k_mat_sample<<<blocks(n), 256>>>(dev_material(*m), n, (float *)a.p, (float *)b.p, (float *)c.p, (float *)o.p);
+    return from_dev(out, o, 9 * n);
+}
+
+rumi_status rumi_test_material_fr(const rumi_material *m, int64_t n, const float *nrm, const float *wi,
+                                  const float *wo, const int32_t *in_object, const float *xi, const float *pdf_path,
+                                  const float *t_in, const float *vol_ratio, float *out) {
+    if (!m || n < 0) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    DevBuf a, b, c, d, e, f, g, h, o;
+    rumi_status st;
+    if ((st = to_dev(a, nrm, 3 * n)) || (st = to_dev(b, wi, 3 * n)) || (st = to_dev(c, wo, 3 * n)) ||
+        (st = to_dev(d, in_object, n)) || (st = to_dev(e, xi, n)) || (st = to_dev(f, pdf_path, n)) ||
+        (st = to_dev(g, t_in, n)) || (st = to_dev(h, vol_ratio, 3 * n)) || (st = to_dev<float>(o, nullptr, 3 * n)))
+        return st;
+    if (n)
+        k_mat_fr<<<blocks(n), 256>>>(dev_material(*m), n, (float *)a.p, (float *)b.p, (float *)c.p, (int32_t *)d.p,
+                                     (float *)e.p, (float *)f.p, (float *)g.p, (float *)h.p, (float *)o.p);
+    return from_dev(out, o, 3 * n);
+}
+
+rumi_status rumi_test_distance_sample(const float *sigma_s, const float *sigma_a, int64_t n, const float *smax,
+                                      const float *xi, const float *xi_absorb, float *out) {
+    if (!sigma_s || !sigma_a || n < 0) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    DevBuf a, b, c, o;
+    rumi_status st;
+    if ((st = to_dev(a, smax, n)) || (st = to_dev(b, xi, n)) || (st = to_dev(c, xi_absorb, n)) ||
+        (st = to_dev<float>(o, nullptr, 9 * n)))
+        return st;
+    if (n)
+        k_dist<<<blocks(n), 256>>>(make_float3(sigma_s[0], sigma_s[1], sigma_s[2]),
+                                   make_float3(sigma_a[0], sigma_a[1], sigma_a[2]), n, (float *)a.p, (float *)b.p,
+                                   (float *)c.p, (float *)o.p);
+    return from_dev(out, o, 9 * n);
+}
+
+rumi_status rumi_test_phase_sample(int64_t n, const float *d, float g, const float *u, float *out) {
+    if (n < 0) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    DevBuf a, b, o;
+    rumi_status st;
+    if ((st = to_dev(a, d, 3 * n)) || (st = to_dev(b, u, 2 * n)) || (st = to_dev<float>(o, nullptr, 4 * n))) return st;
+    if (n) k_phase<<<blocks(n), 256>>>(n, (float *)a.p, g, (float *)b.p, (float *)o.p);
+    return from_dev(out, o, 4 * n);
+}
+
+rumi_status rumi_test_camera_rays(const rumi_camera *cam, int32_t width, int32_t height, int64_t n, const int32_t *pix,
+                                  const float *smp, float *out) {
+    if (!cam || n < 0 || width <= 0 || height <= 0) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    DevCamera dc;
+    memset(&dc, 0, sizeof(dc));
+    dc.p = make_float3(cam->position[0], cam->position[1], cam->position[2]);
+    for (int k = 0; k < 12; ++k) dc.m[k] = cam->basis[k];
+    const float fov = cam->fov_deg > 0.0f ? cam->fov_deg : 20.0f;
+    dc.tanfov = (float)std::tan(3.14159265358979323846 / 180.f * fov * 0.5f);
+    dc.plane_dist = 1.0f;
+    dc.y_ratio = cam->y_ratio;
+    DevBuf a, b, o;
+    rumi_status st;
+    if ((st = to_dev(a, pix, 2 * n)) || (st = to_dev(b, smp, 2 * n)) || (st = to_dev<float>(o, nullptr, 6 * n))) return st;
+    if (n) k_camera<<<blocks(n), 256>>>(dc, width, height, n, (int32_t *)a.p, (float *)b.p, (float *)o.p);
+    return from_dev(out, o, 6 * n);
+}
+
+rumi_status rumi_test_pixel_samples(int64_t n, const int32_t *s, int32_t spp, const int64_t *pixel, uint64_t seed,
+                                    float *out) {
+    if (n < 0 || spp <= 0) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    int d = 0;
+    while ((d + 1) * (d + 1) <= spp) ++d;
+    DevBuf a, b, o;
+    rumi_status st;
+    if ((st = to_dev(a, s, n)) || (st = to_dev(b, pixel, n)) || (st = to_dev<float>(o, nullptr, 2 * n))) return st;
+    if (n)
+        k_pixel_samples<<<blocks(n), 256>>>(n, (int32_t *)a.p, spp, d, d * d == spp, (int64_t *)b.p, (uint32_t)seed,
+                                            (uint32_t)(seed >> 32) ^ 0x5851F42Du, (float *)o.p);
+    return from_dev(out, o, 2 * n);
+}
+
+}  // extern "C"

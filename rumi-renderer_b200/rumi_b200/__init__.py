@@ -102,7 +102,7 @@ class GpuScene:
         return {k: getattr(info, k) for k, _ in info._fields_}
 
     def render(self, spp: int = None, seed: int = 1, tracer=None, wave_paths: int = 0, timing: bool = False,
-               film_device_ptr: int = None, stream: int = None):
+               film_device_ptr: int = None, stream: int = None, count_stats: bool = False):
         """Renders one frame.  Returns (film (H, W, 3) B,G,R sums, stats dict); with
         film_device_ptr the film stays on the device and the first value is None."""
         tr = tracer or self.flat.tracer
@@ -115,7 +115,7 @@ class GpuScene:
         p.spp = int(spp if spp is not None else self.flat.image.n_samples)
         p.seed = int(seed)
         p.wave_paths = int(wave_paths)
-        p.flags = 1 if timing else 0
+        p.flags = (1 if timing else 0) | (2 if count_stats else 0)
         p.stream = stream
         st = _capi.rumi_render_stats()
         if film_device_ptr is not None:

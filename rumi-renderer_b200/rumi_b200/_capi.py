@@ -58,7 +58,8 @@ class rumi_render_stats(C.Structure):
     _fields_ = [("paths", C.c_int64), ("nan_samples", C.c_int64), ("extend_launches", C.c_int64),
                 ("extend_ms", C.c_double), ("shade_launches", C.c_int64), ("shade_ms", C.c_double),
                 ("shadow_launches", C.c_int64), ("shadow_ms", C.c_double), ("total_ms", C.c_double),
-                ("rays_extend", C.c_int64), ("rays_shadow", C.c_int64)]
+                ("rays_extend", C.c_int64), ("rays_shadow", C.c_int64), ("extend_node_fetches", C.c_int64),
+                ("extend_prim_tests", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -69,9 +70,11 @@ class rumi_bvh_info(C.Structure):
                 ("build_ms", C.c_double)]
 
 
-# every symbol the header declares
+# every symbol include/rumi_b200.h and include/rumi_b200_test.h declare
 EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "rumi_render", "rumi_trace_rays",
-           "rumi_last_error_string", "rumi_version"]
+           "rumi_last_error_string", "rumi_version",
+           "rumi_test_philox", "rumi_test_material_sample", "rumi_test_material_fr", "rumi_test_distance_sample",
+           "rumi_test_phase_sample", "rumi_test_camera_rays", "rumi_test_pixel_samples"]
 
 _lib = None
 
@@ -96,6 +99,14 @@ def load(path: str = LIB_PATH):
     L.rumi_trace_rays.restype = C.c_int
     L.rumi_trace_rays.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_void_p]
+    vp = C.c_void_p
+    L.rumi_test_philox.argtypes = [C.c_int64, vp, vp, vp]
+    L.rumi_test_material_sample.argtypes = [C.POINTER(rumi_material), C.c_int64, vp, vp, vp, vp]
+    L.rumi_test_material_fr.argtypes = [C.POINTER(rumi_material), C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.rumi_test_distance_sample.argtypes = [vp, vp, C.c_int64, vp, vp, vp, vp]
+    L.rumi_test_phase_sample.argtypes = [C.c_int64, vp, C.c_float, vp, vp]
+    L.rumi_test_camera_rays.argtypes = [C.POINTER(rumi_camera), C.c_int32, C.c_int32, C.c_int64, vp, vp, vp]
+    L.rumi_test_pixel_samples.argtypes = [C.c_int64, vp, C.c_int32, vp, C.c_uint64, vp]
     L.rumi_last_error_string.restype = C.c_char_p
     L.rumi_version.restype = C.c_char_p
     _lib = L

@@ -1,0 +1,224 @@
+#!/usr/bin/env python3
+"""Generates the golden fixtures of tests/golden/ by running the REFERENCE renderer's own
+routines (oracle/_ref/librumi_ref.so, built from the reference sources by
+oracle/build_ref.py) on seeded inputs.  The reference ships no tests or fixtures, so
+these are its outputs captured here; the fixtures travel with the repository so GPU tests
+need no reference checkout.
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "rumi-renderer_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import refimpl  # noqa: E402
+from rumi_b200 import scenes  # noqa: E402
+from rumi_b200.scene import Matte, Glossy, Specular, Dielectric, Subsurface, Emissive  # noqa: E402
+
+F32 = np.float32
+
+
+def u24(rng, shape):
+    """Uniforms of the exact form m * 2^-24 (what the GPU's Philox conversion yields)."""
+    return (rng.integers(0, 1 << 24, size=shape).astype(np.float64) / float(1 << 24)).astype(F32)
+
+
+def unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v.astype(F32)
+
+
+def rays_in_box(rng, n, lo=0.02, hi=0.98):
+    o = rng.uniform(lo, hi, (n, 3)).astype(F32)
+    d = unit(rng, n)
+    return np.concatenate([o, d, np.full((n, 1), 3.4e38, F32)], 1).astype(F32)
+
+
+def camera_rays(rng, n, cam=(0.5, 0.5, -1.4), lo=(0.05, 0.05, 0.05), hi=(0.95, 0.95, 0.95)):
+    o = np.tile(np.asarray(cam, F32), (n, 1))
+    tgt = rng.uniform(lo, hi, (n, 3)).astype(F32)
+    d = (tgt - o)
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(F32)
+    return np.concatenate([o, d, np.full((n, 1), 3.4e38, F32)], 1).astype(F32)
+
+
+def hit_fixture(scene, rays, path, extra=None):
+    rs = refimpl.RefScene(scene, seed=1)
+    t, ids, nrm = rs.trace(rays, want_normals=True)
+    # shadow queries with a finite tmax (half of each closest-hit distance, or 0.7)
+    tmax = np.where(t > 0, t * 0.5, 0.7).astype(F32)
+    sh = rays.copy()
+    sh[:, 6] = tmax
+    ta, occ = rs.trace(sh, anyhit=True)
+    sh2 = rays.copy()
+    sh2[:, 6] = np.where(t > 0, t + 0.01, 0.7).astype(F32)
+    tb, occ2 = rs.trace(sh2, anyhit=True)
+    data = dict(rays=rays, t=t, prim=ids, normal=nrm, shadow_rays=sh, shadow_occluded=occ, shadow2_rays=sh2,
+                shadow2_occluded=occ2)
+    if extra:
+        data.update(extra)
+    np.savez_compressed(path, **data)
+    rs.close()
+    print(path, "hit fraction", float((ids >= 0).mean()))
+
+
+def material_fixture(path, rng):
+    L = refimpl.lib()
+    mats = {
+        "matte": Matte(0.8, (0.7, 0.4, 0.2)),
+        "glossy": Glossy(0.5, 0.4, 20.0, (0.6, 0.6, 0.9)),
+        "glossy_ks_only": Glossy(0.0, 0.9, 10.0, (1.0, 1.0, 1.0)),
+        "specular": Specular(0.9, (1.0, 0.9, 0.8)),
+        "dielectric": Dielectric(1.5, 1.00029, (0.1, 0.2, 0.3)),
+        "subsurface": Subsurface(1.3, 1.0, (0.8, 0.6, 0.4), (0.05, 0.1, 0.2), 2.0),
+        "emissive": Emissive(3.0, (17.0, 12.0, 4.0)),
+    }
+    N = 256
+    out = {}
+    for name, m in mats.items():
+        p = refimpl.f32(m.ref_params())
+        n = unit(rng, N)
+        wo = unit(rng, N)
+        # a quarter of the cases: wo in the same hemisphere as n, near grazing
+        k = N // 4
+        wo[:k] = np.where((np.sum(wo[:k] * n[:k], 1) < 0)[:, None], -wo[:k], wo[:k])
+        u = u24(rng, (N, 3))
+        samp = np.zeros((N, 9), F32)
+        for i in range(N):
+            # inject the uniforms in the order the reference draws them
+            if m.type == 0:
+                seq = u[i, 1:3]
+            elif m.type == 1:
+                seq = u[i, 0:3]
+            elif m.type in (4, 5):
+                seq = u[i, 0:1]
+            else:
+                seq = u[i, 0:0]
+            keep = refimpl.inject(seq)
+            L.ref_material_sample(m.type, refimpl.P(p), refimpl.P(refimpl.f32(wo[i])), refimpl.P(refimpl.f32(n[i])),
+                                  refimpl.P(samp[i]))
+            L.ref_inject_off()
+            del keep
+        # Fr with the sampled direction and the sampled lobe state
+        inobj = rng.integers(0, 2, N).astype(np.int32)
+        t_in = rng.uniform(0.01, 2.0, N).astype(F32)
+        vr = rng.uniform(0.5, 1.5, (N, 3)).astype(F32)
+        fr = np.zeros((N, 3), F32)
+        for i in range(N):
+            wi = samp[i, 0:3].copy()
+            L.ref_material_fr(m.type, refimpl.P(p), refimpl.P(refimpl.f32(n[i])), refimpl.P(refimpl.f32(wi)),
+                              refimpl.P(refimpl.f32(wo[i])), int(inobj[i]), float(samp[i, 5]), float(samp[i, 6]),
+                              float(t_in[i]), refimpl.P(refimpl.f32(vr[i])), refimpl.P(refimpl.f32([1, 1, 1])),
+                              refimpl.P(fr[i]))
+        out.update({f"{name}_params": p, f"{name}_n": n, f"{name}_wo": wo, f"{name}_u": u, f"{name}_sample": samp,
+                    f"{name}_inobj": inobj, f"{name}_tin": t_in, f"{name}_vr": vr, f"{name}_fr": fr,
+                    f"{name}_type": np.int32(m.type)})
+    # Fresnel over incidence angles and both sides
+    d = unit(rng, N)
+    n = unit(rng, N)
+    kr = np.array([L.ref_fresnel(refimpl.P(refimpl.f32(d[i])), refimpl.P(refimpl.f32(n[i])), 1.5, 1.00029)
+                   for i in range(N)], F32)
+    out.update(fresnel_d=d, fresnel_n=n, fresnel_kr=kr)
+    # isotropic phase
+    dd = unit(rng, N)
+    uu = u24(rng, (N, 2))
+    iso = np.zeros((N, 4), F32)
+    for i in range(N):
+        keep = refimpl.inject(uu[i])
+        L.ref_isotropic_sample(refimpl.P(refimpl.f32(dd[i])), refimpl.P(iso[i]))
+        L.ref_inject_off()
+        del keep
+    out.update(iso_d=dd, iso_u=uu, iso_out=iso)
+    np.savez_compressed(path, **out)
+    print(path)
+
+
+def volume_fixture(path, rng):
+    L = refimpl.lib()
+    N = 512
+    ss = np.array([0.4, 0.3, 0.2], F32)
+    sa = np.array([0.05, 0.1, 0.02], F32)
+    smax = rng.uniform(0.0, 8.0, N).astype(F32)
+    smax[:16] = 0.0
+    xi = u24(rng, N)
+    xa = u24(rng, N)
+    out = np.zeros((N, 10), F32)
+    for i in range(N):
+        keep = refimpl.inject(np.array([xi[i], xa[i]], F32))
+        L.ref_volume_distance_sampling(refimpl.P(ss), refimpl.P(sa), float(smax[i]), refimpl.P(out[i]))
+        L.ref_inject_off()
+        del keep
+    # box segments (Intersect + MaxDistance)
+    bmin, bmax = np.array([0, 0, 0], F32), np.array([1, 1, 1], F32)
+    o = rng.uniform(-0.5, 1.5, (N, 3)).astype(F32)
+    d = unit(rng, N)
+    thit = np.where(rng.uniform(size=N) < 0.5, 0.0, rng.uniform(0.0, 2.0, N)).astype(F32)
+    seg = np.zeros((N, 4), F32)
+    for i in range(N):
+        L.ref_volume_segment(refimpl.P(bmin), refimpl.P(bmax), refimpl.P(refimpl.f32(o[i])),
+                             refimpl.P(refimpl.f32(d[i])), float(thit[i]), refimpl.P(seg[i]))
+    np.savez_compressed(path, sigma_s=ss, sigma_a=sa, smax=smax, xi=xi, xa=xa, out=out, seg_o=o, seg_d=d,
+                        seg_thit=thit, seg_out=seg, bmin=bmin, bmax=bmax)
+    print(path)
+
+
+def camera_fixture(path, rng):
+    L = refimpl.lib()
+    N = 256
+    cam = scenes.cornell_camera()
+    pos, basis = refimpl.f32(cam.position), refimpl.f32(cam.basis)
+    W, H = 96, 64
+    pix = np.stack([rng.integers(0, W, N), rng.integers(0, H, N)], 1).astype(np.int32)
+    smp = u24(rng, (N, 2))
+    out = np.zeros((N, 8), F32)
+    for i in range(N):
+        L.ref_camera_cast(refimpl.P(pos), refimpl.P(basis), 0.75, 40.0, W, H, int(pix[i, 0]), int(pix[i, 1]),
+                          float(smp[i, 0]), float(smp[i, 1]), refimpl.P(out[i]))
+    np.savez_compressed(path, pos=pos, basis=basis, y_ratio=np.float32(0.75), fov=np.float32(40.0), W=W, H=H, pix=pix,
+                        smp=smp, out=out)
+    print(path)
+
+
+def image_fixture(path, size=32, spp=16, depth=8, seeds=64):
+    """Reference renders of the Cornell workload at a small size: per-pixel mean radiance
+    over `seeds` independent frames and its standard error (spread across frames, which
+    includes the frame-level correlation of the reference's shared sample sets)."""
+    sc = scenes.cornell_pt(size, size, spp, depth)
+    frames = []
+    for s in range(seeds):
+        rs = refimpl.RefScene(sc, seed=1000 + s)
+        film, nans = rs.render(7000 + s)
+        frames.append(film / rs.spp)
+        rs.close()
+    fr = np.stack(frames).astype(np.float64)
+    mean = fr.mean(0).astype(F32)
+    stderr = (fr.std(0, ddof=1) / np.sqrt(seeds)).astype(F32)
+    np.savez_compressed(path, mean=mean, stderr=stderr, seeds=seeds, spp=spp, depth=depth, size=size)
+    print(path, "mean", mean.reshape(-1, 3).mean(0))
+
+
+def main():
+    rng = np.random.default_rng(20261203)
+    c1 = scenes.cornell_pt(64, 64, 16, 8)
+    rays = np.concatenate([rays_in_box(rng, 3072), camera_rays(rng, 1024)])
+    hit_fixture(c1, rays, os.path.join(HERE, "hits_cornell.npz"))
+    m5 = scenes.bvh_bound_pt(64, 64, 4, 10, levels=5, seed=7)
+    tris = m5.flatten().tri_vertices
+    rays = np.concatenate([camera_rays(rng, 2048, lo=(0.2, 0.1, 0.2), hi=(0.8, 0.6, 0.8)), rays_in_box(rng, 2048)])
+    hit_fixture(m5, rays, os.path.join(HERE, "hits_mesh5.npz"),
+                extra=dict(mesh_checksum=np.array(scenes.mesh_checksum(tris)), n_tris=np.int32(tris.shape[0])))
+    material_fixture(os.path.join(HERE, "materials.npz"), rng)
+    volume_fixture(os.path.join(HERE, "volume.npz"), rng)
+    camera_fixture(os.path.join(HERE, "camera.npz"), rng)
+    image_fixture(os.path.join(HERE, "image_cornell32.npz"))
+
+
+if __name__ == "__main__":
+    main()

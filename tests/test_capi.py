@@ -1,0 +1,90 @@
+"""Host-side checks that need no GPU: the C-ABI library loads and exports every symbol
+its headers declare, argument validation returns status codes, scene flattening and
+the synthetic workloads are deterministic."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import rumi_b200
+from rumi_b200 import _capi, scenes
+from rumi_b200.scene import Scene, Rect, Sphere, Model, Matte, Emissive, AreaLight, Pinhole, Film, PathTracer
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in ("rumi_b200.h", "rumi_b200_test.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"^\s*(?:rumi_status|const char \*)\s*(rumi_\w+)\s*\(", text, re.M))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = _capi.load()
+    decl = declared_symbols()
+    assert decl == set(_capi.EXPORTS)
+    for name in decl:
+        assert getattr(L, name) is not None
+    assert L.rumi_version().decode().startswith("rumi_b200")
+
+
+def test_invalid_arguments_return_status_without_touching_the_gpu():
+    L = _capi.load()
+    h = C.c_void_p()
+    assert L.rumi_scene_create(None, C.byref(h)) == 1  # RUMI_ERR_INVALID_ARG
+    assert h.value is None
+    assert b"NULL" in L.rumi_last_error_string()
+    d = _capi.rumi_scene_desc()
+    d.width, d.height = 0, 10
+    assert L.rumi_scene_create(C.byref(d), C.byref(h)) == 1
+    # material index out of range
+    sc = scenes.cornell_pt(8, 8, 1, 2)
+    desc, keep = rumi_b200.build_desc(sc.flatten())
+    bad = np.full(desc.n_triangles, 99, np.int32)
+    desc.tri_material = bad.ctypes.data_as(_capi.IP)
+    assert L.rumi_scene_create(C.byref(desc), C.byref(h)) == 1
+    assert b"material index" in L.rumi_last_error_string()
+    # light referring to a missing rect
+    desc, keep = rumi_b200.build_desc(sc.flatten())
+    lights = (_capi.rumi_light * 1)()
+    lights[0].type, lights[0].shape_type, lights[0].shape_index = 0, 1, 7
+    desc.lights = C.cast(lights, C.POINTER(_capi.rumi_light))
+    assert L.rumi_scene_create(C.byref(desc), C.byref(h)) == 1
+    assert L.rumi_render(None, None, None, 0, None) == 1
+    assert L.rumi_trace_rays(None, 1, None, 0, None, None, 0, None, None, None) == 1
+
+
+def test_flatten_canonical_order_and_lights():
+    sc = Scene()
+    r = sc.add(Rect((0, 1, 0), (1, 0, 0), (0, 0, 1)), Emissive(2.0, (1, 1, 1)))
+    sc.add(Sphere((0, 0, 0), 0.5), Matte(1, (0.5, 0.5, 0.5)))
+    tris = np.random.default_rng(0).uniform(size=(3, 3, 3)).astype(np.float32)
+    sc.add(Model(tris), Matte(1, (0.2, 0.3, 0.4)))
+    sc.lights.append(AreaLight(r))
+    sc.camera, sc.image, sc.tracer = Pinhole((0, 0, -2)), Film(4, 4, 1), PathTracer(3)
+    fs = sc.flatten()
+    assert fs.n_prims == 5
+    assert fs.tri_vertices.shape == (3, 3, 3) and fs.rects.shape == (1, 9) and fs.spheres.shape == (1, 4)
+    assert fs.lights == [dict(type=0, shape_type=1, shape_index=0)]
+    # face normals exactly as Normalize(Cross(v1 - v0, v2 - v0)) in float32
+    e1, e2 = tris[:, 1] - tris[:, 0], tris[:, 2] - tris[:, 0]
+    c = np.cross(e1, e2).astype(np.float32)
+    n = c * (np.float32(1) / np.sqrt((c * c).sum(1, dtype=np.float32)))[:, None]
+    np.testing.assert_array_equal(fs.tri_normals[:, 0], n.astype(np.float32))
+
+
+def test_synthetic_meshes_are_deterministic():
+    t5 = scenes.displaced_sphere(5, (0.5, 0.35, 0.5), 0.25, 0.05, 7)
+    assert t5.shape == (4 * 4 ** 5, 3, 3)
+    assert scenes.mesh_checksum(t5) == scenes.mesh_checksum(scenes.displaced_sphere(5, (0.5, 0.35, 0.5), 0.25, 0.05, 7))
+    assert scenes.mesh_checksum(t5) != scenes.mesh_checksum(scenes.displaced_sphere(5, (0.5, 0.35, 0.5), 0.25, 0.05, 8))
+    # the 1,048,576-triangle workload mesh: count is 4 * 4^9
+    assert 4 * 4 ** 9 == 1048576
+    r = np.linalg.norm(t5.reshape(-1, 3) - np.array([0.5, 0.35, 0.5], np.float32), axis=1)
+    assert r.min() > 0.19 and r.max() < 0.31
+    alb = scenes.random_albedo(1000, 8)
+    assert alb.min() >= 0.2 and alb.max() <= 0.8

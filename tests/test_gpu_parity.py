@@ -1,0 +1,262 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the reference's own outputs
+(golden vectors and the live reference build in oracle/_ref) and against the CPU oracle
+on identical seeded inputs.
+
+Tolerances: primitive ids bit-exact except exact-t ties; hit distances bit-exact (the
+intersection arithmetic is restated with correctly rounded operations); BSDF / phase /
+medium / camera routines within 1e-5; renders: per-pixel agreement with the oracle on the
+same random stream, and per-pixel means within 3 sigma of the reference's frames."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oraclelib as O
+import refimpl
+import rumi_b200
+from rumi_b200 import _capi, scenes
+from test_oracle_golden import KAT, MATERIALS, material_from_params, rays8, tie_mask
+
+pytestmark = pytest.mark.gpu
+
+
+def vp(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return _capi.load()
+
+
+def test_gpu_philox_known_answers_and_oracle(lib):
+    rng = np.random.default_rng(5)
+    ctr = rng.integers(0, 2 ** 32, size=(4096, 4), dtype=np.uint64).astype(np.uint32)
+    for c, k, want in KAT:
+        ctr1 = np.array([c], np.uint32)
+        out = np.zeros((1, 4), np.uint32)
+        assert lib.rumi_test_philox(1, vp(ctr1), vp(np.array(k, np.uint32)), vp(out)) == 0
+        assert tuple(int(x) for x in out[0]) == want
+    key = np.array([0x12345678, 0x9ABCDEF0], np.uint32)
+    out = np.zeros((4096, 4), np.uint32)
+    assert lib.rumi_test_philox(4096, vp(ctr), vp(key), vp(out)) == 0
+    for i in range(0, 4096, 97):
+        assert list(out[i]) == O.philox([int(x) for x in ctr[i]], [int(x) for x in key])
+
+
+@pytest.mark.parametrize("fixture,builder", [
+    ("hits_cornell.npz", lambda: scenes.cornell_pt(64, 64, 16, 8)),
+    ("hits_mesh5.npz", lambda: scenes.bvh_bound_pt(64, 64, 4, 10, levels=5, seed=7)),
+])
+def test_gpu_hits_match_reference_golden(golden, fixture, builder):
+    g = golden(fixture)
+    gs = rumi_b200.GpuScene(builder())
+    t, prim, nv, pt = gs.trace(g["rays"])
+    ties = tie_mask(t, prim, g["t"], g["prim"])
+    assert np.all((prim == g["prim"]) | ties)
+    assert ties.mean() < 0.01
+    np.testing.assert_array_equal(t, g["t"])
+    for key in ("shadow", "shadow2"):
+        _, occ, _, _ = gs.trace(g[f"{key}_rays"], anyhit=True)
+        np.testing.assert_array_equal(occ, g[f"{key}_occluded"])
+    gs.close()
+
+
+def test_gpu_hits_1m_mesh_match_live_reference():
+    """The 1,048,576-triangle workload mesh: GPU SAH BVH vs the reference's own BVHAccel."""
+    sc = scenes.bvh_bound_pt(64, 64, 4, 10, levels=9, seed=7)
+    rng = np.random.default_rng(11)
+    n = 16384
+    o = np.tile(np.array([[0.5, 0.5, -1.4]], np.float32), (n, 1))
+    tgt = rng.uniform([0.2, 0.1, 0.2], [0.8, 0.6, 0.8], (n, 3)).astype(np.float32)
+    d = tgt - o
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    rays = np.concatenate([o, d, np.full((n, 1), 3.4e38, np.float32)], 1).astype(np.float32)
+    # secondary rays from inside the box toward the mesh
+    o2 = rng.uniform(0.05, 0.95, (n, 3)).astype(np.float32)
+    d2 = rng.normal(size=(n, 3)).astype(np.float32)
+    d2 /= np.linalg.norm(d2, axis=1, keepdims=True)
+    rays = np.concatenate([rays, np.concatenate([o2, d2, np.full((n, 1), 3.4e38, np.float32)], 1)]).astype(np.float32)
+    gs = rumi_b200.GpuScene(sc)
+    t, prim, nv, pt = gs.trace(rays)
+    rs = refimpl.RefScene(sc, seed=1)
+    rt, rid = rs.trace(rays)
+    ties = tie_mask(t, prim, rt, rid)
+    assert np.all((prim == rid) | ties)
+    np.testing.assert_array_equal(t, rt)
+    sh = rays.copy()
+    sh[:, 6] = np.where(rt > 0, rt * 0.5, 0.5)
+    _, occ, _, _ = gs.trace(sh, anyhit=True)
+    _, rocc = rs.trace(sh, anyhit=True)
+    np.testing.assert_array_equal(occ, rocc)
+    rs.close()
+    gs.close()
+
+
+@pytest.mark.parametrize("name", MATERIALS)
+def test_gpu_material_sample_and_fr_match_reference(golden, lib, name):
+    g = golden("materials.npz")
+    m = O.material_struct(material_from_params(g[f"{name}_type"], g[f"{name}_params"]))
+    n, wo, u, ref = g[f"{name}_n"], g[f"{name}_wo"], g[f"{name}_u"], g[f"{name}_sample"]
+    N = n.shape[0]
+    out = np.zeros((N, 9), np.float32)
+    assert lib.rumi_test_material_sample(C.byref(m), N, vp(wo), vp(n), vp(u), vp(out)) == 0
+    np.testing.assert_allclose(out[:, 0:3], ref[:, 0:3], rtol=0, atol=1e-5)
+    np.testing.assert_array_equal(out[:, 3:5], ref[:, 3:5])
+    np.testing.assert_allclose(out[:, 5:9], ref[:, 5:9], rtol=1e-5, atol=1e-7)
+    fr = np.zeros((N, 3), np.float32)
+    wi = np.ascontiguousarray(ref[:, 0:3])
+    xi = np.ascontiguousarray(ref[:, 5])
+    pp = np.ascontiguousarray(ref[:, 6])
+    inobj = np.ascontiguousarray(g[f"{name}_inobj"].astype(np.int32))
+    assert lib.rumi_test_material_fr(C.byref(m), N, vp(n), vp(wi), vp(wo), vp(inobj), vp(xi), vp(pp),
+                                     vp(g[f"{name}_tin"]), vp(g[f"{name}_vr"]), vp(fr)) == 0
+    np.testing.assert_allclose(fr, g[f"{name}_fr"], rtol=1e-5, atol=1e-7)
+
+
+def test_gpu_medium_phase_camera_match_reference(golden, lib):
+    v = golden("volume.npz")
+    N = v["smax"].shape[0]
+    out = np.zeros((N, 9), np.float32)
+    assert lib.rumi_test_distance_sample(vp(v["sigma_s"]), vp(v["sigma_a"]), N, vp(v["smax"]), vp(v["xi"]),
+                                         vp(v["xa"]), vp(out)) == 0
+    ref = v["out"]
+    outcome = np.where(ref[:, 0] == 1, 1, np.where(ref[:, 2] == 1, 2, 0))
+    np.testing.assert_array_equal(out[:, 0].astype(int), outcome)
+    sc = outcome == 1
+    np.testing.assert_allclose(out[sc, 1], ref[sc, 1], rtol=1e-5)
+    np.testing.assert_allclose(out[:, 2:5], ref[:, 3:6], rtol=1e-5)
+    np.testing.assert_allclose(out[:, 5:8], ref[:, 6:9], rtol=1e-5)
+    g = golden("materials.npz")
+    N = g["iso_d"].shape[0]
+    ph = np.zeros((N, 4), np.float32)
+    assert lib.rumi_test_phase_sample(N, vp(g["iso_d"]), 0.0, vp(g["iso_u"]), vp(ph)) == 0
+    np.testing.assert_allclose(ph, g["iso_out"], rtol=0, atol=1e-5)
+    c = golden("camera.npz")
+    cam = _capi.rumi_camera()
+    cam.position = _capi.f3(*c["pos"])
+    cam.basis = _capi.f16(*c["basis"])
+    cam.y_ratio, cam.fov_deg = float(c["y_ratio"]), float(c["fov"])
+    N = c["pix"].shape[0]
+    co = np.zeros((N, 6), np.float32)
+    assert lib.rumi_test_camera_rays(C.byref(cam), int(c["W"]), int(c["H"]), N, vp(c["pix"].astype(np.int32)),
+                                     vp(c["smp"]), vp(co)) == 0
+    np.testing.assert_allclose(co, c["out"][:, 0:6], rtol=0, atol=1e-6)
+
+
+def test_gpu_hg_phase_matches_oracle(lib):
+    rng = np.random.default_rng(3)
+    N = 2048
+    d = rng.normal(size=(N, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    u = (rng.integers(0, 1 << 24, (N, 2)) / float(1 << 24)).astype(np.float32)
+    for gval in (0.7, -0.3):
+        out = np.zeros((N, 4), np.float32)
+        assert lib.rumi_test_phase_sample(N, vp(d), gval, vp(u), vp(out)) == 0
+        ref = np.zeros(4, np.float32)
+        for i in range(0, N, 7):
+            O.lib().orc_phase_sample(O.P(O.f32(d[i])), gval, float(u[i, 0]), float(u[i, 1]), O.P(ref))
+            np.testing.assert_allclose(out[i], ref, rtol=1e-4, atol=2e-5)
+        # mean cosine of a Henyey-Greenstein lobe is g
+        assert abs(np.mean(np.sum(out[:, 0:3] * d, 1)) - gval) < 0.03
+
+
+def test_gpu_pixel_samples_match_oracle(lib):
+    for spp in (16, 25, 32, 64):
+        n = 4 * spp
+        s = np.tile(np.arange(spp, dtype=np.int32), 4)
+        pix = np.repeat(np.array([0, 7, 1000, 123456], np.int64), spp)
+        out = np.zeros((n, 2), np.float32)
+        assert lib.rumi_test_pixel_samples(n, vp(s), spp, vp(pix), 42, vp(out)) == 0
+        ref = np.zeros(2, np.float32)
+        for i in range(n):
+            O.lib().orc_pixel_sample(int(s[i]), spp, int(pix[i]), 42, O.P(ref))
+            np.testing.assert_array_equal(out[i], ref)
+
+
+def test_gpu_render_matches_oracle_per_pixel():
+    """Same seed, same random stream: the GPU wavefront and the oracle's sequential
+    restatement produce the same pixels up to float rounding (a few paths may branch
+    differently when a decision lands within rounding of its threshold)."""
+    sc = scenes.cornell_pt(48, 48, 16, 8)
+    gs = rumi_b200.GpuScene(sc)
+    film, st = gs.render(spp=16, seed=77)
+    gs.close()
+    ofilm, onan = O.OracleScene(sc).render_pt(8, 16, 77)
+    assert st["nan_samples"] == onan == 0
+    rel = np.abs(film - ofilm) / np.maximum(np.abs(ofilm), 1e-3)
+    bad = np.mean(rel.max(2) > 1e-3)
+    assert bad < 0.02, bad
+    assert abs(film.sum() / ofilm.sum() - 1.0) < 2e-3
+
+
+def test_gpu_render_matches_reference_3sigma(golden):
+    g = golden("image_cornell32.npz")
+    sc = scenes.cornell_pt(32, 32, 16, 8)
+    gs = rumi_b200.GpuScene(sc)
+    frames = []
+    for s in range(32):
+        film, st = gs.render(spp=16, seed=9000 + s)
+        assert st["nan_samples"] == 0
+        frames.append(film / 16.0)
+    gs.close()
+    fr = np.stack(frames).astype(np.float64)
+    m, se = fr.mean(0), fr.std(0, ddof=1) / np.sqrt(fr.shape[0])
+    sig = np.sqrt(se ** 2 + g["stderr"].astype(np.float64) ** 2) + 1e-6
+    z = np.abs(m - g["mean"]) / sig
+    assert np.mean(z > 3.0) < 0.01, np.mean(z > 3.0)
+    assert abs(m.mean() / g["mean"].mean() - 1.0) < 0.01
+
+
+def test_gpu_render_is_deterministic_and_wave_size_invariant():
+    sc = scenes.cornell_pt(40, 24, 9, 6)
+    gs = rumi_b200.GpuScene(sc)
+    a, _ = gs.render(spp=9, seed=5)
+    b, _ = gs.render(spp=9, seed=5)
+    c, _ = gs.render(spp=9, seed=5, wave_paths=999)  # 111 pixels per wave, ragged last wave
+    d, _ = gs.render(spp=9, seed=6)
+    gs.close()
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(a, c)
+    assert not np.array_equal(a, d)
+
+
+def test_gpu_edge_cases():
+    # empty scene: no primitives, no lights -> black film, no error
+    from rumi_b200.scene import Scene, Pinhole, Film, PathTracer
+    sc = Scene()
+    sc.camera, sc.image, sc.tracer = Pinhole((0, 0, -1)), Film(8, 4, 1), PathTracer(3)
+    gs = rumi_b200.GpuScene(sc)
+    film, st = gs.render(spp=1, seed=1)
+    assert film.shape == (4, 8, 3) and not film.any()
+    t, prim, _, _ = gs.trace(np.array([[0, 0, 0, 0, 0, 1, 1e30]], np.float32))
+    assert t[0] == 0 and prim[0] == -1
+    gs.close()
+    # zero-direction ray (BVHAccel::Travel returns a miss), empty batch, depth 1
+    sc = scenes.cornell_pt(8, 8, 1, 1)
+    gs = rumi_b200.GpuScene(sc)
+    t, prim, _, _ = gs.trace(np.array([[0.5, 0.5, 0.5, 0, 0, 0, 1e30]], np.float32))
+    assert t[0] == 0 and prim[0] == -1
+    t, prim, _, _ = gs.trace(np.zeros((0, 7), np.float32))
+    assert t.shape == (0,)
+    film, st = gs.render(spp=1, seed=1)
+    assert np.isfinite(film).all()
+    with pytest.raises(_capi.RumiError):
+        gs.render(spp=0, seed=1)
+    gs.close()
+
+
+def test_gpu_full_size_bvh_bound_workload_properties():
+    """The 1024x1024, 64 spp, depth-10 workload on the 1,048,576-triangle mesh: finite,
+    NaN-free, and two independent seeds agree on the image mean within noise."""
+    sc = scenes.bvh_bound_pt(1024, 1024, 64, 10, levels=9, seed=7)
+    gs = rumi_b200.GpuScene(sc)
+    a, sa = gs.render(seed=1)
+    b, sb = gs.render(seed=2)
+    gs.close()
+    assert sa["paths"] == 1024 * 1024 * 64
+    assert sa["nan_samples"] == 0 and sb["nan_samples"] == 0
+    assert np.isfinite(a).all() and np.isfinite(b).all()
+    ma, mb = a.mean() / 64, b.mean() / 64
+    assert ma > 0.05
+    assert abs(ma / mb - 1.0) < 2e-3
