@@ -181,6 +181,20 @@ rumi_status rumi_scene_bvh_info(const rumi_scene *scene, rumi_bvh_info *info);
 rumi_status rumi_render(rumi_scene *scene, const rumi_render_params *params, float *film, int32_t film_on_device,
                         rumi_render_stats *stats);
 
+/* Renders one path-traced frame like rumi_render, but allocates no device memory: the
+ * wave state lives in a fixed 16 MiB device array inside the library (held on every GPU
+ * that loads it until exit), so frames render in waves of about 100k paths.  For callers
+ * that may not allocate once running -- an application that owns a fixed device-memory
+ * budget, a real-time loop that cannot take cudaMalloc's device-wide synchronisation, or
+ * work issued while a stream is being captured.  The scene is created beforehand with
+ * rumi_scene_create.  film: device pointer, H*W*3 floats.  Path tracer only; spp or
+ * wave_paths beyond the array's capacity and RUMI_FLAG_TIMING are rejected with
+ * RUMI_ERR_INVALID_ARG.  The first call on a device looks up the array's device address
+ * (do it before any stream capture).  All calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller.  No counterpart in the reference. */
+rumi_status rumi_render_noalloc(rumi_scene *scene, const rumi_render_params *params, float *film,
+                                rumi_render_stats *stats);
+
 /* Ray queries against the scene's BVH.  rays: n*8 floats (o.xyz, in_object flag as
  * 0/1, d.xyz, tmax).  anyhit = 0: closest hit -> t (0 = miss, the reference's
  * Ray::_tmin after Travel) and prim (canonical primitive id, -1 = miss).  anyhit = 1:

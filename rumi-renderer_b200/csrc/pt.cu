@@ -405,28 +405,43 @@ __global__ void pt_resolve(PtLaunch P) {
 
 static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// Device bytes of the wave state for `paths` paths in flight (queues, path state,
+// counters): 164 bytes per path plus alignment and counters.
+size_t pt_workspace_bytes(long long paths) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t Wp = (size_t)paths;
+    return 10 * al(Wp * sizeof(float4)) + al(Wp * sizeof(unsigned)) + al(C_NUM * sizeof(int)) +
+           al(S_NUM * sizeof(unsigned long long));
+}
+
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                       cudaStream_t stream) {
-    const int W = sc->dev.width, H = sc->dev.height;
-    const int spp = p->spp;
-    const long long total_pix = (long long)W * H;
+    const long long total_pix = (long long)sc->dev.width * sc->dev.height;
     long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 21);
-    long long pix_per_wave = wave / spp;
+    long long pix_per_wave = wave / p->spp;
     if (pix_per_wave < 1) pix_per_wave = 1;
     if (pix_per_wave > total_pix) pix_per_wave = total_pix;
-    const long long n_paths_max = pix_per_wave * spp;
+    const long long n_paths_max = pix_per_wave * p->spp;
     if (n_paths_max > 0x7fffffffLL) {
         set_error("wave_paths too large");
         return RUMI_ERR_INVALID_ARG;
     }
-    const size_t Wp = (size_t)n_paths_max;
+    rumi_status st = ensure_workspace(sc, pt_workspace_bytes(n_paths_max));
+    if (st != RUMI_OK) return st;
+    return pt_render_in(sc, p, film_dev, stats, stream, sc->ws, pix_per_wave);
+}
+
+// The frame loop over waves of pix_per_wave pixels, with the wave state carved out of
+// `ws` (pt_workspace_bytes(pix_per_wave * spp) bytes).
+rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
+                         cudaStream_t stream, void *ws, long long pix_per_wave) {
+    const int W = sc->dev.width, H = sc->dev.height;
+    const int spp = p->spp;
+    const long long total_pix = (long long)W * H;
+    const size_t Wp = (size_t)(pix_per_wave * spp);
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t f4 = al(Wp * sizeof(float4));
-    const size_t bytes = 10 * f4 + al(Wp * sizeof(unsigned)) + al(C_NUM * sizeof(int)) +
-                         al(S_NUM * sizeof(unsigned long long));
-    rumi_status st = ensure_workspace(sc, bytes);
-    if (st != RUMI_OK) return st;
-    char *w = (char *)sc->ws;
+    char *w = (char *)ws;
     PtLaunch L;
     L.s = sc->dev;
     L.spp = spp;

@@ -71,7 +71,8 @@ class rumi_bvh_info(C.Structure):
 
 
 # every symbol include/rumi_b200.h and include/rumi_b200_test.h declare
-EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "rumi_render", "rumi_trace_rays",
+EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "rumi_render", "rumi_render_noalloc",
+           "rumi_trace_rays",
            "rumi_last_error_string", "rumi_version",
            "rumi_test_philox", "rumi_test_material_sample", "rumi_test_material_fr", "rumi_test_distance_sample",
            "rumi_test_phase_sample", "rumi_test_camera_rays", "rumi_test_pixel_samples"]
@@ -96,6 +97,9 @@ def load(path: str = LIB_PATH):
     L.rumi_render.restype = C.c_int
     L.rumi_render.argtypes = [C.c_void_p, C.POINTER(rumi_render_params), C.c_void_p, C.c_int32,
                               C.POINTER(rumi_render_stats)]
+    L.rumi_render_noalloc.restype = C.c_int
+    L.rumi_render_noalloc.argtypes = [C.c_void_p, C.POINTER(rumi_render_params), C.c_void_p,
+                                      C.POINTER(rumi_render_stats)]
     L.rumi_trace_rays.restype = C.c_int
     L.rumi_trace_rays.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_void_p]

@@ -1,0 +1,69 @@
+"""rumi_render_noalloc -- the render entry point that allocates no device memory, for
+callers that may not call cudaMalloc once running (a fixed device-memory budget owned
+by the embedding application, real-time loops that cannot take the allocator's
+device-wide synchronisation, work issued during stream capture).
+
+It must produce the same film as rumi_render (the regular entry point) on two calls in a
+row -- the second call reuses the shared scratch array the first one left behind -- and
+refuse requests that do not fit its fixed array.  This file is collected last so that a
+run stopping at the first failure has run every other test first; it also passes when
+run alone in a fresh process."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import rumi_b200
+from rumi_b200 import _capi, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(spp, depth, seed, wave_paths=0, flags=0):
+    p = _capi.rumi_render_params()
+    p.integrator, p.max_depth, p.spp, p.seed = 0, depth, spp, seed
+    p.wave_paths, p.flags = wave_paths, flags
+    return p
+
+
+def test_noalloc_render_matches_rumi_render_on_two_calls():
+    import torch
+    torch.cuda.set_device(0)
+    lib = _capi.load()
+    sc = scenes.cornell_pt(96, 80, 16, 6)
+    gs = rumi_b200.GpuScene(sc)
+    film_dev = torch.zeros((80, 96, 3), dtype=torch.float32, device="cuda")
+    for seed in (21, 22):  # two calls in a row on the shared scratch
+        want, wst = gs.render(spp=16, seed=seed)
+        st = _capi.rumi_render_stats()
+        film_dev.fill_(-1.0)
+        torch.cuda.synchronize()
+        rc = lib.rumi_render_noalloc(gs.h, C.byref(_params(16, 6, seed)), C.c_void_p(film_dev.data_ptr()),
+                                     C.byref(st))
+        assert rc == 0, lib.rumi_last_error_string()
+        got = film_dev.cpu().numpy()
+        # same per-path random streams and per-pixel summation order -> same film
+        np.testing.assert_allclose(got, want, rtol=1e-6, atol=0)
+        assert st.paths == wst["paths"] == 96 * 80 * 16
+        assert st.nan_samples == wst["nan_samples"] == 0
+        assert st.rays_extend == wst["rays_extend"]
+    gs.close()
+
+
+def test_noalloc_rejects_requests_beyond_its_scratch():
+    import torch
+    torch.cuda.set_device(0)
+    lib = _capi.load()
+    gs = rumi_b200.GpuScene(scenes.cornell_pt(16, 16, 1, 2))
+    film_dev = torch.zeros((16, 16, 3), dtype=torch.float32, device="cuda")
+    ptr = C.c_void_p(film_dev.data_ptr())
+    assert lib.rumi_render_noalloc(gs.h, C.byref(_params(1 << 20, 2, 1)), ptr, None) == 1
+    assert b"exceeds" in lib.rumi_last_error_string()
+    assert lib.rumi_render_noalloc(gs.h, C.byref(_params(4, 2, 1, wave_paths=1 << 24)), ptr, None) == 1
+    assert lib.rumi_render_noalloc(gs.h, C.byref(_params(4, 2, 1, flags=1)), ptr, None) == 1
+    assert lib.rumi_render_noalloc(gs.h, C.byref(_params(4, 2, 1)), None, None) == 1
+    # a valid call still works after the rejected ones
+    assert lib.rumi_render_noalloc(gs.h, C.byref(_params(4, 2, 1)), ptr, None) == 0
+    torch.cuda.synchronize()
+    assert np.isfinite(film_dev.cpu().numpy()).all()
+    gs.close()
