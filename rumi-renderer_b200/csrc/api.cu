@@ -23,15 +23,45 @@ rumi_status cuda_status(cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? RUMI_ERR_OOM : RUMI_ERR_CUDA;
 }
 
+// Device allocations of scenes and render workspaces come from the device's default
+// stream-ordered memory pool.  The pool keeps up to POOL_KEEP_BYTES of freed memory for
+// reuse within this process, so creating a scene after destroying one does not go back
+// to the driver.
+static constexpr unsigned long long POOL_KEEP_BYTES = 16ull << 30;
+
+void configure_pool(int device) {
+    static bool done[64] = {};
+    if (device < 0 || device >= 64 || done[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        unsigned long long keep = POOL_KEEP_BYTES;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    done[device] = true;
+}
+
+cudaError_t dalloc(void **p, size_t bytes, cudaStream_t s) {
+    cudaError_t e = cudaMallocAsync(p, bytes > 0 ? bytes : 256, s);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+    }
+    return e;
+}
+
+void dfree(void *p, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+}
+
 rumi_status ensure_workspace(rumi_scene *sc, size_t bytes) {
     if (sc->ws_bytes >= bytes) return RUMI_OK;
     if (sc->ws) {
-        cudaStreamSynchronize(sc->stream);
-        cudaFree(sc->ws);
+        dfree(sc->ws, sc->stream);
         sc->ws = nullptr;
         sc->ws_bytes = 0;
     }
-    cudaError_t e = cudaMalloc(&sc->ws, bytes);
+    cudaError_t e = dalloc(&sc->ws, bytes, sc->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return cuda_status(e, "workspace allocation");
@@ -50,11 +80,8 @@ template <typename T>
 rumi_status upload(T **dst, const void *src, size_t bytes, cudaStream_t s) {
     *dst = nullptr;
     if (bytes == 0) return RUMI_OK;
-    cudaError_t e = cudaMalloc((void **)dst, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return cuda_status(e, "cudaMalloc");
-    }
+    cudaError_t e = dalloc((void **)dst, bytes, s);
+    if (e != cudaSuccess) return cuda_status(e, "device allocation");
     e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_status(e, "cudaMemcpyAsync");
     return RUMI_OK;
@@ -64,18 +91,21 @@ float f_len(const float *v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] 
 
 void free_scene(rumi_scene *sc) {
     if (!sc) return;
-    if (sc->stream) cudaStreamSynchronize(sc->stream);
-    cudaFree(sc->nodes);
-    cudaFree(sc->leaf_prims);
-    cudaFree(sc->tri_shade);
-    cudaFree(sc->tri_albedo);
-    cudaFree(sc->rects);
-    cudaFree(sc->spheres);
-    cudaFree(sc->sphere_mat);
-    cudaFree(sc->materials);
-    cudaFree(sc->lights);
-    cudaFree(sc->ws);
-    if (sc->stream) cudaStreamDestroy(sc->stream);
+    cudaStream_t s = sc->stream;
+    dfree(sc->nodes, s);
+    dfree(sc->leaf_prims, s);
+    dfree(sc->tri_shade, s);
+    dfree(sc->tri_albedo, s);
+    dfree(sc->rects, s);
+    dfree(sc->spheres, s);
+    dfree(sc->sphere_mat, s);
+    dfree(sc->materials, s);
+    dfree(sc->lights, s);
+    dfree(sc->ws, s);
+    if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
     delete sc;
 }
 
@@ -146,6 +176,34 @@ DevMaterial make_material(const rumi_material &m) {
     return d;
 }
 
+// tri_shade[3i..3i+2] = (n0, material), (n1, 0), (n2, 0); without normals the face
+// normal Normalize(Cross(v1 - v0, v2 - v0)) as Model::LoadObjectFile computes it
+// (src/Shape/model.cpp:320-323), with correctly rounded operations.
+__global__ void pack_tri_shade_kernel(const float *verts, const float *nrm, const int *mat, int n, float4 *out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float3 n0, n1, n2;
+        if (nrm) {
+            const float *q = nrm + 9 * (size_t)i;
+            n0 = make_float3(q[0], q[1], q[2]);
+            n1 = make_float3(q[3], q[4], q[5]);
+            n2 = make_float3(q[6], q[7], q[8]);
+        } else {
+            const float *v = verts + 9 * (size_t)i;
+            const float3 v0 = make_float3(v[0], v[1], v[2]);
+            const float3 e1 = rn_sub(make_float3(v[3], v[4], v[5]), v0), e2 = rn_sub(make_float3(v[6], v[7], v[8]), v0);
+            n0 = n1 = n2 = normalize_ref(rn_cross(e1, e2));
+        }
+        out[3 * (size_t)i + 0] = make_float4(n0.x, n0.y, n0.z, __int_as_float(mat[i]));
+        out[3 * (size_t)i + 1] = make_float4(n1.x, n1.y, n1.z, 0.0f);
+        out[3 * (size_t)i + 2] = make_float4(n2.x, n2.y, n2.z, 0.0f);
+    }
+}
+
+__global__ void pack_albedo_kernel(const float *a, int n, float4 *out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = make_float4(a[3 * (size_t)i], a[3 * (size_t)i + 1], a[3 * (size_t)i + 2], 0.0f);
+}
+
 }  // namespace
 
 extern "C" {
@@ -170,34 +228,7 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     cudaStream_t s = sc->stream;
     const int nT = d->n_triangles, nR = d->n_rects, nS = d->n_spheres;
     const int N = nT + nR + nS;
-    // ---- shading data (canonical order)
-    std::vector<float4> tri_shade((size_t)nT * 3);
-    for (int i = 0; i < nT; ++i) {
-        const float *v = d->tri_vertices + 9 * (size_t)i;
-        float n[9];
-        if (d->tri_normals) {
-            memcpy(n, d->tri_normals + 9 * (size_t)i, sizeof(n));
-        } else {  // Normalize(Cross(v1 - v0, v2 - v0))
-            const float e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
-            const float e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
-            const float c[3] = {e1[1] * e2[2] - e2[1] * e1[2], e1[2] * e2[0] - e2[2] * e1[0],
-                                e1[0] * e2[1] - e2[0] * e1[1]};
-            const float inv = 1.0f / std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-            for (int k = 0; k < 3; ++k) n[3 * k] = c[0] * inv, n[3 * k + 1] = c[1] * inv, n[3 * k + 2] = c[2] * inv;
-        }
-        int mi = d->tri_material[i];
-        float mif;
-        memcpy(&mif, &mi, 4);
-        tri_shade[3 * (size_t)i + 0] = make_float4(n[0], n[1], n[2], mif);
-        tri_shade[3 * (size_t)i + 1] = make_float4(n[3], n[4], n[5], 0.0f);
-        tri_shade[3 * (size_t)i + 2] = make_float4(n[6], n[7], n[8], 0.0f);
-    }
-    std::vector<float4> tri_albedo;
-    if (d->tri_albedo) {
-        tri_albedo.resize(nT);
-        for (int i = 0; i < nT; ++i)
-            tri_albedo[i] = make_float4(d->tri_albedo[3 * i], d->tri_albedo[3 * i + 1], d->tri_albedo[3 * i + 2], 0.0f);
-    }
+    configure_pool(sc->device);
     std::vector<float4> rects((size_t)nR * 3);
     std::vector<int> rect_emissive(nR);
     std::vector<DevMaterial> mats(d->n_materials);
@@ -285,22 +316,36 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
         dc.dir = make_float3(c.basis[2] + c.basis[3], c.basis[6] + c.basis[7], c.basis[10] + c.basis[11]);
     }
     // ---- uploads
-    float *d_tri_v = nullptr;
-    int *d_rect_em = nullptr;
+    float *d_tri_v = nullptr, *d_tri_n = nullptr, *d_alb = nullptr;
+    int *d_rect_em = nullptr, *d_tri_m = nullptr;
     void *scratch = nullptr;
     auto fail = [&](rumi_status code) {
-        cudaFree(d_tri_v);
-        cudaFree(d_rect_em);
-        cudaFree(scratch);
+        dfree(d_tri_v, s);
+        dfree(d_tri_n, s);
+        dfree(d_tri_m, s);
+        dfree(d_alb, s);
+        dfree(d_rect_em, s);
+        dfree(scratch, s);
         free_scene(sc);
         return code;
     };
+    const int pack_grid = nT > 0 ? (nT + 255) / 256 < sc->num_sms * 8 ? (nT + 255) / 256 : sc->num_sms * 8 : 1;
     if ((st = upload(&d_tri_v, d->tri_vertices, sizeof(float) * 9 * (size_t)nT, s)) != RUMI_OK) return fail(st);
-    if ((st = upload(&sc->tri_shade, tri_shade.data(), sizeof(float4) * tri_shade.size(), s)) != RUMI_OK)
-        return fail(st);
-    if (!tri_albedo.empty() &&
-        (st = upload(&sc->tri_albedo, tri_albedo.data(), sizeof(float4) * tri_albedo.size(), s)) != RUMI_OK)
-        return fail(st);
+    if (nT > 0) {
+        if (d->tri_normals &&
+            (st = upload(&d_tri_n, d->tri_normals, sizeof(float) * 9 * (size_t)nT, s)) != RUMI_OK)
+            return fail(st);
+        if ((st = upload(&d_tri_m, d->tri_material, sizeof(int) * (size_t)nT, s)) != RUMI_OK) return fail(st);
+        e = dalloc((void **)&sc->tri_shade, sizeof(float4) * 3 * (size_t)nT, s);
+        if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
+        pack_tri_shade_kernel<<<pack_grid, 256, 0, s>>>(d_tri_v, d_tri_n, d_tri_m, nT, sc->tri_shade);
+        if (d->tri_albedo) {
+            if ((st = upload(&d_alb, d->tri_albedo, sizeof(float) * 3 * (size_t)nT, s)) != RUMI_OK) return fail(st);
+            e = dalloc((void **)&sc->tri_albedo, sizeof(float4) * (size_t)nT, s);
+            if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
+            pack_albedo_kernel<<<pack_grid, 256, 0, s>>>(d_alb, nT, sc->tri_albedo);
+        }
+    }
     if ((st = upload(&sc->rects, rects.data(), sizeof(float4) * rects.size(), s)) != RUMI_OK) return fail(st);
     if ((st = upload(&d_rect_em, rect_emissive.data(), sizeof(int) * rect_emissive.size(), s)) != RUMI_OK)
         return fail(st);
@@ -310,12 +355,12 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     if ((st = upload(&sc->lights, lights.data(), sizeof(DevLight) * lights.size(), s)) != RUMI_OK) return fail(st);
     // ---- BVH
     sc->n_nodes = bvh_node_capacity(N);
-    e = cudaMalloc(&sc->nodes, sizeof(BvhNode) * (size_t)sc->n_nodes);
-    if (e != cudaSuccess) return fail(cuda_status(e, "cudaMalloc nodes"));
-    e = cudaMalloc(&sc->leaf_prims, sizeof(float4) * 3 * (size_t)(N > 0 ? N : 1));
-    if (e != cudaSuccess) return fail(cuda_status(e, "cudaMalloc prims"));
-    e = cudaMalloc(&scratch, bvh_scratch_bytes(N));
-    if (e != cudaSuccess) return fail(cuda_status(e, "cudaMalloc BVH scratch"));
+    e = dalloc((void **)&sc->nodes, sizeof(BvhNode) * (size_t)sc->n_nodes, s);
+    if (e != cudaSuccess) return fail(cuda_status(e, "device allocation (nodes)"));
+    e = dalloc((void **)&sc->leaf_prims, sizeof(float4) * 3 * (size_t)(N > 0 ? N : 1), s);
+    if (e != cudaSuccess) return fail(cuda_status(e, "device allocation (primitives)"));
+    e = dalloc(&scratch, bvh_scratch_bytes(N), s);
+    if (e != cudaSuccess) return fail(cuda_status(e, "device allocation (BVH scratch)"));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -334,11 +379,14 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
         set_error("bvh_build: internal limit reached");
         return fail(RUMI_ERR_INTERNAL);
     }
-    cudaFree(d_tri_v);
-    d_tri_v = nullptr;
-    cudaFree(d_rect_em);
-    d_rect_em = nullptr;
-    cudaFree(scratch);
+    dfree(d_tri_v, s);
+    dfree(d_tri_n, s);
+    dfree(d_tri_m, s);
+    dfree(d_alb, s);
+    dfree(d_rect_em, s);
+    dfree(scratch, s);
+    d_tri_v = d_tri_n = d_alb = nullptr;
+    d_rect_em = d_tri_m = nullptr;
     scratch = nullptr;
     ds.nodes = sc->nodes;
     ds.leaf_prims = sc->leaf_prims;
@@ -379,30 +427,31 @@ rumi_status rumi_render(rumi_scene *sc, const rumi_render_params *p, float *film
     float *film_dev = film;
     float *tmp = nullptr;
     if (!film_on_device) {
-        cudaError_t e = cudaMalloc(&tmp, film_bytes);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return cuda_status(e, "cudaMalloc film");
-        }
+        cudaError_t e = dalloc((void **)&tmp, film_bytes, s);
+        if (e != cudaSuccess) return cuda_status(e, "device allocation (film)");
         film_dev = tmp;
     }
     rumi_status st;
     if (p->integrator == RUMI_PATH_TRACER) {
         if (p->max_depth <= 0) {
-            cudaFree(tmp);
+            dfree(tmp, s);
             return set_error("max_depth must be positive"), RUMI_ERR_INVALID_ARG;
         }
         st = pt_render(sc, p, film_dev, stats, s);
+    } else if (p->integrator == RUMI_BDPT) {
+        st = bdpt_render(sc, p, film_dev, stats, s);
     } else {
-        cudaFree(tmp);
-        return set_error("integrator not available"), RUMI_ERR_INVALID_ARG;
+        dfree(tmp, s);
+        return set_error("unknown integrator"), RUMI_ERR_INVALID_ARG;
     }
     if (st == RUMI_OK && !film_on_device) {
         cudaError_t e = cudaMemcpyAsync(film, film_dev, film_bytes, cudaMemcpyDeviceToHost, s);
+        dfree(tmp, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = cuda_status(e, "film copy");
+    } else {
+        dfree(tmp, s);
     }
-    cudaFree(tmp);
     return st;
 }
 
@@ -414,13 +463,10 @@ rumi_status rumi_trace_rays(rumi_scene *sc, int64_t n, const float *rays, int32_
     float *dr = nullptr, *dt = nullptr;
     int32_t *dp = nullptr;
     rumi_status st = RUMI_OK;
-    cudaError_t e = cudaMalloc(&dr, sizeof(float) * 8 * (size_t)(n > 0 ? n : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&dt, sizeof(float) * (size_t)(n > 0 ? n : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&dp, sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        st = cuda_status(e, "cudaMalloc rays");
-    }
+    cudaError_t e = dalloc((void **)&dr, sizeof(float) * 8 * (size_t)(n > 0 ? n : 1), s);
+    if (e == cudaSuccess) e = dalloc((void **)&dt, sizeof(float) * (size_t)(n > 0 ? n : 1), s);
+    if (e == cudaSuccess) e = dalloc((void **)&dp, sizeof(int32_t) * (size_t)(n > 0 ? n : 1), s);
+    if (e != cudaSuccess) st = cuda_status(e, "device allocation (rays)");
     if (st == RUMI_OK) {
         cudaMemcpyAsync(dr, rays, sizeof(float) * 8 * (size_t)n, cudaMemcpyHostToDevice, s);
         st = trace_rays(sc, n, dr, anyhit, dt, dp, node_visits, prim_tests, s);
@@ -431,9 +477,10 @@ rumi_status rumi_trace_rays(rumi_scene *sc, int64_t n, const float *rays, int32_
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = cuda_status(e, "trace copy");
     }
-    cudaFree(dr);
-    cudaFree(dt);
-    cudaFree(dp);
+    dfree(dr, s);
+    dfree(dt, s);
+    dfree(dp, s);
+    cudaStreamSynchronize(s);
     return st;
 }
 

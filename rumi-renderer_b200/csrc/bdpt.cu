@@ -1,0 +1,819 @@
+// Bidirectional path tracing with multiple importance sampling, restating
+// BidirectionalPathTracer (src/Integrator/bidirectionalpathtracer.cpp):
+//   Trace                 :121-394  all (s, t) strategies of one camera sample
+//   ConstructViewPath     :396-711  camera subpath with area-measure pdfs and throughput
+//   ConstructLightPath    :713-1016 light subpath
+//   VisibilityTest        :1018-1050
+//   VolumetricTest        :1052-1094
+//   MISWeight             :1096-1586 balance heuristic over pdf ratios, "locked" rule
+// One thread renders one camera sample: both subpaths live in per-thread arrays
+// (the reference's Path[] / Color[] members), pdfs are RGB because medium pdfs are.
+// Light-tracing strategies (t = 1, the camera vertex) splat through the film plane
+// into a separate buffer with atomic adds, added to the pixel sums at the end (the
+// reference's Film::LightPixel + CombineBuffer, src/Camera/film.cpp:99-150).
+#include "renderer.h"
+#include "traverse.cuh"
+#include "shading.cuh"
+#include "camera.cuh"
+
+namespace rumi {
+
+static constexpr int BD_THREADS = 64;
+static constexpr int BD_STACK = 32;
+static constexpr int BD_MAXV = 16;  // vertices per subpath (nE, nL <= 16)
+
+struct BVert {
+    float3 p, n;
+    float3 pdf_fwd, pdf_bwd;  // _pdf_pforward / _pdf_pbackward (area measure)
+    float pdf_dir;            // _pdf_wi (eye) / _pdf_wo (light) of the sampled outgoing direction
+    float pdf_path;           // _pdf_path (lobe probability)
+    float cos_a;              // eye: _costheta_i, light: _costheta_o (outgoing side)
+    float cos_b;              // eye: _costheta_o, light: _costheta_i (arriving side)
+    bool dirac, onsurface;
+    // Intersection of the segment arriving at this vertex
+    int mat;                  // material index of the hit surface (-1: none)
+    int prim;
+    float xi;                 // _rand
+    bool in_obj;              // _in_object
+    float t_in;               // ray _tmin
+    float3 d_in;              // direction of the arriving segment
+    float3 vtau, vpdf;        // _volumetric_tau / _volumetric_pdf
+};
+
+RUMI_D void bvert_clear(BVert &v) {
+    v.p = v.n = mk3(0, 0, 0);
+    v.pdf_fwd = v.pdf_bwd = mk3(1, 1, 1);
+    v.pdf_dir = 1.0f;
+    v.pdf_path = 1.0f;
+    v.cos_a = v.cos_b = 1.0f;
+    v.dirac = false;
+    v.onsurface = true;
+    v.mat = -1;
+    v.prim = -1;
+    v.xi = 1.0f;
+    v.in_obj = false;
+    v.t_in = 0.0f;
+    v.d_in = mk3(0, 0, 0);
+    v.vtau = v.vpdf = mk3(1, 1, 1);
+}
+
+struct BdLaunch {
+    DevScene s;
+    int nL, nE, spp;
+    uint32_t k0, k1;
+    int grid_d, square;
+    long long path0;
+    int n_paths, pix0;
+    float4 *L;           // per-path radiance (sample value of Trace)
+    float *light_film;   // H*W*3 (B,G,R) light-tracing splats
+    float3 right, up;    // camera basis (film plane)
+};
+
+RUMI_D float3 c3(float v) { return mk3(v, v, v); }
+
+// HomogeneousVolume::Tr over [0, s] (homogeneousvolume.cpp:46-54)
+RUMI_D float3 vol_tr(const DevVolume &V, float s) {
+    return mk3(expf(V.sigma_t.x * -s), expf(V.sigma_t.y * -s), expf(V.sigma_t.z * -s));
+}
+// HomogeneousVolume::PdfDistance (homogeneousvolume.cpp:100-111)
+RUMI_D float3 vol_pdf_distance(const DevVolume &V, float s) {
+    float3 pdf = vol_tr(V, s) * V.sigma_t;
+    if (pdf.x == 0.0f && pdf.y == 0.0f && pdf.z == 0.0f) pdf = c3(1e-4f);
+    return pdf;
+}
+// Scattering-ray segment as MISWeight / the subpath loops form it: Intersect (return
+// value ignored where the reference ignores it), MaxDistance.
+RUMI_D float vol_segment(const DevVolume &V, float3 o, float3 d, float tmax, bool &hit) {
+    float tn, tf;
+    hit = volume_intersect(V, o, d, 0.0f, tn, tf);
+    return volume_max_distance(tmax, tn, tf);
+}
+
+// Pinhole::FilmPlaneIntersection (pinhole.cpp:138-167) with the film plane of
+// Pinhole::AddFilmPlane (pinhole.cpp:64-82).
+RUMI_D bool film_plane_pixel(const BdLaunch &P, float3 pos, int &wi, int &hi) {
+    const DevCamera &c = P.s.camera;
+    const float width = 2.0f * c.tanfov, height = 2.0f * c.tanfov * c.y_ratio;
+    float3 sp = c.p - P.right * (0.5f * width);
+    sp = sp - P.up * (0.5f * height);
+    sp = sp + c.dir * c.plane_dist;
+    const float3 lv = P.right * width, wv = P.up * height;
+    const float3 d = normalize_ref(c.p - pos);
+    float t;
+    // the film plane Rect carries no material: two-sided
+    if (!isect_rect(pos, d, FLT_MAX, 0.0f, make_float4(sp.x, sp.y, sp.z, 0), make_float4(lv.x, lv.y, lv.z, 0),
+                    make_float4(wv.x, wv.y, wv.z, 0), true, t))
+        return false;
+    const float3 ip = pos + d * t;
+    const float3 on = ip - sp;
+    const float llen = sqrtf(dot3(lv, lv)), wlen = sqrtf(dot3(wv, wv));
+    float u = dot3(on, lv) / (llen * llen);
+    float v = dot3(on, wv) / (wlen * wlen);
+    u = (float)P.s.width * (1.0f - u);
+    v = (float)P.s.height * (1.0f - v);
+    if (u == (float)P.s.width) u -= 1.0f;
+    if (v == (float)P.s.height) v -= 1.0f;
+    wi = (int)u;
+    hi = (int)v;
+    return true;
+}
+
+// Hit -> vertex fields (position, normal, material).
+RUMI_D void record_hit(const DevScene &S, const HitRec &h, float3 o, float3 d, BVert &v) {
+    v.p = o + d * h.t;
+    v.prim = h.id;
+    v.mat = prim_material(S, h.id);
+    v.n = surface_normal(S, h.id, h.back != 0, h.u, h.v, o, v.p, S.materials[v.mat]);
+}
+
+RUMI_D float3 vert_albedo(const DevScene &S, const BVert &v, const DevMaterial &m) {
+    if (S.tri_albedo && v.prim >= 0 && v.prim < S.n_tris) return f4xyz(__ldg(&S.tri_albedo[v.prim]));
+    return m.rgb;
+}
+
+// Material::Fr with the vertex's arriving Intersection state.
+RUMI_D float3 vert_fr(const DevScene &S, const BVert &v, float3 n, float3 wi, float3 wo) {
+    const DevMaterial m = S.materials[v.mat];
+    return material_fr(m, vert_albedo(S, v, m), n, wi, wo, v.in_obj, v.xi, v.pdf_path, v.t_in, v.vtau / v.vpdf);
+}
+
+// Subpath construction shared by both directions.  EYE: ConstructViewPath, else
+// ConstructLightPath.  V[0] is prepared by the caller; seg_d[k] receives the direction of
+// the segment from V[k] to V[k+1]; alpha[] the subpath throughputs.  Returns the vertex count.
+template <bool EYE>
+RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, uint32_t stream_base, float3 o,
+                             float3 d, BVert *V, float3 *seg_d, float3 *alpha, const DevLight &light, float3 light_n,
+                             int *stack, TraceStats &st) {
+    const DevScene &S = P.s;
+    const DevVolume &vol = S.volume;
+    bool le = true, in_object = false;
+    alpha[0] = c3(1.0f);
+    int n_vertex = 1;
+    int prev_mat = -1;
+    float3 prev_w = mk3(0, 0, 0);  // prev_wo (eye) / prev_wi (light)
+    const int max_seg = max_depth - 1;  // the reference's Path[max_depth - 1] array
+    for (int depth = 0; depth < max_depth && depth < max_seg; ++depth) {
+        BVert &start = V[depth];
+        BVert &end = V[depth + 1];
+        bvert_clear(end);
+        end.in_obj = in_object;
+        end.d_in = d;
+        seg_d[depth] = d;
+        const Uniform4 U0 = path_uniforms(path, stream_base + depth, 0, P.k0, P.k1);
+        const Uniform4 U1 = path_uniforms(path, stream_base + depth, 1, P.k0, P.k1);
+        const HitRec h = trace_ray<false, BD_STACK, false>(S, o, d, FLT_MAX, in_object, stack, BD_THREADS, st);
+        const bool hit = h.t > 0.0f;
+        end.t_in = h.t;
+        if (hit) record_hit(S, h, o, d, end);
+        float vol_s = 0.0f;
+        bool absorb = false;
+        if (vol.present && !in_object) {
+            float tn, tf;
+            if (volume_intersect(vol, o, d, h.t, tn, tf)) {
+                const float smax = volume_max_distance(h.t, tn, tf);
+                const DistSample ds = distance_sample(vol.sigma_t, vol.avg_sigma_t, vol.absorb, smax, U1.u[2], U1.u[3]);
+                if (ds.outcome == 2) {
+                    absorb = true;
+                } else {
+                    end.vtau = ds.tau;
+                    end.vpdf = ds.pdf;
+                    if (ds.outcome == 1) {
+                        vol_s = ds.s;
+                        end.p = o + d * (tn < 0.0f ? ds.s : tn + ds.s);
+                        end.onsurface = false;
+                    }
+                }
+            }
+            if (absorb) break;
+        }
+        if (!hit && vol_s == 0.0f) break;
+        ++n_vertex;
+        const bool has_mat = end.mat >= 0;
+        DevMaterial m;
+        if (has_mat) m = S.materials[end.mat];
+        const float3 wrev = -d;  // wo (eye) / wi (light)
+        float3 w, n;
+        float pdf_dir = 1.0f;
+        if (end.onsurface) {
+            n = end.n;
+            const BsdfSample b = material_sample(m, wrev, n, U0.u[0], U0.u[1], U0.u[2]);
+            w = b.w;
+            le = b.le;
+            in_object = b.go_in;
+            end.xi = b.xi;
+            end.pdf_path = b.pdf_path;
+            end.cos_a = b.cost;
+            pdf_dir = b.pdfw;
+            end.pdf_dir = pdf_dir;
+            end.dirac = material_dirac(m, b.xi);
+        } else {
+            n = mk3(0, 0, 0);
+            if (vol.g == 0.0f) {
+                w = isotropic_dir(d, U0.u[1], U0.u[2]);
+                pdf_dir = 1.0f / (4.0f * RUMI_PI_F);
+            } else {
+                w = hg_sample(d, vol.g, U0.u[1], U0.u[2], pdf_dir);
+            }
+            le = false;
+            in_object = false;
+            end.pdf_dir = pdf_dir;
+            end.dirac = false;
+        }
+        // cosine at the start vertex on its outgoing side
+        float cos_s;
+        if (start.onsurface) {
+            const bool use_stored = EYE ? (depth == 0 || !start.dirac) : !start.dirac;
+            if (use_stored) {
+                cos_s = start.cos_a;
+            } else {
+                cos_s = !end.in_obj ? dot3(d, start.n) : -dot3(d, start.n);
+                if (cos_s <= 0.0f) cos_s = 1e-4f;
+                start.cos_a = cos_s;
+            }
+        } else {
+            cos_s = 1.0f;
+            start.cos_a = 1.0f;
+        }
+        // cosine at the end vertex on its arriving side
+        float cos_e;
+        if (end.onsurface) {
+            cos_e = !end.in_obj ? -dot3(d, end.n) : dot3(d, end.n);
+            if (cos_e <= 0.0f) cos_e = 1e-4f;
+        } else {
+            cos_e = 1.0f;
+        }
+        end.cos_b = cos_e;
+        // forward pdf of the end vertex
+        const float3 se = end.p - start.p;
+        const float dist = sqrtf(dot3(se, se));
+        float dwda = cos_e / (dist * dist);
+        float fwd;
+        if (start.onsurface) {
+            const bool plain = EYE ? (depth == 0 || !start.dirac) : !start.dirac;
+            fwd = plain ? start.pdf_dir * dwda : start.pdf_dir * dwda * start.cos_a;
+        } else {
+            fwd = start.pdf_dir * dwda * start.cos_a;
+        }
+        end.pdf_fwd = c3(fwd);
+        if (vol.present && !end.in_obj) end.pdf_fwd = end.pdf_fwd * end.vpdf;
+        // backward pdf of the start vertex
+        dwda = cos_s / (dist * dist);
+        const bool end_le = has_mat && m.type == MAT_EMISSIVE;
+        float3 bwd;
+        if (start.onsurface) {
+            if (end.onsurface) {
+                float pw;
+                if (end_le) {
+                    // AreaLight::Pdfw(w) with the light's stored normal
+                    float c = dot3(wrev, light_n);
+                    if (c <= 0.0f) c = 1e-4f;
+                    pw = RUMI_INV_PI_F * c;
+                    if (pw <= 0.0f) pw = 1e-4f;
+                    bwd = c3(pw * dwda);
+                } else {
+                    pw = material_pdfw(m, end.xi, n, w, wrev);
+                    bwd = end.dirac ? c3(pw * dwda * end.cos_b) : c3(pw * dwda);
+                }
+                if (vol.present && !end.in_obj) bwd = bwd * end.vpdf;
+            } else {
+                bool vh;
+                const float sm = vol_segment(vol, end.p, -d, dist, vh);
+                bwd = vol_tr(vol, sm) * (phase_value(vol, w, wrev) * dwda * end.cos_b);
+            }
+        } else {
+            bool vh;
+            const float sm = vol_segment(vol, end.p, -d, dist, vh);
+            const float3 pdf_s = vol_pdf_distance(vol, sm);
+            if (end.onsurface) {
+                if (end_le) {
+                    float c = dot3(wrev, light_n);
+                    if (c <= 0.0f) c = 1e-4f;
+                    float pw = RUMI_INV_PI_F * c;
+                    if (pw <= 0.0f) pw = 1e-4f;
+                    bwd = pdf_s * (pw * dwda);
+                } else {
+                    const float pw = material_pdfw(m, end.xi, n, w, wrev);
+                    bwd = end.dirac ? pdf_s * (pw * dwda * end.cos_b) : pdf_s * (pw * dwda);
+                }
+            } else {
+                bwd = pdf_s * (phase_value(vol, w, wrev) * dwda * end.cos_b);
+            }
+        }
+        start.pdf_bwd = bwd;
+        // throughput
+        const float G = cos_s * cos_e / (dist * dist);
+        float3 a = alpha[depth];
+        if (start.onsurface) {
+            if (depth == 0) {
+                if (EYE) {
+                    const DevCamera &c = S.camera;
+                    const float cs = start.cos_a;
+                    const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
+                    a = a * (We / avg3(start.pdf_fwd) * G);
+                } else {
+                    a = a * (light.le / start.pdf_fwd * G);  // Light::L / pick pdf
+                }
+            } else {
+                const float3 fr = EYE ? vert_fr(S, start, start.n, d, prev_w) : vert_fr(S, start, start.n, prev_w, d);
+                a = a * (fr / (start.pdf_fwd * start.pdf_path) * G);
+            }
+        } else {
+            const float fp = EYE ? phase_value(vol, d, prev_w) : phase_value(vol, prev_w, d);
+            a = a * ((vol.sigma_s * fp) / (start.pdf_fwd * start.pdf_path) * G);
+        }
+        if (vol.present && !end.in_obj) a = a * end.vtau;
+        alpha[depth + 1] = a;
+        if (EYE) {
+            if (end_le) {
+                const float3 fr = end.onsurface ? vert_fr(S, end, n, w, wrev) : mk3(0, 0, 0);
+                alpha[depth + 2] = a * (fr / (end.pdf_fwd * end.pdf_path));
+                end.pdf_bwd = c3(light.inv_area * (float)S.n_lights);  // Light::Pdf() * LightCount()
+                break;
+            }
+        } else {
+            if (end.onsurface && end_le) break;
+        }
+        prev_mat = end.mat;
+        prev_w = wrev;
+        o = end.p;
+        d = w;
+    }
+    (void)prev_mat;
+    return n_vertex;
+}
+
+// AreaLight::Pdfw (arealight.cpp:62-73) with the light's normal.
+RUMI_D float light_pdfw(float3 w, float3 light_n) {
+    float c = dot3(w, light_n);
+    if (c <= 0.0f) c = 1e-4f;
+    float pdf = RUMI_INV_PI_F * c;
+    return pdf <= 0.0f ? 1e-4f : pdf;
+}
+
+// Pinhole::Pdfw (pinhole.cpp:58-62)
+RUMI_D float camera_pdfw(const DevCamera &c, float3 w) {
+    const float ct = dot3(w, c.dir);
+    return c.plane_dist * c.plane_dist / (ct * ct * ct * c.film_area);
+}
+
+// BidirectionalPathTracer::MISWeight (bidirectionalpathtracer.cpp:1096-1586).
+// ns / nt: vertices used on the light / eye side; VL / VE the subpaths, segL / segE
+// their segment directions.
+RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, const BVert *VE, const float3 *segE,
+                        int ns, int nt, float3 connect_wi, float3 connect_wo, float3 light_n) {
+    if (ns + nt <= 2) return 1.0f;
+    const DevScene &S = P.s;
+    const DevVolume &vol = S.volume;
+    float3 sb[BD_MAXV], sf[BD_MAXV], tb[BD_MAXV], tf[BD_MAXV];
+    const BVert *s_connect = nullptr, *s_prev = nullptr, *t_connect = nullptr, *t_prev = nullptr;
+    float3 s_wi = mk3(0, 0, 0), t_wo = mk3(0, 0, 0);
+    if (ns > 0) {
+        s_connect = &VL[ns - 1];
+        if (ns >= 2) {
+            s_prev = &VL[ns - 2];
+            s_wi = -segL[ns - 2];
+        }
+    }
+    if (nt > 0) {
+        t_connect = &VE[nt - 1];
+        if (nt >= 2) {
+            t_prev = &VE[nt - 2];
+            t_wo = -segE[nt - 2];
+        }
+    }
+    float connect_d = 1.0f, sd = 1.0f, td = 1.0f;
+    if (s_connect && t_connect) connect_d = sqrtf(dot3(s_connect->p - t_connect->p, s_connect->p - t_connect->p));
+    if (s_connect && s_prev) sd = sqrtf(dot3(s_connect->p - s_prev->p, s_connect->p - s_prev->p));
+    if (t_connect && t_prev) td = sqrtf(dot3(t_connect->p - t_prev->p, t_connect->p - t_prev->p));
+
+    // pdf of sampling `to` from `from` along direction dir (length len) in the
+    // reference's form: Tr (surface end) or PdfDistance (medium end) of the segment.
+    if (s_connect) {
+        float3 pdf_s = c3(1.0f);
+        float dwda;
+        if (s_connect->onsurface) {
+            if (vol.present) {
+                bool vh;
+                const float sm = vol_segment(vol, t_connect->p, connect_wi, connect_d, vh);
+                if (vh) pdf_s = vol_tr(vol, sm);
+            }
+            dwda = dot3(s_connect->n, connect_wo) / (connect_d * connect_d);
+        } else {
+            dwda = 1.0f / (connect_d * connect_d);
+            bool vh;
+            const float sm = vol_segment(vol, t_connect->p, connect_wi, connect_d, vh);
+            if (vh) pdf_s = vol_pdf_distance(vol, sm);
+        }
+        float pw;
+        if (t_connect->onsurface)
+            pw = nt > 1 ? material_pdfw(S.materials[t_connect->mat], t_connect->xi, t_connect->n, t_wo, connect_wi)
+                        : camera_pdfw(S.camera, connect_wi);
+        else
+            pw = phase_value(vol, t_wo, connect_wi);
+        sb[ns - 1] = pdf_s * (pw * dwda);
+        sf[ns - 1] = s_connect->pdf_fwd;
+        if (s_prev) {
+            if (s_prev->onsurface && s_prev->dirac) {
+                sb[ns - 2] = c3(1.0f);
+                sf[ns - 2] = c3(1.0f);
+            } else {
+                float3 ps = c3(1.0f);
+                float dw;
+                if (s_prev->onsurface) {
+                    if (vol.present) {
+                        bool vh;
+                        const float sm = vol_segment(vol, s_connect->p, s_wi, sd, vh);
+                        if (vh) ps = vol_tr(vol, sm);
+                    }
+                    dw = -dot3(s_prev->n, s_wi) / (sd * sd);
+                } else {
+                    dw = 1.0f / (sd * sd);
+                    bool vh;
+                    const float sm = vol_segment(vol, s_connect->p, s_wi, sd, vh);
+                    if (vh) ps = vol_pdf_distance(vol, sm);
+                }
+                const float pw2 = s_connect->onsurface ? material_pdfw(S.materials[s_connect->mat], s_connect->xi,
+                                                                       s_connect->n, connect_wo, s_wi)
+                                                       : phase_value(vol, connect_wo, s_wi);
+                sb[ns - 2] = ps * (pw2 * dw);
+                sf[ns - 2] = s_prev->pdf_fwd;
+            }
+        }
+    }
+    if (t_connect) {
+        if (ns > 0) {
+            float3 pdf_s = c3(1.0f);
+            float dwda;
+            if (t_connect->onsurface) {
+                if (vol.present) {
+                    bool vh;
+                    const float sm = vol_segment(vol, s_connect->p, connect_wo, connect_d, vh);
+                    if (vh) pdf_s = vol_tr(vol, sm);
+                }
+                dwda = dot3(t_connect->n, connect_wi) / (connect_d * connect_d);
+            } else {
+                dwda = 1.0f / (connect_d * connect_d);
+                bool vh;
+                const float sm = vol_segment(vol, s_connect->p, connect_wo, connect_d, vh);
+                if (vh) pdf_s = vol_pdf_distance(vol, sm);
+            }
+            float pw;
+            if (s_connect->onsurface)
+                pw = ns > 1 ? material_pdfw(S.materials[s_connect->mat], s_connect->xi, s_connect->n, s_wi, connect_wo)
+                            : light_pdfw(connect_wo, light_n);
+            else
+                pw = phase_value(vol, s_wi, connect_wo);
+            tb[nt - 1] = pdf_s * (pw * dwda);
+            tf[nt - 1] = t_connect->pdf_fwd;
+            if (t_prev) {
+                if (t_prev->onsurface && t_prev->dirac) {
+                    tb[nt - 2] = c3(1.0f);
+                    tf[nt - 2] = c3(1.0f);
+                } else {
+                    float3 ps = c3(1.0f);
+                    float dw;
+                    if (t_prev->onsurface) {
+                        if (vol.present) {
+                            bool vh;
+                            const float sm = vol_segment(vol, t_connect->p, t_wo, td, vh);
+                            if (vh) ps = vol_tr(vol, sm);
+                        }
+                        dw = -dot3(t_prev->n, t_wo) / (td * td);
+                    } else {
+                        dw = 1.0f / (td * td);
+                        bool vh;
+                        const float sm = vol_segment(vol, t_connect->p, t_wo, td, vh);
+                        if (vh) ps = vol_pdf_distance(vol, sm);
+                    }
+                    const float pw2 = t_connect->onsurface ? material_pdfw(S.materials[t_connect->mat], t_connect->xi,
+                                                                           t_connect->n, connect_wi, t_wo)
+                                                           : phase_value(vol, connect_wi, t_wo);
+                    tb[nt - 2] = ps * (pw2 * dw);
+                    tf[nt - 2] = t_prev->pdf_fwd;
+                }
+            }
+        } else {
+            // the eye subpath reached a light by itself ("kajiya" strategy)
+            tb[nt - 1] = VE[nt - 1].pdf_bwd;
+            tf[nt - 1] = VE[nt - 1].pdf_fwd;
+            if (t_prev->dirac) {
+                tb[nt - 2] = c3(1.0f);
+                tf[nt - 2] = c3(1.0f);
+            } else {
+                tb[nt - 2] = VE[nt - 2].pdf_bwd;
+                tf[nt - 2] = VE[nt - 2].pdf_fwd;
+            }
+        }
+    }
+    for (int i = 0; i < ns - 2; ++i) {
+        if (VL[i].dirac) {
+            sf[i] = sb[i] = c3(1.0f);
+        } else {
+            sf[i] = VL[i].pdf_fwd;
+            sb[i] = VL[i].pdf_bwd;
+        }
+    }
+    for (int i = 0; i < nt - 2; ++i) {
+        if (VE[i].dirac) {
+            tf[i] = tb[i] = c3(1.0f);
+        } else {
+            tf[i] = VE[i].pdf_fwd;
+            tb[i] = VE[i].pdf_bwd;
+        }
+    }
+    // leading specular chain seen from the camera ("locked", :1523-1540)
+    int locked = -1;
+    if (VE[0].dirac && VE[1].dirac) {
+        int i = 0;
+        for (; i < nt - 1; ++i) {
+            if (VE[i].dirac || VE[i + 1].dirac) continue;
+            locked = i;
+            break;
+        }
+        if (i == nt - 1) locked = i;
+    }
+    float sum = 1.0f, pi = 1.0f;
+    for (int i = nt - 1; i >= 0; --i) {
+        pi *= avg3(tb[i] / tf[i]);
+        if (locked != -1 && i <= locked) break;
+        if (i < nt - 1 && VE[i].dirac) continue;
+        if (i == 0 && VE[0].dirac) continue;
+        sum += pi;
+    }
+    pi = 1.0f;
+    for (int i = ns - 1; i >= 0; --i) {
+        pi *= avg3(sb[i] / sf[i]);
+        if (0 < i && i < ns - 1 && VL[i].dirac) continue;
+        if (i == 0 && VL[0].dirac) continue;
+        sum += pi;
+    }
+    return 1.0f / sum;
+}
+
+// VisibilityTest (:1018-1050): shadow ray between the two vertices, from the eye vertex
+// unless the eye vertex is the camera.
+RUMI_D bool visible(const DevScene &S, int ns, int nt, float3 sp, float3 tp, int *stack, TraceStats &st) {
+    float3 o, dir;
+    float tmax;
+    if (nt == 1) {
+        o = sp;
+        dir = normalize_ref(tp - sp);
+        tmax = sqrtf(dot3(tp - sp, tp - sp));
+    } else {
+        o = tp;
+        dir = normalize_ref(sp - tp);
+        tmax = sqrtf(dot3(sp - tp, sp - tp));
+    }
+    const HitRec h = trace_ray<true, BD_STACK, false>(S, o, dir, tmax, false, stack, BD_THREADS, st);
+    return !(h.t > 0.0f && tmax - h.t > 1e-4f);
+}
+
+// VolumetricTest (:1052-1094): binary transmittance between the vertices.
+RUMI_D bool volumetric_ok(const DevVolume &V, float3 sp, float3 tp, float xi) {
+    if (!V.present) return true;
+    const float3 dir = normalize_ref(tp - sp);
+    const float tmax = sqrtf(dot3(tp - sp, tp - sp));
+    float tn, tf;
+    if (!volume_intersect(V, sp, dir, 0.0f, tn, tf)) return true;
+    const float sm = volume_max_distance(tmax, tn, tf);
+    return !(xi < 1.0f - expf(avg3(V.sigma_t) * -sm));
+}
+
+__global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
+    __shared__ int stack[BD_STACK * BD_THREADS];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_paths) return;
+    const DevScene &S = P.s;
+    const uint64_t path = (uint64_t)(P.path0 + j);
+    const long long pixel = (long long)P.pix0 + j / P.spp;
+    const int sidx = j % P.spp;
+    const int W = S.width, H = S.height;
+    const int pw_ = (int)(pixel % W), ph_ = (int)(pixel / W);
+    TraceStats st{0, 0};
+    int *stk = stack + threadIdx.x;
+
+    BVert VE[BD_MAXV], VL[BD_MAXV];
+    float3 segE[BD_MAXV], segL[BD_MAXV], aE[BD_MAXV + 2], aL[BD_MAXV + 2];
+    // Scene::LightsUniformSampling + AreaLight::SolidAngleSampling
+    const Uniform4 UL = path_uniforms(path, 1000u, 0, P.k0, P.k1);
+    const Uniform4 UD = path_uniforms(path, 1000u, 1, P.k0, P.k1);
+    const int li = pick_light(S, UL.u[0]);
+    const DevLight light = S.lights[li];
+    const LightSample ls = sample_light(S, UL.u[0], UL.u[1], UL.u[2]);
+    const float3 light_n = ls.nL;
+    // eye subpath start (Pinhole::CastViewRay, pinhole.cpp:97-136)
+    const float2 smp = pixel_sample(sidx, P.spp, P.grid_d, P.square != 0, pixel, P.k0, P.k1);
+    float3 eo, ed;
+    camera_ray(S.camera, W, H, pw_, ph_, smp.x, smp.y, eo, ed);
+    {
+        const DevCamera &c = S.camera;
+        const float hw = W * 0.5f, hh = H * 0.5f;
+        const float x = -(((float)pw_ - hw) + smp.x) / hw * c.tanfov;
+        const float y = -(((float)ph_ - hh) + smp.y) / hh * c.tanfov * c.y_ratio;
+        const float3 l = normalize_ref(mk3(x, y, c.plane_dist));
+        bvert_clear(VE[0]);
+        VE[0].p = eo;
+        VE[0].n = c.dir;
+        VE[0].dirac = true;
+        VE[0].cos_a = l.z;
+        VE[0].pdf_dir = c.plane_dist * c.plane_dist / (l.z * l.z * l.z * c.film_area);
+        VE[0].pdf_fwd = c3(1.0f);
+    }
+    const int nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
+    // light subpath start
+    const LobeSample emit = lambert_sample(light_n, UD.u[0], UD.u[1]);
+    bvert_clear(VL[0]);
+    VL[0].p = ls.P;
+    VL[0].n = light_n;
+    VL[0].pdf_dir = emit.pdf;
+    VL[0].cos_a = dot3(emit.wi, light_n);
+    VL[0].pdf_fwd = c3(ls.pdf);
+    const int nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit.wi, VL, segL, aL, light, light_n, stk, st);
+
+    float3 L = mk3(0, 0, 0);
+    const int max_len = nE + nLv - 1;
+    for (int len = 1; len <= max_len; ++len) {
+        for (int t = 0; t <= len; ++t) {
+            if (t >= nE) break;
+            const BVert &tc = VE[t];
+            float3 t_wo = mk3(0, 0, 0);
+            if (t > 0) {
+                t_wo = -segE[t - 1];
+                if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
+                    if (len == nE - 1) {
+                        const float w = mis_weight(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n);
+                        L = L + aE[t + 1] * w;
+                    }
+                    break;
+                }
+                if (tc.dirac) continue;
+            }
+            const int s = len - (t + 1);
+            if (s >= nLv || s <= -1) continue;
+            const BVert &sc = VL[s];
+            float3 s_wi = mk3(0, 0, 0);
+            if (s > 0) {
+                s_wi = -segL[s - 1];
+                if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) continue;
+                if (sc.dirac) continue;
+            }
+            if (!visible(S, s + 1, t + 1, sc.p, tc.p, stk, st)) continue;
+            const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
+            if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) continue;
+            const float3 cwi = normalize_ref(sc.p - tc.p);
+            const float3 cwo = normalize_ref(tc.p - sc.p);
+            const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
+            if (ci < 1e-4f) continue;
+            const float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
+            if (co < 1e-4f) continue;
+            const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+            if (dist <= 0.0f) continue;
+            const float G = ci * co / (dist * dist);
+            if (G <= 0.0f) continue;
+            float3 cE, cL;
+            if (t == 0) {
+                const DevCamera &c = S.camera;
+                const float cs = dot3(tc.n, cwi);
+                const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
+                cE = c3(We / avg3(tc.pdf_fwd));
+            } else if (tc.onsurface) {
+                cE = vert_fr(S, tc, tc.n, cwi, t_wo) / (tc.pdf_fwd * tc.pdf_path);
+            } else {
+                cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
+            }
+            if (s == 0) {
+                cL = light.le / sc.pdf_fwd;
+            } else if (sc.onsurface) {
+                cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
+            } else {
+                cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
+            }
+            if (t == 0) {
+                int wi, hi;
+                if (!film_plane_pixel(P, sc.p, wi, hi)) continue;
+                if (wi == W || hi == H) continue;
+                if (wi < 0 || hi < 0 || wi > W || hi > H) continue;
+                float3 lo = aE[t] * cE * G * cL * aL[s];
+                lo = lo * mis_weight(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n);
+                float *dst = P.light_film + ((size_t)hi * W + wi) * 3;
+                atomicAdd(dst + 0, lo.z);
+                atomicAdd(dst + 1, lo.y);
+                atomicAdd(dst + 2, lo.x);
+            } else {
+                float3 lo = aE[t] * cE * G * cL * aL[s];
+                lo = lo * mis_weight(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n);
+                L = L + lo;
+            }
+        }
+    }
+    P.L[j] = make_float4(L.x, L.y, L.z, 0.0f);
+}
+
+__global__ void bdpt_write_film(BdLaunch P, int n_pix, float *film, unsigned long long *nan_count) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_pix) return;
+    float3 acc = mk3(0, 0, 0);
+    int nan = 0;
+    for (int s = 0; s < P.spp; ++s) {
+        const float4 l = P.L[(size_t)q * P.spp + s];
+        if (l.x != l.x || l.y != l.y || l.z != l.z)
+            ++nan;
+        else {
+            acc.x += l.x; acc.y += l.y; acc.z += l.z;
+        }
+    }
+    const size_t px = (size_t)(P.pix0 + q) * 3;
+    film[px + 0] = acc.z;
+    film[px + 1] = acc.y;
+    film[px + 2] = acc.x;
+    if (nan) atomicAdd(nan_count, (unsigned long long)nan);
+}
+
+__global__ void add_light_film(float *film, const float *light, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        film[i] += light[i];
+}
+
+rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
+                        cudaStream_t stream) {
+    const DevScene &S = sc->dev;
+    if (p->n_light < 2 || p->n_eye < 2 || p->n_light > BD_MAXV || p->n_eye > BD_MAXV) {
+        set_error("BDPT needs 2 <= n_light, n_eye <= 16");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    if (S.n_lights <= 0) {
+        set_error("BDPT needs a light");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    const int W = S.width, H = S.height, spp = p->spp;
+    const long long total_pix = (long long)W * H;
+    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 20);
+    long long pix_per_wave = wave / spp;
+    if (pix_per_wave < 1) pix_per_wave = 1;
+    if (pix_per_wave > total_pix) pix_per_wave = total_pix;
+    const size_t npaths = (size_t)(pix_per_wave * spp);
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t film_bytes = sizeof(float) * 3 * (size_t)total_pix;
+    const size_t bytes = al(npaths * sizeof(float4)) + al(film_bytes) + al(64);
+    rumi_status st = ensure_workspace(sc, bytes);
+    if (st != RUMI_OK) return st;
+    char *w = (char *)sc->ws;
+    BdLaunch B;
+    B.s = S;
+    B.nL = p->n_light;
+    B.nE = p->n_eye;
+    B.spp = spp;
+    B.k0 = (uint32_t)p->seed;
+    B.k1 = (uint32_t)(p->seed >> 32) ^ 0x5851F42Du;
+    int d = 0;
+    while ((d + 1) * (d + 1) <= spp) ++d;
+    B.grid_d = d;
+    B.square = d * d == spp;
+    B.L = (float4 *)w; w += al(npaths * sizeof(float4));
+    B.light_film = (float *)w; w += al(film_bytes);
+    unsigned long long *nan_count = (unsigned long long *)w;
+    const DevCamera &c = S.camera;
+    B.right = mk3(c.m[0] + c.m[3], c.m[4] + c.m[7], c.m[8] + c.m[11]);
+    B.up = mk3(c.m[1] + c.m[3], c.m[5] + c.m[7], c.m[9] + c.m[11]);
+    cudaMemsetAsync(B.light_film, 0, film_bytes, stream);
+    cudaMemsetAsync(nan_count, 0, sizeof(unsigned long long), stream);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const bool timing = (p->flags & RUMI_FLAG_TIMING) != 0;
+    if (timing) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, stream);
+    }
+    long long launches = 0;
+    for (long long pix0 = 0; pix0 < total_pix; pix0 += pix_per_wave) {
+        const long long n_pix = pix0 + pix_per_wave <= total_pix ? pix_per_wave : total_pix - pix0;
+        B.pix0 = (int)pix0;
+        B.n_paths = (int)(n_pix * spp);
+        B.path0 = pix0 * spp;
+        bdpt_kernel<<<(B.n_paths + BD_THREADS - 1) / BD_THREADS, BD_THREADS, 0, stream>>>(B);
+        bdpt_write_film<<<(int)((n_pix + 255) / 256), 256, 0, stream>>>(B, (int)n_pix, film_dev, nan_count);
+        launches += 2;
+    }
+    add_light_film<<<sc->num_sms * 4, 256, 0, stream>>>(film_dev, B.light_film, (size_t)total_pix * 3);
+    if (timing) cudaEventRecord(e1, stream);
+    unsigned long long h_nan = 0;
+    cudaMemcpyAsync(&h_nan, nan_count, sizeof(h_nan), cudaMemcpyDeviceToHost, stream);
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_status(e, "bdpt_render");
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->paths = total_pix * spp;
+        stats->nan_samples = (int64_t)h_nan;
+        stats->extend_launches = launches;
+        if (timing) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            stats->total_ms = ms;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return RUMI_OK;
+}
+
+}  // namespace rumi

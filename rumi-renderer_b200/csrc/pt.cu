@@ -82,28 +82,52 @@ __global__ void pt_reset(PtLaunch P, int bounce) {
 
 __global__ void pt_finish(PtLaunch P) { P.stats[S_RAYS_SH] += (unsigned long long)P.cnt[C_SHADOW]; }
 
-// Persistent closest-hit kernel: warps fetch 32 rays at a time from the queue.
+// Persistent traversal kernels with per-lane refill: every lane holds one ray and
+// advances it one node pair per iteration; lanes whose ray finished take new rays from
+// the queue together (one warp-aggregated atomic) once REFILL_MIN of them are idle, so
+// warps stay full until the queue drains.
+static constexpr int REFILL_MIN = 8;
+static constexpr int SPILL = RUMI_MAX_BVH_DEPTH - STACK_SMEM;
+
 template <bool STATS>
 __global__ void __launch_bounds__(TRACE_THREADS) pt_extend(PtLaunch P, int bounce) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
     const int cur = bounce & 1;
     const int n = P.cnt[cur];
     const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int *my_stack = stack + threadIdx.x;
+    int spill[SPILL];
     TraceStats st{0, 0};
+    TravState T;
+    int ray = -1;
+    bool exhausted = false;
     for (;;) {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(&P.cnt[C_FETCH_EXT], 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const int i = base + lane;
-        if (i < n) {
-            const float4 o4 = P.ray_o[cur][i];
-            const float4 d4 = P.ray_d[cur][i];
-            const bool in_obj = (__float_as_uint(o4.w) >> 31) != 0;
-            const HitRec h = trace_ray<false, STACK_SMEM, STATS>(P.s, f4xyz(o4), f4xyz(d4), d4.w, in_obj,
-                                                                 stack + threadIdx.x, TRACE_THREADS, st);
-            const int code = h.t > 0.0f ? (h.id | (h.back ? (int)0x80000000 : 0)) : -1;
-            P.hit[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
+        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
+        if (!exhausted && idle && (__popc(idle) >= REFILL_MIN || idle == 0xffffffffu)) {
+            int base = 0;
+            const int leader = __ffs(idle) - 1;
+            if (lane == leader) base = atomicAdd(&P.cnt[C_FETCH_EXT], __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= n) exhausted = true;
+            if (ray < 0) {
+                const int r = base + __popc(idle & lt);
+                if (r < n) {
+                    ray = r;
+                    const float4 o4 = P.ray_o[cur][r];
+                    const float4 d4 = P.ray_d[cur][r];
+                    trav_begin<false, STATS>(P.s, T, f4xyz(o4), f4xyz(d4), d4.w, (__float_as_uint(o4.w) >> 31) != 0, st);
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, ray >= 0) == 0) break;
+        if (ray >= 0) {
+            if (T.cur != -2) trav_step<false, STACK_SMEM, STATS>(P.s, T, my_stack, TRACE_THREADS, spill, st);
+            if (T.cur == -2) {
+                const int code = T.h.t > 0.0f ? (T.h.id | (T.h.back ? (int)0x80000000 : 0)) : -1;
+                P.hit[ray] = make_float4(T.h.t, __int_as_float(code), T.h.u, T.h.v);
+                ray = -1;
+            }
         }
     }
     if (STATS) {
@@ -116,24 +140,43 @@ __global__ void __launch_bounds__(TRACE_THREADS) pt_shadow(PtLaunch P) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
     const int n = P.cnt[C_SHADOW];
     const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int *my_stack = stack + threadIdx.x;
+    int spill[SPILL];
     TraceStats st{0, 0};
+    TravState T;
+    int ray = -1;
+    bool exhausted = false;
     for (;;) {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(&P.cnt[C_FETCH_SH], 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const int i = base + lane;
-        if (i < n) {
-            const float4 o4 = P.sh_o[i];
-            const float4 d4 = P.sh_d[i];
-            const HitRec h = trace_ray<true, STACK_SMEM, false>(P.s, f4xyz(o4), f4xyz(d4), d4.w, false,
-                                                                stack + threadIdx.x, TRACE_THREADS, st);
-            if (h.t == 0.0f) {
-                const int slot = __float_as_int(o4.w);
-                const float4 c = P.sh_c[i];
-                float4 l = P.L[slot];
-                l.x += c.x; l.y += c.y; l.z += c.z;
-                P.L[slot] = l;
+        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
+        if (!exhausted && idle && (__popc(idle) >= REFILL_MIN || idle == 0xffffffffu)) {
+            int base = 0;
+            const int leader = __ffs(idle) - 1;
+            if (lane == leader) base = atomicAdd(&P.cnt[C_FETCH_SH], __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= n) exhausted = true;
+            if (ray < 0) {
+                const int r = base + __popc(idle & lt);
+                if (r < n) {
+                    ray = r;
+                    const float4 o4 = P.sh_o[r];
+                    const float4 d4 = P.sh_d[r];
+                    trav_begin<true, false>(P.s, T, f4xyz(o4), f4xyz(d4), d4.w, false, st);
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, ray >= 0) == 0) break;
+        if (ray >= 0) {
+            if (T.cur != -2) trav_step<true, STACK_SMEM, false>(P.s, T, my_stack, TRACE_THREADS, spill, st);
+            if (T.cur == -2) {
+                if (T.h.t == 0.0f) {
+                    const int slot = __float_as_int(P.sh_o[ray].w);
+                    const float4 c = P.sh_c[ray];
+                    float4 l = P.L[slot];
+                    l.x += c.x; l.y += c.y; l.z += c.z;
+                    P.L[slot] = l;
+                }
+                ray = -1;
             }
         }
     }

@@ -37,10 +37,15 @@ rumi_status cuda_status(cudaError_t e, const char *what);
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                       cudaStream_t stream);
 size_t pt_workspace_bytes(long long paths);
+rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
+                        cudaStream_t stream);
 rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                          cudaStream_t stream, void *ws, long long pix_per_wave);
 rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, float *t_dev, int32_t *prim_dev,
                        int64_t *node_visits, int64_t *prim_tests, cudaStream_t stream);
 rumi_status ensure_workspace(rumi_scene *sc, size_t bytes);
+cudaError_t dalloc(void **p, size_t bytes, cudaStream_t s);
+void dfree(void *p, cudaStream_t s);
+void configure_pool(int device);
 
 }  // namespace rumi

@@ -470,3 +470,52 @@ RUMI_D float volume_shadow_tr(const DevVolume &v, float3 o, float3 d, float tmax
     if (xi < 1.0f - expf(v.avg_sigma_t * -smax)) return 0.0f;
     return 1.0f;
 }
+
+// Material::Pdfw (Matte: Lambertian::Pdfw; Glossy: the lobe recorded in xi; Dirac and
+// emissive materials: 1), src/Material/{matte,glossy,specular,dielectric}.cpp.
+RUMI_D float material_pdfw(const DevMaterial &m, float xi, float3 n, float3 w, float3 w_pdf) {
+    if (m.type == MAT_MATTE) return lambert_pdf(n, w_pdf);
+    if (m.type == MAT_GLOSSY) {
+        if (m.kd != 0.0f && xi <= m.kd_pdf) return lambert_pdf(n, w_pdf);
+        return phong_pdf(n, w, w_pdf, m.e, m.phong_norm);
+    }
+    return 1.0f;
+}
+
+RUMI_D bool material_dirac(const DevMaterial &m, float xi) {
+    if (m.type == MAT_SPECULAR || m.type == MAT_DIELECTRIC || m.type == MAT_SUBSURFACE) return true;
+    if (m.type == MAT_GLOSSY) return !(m.kd != 0.0f && xi <= m.kd_pdf);
+    return false;
+}
+
+// Phase value / pdf for directions a and b pointing away from the scattering point
+// toward its two neighbours (the scattering cosine is -dot(a, b)).  g = 0: the
+// reference's Isotropic (1 / 4 pi).
+RUMI_D float phase_value(const DevVolume &v, float3 a, float3 b) {
+    return v.g == 0.0f ? 1.0f / (4.0f * RUMI_PI_F) : hg_eval(-dot3(a, b), v.g);
+}
+
+// Surface normal at a hit as the shapes' Intersect routines record it
+// (triangle.cpp:109-115 with the Q3 barycentric order, rect.cpp:113-119,
+// sphere.cpp:111-128).  o: ray origin, p: hit point.
+RUMI_D float3 surface_normal(const DevScene &S, int id, bool back, float u, float v, float3 o, float3 p,
+                             const DevMaterial &m) {
+    if (id < S.n_tris) {
+        const float4 n0 = __ldg(&S.tri_shade[3 * id]), n1 = __ldg(&S.tri_shade[3 * id + 1]),
+                     n2 = __ldg(&S.tri_shade[3 * id + 2]);
+        float3 nrm = f4xyz(n0) * (1.0f - u - v) + f4xyz(n1) * u + f4xyz(n2) * v;
+        if (back && material_opaque(m)) nrm = -nrm;
+        return nrm;
+    }
+    if (id < S.n_tris + S.n_rects) {
+        const int r = id - S.n_tris;
+        return normalize_ref(cross3(f4xyz(S.rects[3 * r + 1]), f4xyz(S.rects[3 * r + 2])));
+    }
+    const float4 c = S.spheres[id - S.n_tris - S.n_rects];
+    const float3 cc = f4xyz(c);
+    if (m.type == MAT_EMISSIVE) {
+        const float3 oc = o - cc;
+        return sqrtf(dot3(oc, oc)) > c.w ? normalize_ref(p - cc) : normalize_ref(cc - p);
+    }
+    return normalize_ref(p - cc);
+}

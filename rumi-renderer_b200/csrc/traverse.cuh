@@ -251,3 +251,110 @@ RUMI_D HitRec trace_ray(const DevScene &s, float3 o, float3 d, float tmax, bool 
     }
     return h;
 }
+
+// ------------------------------------------------------------ resumable form
+// The same traversal split into single node-pair steps, so a warp can refill a lane with
+// a new ray as soon as that lane's ray finishes (dynamic fetch) instead of waiting for
+// the slowest of its 32 rays.  cur: next node pair, -1: pop the stack, -2: finished.
+struct TravState {
+    float3 o, d, inv, oinv;
+    float tmax;
+    int cur, sp, steps;
+    bool in_obj;
+    HitRec h;
+};
+
+template <bool ANYHIT, bool STATS>
+RUMI_D void trav_begin(const DevScene &s, TravState &T, float3 o, float3 d, float tmax, bool in_obj,
+                       TraceStats &st) {
+    T.o = o;
+    T.d = d;
+    T.tmax = tmax;
+    T.in_obj = in_obj;
+    T.sp = 0;
+    T.steps = 0;
+    T.h.t = 0.0f;
+    T.h.id = -1;
+    T.h.u = T.h.v = 0.0f;
+    T.h.back = 0;
+    T.cur = -2;
+    if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) return;  // bvh.cpp:161-162
+    T.inv = mk3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    T.oinv = mk3(o.x * T.inv.x, o.y * T.inv.y, o.z * T.inv.z);
+    const float4 *rp = reinterpret_cast<const float4 *>(s.nodes);
+    const float4 a = __ldg(rp), b = __ldg(rp + 1);
+    if (STATS) st.nodes++;
+    float tn;
+    if (!slab(a, b, T.inv, T.oinv, tmax, tn)) return;
+    const int first = __float_as_int(b.z), count = __float_as_int(b.w);
+    if (count > 0) {
+        leaf_isect<ANYHIT, STATS>(s, first, count, o, d, tmax, in_obj, T.h, st);
+        return;
+    }
+    if ((unsigned)first >= (unsigned)(s.n_nodes - 1)) return;
+    T.cur = first;
+}
+
+template <bool ANYHIT, int STACK_SMEM, bool STATS>
+RUMI_D void trav_step(const DevScene &s, TravState &T, int *smem_stack, int stride, int *spill, TraceStats &st) {
+    if (T.cur == -1) {
+        if (T.sp == 0) {
+            T.cur = -2;
+            return;
+        }
+        --T.sp;
+        T.cur = T.sp < STACK_SMEM ? smem_stack[T.sp * stride] : spill[T.sp - STACK_SMEM];
+    }
+    if ((unsigned)T.cur >= (unsigned)(s.n_nodes - 1) || ++T.steps > s.n_nodes) {  // malformed tree guard
+        T.cur = -2;
+        return;
+    }
+    const float4 *np = reinterpret_cast<const float4 *>(s.nodes + T.cur);
+    const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
+    if (STATS) st.nodes += 2;
+    const float lim = T.h.t > 0.0f ? fminf(T.h.t, T.tmax) : T.tmax;
+    float tn0, tn1;
+    const bool h0 = slab(a0, b0, T.inv, T.oinv, lim, tn0);
+    const bool h1 = slab(a1, b1, T.inv, T.oinv, lim, tn1);
+    const int f0 = __float_as_int(b0.z), c0 = __float_as_int(b0.w);
+    const int f1 = __float_as_int(b1.z), c1 = __float_as_int(b1.w);
+    const bool l0 = h0 && c0 > 0, l1 = h1 && c1 > 0;
+    if (l0 || l1) {
+        int fa = f0, ca = c0, fb = f1, cb = c1;
+        float tnb = tn1;
+        bool lb = l1;
+        if (l0 && l1 && tn1 < tn0) {
+            fa = f1; ca = c1; fb = f0; cb = c0; tnb = tn0;
+        }
+        if (!l0) {
+            fa = f1; ca = c1; lb = false;
+        }
+        if (leaf_isect<ANYHIT, STATS>(s, fa, ca, T.o, T.d, T.tmax, T.in_obj, T.h, st)) {
+            T.cur = -2;
+            return;
+        }
+        if (lb && (T.h.t <= 0.0f || tnb <= T.h.t))
+            if (leaf_isect<ANYHIT, STATS>(s, fb, cb, T.o, T.d, T.tmax, T.in_obj, T.h, st)) {
+                T.cur = -2;
+                return;
+            }
+    }
+    const bool i0 = h0 && c0 == 0 && (T.h.t <= 0.0f || tn0 <= T.h.t);
+    const bool i1 = h1 && c1 == 0 && (T.h.t <= 0.0f || tn1 <= T.h.t);
+    if (i0 && i1) {
+        const bool swap01 = tn1 < tn0;
+        const int near_ = swap01 ? f1 : f0, far_ = swap01 ? f0 : f1;
+        if (T.sp < STACK_SMEM)
+            smem_stack[T.sp * stride] = far_;
+        else if (T.sp < RUMI_MAX_BVH_DEPTH)
+            spill[T.sp - STACK_SMEM] = far_;
+        if (T.sp < RUMI_MAX_BVH_DEPTH) ++T.sp;
+        T.cur = near_;
+    } else if (i0) {
+        T.cur = f0;
+    } else if (i1) {
+        T.cur = f1;
+    } else {
+        T.cur = -1;
+    }
+}

@@ -13,7 +13,7 @@ import math
 
 import numpy as np
 
-from .scene import (Scene, Rect, Sphere, Model, Matte, Specular, Emissive, Dielectric, AreaLight,
+from .scene import (Scene, Rect, Sphere, Model, Matte, Specular, Emissive, Dielectric, Glossy, Subsurface, AreaLight,
                     SpotLight, HomogeneousVolume, Pinhole, Film, PathTracer, BidirectionalPathTracer,
                     identity16)
 
@@ -173,6 +173,55 @@ def bvh_bound_pt(width: int = 1024, height: int = 1024, spp: int = 64, max_depth
     tris = displaced_sphere(levels, (0.5, 0.35, 0.5), 0.25, 0.05, seed)
     alb = random_albedo(tris.shape[0], seed + 1)
     sc.add(Model(tris, albedo=alb), Matte(1.0, WHITE))
+    sc.camera = cornell_camera()
+    sc.image = Film(width, height, spp)
+    sc.tracer = PathTracer(max_depth)
+    return sc
+
+
+def volumetric_caustic(width: int = 512, height: int = 512, spp: int = 32, nL: int = 6, nE: int = 7,
+                       parity: bool = False) -> Scene:
+    """BDPT with MIS, volumetric caustic: a glass sphere (IOR 1.5, r=0.3) at (0.5, 0.35, 0.5)
+    inside the Cornell box filled with a homogeneous medium (sigma_a=0.05, sigma_s=0.4,
+    RGB-uniform).  Workload: Henyey-Greenstein g=0.7, 30 degree spot light of intensity 50
+    at (0.5, 0.98, 0.5) pointing down.  ``parity``: the reference-expressible variant -- the
+    reference's isotropic phase (g=0) and a small area light under the ceiling in place of
+    the spot (the reference's "Volumetric Caustics" preset uses the same arrangement).
+    Max path length nL + nE - 1."""
+    sc = Scene()
+    for tris, alb in cornell_walls():
+        sc.add(Model(tris), Matte(1.0, alb))
+    sc.add(Sphere((0.5, 0.35, 0.5), 0.3), Dielectric(1.5, 1.0, (0.0, 0.0, 0.0)))
+    if parity:
+        light = Rect((0.45, 0.98, 0.45), (0.1, 0.0, 0.0), (0.0, 0.0, 0.1), 64)
+        sc.add(light, Emissive(1.0, (120.0, 120.0, 120.0)))
+        sc.lights.append(AreaLight(light))
+        g = 0.0
+    else:
+        sc.lights.append(SpotLight((0.5, 0.98, 0.5), (0.0, -1.0, 0.0), 30.0, (50.0, 50.0, 50.0)))
+        g = 0.7
+    sc.volume = HomogeneousVolume((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.4, 0.4, 0.4), (0.05, 0.05, 0.05), g)
+    sc.camera = cornell_camera()
+    sc.image = Film(width, height, spp)
+    sc.tracer = BidirectionalPathTracer(nL, nE)
+    return sc
+
+
+def cornell_bdpt(width: int = 32, height: int = 32, spp: int = 16, nL: int = 4, nE: int = 5) -> Scene:
+    """The plain path-tracer Cornell scene rendered by BDPT (parity scene without a medium)."""
+    sc = cornell_pt(width, height, spp, 8)
+    sc.tracer = BidirectionalPathTracer(nL, nE)
+    return sc
+
+
+def subsurface_cornell(width: int = 32, height: int = 32, spp: int = 16, max_depth: int = 12) -> Scene:
+    """The Cornell box with a subsurface-scattering sphere (Subsurface(1.3, 1.0, sigma_s,
+    sigma_a)) and a glossy sphere, path traced (reference semantics of
+    src/Material/subsurface.cpp and src/Material/glossy.cpp)."""
+    sc = Scene()
+    add_cornell_box(sc)
+    sc.add(Sphere((0.35, 0.2, 0.55), 0.2), Subsurface(1.3, 1.0, (6.0, 4.0, 2.0), (0.3, 0.6, 1.2), 1.0))
+    sc.add(Sphere((0.72, 0.15, 0.35), 0.15), Glossy(0.5, 0.5, 30.0, (0.8, 0.7, 0.6)))
     sc.camera = cornell_camera()
     sc.image = Film(width, height, spp)
     sc.tracer = PathTracer(max_depth)

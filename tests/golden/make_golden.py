@@ -186,11 +186,11 @@ def camera_fixture(path, rng):
     print(path)
 
 
-def image_fixture(path, size=32, spp=16, depth=8, seeds=64):
-    """Reference renders of the Cornell workload at a small size: per-pixel mean radiance
-    over `seeds` independent frames and its standard error (spread across frames, which
+def image_fixture(path, size=32, spp=16, depth=8, seeds=64, scene=None):
+    """Reference renders of a workload at a small size: per-pixel mean radiance over
+    `seeds` independent frames and its standard error (spread across frames, which
     includes the frame-level correlation of the reference's shared sample sets)."""
-    sc = scenes.cornell_pt(size, size, spp, depth)
+    sc = scene if scene is not None else scenes.cornell_pt(size, size, spp, depth)
     frames = []
     for s in range(seeds):
         rs = refimpl.RefScene(sc, seed=1000 + s)
@@ -205,6 +205,17 @@ def image_fixture(path, size=32, spp=16, depth=8, seeds=64):
 
 
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "media":
+        sc = scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)
+        sc.tracer = scenes.PathTracer(8)
+        image_fixture(os.path.join(HERE, "image_caustic_pt32.npz"), scene=sc)
+        image_fixture(os.path.join(HERE, "image_sss_pt32.npz"), scene=scenes.subsurface_cornell(32, 32, 16, 12))
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == "bdpt":
+        image_fixture(os.path.join(HERE, "image_cornell_bdpt32.npz"), scene=scenes.cornell_bdpt(32, 32, 16, 4, 5))
+        image_fixture(os.path.join(HERE, "image_caustic_bdpt32.npz"),
+                      scene=scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True))
+        return
     rng = np.random.default_rng(20261203)
     c1 = scenes.cornell_pt(64, 64, 16, 8)
     rays = np.concatenate([rays_in_box(rng, 3072), camera_rays(rng, 1024)])
@@ -218,6 +229,13 @@ def main():
     volume_fixture(os.path.join(HERE, "volume.npz"), rng)
     camera_fixture(os.path.join(HERE, "camera.npz"), rng)
     image_fixture(os.path.join(HERE, "image_cornell32.npz"))
+    image_fixture(os.path.join(HERE, "image_cornell_bdpt32.npz"), scene=scenes.cornell_bdpt(32, 32, 16, 4, 5))
+    image_fixture(os.path.join(HERE, "image_caustic_bdpt32.npz"),
+                  scene=scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True))
+    sc = scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)
+    sc.tracer = scenes.PathTracer(8)
+    image_fixture(os.path.join(HERE, "image_caustic_pt32.npz"), scene=sc)
+    image_fixture(os.path.join(HERE, "image_sss_pt32.npz"), scene=scenes.subsurface_cornell(32, 32, 16, 12))
 
 
 if __name__ == "__main__":

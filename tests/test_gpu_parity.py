@@ -263,3 +263,37 @@ def test_gpu_full_size_bvh_bound_workload_properties():
     ma, mb = a.mean() / 64, b.mean() / 64
     assert ma > 0.05
     assert abs(ma / mb - 1.0) < 2e-3
+
+
+def gpu_frames(sc, n, seed0, spp=16):
+    gs = rumi_b200.GpuScene(sc)
+    frames = []
+    for s in range(n):
+        film, st = gs.render(spp=spp, seed=seed0 + s)
+        assert st["nan_samples"] == 0
+        frames.append(film / float(spp))
+    gs.close()
+    return frames
+
+
+def test_gpu_pt_medium_and_glass_match_reference_3sigma(golden):
+    from test_oracle_golden import frames_vs_reference
+    sc = scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)
+    sc.tracer = scenes.PathTracer(8)
+    frames_vs_reference(gpu_frames(sc, 32, 11000), golden("image_caustic_pt32.npz"))
+
+
+def test_gpu_pt_subsurface_matches_reference_3sigma(golden):
+    from test_oracle_golden import frames_vs_reference
+    frames_vs_reference(gpu_frames(scenes.subsurface_cornell(32, 32, 16, 12), 32, 12000), golden("image_sss_pt32.npz"))
+
+
+@pytest.mark.parametrize("fixture,builder", [
+    ("image_cornell_bdpt32.npz", lambda: scenes.cornell_bdpt(32, 32, 16, 4, 5)),
+    ("image_caustic_bdpt32.npz", lambda: scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)),
+])
+def test_gpu_bdpt_matches_reference_3sigma(golden, fixture, builder):
+    """BDPT with MIS (all strategies incl. light tracing splats through the film plane)
+    against the reference's BidirectionalPathTracer frames."""
+    from test_oracle_golden import frames_vs_reference
+    frames_vs_reference(gpu_frames(builder(), 32, 13000), golden(fixture))

@@ -158,21 +158,47 @@ def test_pixel_sampler_is_a_stratified_permutation():
             assert sorted(L.orc_perm(i, n, 0xABCDEF) for i in range(n)) == list(range(n))
 
 
-def test_oracle_image_matches_reference_3sigma(golden):
-    """Oracle PT frames of the Cornell workload (32x32) against the reference's frames:
-    per-pixel means within 3 sigma (sigma from both sides' frame-to-frame spread)."""
-    g = golden("image_cornell32.npz")
-    sc = scenes.cornell_pt(32, 32, 16, 8)
-    os_ = O.OracleScene(sc)
-    frames = []
-    for s in range(24):
-        film, nan = os_.render_pt(8, 16, seed=500 + s)
-        assert nan == 0
-        frames.append(film / 16.0)
+def frames_vs_reference(frames, g, max_frac=0.01):
+    """Per-pixel means within 3 sigma of the reference's frames (sigma from both sides'
+    frame-to-frame spread) on all but max_frac of the pixels, and the image mean within 4
+    sigma of the reference's (sigma of the image mean from the same spreads, at least 0.2%:
+    caustic and medium scenes carry ~1% of image-mean noise at these frame counts)."""
     fr = np.stack(frames).astype(np.float64)
     m, se = fr.mean(0), fr.std(0, ddof=1) / np.sqrt(fr.shape[0])
-    sig = np.sqrt(se ** 2 + g["stderr"].astype(np.float64) ** 2) + 1e-6
+    gse = g["stderr"].astype(np.float64)
+    sig = np.sqrt(se ** 2 + gse ** 2) + 1e-6
     z = np.abs(m - g["mean"]) / sig
-    assert np.mean(z > 3.0) < 0.01, np.mean(z > 3.0)
-    # image-level energy agrees far inside the noise
-    assert abs(m.mean() / g["mean"].mean() - 1.0) < 0.01
+    frac = float(np.mean(z > 3.0))
+    ratio = float(m.mean() / g["mean"].mean())
+    rel_sigma = np.sqrt((se ** 2).sum() + (gse ** 2).sum()) / g["mean"].astype(np.float64).sum()
+    assert frac < max_frac, (frac, ratio)
+    assert abs(ratio - 1.0) < max(4.0 * rel_sigma, 0.002), (frac, ratio, rel_sigma)
+    return frac, ratio
+
+
+def oracle_frames(sc, depth, n, seed0):
+    os_ = O.OracleScene(sc)
+    frames = []
+    for s in range(n):
+        film, nan = os_.render_pt(depth, 16, seed=seed0 + s)
+        assert nan == 0
+        frames.append(film / 16.0)
+    return frames
+
+
+def test_oracle_image_matches_reference_3sigma(golden):
+    """Oracle PT frames of the Cornell workload (32x32) against the reference's frames."""
+    frames_vs_reference(oracle_frames(scenes.cornell_pt(32, 32, 16, 8), 8, 24, 500), golden("image_cornell32.npz"))
+
+
+def test_oracle_medium_and_glass_match_reference_3sigma(golden):
+    """Homogeneous medium (free flight, absorption roulette, binary shadow transmittance,
+    isotropic phase) around a glass sphere, path traced."""
+    sc = scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)
+    frames_vs_reference(oracle_frames(sc, 8, 24, 700), golden("image_caustic_pt32.npz"))
+
+
+def test_oracle_subsurface_matches_reference_3sigma(golden):
+    """Subsurface random walk and a glossy sphere, path traced to depth 12."""
+    frames_vs_reference(oracle_frames(scenes.subsurface_cornell(32, 32, 16, 12), 12, 24, 900),
+                        golden("image_sss_pt32.npz"))
