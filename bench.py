@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--wave-paths", type=int, default=0)
     ap.add_argument("--small", action="store_true", help="256x256 at 16 spp (profiling runs)")
+    ap.add_argument("--workload", default="bvh_bound", choices=["bvh_bound", "batched"],
+                    help="batched: 256 seeded scenes as one frame vs the per-scene loop")
+    ap.add_argument("--scenes", type=int, default=256, help="batched workload: number of scenes")
     return ap.parse_args()
 
 
@@ -385,7 +388,7 @@ def our_arm(args):
                     config=dict(workload="bvh_bound_pt: Cornell box + displaced sphere", width=w["width"],
                                 height=w["height"], spp=w["spp"], max_depth=w["max_depth"],
                                 triangles=4 * 4 ** w["levels"], parallelism=f"replicas x{world} (spp shards)",
-                                l2="inputs larger than L2 (scene ~170 MB + wave queues ~330 MB per GPU)",
+                                l2="inputs larger than L2 (scene ~170 MB + wave queues ~690 MB per GPU)",
                                 bvh_build_ms=bvh["build_ms"]),
                     rays_per_sec=rays_per_s, roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=launches,
                     clocks=clocks_info)
@@ -396,10 +399,123 @@ def our_arm(args):
     return 0
 
 
+def batched_arm(args):
+    """Batched wavefront workload: scene i (scenes.batch_scene) has a log-uniform 1k-200k
+    triangle terrain, a resolution from {64,128,256,512}^2 and spp from {4,16,64}, depth 8.
+    One step renders every scene once.  Plain arm: the scenes one at a time through
+    rumi_render; batched arm: one rumi_render_batch frame replayed from its CUDA graph.
+    Both arms produce bit-identical films for the same seeds (checked on the last step),
+    so their RMSE is equal and samples/sec compare directly."""
+    import torch
+    import rumi_b200
+    from rumi_b200 import scenes
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    depth = 8
+    # scenes are sharded across ranks (scene i on rank i % world); no exchange
+    ids = [i for i in range(args.scenes) if i % world == rank]
+    t0 = time.perf_counter()
+    gss = [rumi_b200.GpuScene(scenes.batch_scene(i, depth)) for i in ids]
+    setup_s = time.perf_counter() - t0
+    spp = [g.flat.image.n_samples for g in gss]
+    paths = sum(g.width * g.height * s for g, s in zip(gss, spp))
+    tris = sum(int(g.flat.tri_vertices.shape[0]) for g in gss)
+    batch = rumi_b200.GpuBatch(gss)
+    films_plain = torch.zeros(batch.n_floats, dtype=torch.float32, device="cuda")
+    films_batch = torch.zeros(batch.n_floats, dtype=torch.float32, device="cuda")
+    offs, o = [], 0
+    for g in gss:
+        offs.append(o)
+        o += g.width * g.height * 3
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def seeds(step):
+        return [1 + i + 100000 * step for i in ids]
+
+    def plain(step):
+        for g, s, sd, off in zip(gss, spp, seeds(step), offs):
+            g.render(spp=s, seed=sd, film_device_ptr=films_plain.data_ptr() + 4 * off, stream=stream)
+        return len(gss) * (3 + 4 * depth)
+
+    def batched(step):
+        _, st = batch.render(spp, seeds(step), depth, graph=True, films_device_ptr=films_batch.data_ptr(),
+                             stream=stream)
+        waves = st["extend_launches"] // depth
+        return waves * (3 + 4 * depth)
+
+    def timed(fn):
+        for s in range(args.warmup):
+            fn(s)
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        launches = 0
+        for s in range(args.steps):
+            launches += fn(args.warmup + s)
+        ev1.record()
+        barrier()
+        return max_over_ranks(ev0.elapsed_time(ev1)), launches
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_plain, l_plain = timed(plain)
+    ms_batch, l_batch = timed(batched)
+    clocks_info = clocks.stop()
+    equal = bool(torch.equal(films_plain, films_batch))
+    batch.close()
+    for g in gss:
+        g.close()
+    all_paths = paths
+    if dist:
+        t = torch.tensor([paths], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        all_paths = float(t.item())
+    value = all_paths * args.steps / (ms_batch / 1000.0)
+    plain_value = all_paths * args.steps / (ms_plain / 1000.0)
+    if rank == 0:
+        line = dict(metric="path samples/sec at equal RMSE (batched vs plain per-scene loop)", value=value,
+                    unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=ms_batch / args.steps,
+                    higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                    data="synthetic (seeded fBm terrains in the Cornell box)",
+                    config=dict(workload=f"batched: {args.scenes} scenes, tris log-uniform 1k-200k, res "
+                                         "{64..512}^2, spp {4,16,64}, depth 8", scenes=len(gss), paths=paths,
+                                triangles=tris, setup_s=setup_s, parallelism=f"scene shards x{world}",
+                                l2="inputs larger than L2 (scenes + wave queues)"),
+                    plain_loop=dict(value=plain_value, ms_per_step=ms_plain / args.steps, gpu_launches=l_plain),
+                    speedup_vs_plain=value / plain_value, equal_images=equal, gpu_launches=l_batch,
+                    clocks=clocks_info)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0 if equal else 1
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "batched":
+        return batched_arm(args)
     return our_arm(args)
 
 

@@ -141,6 +141,11 @@ typedef struct {
     int32_t wave_paths;    /* paths in flight per wave; 0 = library default */
     int32_t flags;         /* RUMI_FLAG_* */
     void *stream;          /* cudaStream_t, NULL = the library's own stream */
+    /* launch tuning (0 = library default; chosen by rumi_b200.autotune) */
+    int32_t trace_mode;    /* 1: a warp traces 32 rays to completion; 2: per-lane ray refill;
+                              3: per-lane refill with leaves intersected warp-wide */
+    int32_t blocks_per_sm; /* persistent traversal blocks (128 threads) per SM, capped by occupancy */
+    int32_t refill_min;    /* idle lanes that trigger a refill (modes 2, 3) */
 } rumi_render_params;
 
 typedef struct {
@@ -194,6 +199,32 @@ rumi_status rumi_render(rumi_scene *scene, const rumi_render_params *params, flo
  * the GPU race and must be serialised by the caller.  No counterpart in the reference. */
 rumi_status rumi_render_noalloc(rumi_scene *scene, const rumi_render_params *params, float *film,
                                 rumi_render_stats *stats);
+
+/* Multi-scene batches: many scenes of uneven size and sample count rendered as one frame
+ * from shared ray queues (no counterpart in the reference, which renders one scene per
+ * process).  The batch references its scenes (which must outlive it and live on the
+ * current device); films are the scenes' films concatenated in scene order
+ * (rumi_batch_film_floats floats in total).  Scene i uses seeds[i] and its own path
+ * numbering, so its image equals rumi_render's for that scene and seed. */
+typedef struct rumi_batch rumi_batch;
+
+enum { RUMI_BATCH_GRAPH = 4 };  /* capture the frame as a CUDA graph on first use, then replay */
+
+typedef struct {
+    int32_t max_depth;       /* path tracer depth shared by the batch */
+    const int32_t *spp;      /* samples per pixel of each scene */
+    const uint64_t *seeds;   /* Philox seed of each scene */
+    int32_t wave_paths;      /* paths in flight per wave (queue capacity); 0 = default */
+    int32_t flags;           /* RUMI_FLAG_TIMING, RUMI_BATCH_GRAPH */
+    int32_t blocks_per_sm;   /* persistent traversal blocks per SM; 0 = occupancy limit */
+    void *stream;            /* cudaStream_t; NULL = the batch's own stream */
+} rumi_batch_params;
+
+rumi_status rumi_batch_create(rumi_scene *const *scenes, int32_t n, rumi_batch **out);
+rumi_status rumi_batch_destroy(rumi_batch *batch);
+int64_t rumi_batch_film_floats(const rumi_batch *batch);
+rumi_status rumi_render_batch(rumi_batch *batch, const rumi_batch_params *params, float *films,
+                              int32_t films_on_device, rumi_render_stats *stats);
 
 /* Ray queries against the scene's BVH.  rays: n*8 floats (o.xyz, in_object flag as
  * 0/1, d.xyz, tmax).  anyhit = 0: closest hit -> t (0 = miss, the reference's

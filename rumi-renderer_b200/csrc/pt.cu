@@ -50,19 +50,62 @@ struct PtLaunch {
     int *cnt;
     unsigned long long *stats;
     float *film;
+    int refill_min;
+    // multi-scene batches (scenes == nullptr: the single scene s)
+    const DevScene *scenes;
+    const long long *scene_path0;  // n_scenes + 1 prefix: first global path of each scene
+    const long long *scene_pix0;   // n_scenes + 1 prefix: first global pixel of each scene
+    const uint32_t *scene_key;     // Philox key per scene (2 words)
+    const int *scene_spp;
+    int n_scenes;
+    int *slot_scene;               // scene of each wave slot
 };
+
+// Largest k with prefix[k] <= g (prefix has n + 1 ascending entries).
+RUMI_D int find_scene(const long long *prefix, int n, long long g) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (prefix[mid] <= g)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+RUMI_D int isqrt_floor(int n) {
+    int d = 0;
+    while ((d + 1) * (d + 1) <= n) ++d;
+    return d;
+}
 
 __global__ void pt_generate(PtLaunch P) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j == 0) P.cnt[C_RAY0] = P.n_paths;
     if (j >= P.n_paths) return;
-    const long long pixel = (long long)P.pix0 + j / P.spp;
-    const int s = j % P.spp;
-    const int W = P.s.width;
-    const int w = (int)(pixel % W), h = (int)(pixel / W);
-    const float2 smp = pixel_sample(s, P.spp, P.grid_d, P.square != 0, pixel, P.k0, P.k1);
     float3 o, d;
-    camera_ray(P.s.camera, W, P.s.height, w, h, smp.x, smp.y, o, d);
+    if (P.scenes) {
+        const long long g = P.path0 + j;
+        const int k = find_scene(P.scene_path0, P.n_scenes, g);
+        const DevScene &S = P.scenes[k];
+        const int spp = P.scene_spp[k];
+        const long long local = g - P.scene_path0[k];
+        const long long pixel = local / spp;
+        const int s = (int)(local % spp);
+        const int gd = isqrt_floor(spp);
+        const int w = (int)(pixel % S.width), h = (int)(pixel / S.width);
+        const float2 smp = pixel_sample(s, spp, gd, gd * gd == spp, pixel, P.scene_key[2 * k], P.scene_key[2 * k + 1]);
+        camera_ray(S.camera, S.width, S.height, w, h, smp.x, smp.y, o, d);
+        P.slot_scene[j] = k;
+    } else {
+        const long long pixel = (long long)P.pix0 + j / P.spp;
+        const int s = j % P.spp;
+        const int W = P.s.width;
+        const int w = (int)(pixel % W), h = (int)(pixel / W);
+        const float2 smp = pixel_sample(s, P.spp, P.grid_d, P.square != 0, pixel, P.k0, P.k1);
+        camera_ray(P.s.camera, W, P.s.height, w, h, smp.x, smp.y, o, d);
+    }
     P.ray_o[0][j] = make_float4(o.x, o.y, o.z, __int_as_float(j));
     P.ray_d[0][j] = make_float4(d.x, d.y, d.z, FLT_MAX);
     P.beta[j] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -82,101 +125,91 @@ __global__ void pt_reset(PtLaunch P, int bounce) {
 
 __global__ void pt_finish(PtLaunch P) { P.stats[S_RAYS_SH] += (unsigned long long)P.cnt[C_SHADOW]; }
 
-// Persistent traversal kernels with per-lane refill: every lane holds one ray and
-// advances it one node pair per iteration; lanes whose ray finished take new rays from
-// the queue together (one warp-aggregated atomic) once REFILL_MIN of them are idle, so
-// warps stay full until the queue drains.
-static constexpr int REFILL_MIN = 8;
-static constexpr int SPILL = RUMI_MAX_BVH_DEPTH - STACK_SMEM;
-
-template <bool STATS>
+// Persistent traversal kernels: every block takes rays from the bounce's queue until it
+// is empty (traverse_queue in traverse.cuh; MODE selects the scheme, see there).
+template <int MODE, bool STATS>
 __global__ void __launch_bounds__(TRACE_THREADS) pt_extend(PtLaunch P, int bounce) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
     const int cur = bounce & 1;
-    const int n = P.cnt[cur];
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    int *my_stack = stack + threadIdx.x;
-    int spill[SPILL];
     TraceStats st{0, 0};
-    TravState T;
-    int ray = -1;
-    bool exhausted = false;
-    for (;;) {
-        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
-        if (!exhausted && idle && (__popc(idle) >= REFILL_MIN || idle == 0xffffffffu)) {
-            int base = 0;
-            const int leader = __ffs(idle) - 1;
-            if (lane == leader) base = atomicAdd(&P.cnt[C_FETCH_EXT], __popc(idle));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (base + __popc(idle) >= n) exhausted = true;
-            if (ray < 0) {
-                const int r = base + __popc(idle & lt);
-                if (r < n) {
-                    ray = r;
-                    const float4 o4 = P.ray_o[cur][r];
-                    const float4 d4 = P.ray_d[cur][r];
-                    trav_begin<false, STATS>(P.s, T, f4xyz(o4), f4xyz(d4), d4.w, (__float_as_uint(o4.w) >> 31) != 0, st);
-                }
-            }
-        }
-        if (__ballot_sync(0xffffffffu, ray >= 0) == 0) break;
-        if (ray >= 0) {
-            if (T.cur != -2) trav_step<false, STACK_SMEM, STATS>(P.s, T, my_stack, TRACE_THREADS, spill, st);
-            if (T.cur == -2) {
-                const int code = T.h.t > 0.0f ? (T.h.id | (T.h.back ? (int)0x80000000 : 0)) : -1;
-                P.hit[ray] = make_float4(T.h.t, __int_as_float(code), T.h.u, T.h.v);
-                ray = -1;
-            }
-        }
-    }
+    auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
+        const float4 o4 = P.ray_o[cur][i];
+        const float4 d4 = P.ray_d[cur][i];
+        o = f4xyz(o4);
+        d = f4xyz(d4);
+        tmax = d4.w;
+        in_obj = (__float_as_uint(o4.w) >> 31) != 0;
+    };
+    auto finish = [&](int i, const HitRec &h) {
+        const int code = h.t > 0.0f ? (h.id | (h.back ? (int)0x80000000 : 0)) : -1;
+        P.hit[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
+    };
+    traverse_queue<MODE, false, STACK_SMEM, STATS>(P.s, P.cnt[cur], &P.cnt[C_FETCH_EXT], P.refill_min,
+                                                   stack + threadIdx.x, TRACE_THREADS, fetch, finish, st);
     if (STATS) {
         atomicAdd(&P.stats[S_NODES], (unsigned long long)st.nodes);
         atomicAdd(&P.stats[S_PRIMS], (unsigned long long)st.prims);
     }
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(TRACE_THREADS) pt_shadow(PtLaunch P) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
-    const int n = P.cnt[C_SHADOW];
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    int *my_stack = stack + threadIdx.x;
-    int spill[SPILL];
     TraceStats st{0, 0};
-    TravState T;
-    int ray = -1;
-    bool exhausted = false;
-    for (;;) {
-        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
-        if (!exhausted && idle && (__popc(idle) >= REFILL_MIN || idle == 0xffffffffu)) {
-            int base = 0;
-            const int leader = __ffs(idle) - 1;
-            if (lane == leader) base = atomicAdd(&P.cnt[C_FETCH_SH], __popc(idle));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (base + __popc(idle) >= n) exhausted = true;
-            if (ray < 0) {
-                const int r = base + __popc(idle & lt);
-                if (r < n) {
-                    ray = r;
-                    const float4 o4 = P.sh_o[r];
-                    const float4 d4 = P.sh_d[r];
-                    trav_begin<true, false>(P.s, T, f4xyz(o4), f4xyz(d4), d4.w, false, st);
-                }
-            }
+    auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
+        const float4 o4 = P.sh_o[i];
+        const float4 d4 = P.sh_d[i];
+        o = f4xyz(o4);
+        d = f4xyz(d4);
+        tmax = d4.w;
+        in_obj = false;
+    };
+    auto finish = [&](int i, const HitRec &h) {
+        if (h.t == 0.0f) {
+            const int slot = __float_as_int(P.sh_o[i].w);
+            const float4 c = P.sh_c[i];
+            float4 l = P.L[slot];
+            l.x += c.x; l.y += c.y; l.z += c.z;
+            P.L[slot] = l;
         }
-        if (__ballot_sync(0xffffffffu, ray >= 0) == 0) break;
-        if (ray >= 0) {
-            if (T.cur != -2) trav_step<true, STACK_SMEM, false>(P.s, T, my_stack, TRACE_THREADS, spill, st);
-            if (T.cur == -2) {
-                if (T.h.t == 0.0f) {
-                    const int slot = __float_as_int(P.sh_o[ray].w);
-                    const float4 c = P.sh_c[ray];
+    };
+    traverse_queue<MODE, true, STACK_SMEM, false>(P.s, P.cnt[C_SHADOW], &P.cnt[C_FETCH_SH], P.refill_min,
+                                                  stack + threadIdx.x, TRACE_THREADS, fetch, finish, st);
+}
+
+// Multi-scene batches: the warp-batch traversal with each ray's own scene.
+template <bool ANYHIT>
+__global__ void __launch_bounds__(TRACE_THREADS) pt_trace_multi(PtLaunch P, int bounce) {
+    __shared__ int stack[STACK_SMEM * TRACE_THREADS];
+    const int cur = bounce & 1;
+    const int n = ANYHIT ? P.cnt[C_SHADOW] : P.cnt[cur];
+    int *counter = ANYHIT ? &P.cnt[C_FETCH_SH] : &P.cnt[C_FETCH_EXT];
+    const int lane = threadIdx.x & 31;
+    TraceStats st{0, 0};
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const int i = base + lane;
+        if (i < n) {
+            const float4 o4 = ANYHIT ? P.sh_o[i] : P.ray_o[cur][i];
+            const float4 d4 = ANYHIT ? P.sh_d[i] : P.ray_d[cur][i];
+            const int slot = __float_as_int(o4.w) & 0x7fffffff;
+            const DevScene &S = P.scenes[P.slot_scene[slot]];
+            const bool in_obj = !ANYHIT && (__float_as_uint(o4.w) >> 31) != 0;
+            const HitRec h = trace_ray<ANYHIT, STACK_SMEM, false>(S, f4xyz(o4), f4xyz(d4), d4.w, in_obj,
+                                                                 stack + threadIdx.x, TRACE_THREADS, st);
+            if (ANYHIT) {
+                if (h.t == 0.0f) {
+                    const float4 c = P.sh_c[i];
                     float4 l = P.L[slot];
                     l.x += c.x; l.y += c.y; l.z += c.z;
                     P.L[slot] = l;
                 }
-                ray = -1;
+            } else {
+                const int code = h.t > 0.0f ? (h.id | (h.back ? (int)0x80000000 : 0)) : -1;
+                P.hit[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
             }
         }
     }
@@ -204,7 +237,6 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
     const int n = P.cnt[cur];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < n;
-    const DevScene &S = P.s;
 
     bool want_next = false, want_sh = false;
     float3 nx_o = mk3(0, 0, 0), nx_d = mk3(0, 0, 0);
@@ -219,6 +251,17 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
         const float4 d4 = P.ray_d[cur][i];
         const float4 hv = P.hit[i];
         slot = __float_as_int(o4.w) & 0x7fffffff;
+        const DevScene *Sp = &P.s;
+        uint32_t k0 = P.k0, k1 = P.k1;
+        uint64_t path = (uint64_t)(P.path0 + slot);
+        if (P.scenes) {
+            const int sk = P.slot_scene[slot];
+            Sp = &P.scenes[sk];
+            k0 = P.scene_key[2 * sk];
+            k1 = P.scene_key[2 * sk + 1];
+            path = (uint64_t)(P.path0 + slot - P.scene_path0[sk]);
+        }
+        const DevScene &S = *Sp;
         const float3 o = f4xyz(o4), d = f4xyz(d4);
         const float t = hv.x;
         const bool hit = t > 0.0f;
@@ -226,9 +269,8 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
         const unsigned fl = P.pflags[slot];
         const bool le = (fl & PFL_LE) != 0, inobj = (fl & PFL_IN) != 0;
         beta = f4xyz(P.beta[slot]);
-        const uint64_t path = (uint64_t)(P.path0 + slot);
-        const Uniform4 U0 = path_uniforms(path, bounce, 0, P.k0, P.k1);
-        const Uniform4 U1 = path_uniforms(path, bounce, 1, P.k0, P.k1);
+        const Uniform4 U0 = path_uniforms(path, bounce, 0, k0, k1);
+        const Uniform4 U1 = path_uniforms(path, bounce, 1, k0, k1);
         const bool last = bounce + 1 >= P.max_depth;
         float3 addL = mk3(0, 0, 0);
         bool done = false;
@@ -252,7 +294,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                         float3 wi;
                         float dist, G;
                         if (nee_setup(ls, p, wi, dist, G)) {
-                            const Uniform4 U2 = path_uniforms(path, bounce, 2, P.k0, P.k1);
+                            const Uniform4 U2 = path_uniforms(path, bounce, 2, k0, k1);
                             const float tr = volume_shadow_tr(V, p, wi, dist, U2.u[2]);
                             if (tr > 0.0f) {
                                 const float fp = V.g == 0.0f ? 1.0f / (4.0f * RUMI_PI_F) : hg_eval(dot3(d, wi), V.g);
@@ -327,7 +369,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                 bool walk_scatter = false, absorbed = false;
                 if (m.type == MAT_SUBSURFACE && inobj) {
                     // Subsurface::PhaseSampling (subsurface.cpp:121-142): random walk step
-                    const Uniform4 U2 = path_uniforms(path, bounce, 2, P.k0, P.k1);
+                    const Uniform4 U2 = path_uniforms(path, bounce, 2, k0, k1);
                     const DistSample ws = distance_sample(m.sigma_t, m.avg_sigma_t, m.absorb, t, U2.u[0], U2.u[1]);
                     if (ws.outcome == 1) {
                         walk_scatter = true;
@@ -366,7 +408,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                             if (m.type == MAT_GLOSSY) direct = direct * (1.0f / m.kd_pdf);
                             float tr = 1.0f;
                             if (V.present) {
-                                const Uniform4 U2 = path_uniforms(path, bounce, 2, P.k0, P.k1);
+                                const Uniform4 U2 = path_uniforms(path, bounce, 2, k0, k1);
                                 tr = volume_shadow_tr(V, p, wi, dist, U2.u[2]);
                             }
                             if (tr > 0.0f) {
@@ -420,12 +462,19 @@ __global__ void pt_resolve(PtLaunch P) {
     if (warp >= P.n_pix) return;
     float3 acc = mk3(0.0f, 0.0f, 0.0f);
     int nan = 0;
-    const size_t base = (size_t)warp * P.spp;
-    for (int s0 = 0; s0 < P.spp; s0 += 32) {
+    const long long gp = (long long)P.pix0 + warp;
+    int spp = P.spp;
+    size_t base = (size_t)warp * P.spp;
+    if (P.scenes) {
+        const int k = find_scene(P.scene_pix0, P.n_scenes, gp);
+        spp = P.scene_spp[k];
+        base = (size_t)(P.scene_path0[k] + (gp - P.scene_pix0[k]) * spp - P.path0);
+    }
+    for (int s0 = 0; s0 < spp; s0 += 32) {
         const int s = s0 + lane;
         float4 l = make_float4(0, 0, 0, 0);
-        if (s < P.spp) l = P.L[base + s];
-        const int cnt = min(32, P.spp - s0);
+        if (s < spp) l = P.L[base + s];
+        const int cnt = min(32, spp - s0);
         for (int k = 0; k < cnt; ++k) {
             const float x = __shfl_sync(0xffffffffu, l.x, k);
             const float y = __shfl_sync(0xffffffffu, l.y, k);
@@ -438,7 +487,7 @@ __global__ void pt_resolve(PtLaunch P) {
         }
     }
     if (lane == 0) {
-        const size_t px = (size_t)(P.pix0 + warp) * 3;
+        const size_t px = (size_t)gp * 3;
         P.film[px + 0] = acc.z;  // B
         P.film[px + 1] = acc.y;  // G
         P.film[px + 2] = acc.x;  // R
@@ -460,7 +509,7 @@ size_t pt_workspace_bytes(long long paths) {
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                       cudaStream_t stream) {
     const long long total_pix = (long long)sc->dev.width * sc->dev.height;
-    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 21);
+    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 22);
     long long pix_per_wave = wave / p->spp;
     if (pix_per_wave < 1) pix_per_wave = 1;
     if (pix_per_wave > total_pix) pix_per_wave = total_pix;
@@ -509,16 +558,36 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     L.cnt = (int *)w; w += al(C_NUM * sizeof(int));
     L.stats = (unsigned long long *)w; w += al(S_NUM * sizeof(unsigned long long));
     L.film = film_dev;
+    L.scenes = nullptr;
+    L.scene_path0 = L.scene_pix0 = nullptr;
+    L.scene_key = nullptr;
+    L.scene_spp = nullptr;
+    L.n_scenes = 0;
+    L.slot_scene = nullptr;
     cudaMemsetAsync(L.cnt, 0, C_NUM * sizeof(int), stream);
     cudaMemsetAsync(L.stats, 0, S_NUM * sizeof(unsigned long long), stream);
 
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<false>, TRACE_THREADS, 0);
+    // traversal scheme and persistent grid (autotuner knobs; 0 = defaults)
+    const int mode = p->trace_mode >= 1 && p->trace_mode <= 3 ? p->trace_mode - 1 : 0;
+    L.refill_min = p->refill_min > 0 ? p->refill_min : 8;
+    int occ = 0, occ_sh = 0;
+    if (mode == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<0, false>, TRACE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<0>, TRACE_THREADS, 0);
+    } else if (mode == 1) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<1, false>, TRACE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<1>, TRACE_THREADS, 0);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<2, false>, TRACE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<2>, TRACE_THREADS, 0);
+    }
     if (occ < 1) occ = 1;
-    const int trace_grid = sc->num_sms * occ;
-    int occ_sh = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow, TRACE_THREADS, 0);
     if (occ_sh < 1) occ_sh = 1;
+    if (p->blocks_per_sm > 0) {
+        occ = p->blocks_per_sm < occ ? p->blocks_per_sm : occ;
+        occ_sh = p->blocks_per_sm < occ_sh ? p->blocks_per_sm : occ_sh;
+    }
+    const int trace_grid = sc->num_sms * occ;
     const int shadow_grid = sc->num_sms * occ_sh;
 
     const bool timing = (p->flags & RUMI_FLAG_TIMING) != 0;
@@ -546,15 +615,24 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
             int e0 = 0;
             if (timing) { e0 = (int)evs.size(); mark(); }
             if (count_stats)
-                pt_extend<true><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
+                pt_extend<0, true><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
+            else if (mode == 0)
+                pt_extend<0, false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
+            else if (mode == 1)
+                pt_extend<1, false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
             else
-                pt_extend<false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
+                pt_extend<2, false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
             if (timing) { mark(); ext_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
             pt_shade<<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
             if (timing) { mark(); shade_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
-            pt_shadow<<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
+            if (mode == 0)
+                pt_shadow<0><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
+            else if (mode == 1)
+                pt_shadow<1><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
+            else
+                pt_shadow<2><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
             if (timing) { mark(); sh_ev.push_back({e0, e0 + 1}); }
         }
         pt_finish<<<1, 1, 0, stream>>>(L);
@@ -593,6 +671,86 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     }
     for (auto ev : evs) cudaEventDestroy(ev);
     return RUMI_OK;
+}
+
+// ---------------------------------------------------------------- scene batches
+// Device bytes of a multi-scene wave: the single-scene wave state plus each slot's scene.
+size_t pt_batch_workspace_bytes(long long wave_paths) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    return pt_workspace_bytes(wave_paths) + al((size_t)wave_paths * sizeof(int));
+}
+
+// Enqueues one frame of a multi-scene batch without synchronising, so the sequence can
+// be captured into a CUDA graph: waves over the batch's global pixel / path index space,
+// every stage serving all scenes from shared queues.
+rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaStream_t stream, int num_sms) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t Wp = (size_t)F.wave_paths;
+    const size_t f4 = al(Wp * sizeof(float4));
+    char *w = (char *)ws;
+    PtLaunch L;
+    memset(&L, 0, sizeof(L));
+    L.max_depth = F.max_depth;
+    L.ray_o[0] = (float4 *)w; w += f4;
+    L.ray_o[1] = (float4 *)w; w += f4;
+    L.ray_d[0] = (float4 *)w; w += f4;
+    L.ray_d[1] = (float4 *)w; w += f4;
+    L.hit = (float4 *)w; w += f4;
+    L.sh_o = (float4 *)w; w += f4;
+    L.sh_d = (float4 *)w; w += f4;
+    L.sh_c = (float4 *)w; w += f4;
+    L.beta = (float4 *)w; w += f4;
+    L.L = (float4 *)w; w += f4;
+    L.pflags = (unsigned *)w; w += al(Wp * sizeof(unsigned));
+    L.cnt = (int *)w; w += al(C_NUM * sizeof(int));
+    L.stats = (unsigned long long *)w; w += al(S_NUM * sizeof(unsigned long long));
+    L.slot_scene = (int *)w;
+    L.film = films;
+    L.scenes = F.scenes;
+    L.scene_path0 = F.scene_path0;
+    L.scene_pix0 = F.scene_pix0;
+    L.scene_key = F.scene_key;
+    L.scene_spp = F.scene_spp;
+    L.n_scenes = F.n_scenes;
+    L.spp = 1;
+    L.refill_min = 8;
+    cudaMemsetAsync(L.cnt, 0, C_NUM * sizeof(int), stream);
+    cudaMemsetAsync(L.stats, 0, S_NUM * sizeof(unsigned long long), stream);
+    int occ = 0, occ_sh = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_trace_multi<false>, TRACE_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_trace_multi<true>, TRACE_THREADS, 0);
+    if (occ < 1) occ = 1;
+    if (occ_sh < 1) occ_sh = 1;
+    if (F.blocks_per_sm > 0) {
+        occ = F.blocks_per_sm < occ ? F.blocks_per_sm : occ;
+        occ_sh = F.blocks_per_sm < occ_sh ? F.blocks_per_sm : occ_sh;
+    }
+    for (const BatchWave &wv : F.waves) {
+        L.pix0 = (int)wv.pix0;
+        L.n_pix = (int)(wv.pix1 - wv.pix0);
+        L.path0 = wv.path0;
+        L.n_paths = (int)(wv.path1 - wv.path0);
+        pt_generate<<<cdiv(L.n_paths, 256), 256, 0, stream>>>(L);
+        for (int b = 0; b < F.max_depth; ++b) {
+            pt_reset<<<1, 1, 0, stream>>>(L, b);
+            pt_trace_multi<false><<<num_sms * occ, TRACE_THREADS, 0, stream>>>(L, b);
+            pt_shade<<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
+            pt_trace_multi<true><<<num_sms * occ_sh, TRACE_THREADS, 0, stream>>>(L, b);
+        }
+        pt_finish<<<1, 1, 0, stream>>>(L);
+        pt_resolve<<<cdiv(L.n_pix * 32LL, 256), 256, 0, stream>>>(L);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "batch launch");
+    return RUMI_OK;
+}
+
+// Device address of the 64-bit statistics inside a batch workspace.
+unsigned long long *pt_batch_stats_ptr(void *ws, long long wave_paths) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t Wp = (size_t)wave_paths;
+    const size_t off = 10 * al(Wp * sizeof(float4)) + al(Wp * sizeof(unsigned)) + al(C_NUM * sizeof(int));
+    return (unsigned long long *)((char *)ws + off);
 }
 
 // ---------------------------------------------------------------- ray batches

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <string>
+#include <vector>
 #include "../../include/rumi_b200.h"
 #include "scene.cuh"
 #include "bvh_build.h"
@@ -30,6 +31,27 @@ struct rumi_scene {
 };
 
 namespace rumi {
+
+struct BatchWave {
+    long long pix0, pix1, path0, path1;  // global pixel / path ranges of one wave
+};
+
+// One frame of a multi-scene batch (device tables; `waves` on the host).
+struct BatchFrame {
+    const DevScene *scenes;
+    const long long *scene_path0, *scene_pix0;
+    const uint32_t *scene_key;
+    const int *scene_spp;
+    int n_scenes;
+    int max_depth;
+    long long wave_paths;
+    int blocks_per_sm;
+    std::vector<BatchWave> waves;
+};
+
+size_t pt_batch_workspace_bytes(long long wave_paths);
+rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaStream_t stream, int num_sms);
+unsigned long long *pt_batch_stats_ptr(void *ws, long long wave_paths);
 
 void set_error(const std::string &msg);
 rumi_status cuda_status(cudaError_t e, const char *what);

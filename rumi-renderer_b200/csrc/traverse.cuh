@@ -358,3 +358,155 @@ RUMI_D void trav_step(const DevScene &s, TravState &T, int *smem_stack, int stri
         T.cur = -1;
     }
 }
+
+// Step with postponed leaves: leaves reached by this node pair are recorded in the
+// state (at most the pair's two children) instead of being intersected, so a warp can
+// intersect the leaves of all its lanes together ("while-while" traversal).
+struct PendingLeaves {
+    int f0, c0, f1, c1;
+    float tn1;
+    int n;
+};
+
+template <int STACK_SMEM, bool STATS>
+RUMI_D void trav_step_postpone(const DevScene &s, TravState &T, PendingLeaves &pl, int *smem_stack, int stride,
+                               int *spill, TraceStats &st) {
+    if (T.cur == -1) {
+        if (T.sp == 0) {
+            T.cur = -2;
+            return;
+        }
+        --T.sp;
+        T.cur = T.sp < STACK_SMEM ? smem_stack[T.sp * stride] : spill[T.sp - STACK_SMEM];
+    }
+    if ((unsigned)T.cur >= (unsigned)(s.n_nodes - 1) || ++T.steps > s.n_nodes) {
+        T.cur = -2;
+        return;
+    }
+    const float4 *np = reinterpret_cast<const float4 *>(s.nodes + T.cur);
+    const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
+    if (STATS) st.nodes += 2;
+    const float lim = T.h.t > 0.0f ? fminf(T.h.t, T.tmax) : T.tmax;
+    float tn0, tn1;
+    const bool h0 = slab(a0, b0, T.inv, T.oinv, lim, tn0);
+    const bool h1 = slab(a1, b1, T.inv, T.oinv, lim, tn1);
+    const int f0 = __float_as_int(b0.z), c0 = __float_as_int(b0.w);
+    const int f1 = __float_as_int(b1.z), c1 = __float_as_int(b1.w);
+    const bool l0 = h0 && c0 > 0, l1 = h1 && c1 > 0;
+    pl.n = 0;
+    if (l0 && l1) {
+        const bool sw = tn1 < tn0;
+        pl.f0 = sw ? f1 : f0; pl.c0 = sw ? c1 : c0;
+        pl.f1 = sw ? f0 : f1; pl.c1 = sw ? c0 : c1;
+        pl.tn1 = sw ? tn0 : tn1;
+        pl.n = 2;
+    } else if (l0) {
+        pl.f0 = f0; pl.c0 = c0; pl.n = 1;
+    } else if (l1) {
+        pl.f0 = f1; pl.c0 = c1; pl.n = 1;
+    }
+    const bool i0 = h0 && c0 == 0 && (T.h.t <= 0.0f || tn0 <= T.h.t);
+    const bool i1 = h1 && c1 == 0 && (T.h.t <= 0.0f || tn1 <= T.h.t);
+    if (i0 && i1) {
+        const bool swap01 = tn1 < tn0;
+        const int near_ = swap01 ? f1 : f0, far_ = swap01 ? f0 : f1;
+        if (T.sp < STACK_SMEM)
+            smem_stack[T.sp * stride] = far_;
+        else if (T.sp < RUMI_MAX_BVH_DEPTH)
+            spill[T.sp - STACK_SMEM] = far_;
+        if (T.sp < RUMI_MAX_BVH_DEPTH) ++T.sp;
+        T.cur = near_;
+    } else if (i0) {
+        T.cur = f0;
+    } else if (i1) {
+        T.cur = f1;
+    } else {
+        T.cur = -1;
+    }
+}
+
+// Intersects the postponed leaves; returns true when ANYHIT found a hit.
+template <bool ANYHIT, bool STATS>
+RUMI_D bool run_pending(const DevScene &s, TravState &T, PendingLeaves &pl, TraceStats &st) {
+    bool found = false;
+    if (pl.n > 0) found = leaf_isect<ANYHIT, STATS>(s, pl.f0, pl.c0, T.o, T.d, T.tmax, T.in_obj, T.h, st);
+    if (!found && pl.n > 1 && (T.h.t <= 0.0f || pl.tn1 <= T.h.t))
+        found = leaf_isect<ANYHIT, STATS>(s, pl.f1, pl.c1, T.o, T.d, T.tmax, T.in_obj, T.h, st);
+    pl.n = 0;
+    return found;
+}
+
+// Persistent queue traversal shared by every ray kernel.
+//   MODE 0: a warp takes 32 rays and traces each to completion.
+//   MODE 1: per-lane refill; every iteration advances each ray by one node pair.
+//   MODE 2: per-lane refill; interior node pairs until every busy lane holds postponed
+//           leaves, then the warp intersects those leaves together.
+// fetch(i, o, d, tmax, in_obj) loads ray i; finish(i, hit) consumes its result.
+template <int MODE, bool ANYHIT, int STACK_SMEM, bool STATS, typename Fetch, typename Finish>
+RUMI_D void traverse_queue(const DevScene &s, int n, int *counter, int refill_min, int *smem_stack, int stride,
+                           Fetch fetch, Finish finish, TraceStats &st) {
+    const int lane = threadIdx.x & 31;
+    int spill[RUMI_MAX_BVH_DEPTH - STACK_SMEM > 0 ? RUMI_MAX_BVH_DEPTH - STACK_SMEM : 1];
+    if (MODE == 0) {
+        for (;;) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(counter, 32);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= n) break;
+            const int i = base + lane;
+            if (i < n) {
+                float3 o, d;
+                float tmax;
+                bool in_obj;
+                fetch(i, o, d, tmax, in_obj);
+                const HitRec h = trace_ray<ANYHIT, STACK_SMEM, STATS>(s, o, d, tmax, in_obj, smem_stack, stride, st);
+                finish(i, h);
+            }
+        }
+        return;
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    TravState T;
+    PendingLeaves pl;
+    pl.n = 0;
+    int ray = -1;
+    bool exhausted = false;
+    for (int outer = 0;; ++outer) {
+        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
+        if (!exhausted && idle && (__popc(idle) >= refill_min || idle == 0xffffffffu)) {
+            int base = 0;
+            const int leader = __ffs(idle) - 1;
+            if (lane == leader) base = atomicAdd(counter, __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= n) exhausted = true;
+            if (ray < 0) {
+                const int r = base + __popc(idle & lt);
+                if (r < n) {
+                    ray = r;
+                    float3 o, d;
+                    float tmax;
+                    bool in_obj;
+                    fetch(r, o, d, tmax, in_obj);
+                    trav_begin<ANYHIT, STATS>(s, T, o, d, tmax, in_obj, st);
+                    pl.n = 0;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, ray >= 0) == 0) break;
+        if (MODE == 1) {
+            if (ray >= 0 && T.cur != -2) trav_step<ANYHIT, STACK_SMEM, STATS>(s, T, smem_stack, stride, spill, st);
+        } else {
+            for (int it = 0; it < 4 * RUMI_MAX_BVH_DEPTH; ++it) {
+                const bool want = ray >= 0 && pl.n == 0 && T.cur != -2;
+                if (__ballot_sync(0xffffffffu, want) == 0) break;
+                if (want) trav_step_postpone<STACK_SMEM, STATS>(s, T, pl, smem_stack, stride, spill, st);
+            }
+            if (ray >= 0 && pl.n > 0)
+                if (run_pending<ANYHIT, STATS>(s, T, pl, st)) T.cur = -2;
+        }
+        if (ray >= 0 && T.cur == -2 && pl.n == 0) {
+            finish(ray, T.h);
+            ray = -1;
+        }
+    }
+}

@@ -102,7 +102,8 @@ class GpuScene:
         return {k: getattr(info, k) for k, _ in info._fields_}
 
     def render(self, spp: int = None, seed: int = 1, tracer=None, wave_paths: int = 0, timing: bool = False,
-               film_device_ptr: int = None, stream: int = None, count_stats: bool = False):
+               film_device_ptr: int = None, stream: int = None, count_stats: bool = False, trace_mode: int = 0,
+               blocks_per_sm: int = 0, refill_min: int = 0, tuning: dict = None):
         """Renders one frame.  Returns (film (H, W, 3) B,G,R sums, stats dict); with
         film_device_ptr the film stays on the device and the first value is None."""
         tr = tracer or self.flat.tracer
@@ -117,6 +118,12 @@ class GpuScene:
         p.wave_paths = int(wave_paths)
         p.flags = (1 if timing else 0) | (2 if count_stats else 0)
         p.stream = stream
+        t = dict(tuning or {})
+        p.trace_mode = int(t.get("trace_mode", trace_mode))
+        p.blocks_per_sm = int(t.get("blocks_per_sm", blocks_per_sm))
+        p.refill_min = int(t.get("refill_min", refill_min))
+        if "wave_paths" in t and not wave_paths:
+            p.wave_paths = int(t["wave_paths"])
         st = _capi.rumi_render_stats()
         if film_device_ptr is not None:
             _capi.check(self.lib.rumi_render(self.h, C.byref(p), C.c_void_p(film_device_ptr), 1, C.byref(st)),
@@ -159,6 +166,61 @@ class GpuScene:
     def close(self):
         if getattr(self, "h", None):
             self.lib.rumi_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuBatch:
+    """Many GpuScenes path traced as one frame from shared ray queues (rumi_batch).  The
+    scenes must stay open while the batch lives."""
+
+    def __init__(self, scenes):
+        self.lib = _capi.load()
+        self.scenes = list(scenes)
+        arr = (C.c_void_p * len(self.scenes))(*[g.h.value for g in self.scenes])
+        h = C.c_void_p()
+        _capi.check(self.lib.rumi_batch_create(arr, len(self.scenes), C.byref(h)), "rumi_batch_create")
+        self.h = h
+        self.sizes = [(g.height, g.width) for g in self.scenes]
+        self.n_floats = int(self.lib.rumi_batch_film_floats(self.h))
+
+    def render(self, spp, seeds, max_depth: int, graph: bool = False, timing: bool = False, wave_paths: int = 0,
+               blocks_per_sm: int = 0, films_device_ptr: int = None, stream: int = None):
+        """One frame of every scene.  Returns (list of (H, W, 3) films, stats dict); with
+        films_device_ptr the concatenated films stay on the device and the list is None."""
+        n = len(self.scenes)
+        spp_a = (C.c_int32 * n)(*[int(x) for x in (spp if hasattr(spp, "__len__") else [spp] * n)])
+        seed_a = (C.c_uint64 * n)(*[int(x) for x in (seeds if hasattr(seeds, "__len__") else [seeds] * n)])
+        p = _capi.rumi_batch_params()
+        p.max_depth = int(max_depth)
+        p.spp = spp_a
+        p.seeds = seed_a
+        p.wave_paths = int(wave_paths)
+        p.flags = (1 if timing else 0) | (_capi.BATCH_GRAPH if graph else 0)
+        p.blocks_per_sm = int(blocks_per_sm)
+        p.stream = stream
+        st = _capi.rumi_render_stats()
+        if films_device_ptr is not None:
+            _capi.check(self.lib.rumi_render_batch(self.h, C.byref(p), C.c_void_p(films_device_ptr), 1, C.byref(st)),
+                        "rumi_render_batch")
+            return None, st.as_dict()
+        flat = np.zeros(self.n_floats, np.float32)
+        _capi.check(self.lib.rumi_render_batch(self.h, C.byref(p), flat.ctypes.data_as(C.c_void_p), 0, C.byref(st)),
+                    "rumi_render_batch")
+        films, o = [], 0
+        for H, W in self.sizes:
+            films.append(flat[o:o + H * W * 3].reshape(H, W, 3))
+            o += H * W * 3
+        return films, st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rumi_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

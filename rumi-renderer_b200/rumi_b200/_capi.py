@@ -51,7 +51,8 @@ class rumi_scene_desc(C.Structure):
 class rumi_render_params(C.Structure):
     _fields_ = [("integrator", C.c_int32), ("max_depth", C.c_int32), ("n_light", C.c_int32), ("n_eye", C.c_int32),
                 ("spp", C.c_int32), ("seed", C.c_uint64), ("wave_paths", C.c_int32), ("flags", C.c_int32),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("trace_mode", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("refill_min", C.c_int32)]
 
 
 class rumi_render_stats(C.Structure):
@@ -65,6 +66,15 @@ class rumi_render_stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class rumi_batch_params(C.Structure):
+    _fields_ = [("max_depth", C.c_int32), ("spp", C.POINTER(C.c_int32)), ("seeds", C.POINTER(C.c_uint64)),
+                ("wave_paths", C.c_int32), ("flags", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("stream", C.c_void_p)]
+
+
+BATCH_GRAPH = 4
+
+
 class rumi_bvh_info(C.Structure):
     _fields_ = [("large_levels", C.c_int32), ("small_tasks", C.c_int32), ("n_nodes", C.c_int32),
                 ("build_ms", C.c_double)]
@@ -72,7 +82,8 @@ class rumi_bvh_info(C.Structure):
 
 # every symbol include/rumi_b200.h and include/rumi_b200_test.h declare
 EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "rumi_render", "rumi_render_noalloc",
-           "rumi_trace_rays",
+           "rumi_trace_rays", "rumi_batch_create", "rumi_batch_destroy", "rumi_batch_film_floats",
+           "rumi_render_batch",
            "rumi_last_error_string", "rumi_version",
            "rumi_test_philox", "rumi_test_material_sample", "rumi_test_material_fr", "rumi_test_distance_sample",
            "rumi_test_phase_sample", "rumi_test_camera_rays", "rumi_test_pixel_samples"]
@@ -103,6 +114,15 @@ def load(path: str = LIB_PATH):
     L.rumi_trace_rays.restype = C.c_int
     L.rumi_trace_rays.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_void_p]
+    L.rumi_batch_create.restype = C.c_int
+    L.rumi_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]
+    L.rumi_batch_destroy.restype = C.c_int
+    L.rumi_batch_destroy.argtypes = [C.c_void_p]
+    L.rumi_batch_film_floats.restype = C.c_int64
+    L.rumi_batch_film_floats.argtypes = [C.c_void_p]
+    L.rumi_render_batch.restype = C.c_int
+    L.rumi_render_batch.argtypes = [C.c_void_p, C.POINTER(rumi_batch_params), C.c_void_p, C.c_int32,
+                                    C.POINTER(rumi_render_stats)]
     vp = C.c_void_p
     L.rumi_test_philox.argtypes = [C.c_int64, vp, vp, vp]
     L.rumi_test_material_sample.argtypes = [C.POINTER(rumi_material), C.c_int64, vp, vp, vp, vp]

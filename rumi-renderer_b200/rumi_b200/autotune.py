@@ -1,0 +1,79 @@
+"""Autotuner of the renderer's launch parameters.
+
+Knobs (fields of rumi_render_params): ``trace_mode`` (traversal scheme of the persistent
+ray kernels), ``blocks_per_sm`` (persistent traversal blocks per SM, i.e. warps per SM in
+steps of 4), ``refill_min`` (idle lanes that trigger a per-lane refill) and ``wave_paths``
+(queue capacity: paths in flight per wave).  Each candidate renders the given scene and is
+timed on the device (RUMI_FLAG_TIMING); the search is coordinate descent from the library
+defaults.  Results are cached per GPU model and workload key in a JSON file.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+
+DEFAULTS = dict(trace_mode=1, blocks_per_sm=0, refill_min=8, wave_paths=1 << 22)
+SPACE = dict(trace_mode=[1, 2, 3], blocks_per_sm=[0, 4, 5, 6], refill_min=[4, 8, 16],
+             wave_paths=[1 << 21, 1 << 22, 1 << 23])
+CACHE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tuning", "autotune_cache.json")
+
+
+def gpu_name() -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(0)
+    except Exception:
+        return "unknown-gpu"
+
+
+def measure(gs, tuning: dict, spp: int, seed: int = 12345, repeats: int = 1, film_ptr=None) -> float:
+    """Device milliseconds of one frame with these launch parameters (best of repeats)."""
+    best = float("inf")
+    for r in range(repeats):
+        _, st = gs.render(spp=spp, seed=seed + r, timing=True, tuning=tuning, film_device_ptr=film_ptr)
+        best = min(best, st["total_ms"])
+    return best
+
+
+def tune(gs, spp: int, key: str, space: dict = None, repeats: int = 2, film_ptr=None, log=None,
+         cache_path: str = CACHE) -> dict:
+    """Coordinate descent over the knobs; returns the best parameters and caches them."""
+    space = space or SPACE
+    cur = dict(DEFAULTS)
+    cur_ms = measure(gs, cur, spp, repeats=repeats, film_ptr=film_ptr)
+    history = [(dict(cur), cur_ms)]
+    for knob in ("trace_mode", "blocks_per_sm", "refill_min", "wave_paths"):
+        for v in space[knob]:
+            if v == cur[knob]:
+                continue
+            cand = dict(cur)
+            cand[knob] = v
+            ms = measure(gs, cand, spp, repeats=repeats, film_ptr=film_ptr)
+            history.append((dict(cand), ms))
+            if log:
+                log(f"{knob}={v}: {ms:.2f} ms (best {cur_ms:.2f})")
+            if ms < cur_ms:
+                cur, cur_ms = cand, ms
+    result = dict(params=cur, ms=cur_ms, gpu=gpu_name(), key=key, when=time.strftime("%Y-%m-%dT%H:%M:%S"),
+                  history=[dict(params=p, ms=m) for p, m in history])
+    save(key, result, cache_path)
+    return result
+
+
+def load(key: str, cache_path: str = CACHE):
+    try:
+        data = json.load(open(cache_path))
+    except Exception:
+        return None
+    return data.get(f"{gpu_name()}|{key}")
+
+
+def save(key: str, result: dict, cache_path: str = CACHE):
+    os.makedirs(os.path.dirname(cache_path), exist_ok=True)
+    try:
+        data = json.load(open(cache_path))
+    except Exception:
+        data = {}
+    data[f"{result['gpu']}|{key}"] = result
+    json.dump(data, open(cache_path, "w"), indent=1)

@@ -226,3 +226,55 @@ def subsurface_cornell(width: int = 32, height: int = 32, spp: int = 16, max_dep
     sc.image = Film(width, height, spp)
     sc.tracer = PathTracer(max_depth)
     return sc
+
+
+def heightfield(n_target: int, seed: int, lo=(0.1, 0.1), hi=(0.9, 0.9), base: float = 0.12, amp: float = 0.12):
+    """Seeded fBm terrain over [lo, hi] in x/z: an nx-by-nx grid split into 2 nx^2
+    triangles, nx = max(2, round(sqrt(n_target / 2))).  Returns (F,3,3) float32."""
+    nx = max(2, int(round(math.sqrt(n_target / 2.0))))
+    g = np.arange(nx + 1, dtype=F32) / F32(nx)
+    x = (F32(lo[0]) + g * F32(hi[0] - lo[0])).astype(F32)
+    z = (F32(lo[1]) + g * F32(hi[1] - lo[1])).astype(F32)
+    X, Z = np.meshgrid(x, z, indexing="ij")
+    p = np.stack([X, np.zeros_like(X), Z], -1).reshape(-1, 3).astype(F32)
+    y = (F32(base) + F32(amp) * fbm((p * F32(4.0)).astype(F32), seed)).astype(F32)
+    p[:, 1] = y
+    P = p.reshape(nx + 1, nx + 1, 3)
+    a, b, c, d = P[:-1, :-1], P[1:, :-1], P[1:, 1:], P[:-1, 1:]
+    t0 = np.stack([a, c, b], -2).reshape(-1, 3, 3)
+    t1 = np.stack([a, d, c], -2).reshape(-1, 3, 3)
+    return np.ascontiguousarray(np.concatenate([t0, t1]), dtype=F32)
+
+
+BATCH_RESOLUTIONS = (64, 128, 256, 512)
+BATCH_SPP = (4, 16, 64)
+
+
+def batch_scene(i: int, max_depth: int = 8, res: int = None, spp: int = None, n_tris: int = None) -> Scene:
+    """Scene i of the batched workload: the Cornell box holding a seeded fBm terrain whose
+    triangle count is drawn log-uniform in [1k, 200k] (rounded to the terrain grid), with
+    per-triangle albedo, and a sphere; the terrain is Lambertian and the sphere glass, or
+    the other way round, by the seed.  Resolution from {64,128,256,512}^2, spp from
+    {4,16,64}, path depth 8.  res / spp / n_tris override the draws."""
+    rng = np.random.Generator(np.random.PCG64(1000 + i))
+    u_tris, u_res, u_spp, u_mat, u_pos = rng.random(5)
+    if n_tris is None:
+        n_tris = int(round(math.exp(math.log(1000.0) + u_tris * (math.log(200000.0) - math.log(1000.0)))))
+    if res is None:
+        res = BATCH_RESOLUTIONS[min(3, int(u_res * 4))]
+    if spp is None:
+        spp = BATCH_SPP[min(2, int(u_spp * 3))]
+    sc = Scene()
+    add_cornell_box(sc)
+    tris = heightfield(n_tris, 50 + i)
+    glass_terrain = u_mat < 0.5
+    if glass_terrain:
+        sc.add(Model(tris), Dielectric(1.5, 1.00029, (0.0, 0.0, 0.0)))
+        sc.add(Sphere((0.3 + 0.4 * float(u_pos), 0.55, 0.5), 0.12), Matte(1.0, WHITE))
+    else:
+        sc.add(Model(tris, albedo=random_albedo(tris.shape[0], 70 + i)), Matte(1.0, WHITE))
+        sc.add(Sphere((0.3 + 0.4 * float(u_pos), 0.55, 0.5), 0.12), Dielectric(1.5, 1.00029, (0.0, 0.0, 0.0)))
+    sc.camera = cornell_camera()
+    sc.image = Film(res, res, spp)
+    sc.tracer = PathTracer(max_depth)
+    return sc

@@ -19,7 +19,7 @@ def declared_symbols():
     names = set()
     for h in ("rumi_b200.h", "rumi_b200_test.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
-        names |= set(re.findall(r"^\s*(?:rumi_status|const char \*)\s*(rumi_\w+)\s*\(", text, re.M))
+        names |= set(re.findall(r"^\s*(?:rumi_status|const char \*|int64_t)\s*(rumi_\w+)\s*\(", text, re.M))
     return names
 
 
