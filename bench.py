@@ -44,8 +44,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--wave-paths", type=int, default=0)
     ap.add_argument("--small", action="store_true", help="256x256 at 16 spp (profiling runs)")
-    ap.add_argument("--workload", default="bvh_bound", choices=["bvh_bound", "batched"],
-                    help="batched: 256 seeded scenes as one frame vs the per-scene loop")
+    ap.add_argument("--workload", default="bvh_bound", choices=["bvh_bound", "batched", "adjoint"],
+                    help="batched: 256 seeded scenes as one frame vs the per-scene loop; "
+                         "adjoint: inverse rendering with the path-replay adjoint")
+    ap.add_argument("--adam-steps", type=int, default=200, help="adjoint workload: optimisation steps")
     ap.add_argument("--scenes", type=int, default=256, help="batched workload: number of scenes")
     return ap.parse_args()
 
@@ -510,12 +512,100 @@ def batched_arm(args):
     return 0 if equal else 1
 
 
+def adjoint_arm(args):
+    """Differentiable inverse rendering: the Cornell box with a seeded 65,536-triangle
+    displaced sphere (per-triangle RGB albedo, 196,608 parameters) in a homogeneous medium
+    (sigma_s, sigma_a RGB and HG g: 7 parameters); target rendered from the hidden
+    parameters at 256x256, 64 spp, depth 8; L2 image loss; Adam (lr 1e-2) from a uniform
+    0.5 albedo and a wrong medium.  One step = forward + path-replay backward + update.
+    value = gradient evaluations (of all parameters) per second over the timed steps."""
+    import numpy as np
+    import torch
+    import rumi_b200
+    from rumi_b200 import scenes
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from adjoint_torch import render
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    size, spp, depth = 256, 64, 8
+    gt = rumi_b200.GpuScene(scenes.inverse_rendering(size, size, spp, depth))
+    target = torch.from_numpy(gt.forward(seed=1)[0] / spp).cuda()
+    gt.close()
+    n_mesh = 4 * 4 ** 7
+    hidden = scenes.random_albedo(n_mesh, 23)
+    start = scenes.inverse_rendering(size, size, spp, depth, albedo=np.full((n_mesh, 3), 0.5, np.float32),
+                                     medium=scenes.INVERSE_START_MEDIUM)
+    g = rumi_b200.GpuScene(start)
+    alb_all = torch.from_numpy(start.flatten().tri_albedo.copy()).cuda()
+    walls = alb_all[:-n_mesh].clone()
+    mesh = torch.nn.Parameter(alb_all[-n_mesh:].clone())
+    m0 = scenes.INVERSE_START_MEDIUM
+    med = torch.nn.Parameter(torch.tensor(list(m0["sigma_s"]) + list(m0["sigma_a"]) + [m0["g"]],
+                                          dtype=torch.float32, device="cuda"))
+    opt = torch.optim.Adam([mesh, med], lr=1e-2)
+    hidden_t = torch.from_numpy(hidden).cuda()
+
+    def step(it):
+        film = render(torch.cat([walls, mesh]), med, g, spp, 100 + it) / spp
+        loss = ((film - target) ** 2).mean()
+        opt.zero_grad()
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            mesh.clamp_(0.01, 1.0)
+            med[0:6].clamp_(1e-3, 5.0)
+            med[6].clamp_(-0.9, 0.9)
+        return loss.detach()
+
+    # forward / backward split, measured on the start parameters before optimising
+    d = np.ones((size, size, 3), np.float32)
+    for _ in range(3):
+        g.forward(seed=7, timing=True)
+        g.backward(d, seed=7, timing=True)
+    fwd_ms = statistics.median(g.forward(seed=8 + i, timing=True)[1]["total_ms"] for i in range(5))
+    bwd_ms = statistics.median(g.backward(d, seed=8 + i, timing=True)[2]["total_ms"] for i in range(5))
+    alb_rmse0 = float(((mesh.detach() - hidden_t) ** 2).mean().sqrt())
+    for it in range(args.warmup):
+        step(-1 - it)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    losses = []
+    for it in range(args.adam_steps):
+        losses.append(step(it))
+    ev1.record()
+    torch.cuda.synchronize()
+    clocks_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    losses = [float(x) for x in losses]
+    alb_rmse = float(((mesh.detach() - hidden_t) ** 2).mean().sqrt())
+    t = scenes.INVERSE_TARGET_MEDIUM
+    line = dict(metric="adjoint grads/s", value=args.adam_steps / (ms / 1000.0), unit="gradient evaluations/s",
+                n_gpus=1, steps=args.adam_steps, warmup=args.warmup, ms_per_step=ms / args.adam_steps,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                data="synthetic (seeded 65,536-triangle displaced sphere, hidden seeded albedo and medium)",
+                config=dict(workload="inverse rendering: 256x256, 64 spp, depth 8, 65,536 triangles in a medium",
+                            params=3 * n_mesh + 7, optimiser="Adam lr 1e-2", loss="L2 image"),
+                forward_ms=fwd_ms, backward_ms=bwd_ms, backward_over_forward=bwd_ms / fwd_ms,
+                paths_per_step=size * size * spp, loss_first=losses[0], loss_last=losses[-1],
+                albedo_rmse_start=alb_rmse0, albedo_rmse_end=alb_rmse,
+                medium_end=[float(x) for x in med.detach().cpu()],
+                medium_target=list(t["sigma_s"]) + list(t["sigma_a"]) + [t["g"]],
+                gpu_launches=args.adam_steps * 3 * (3 + 4 * depth), clocks=clocks_info)
+    print(json.dumps(line), flush=True)
+    g.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
     if args.workload == "batched":
         return batched_arm(args)
+    if args.workload == "adjoint":
+        return adjoint_arm(args)
     return our_arm(args)
 
 

@@ -10,6 +10,8 @@
  *   rumi_render         <- Scene::Rendering + PathTracer::Trace / BidirectionalPathTracer::Trace
  *                          (src/Integrator/pathtracer.cpp:117-354,
  *                           src/Integrator/bidirectionalpathtracer.cpp:121-394)
+ *   rumi_render_batch   <- many Scene::Rendering calls, one frame from shared queues
+ *   rumi_forward / rumi_backward  <- path-replay adjoint of PathTracer::Trace (new)
  *   rumi_trace_rays     <- BVHAccel::Travel (src/Acceleration/bvh.cpp:150-213), closest-hit
  *                          (isect != NULL) and shadow (isect == NULL) forms
  *
@@ -225,6 +227,39 @@ rumi_status rumi_batch_destroy(rumi_batch *batch);
 int64_t rumi_batch_film_floats(const rumi_batch *batch);
 rumi_status rumi_render_batch(rumi_batch *batch, const rumi_batch_params *params, float *films,
                               int32_t films_on_device, rumi_render_stats *stats);
+
+/* Path-replay adjoint of the path tracer (no counterpart in the reference).
+ *
+ * rumi_forward renders exactly what rumi_render renders (integrator RUMI_PATH_TRACER).
+ * rumi_backward, given d_film = dLoss/dfilm (H*W*3 floats, the film's B,G,R layout) and
+ * the same params (seed, spp, depth, wave_paths), writes the gradient of
+ * sum(d_film * film) with respect to
+ *   grad_albedo: the per-triangle albedo (n_triangles * 3 floats, r,g,b, the layout of
+ *                rumi_scene_desc.tri_albedo); only Lambertian (Matte) triangles receive
+ *                gradient; NULL = not wanted;
+ *   grad_volume: the medium (7 floats: sigma_s r,g,b, sigma_a r,g,b, g); NULL = not wanted.
+ * Paths are replayed from their Philox streams (no per-vertex tape): each wave is traced
+ * once to record every path's radiance and once more to weight each event's score with
+ * the radiance that follows it.  Albedo gradients are exact for the estimator (albedo
+ * drives no sampling decision); medium gradients are score-function estimates of the
+ * derivative of the expected image (free-flight, absorption and shadow-transmittance
+ * decisions and the phase direction depend on the coefficients).  NaN samples, which
+ * the film drops, receive no gradient.  on_device: all buffers are device pointers.
+ * With the forward's seed the result is the exact derivative of that frame's
+ * <d_film, film>; for a loss that is nonlinear in the film (L2) give the backward a
+ * different seed, so that the residual and the derivative come from independent paths
+ * and the gradient is unbiased. */
+rumi_status rumi_forward(rumi_scene *scene, const rumi_render_params *params, float *film,
+                         int32_t film_on_device, rumi_render_stats *stats);
+rumi_status rumi_backward(rumi_scene *scene, const rumi_render_params *params, const float *d_film,
+                          float *grad_albedo, float *grad_volume, int32_t on_device,
+                          rumi_render_stats *stats);
+
+/* Parameter updates between optimisation steps (the BVH is kept).  albedo: n_triangles*3
+ * floats (r,g,b); the scene must have been created with tri_albedo.  volume: replaces the
+ * medium (box and coefficients; present = 0 removes it). */
+rumi_status rumi_scene_set_albedo(rumi_scene *scene, const float *albedo, int32_t on_device);
+rumi_status rumi_scene_set_volume(rumi_scene *scene, const rumi_volume *volume);
 
 /* Ray queries against the scene's BVH.  rays: n*8 floats (o.xyz, in_object flag as
  * 0/1, d.xyz, tmax).  anyhit = 0: closest hit -> t (0 = miss, the reference's

@@ -1,0 +1,123 @@
+// Path-replay adjoint of the path tracer (rumi_forward / rumi_backward in
+// include/rumi_b200.h) and the parameter updates an optimiser needs between steps
+// (rumi_scene_set_albedo, rumi_scene_set_volume).  The kernels live in pt.cu
+// (pt_shade<true>, pt_shadow<0, true>, pt_backward).
+#include "renderer.h"
+
+using namespace rumi;
+
+extern "C" {
+
+rumi_status rumi_forward(rumi_scene *sc, const rumi_render_params *p, float *film, int32_t film_on_device,
+                         rumi_render_stats *stats) {
+    if (p && p->integrator != RUMI_PATH_TRACER) {
+        set_error("rumi_forward: the adjoint covers the path tracer only");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    return rumi_render(sc, p, film, film_on_device, stats);
+}
+
+rumi_status rumi_backward(rumi_scene *sc, const rumi_render_params *p, const float *d_film, float *grad_albedo,
+                          float *grad_volume, int32_t on_device, rumi_render_stats *stats) {
+    if (!sc || !p || !d_film) {
+        set_error("rumi_backward: NULL argument");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    if (p->integrator != RUMI_PATH_TRACER) {
+        set_error("rumi_backward: the adjoint covers the path tracer only");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    if (p->spp <= 0 || p->max_depth <= 0) {
+        set_error("rumi_backward: spp and max_depth must be positive");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    if (grad_albedo && !sc->tri_albedo) {
+        set_error("rumi_backward: the scene has no per-triangle albedo to differentiate");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    if (grad_volume && !sc->dev.volume.present) {
+        set_error("rumi_backward: the scene has no medium to differentiate");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = p->stream ? (cudaStream_t)p->stream : sc->stream;
+    const size_t film_bytes = sizeof(float) * 3 * (size_t)sc->dev.width * sc->dev.height;
+    const size_t alb_bytes = sizeof(float) * 3 * (size_t)sc->dev.n_tris;
+    const size_t vol_bytes = sizeof(float) * 7;
+    const float *df = d_film;
+    float *ga = grad_albedo, *gv = grad_volume;
+    float *t_df = nullptr, *t_ga = nullptr, *t_gv = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (!on_device) {
+        e = dalloc((void **)&t_df, film_bytes, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(t_df, d_film, film_bytes, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && grad_albedo) e = dalloc((void **)&t_ga, alb_bytes, s);
+        if (e == cudaSuccess && grad_volume) e = dalloc((void **)&t_gv, vol_bytes, s);
+        df = t_df;
+        ga = t_ga;
+        gv = t_gv;
+    }
+    rumi_status st = e == cudaSuccess ? RUMI_OK : cuda_status(e, "rumi_backward buffers");
+    if (st == RUMI_OK) st = pt_backward(sc, p, df, ga, gv, stats, s);
+    if (st == RUMI_OK && !on_device) {
+        if (grad_albedo) e = cudaMemcpyAsync(grad_albedo, t_ga, alb_bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && grad_volume) e = cudaMemcpyAsync(grad_volume, t_gv, vol_bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_status(e, "rumi_backward copy");
+    }
+    dfree(t_df, s);
+    dfree(t_ga, s);
+    dfree(t_gv, s);
+    return st;
+}
+
+rumi_status rumi_scene_set_albedo(rumi_scene *sc, const float *albedo, int32_t on_device) {
+    if (!sc || !albedo) {
+        set_error("rumi_scene_set_albedo: NULL argument");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    if (!sc->tri_albedo) {
+        set_error("rumi_scene_set_albedo: the scene was created without per-triangle albedo");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    const int n = sc->dev.n_tris;
+    const size_t bytes = sizeof(float) * 3 * (size_t)n;
+    cudaStream_t s = sc->stream;
+    const float *src = albedo;
+    float *tmp = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (!on_device) {
+        e = dalloc((void **)&tmp, bytes, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, albedo, bytes, cudaMemcpyHostToDevice, s);
+        src = tmp;
+    }
+    if (e == cudaSuccess) pack_albedo(src, n, sc->tri_albedo, s);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    dfree(tmp, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? RUMI_OK : cuda_status(e, "rumi_scene_set_albedo");
+}
+
+rumi_status rumi_scene_set_volume(rumi_scene *sc, const rumi_volume *v) {
+    if (!sc || !v) {
+        set_error("rumi_scene_set_volume: NULL argument");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    if (v->present) {
+        for (int c = 0; c < 3; ++c) {
+            if (!(v->sigma_s[c] >= 0.0f) || !(v->sigma_a[c] >= 0.0f) || !(v->sigma_s[c] + v->sigma_a[c] > 0.0f)) {
+                set_error("rumi_scene_set_volume: coefficients must be >= 0 with positive extinction");
+                return RUMI_ERR_INVALID_ARG;
+            }
+        }
+        if (!(v->g > -1.0f && v->g < 1.0f)) {
+            set_error("rumi_scene_set_volume: g must lie in (-1, 1)");
+            return RUMI_ERR_INVALID_ARG;
+        }
+    }
+    DevVolume dv{};
+    if (v->present) fill_dev_volume(dv, *v);
+    sc->dev.volume = dv;
+    return RUMI_OK;
+}
+
+}  // extern "C"

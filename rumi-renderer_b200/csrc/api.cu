@@ -206,6 +206,30 @@ __global__ void pack_albedo_kernel(const float *a, int n, float4 *out) {
 
 }  // namespace
 
+namespace rumi {
+
+// HomogeneousVolume's constructor (src/Volume/homogeneousvolume.cpp:24-44): the box, the
+// coefficients and the derived mean extinction and absorption probability.
+void fill_dev_volume(DevVolume &dv, const rumi_volume &v) {
+    dv.present = v.present ? 1 : 0;
+    dv.bmin = make_float3(v.pmin[0], v.pmin[1], v.pmin[2]);
+    dv.bmax = make_float3(v.pmax[0], v.pmax[1], v.pmax[2]);
+    dv.sigma_s = make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]);
+    dv.sigma_a = make_float3(v.sigma_a[0], v.sigma_a[1], v.sigma_a[2]);
+    dv.sigma_t = make_float3(v.sigma_a[0] + v.sigma_s[0], v.sigma_a[1] + v.sigma_s[1], v.sigma_a[2] + v.sigma_s[2]);
+    dv.avg_sigma_t = (dv.sigma_t.z + dv.sigma_t.y + dv.sigma_t.x) * 0.33333333333f;
+    const float3 r = make_float3(dv.sigma_a.x / dv.sigma_t.x, dv.sigma_a.y / dv.sigma_t.y, dv.sigma_a.z / dv.sigma_t.z);
+    dv.absorb = (r.z + r.y + r.x) * 0.33333333333f;
+    dv.g = v.g;
+}
+
+void pack_albedo(const float *a_dev, int n, float4 *out, cudaStream_t s) {
+    const int grid = n < 256 * 1184 ? (n + 255) / 256 : 1184;
+    if (n > 0) pack_albedo_kernel<<<grid, 256, 0, s>>>(a_dev, n, out);
+}
+
+}  // namespace rumi
+
 extern "C" {
 
 const char *rumi_last_error_string(void) { return g_last_error.c_str(); }
@@ -288,20 +312,7 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     ds.n_materials = d->n_materials;
     ds.n_lights = d->n_lights;
     // volume
-    if (d->volume.present) {
-        const rumi_volume &v = d->volume;
-        DevVolume &dv = ds.volume;
-        dv.present = 1;
-        dv.bmin = make_float3(v.pmin[0], v.pmin[1], v.pmin[2]);
-        dv.bmax = make_float3(v.pmax[0], v.pmax[1], v.pmax[2]);
-        dv.sigma_s = make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]);
-        dv.sigma_a = make_float3(v.sigma_a[0], v.sigma_a[1], v.sigma_a[2]);
-        dv.sigma_t = make_float3(v.sigma_a[0] + v.sigma_s[0], v.sigma_a[1] + v.sigma_s[1], v.sigma_a[2] + v.sigma_s[2]);
-        dv.avg_sigma_t = (dv.sigma_t.z + dv.sigma_t.y + dv.sigma_t.x) * 0.33333333333f;
-        const float3 r = make_float3(dv.sigma_a.x / dv.sigma_t.x, dv.sigma_a.y / dv.sigma_t.y, dv.sigma_a.z / dv.sigma_t.z);
-        dv.absorb = (r.z + r.y + r.x) * 0.33333333333f;
-        dv.g = v.g;
-    }
+    if (d->volume.present) fill_dev_volume(ds.volume, d->volume);
     // camera
     {
         const rumi_camera &c = d->camera;

@@ -56,27 +56,35 @@ RUMI_D float2 pixel_sample(int s, int spp, int grid_d, bool square, long long pi
     const int ky = perm_index(s, spp, mix32(pk ^ k1) ^ 0xB5297A4Du);
     const Philox4 jx = philox4x32_10((uint32_t)kx, 0u, 0xFFFFFFFFu, 0u, k0, k1);
     const Philox4 jy = philox4x32_10((uint32_t)ky, 0u, 0xFFFFFFFFu, 0u, k0, k1);
+    // correctly rounded operations in source order: no contraction into the caller's
+    // arithmetic, so every inlined copy yields the same bits
     float2 r;
     if (square) {
-        const float normalize = 1.0f / (float)grid_d;
-        r.x = ((float)(kx % grid_d) + u01(jx.v[0])) * normalize;
-        r.y = ((float)(ky / grid_d) + u01(jy.v[1])) * normalize;
+        const float normalize = __fdiv_rn(1.0f, (float)grid_d);
+        r.x = __fmul_rn(__fadd_rn((float)(kx % grid_d), u01(jx.v[0])), normalize);
+        r.y = __fmul_rn(__fadd_rn((float)(ky / grid_d), u01(jy.v[1])), normalize);
     } else {
-        const float normalize = 1.0f / (float)spp;
-        r.x = ((float)kx + u01(jx.v[0])) * normalize;
-        r.y = ((float)ky + u01(jy.v[1])) * normalize;
+        const float normalize = __fdiv_rn(1.0f, (float)spp);
+        r.x = __fmul_rn(__fadd_rn((float)kx, u01(jx.v[0])), normalize);
+        r.y = __fmul_rn(__fadd_rn((float)ky, u01(jy.v[1])), normalize);
     }
     return r;
 }
 
 // Pinhole::CastViewRay (src/Camera/pinhole.cpp:97-136) without depth of field.
 RUMI_D void camera_ray(const DevCamera &c, int W, int H, int w, int h, float sx, float sy, float3 &o, float3 &d) {
-    const float half_w = W * 0.5f, half_h = H * 0.5f;
-    const float x = -(((float)w - half_w) + sx) / half_w * c.tanfov;
-    const float y = -(((float)h - half_h) + sy) / half_h * c.tanfov * c.y_ratio;
+    // correctly rounded operations in the reference's order (no FMA contraction)
+    const float half_w = __fmul_rn((float)W, 0.5f), half_h = __fmul_rn((float)H, 0.5f);
+    const float x = -__fmul_rn(__fdiv_rn(__fadd_rn(__fsub_rn((float)w, half_w), sx), half_w), c.tanfov);
+    const float y = -__fmul_rn(__fmul_rn(__fdiv_rn(__fadd_rn(__fsub_rn((float)h, half_h), sy), half_h), c.tanfov),
+                               c.y_ratio);
     const float3 l = normalize_ref(mk3(x, y, c.plane_dist));
-    d = mk3(c.m[0] * l.x + c.m[1] * l.y + c.m[2] * l.z + c.m[3], c.m[4] * l.x + c.m[5] * l.y + c.m[6] * l.z + c.m[7],
-            c.m[8] * l.x + c.m[9] * l.y + c.m[10] * l.z + c.m[11]);
+    auto row = [&](int r) {
+        return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.m[4 * r], l.x), __fmul_rn(c.m[4 * r + 1], l.y)),
+                                   __fmul_rn(c.m[4 * r + 2], l.z)),
+                         c.m[4 * r + 3]);
+    };
+    d = mk3(row(0), row(1), row(2));
     o = c.p;
 }
 

@@ -59,7 +59,51 @@ struct PtLaunch {
     const int *scene_spp;
     int n_scenes;
     int *slot_scene;               // scene of each wave slot
+    // path-replay adjoint (dls == nullptr: plain rendering)
+    const float4 *Lt;              // per slot: the path's radiance from the first pass
+    float4 *dls;                   // per slot: dLoss / d(path radiance), RGB (0 for NaN paths)
+    const float *dfilm;            // dLoss / dfilm, H*W*3 in B,G,R order
+    float2 *sh_s;                  // per shadow ray: (d log / d sigma coefficient, d log / d g)
+    float *g_albedo;               // n_tris * 3 RGB, or nullptr
+    float *g_medium;               // 7: sigma_s rgb, sigma_a rgb, g
 };
+
+// Parameter order of the medium gradient.
+enum { GM_SIGMA_S = 0, GM_SIGMA_A = 3, GM_G = 6, GM_NUM = 7 };
+
+// d/dg log p_HG(cos; g): the score of a direction drawn from (or weighted by) the
+// Henyey-Greenstein phase function.
+RUMI_D float hg_dlog_dg(float c, float g) {
+    const float denom = 1.0f + g * g - 2.0f * g * c;
+    return -2.0f * g / (1.0f - g * g) - 3.0f * (g - c) / denom;
+}
+
+// Sums `v` over the lanes of the warp that share `key` (>= 0) and adds the sums to
+// base[3 * key + 0..2] with one atomic per group.  Called by all 32 lanes.
+RUMI_D void warp_add3_by_key(float *base, int key, float3 v) {
+    const unsigned act = __ballot_sync(0xffffffffu, key >= 0);
+    if (key < 0) return;
+    const unsigned grp = __match_any_sync(act, key);
+    float3 acc = mk3(0.0f, 0.0f, 0.0f);
+    unsigned m = grp;
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        acc.x += __shfl_sync(grp, v.x, src);
+        acc.y += __shfl_sync(grp, v.y, src);
+        acc.z += __shfl_sync(grp, v.z, src);
+    }
+    if ((int)(threadIdx.x & 31) == __ffs(grp) - 1) {
+        atomicAdd(base + 3 * key + 0, acc.x);
+        atomicAdd(base + 3 * key + 1, acc.y);
+        atomicAdd(base + 3 * key + 2, acc.z);
+    }
+}
+
+RUMI_D float warp_sum(float x) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
 
 // Largest k with prefix[k] <= g (prefix has n + 1 ascending entries).
 RUMI_D int find_scene(const long long *prefix, int n, long long g) {
@@ -84,33 +128,48 @@ __global__ void pt_generate(PtLaunch P) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j == 0) P.cnt[C_RAY0] = P.n_paths;
     if (j >= P.n_paths) return;
-    float3 o, d;
+    // one call site of the sampler and camera for both forms, so a batched scene's rays
+    // are bit-identical to the single-scene ones
+    const DevScene *S = &P.s;
+    long long pixel;
+    int s, spp = P.spp, gd = P.grid_d;
+    bool square = P.square != 0;
+    uint32_t k0 = P.k0, k1 = P.k1;
     if (P.scenes) {
         const long long g = P.path0 + j;
         const int k = find_scene(P.scene_path0, P.n_scenes, g);
-        const DevScene &S = P.scenes[k];
-        const int spp = P.scene_spp[k];
+        S = &P.scenes[k];
+        spp = P.scene_spp[k];
         const long long local = g - P.scene_path0[k];
-        const long long pixel = local / spp;
-        const int s = (int)(local % spp);
-        const int gd = isqrt_floor(spp);
-        const int w = (int)(pixel % S.width), h = (int)(pixel / S.width);
-        const float2 smp = pixel_sample(s, spp, gd, gd * gd == spp, pixel, P.scene_key[2 * k], P.scene_key[2 * k + 1]);
-        camera_ray(S.camera, S.width, S.height, w, h, smp.x, smp.y, o, d);
+        pixel = local / spp;
+        s = (int)(local % spp);
+        gd = isqrt_floor(spp);
+        square = gd * gd == spp;
+        k0 = P.scene_key[2 * k];
+        k1 = P.scene_key[2 * k + 1];
         P.slot_scene[j] = k;
     } else {
-        const long long pixel = (long long)P.pix0 + j / P.spp;
-        const int s = j % P.spp;
-        const int W = P.s.width;
-        const int w = (int)(pixel % W), h = (int)(pixel / W);
-        const float2 smp = pixel_sample(s, P.spp, P.grid_d, P.square != 0, pixel, P.k0, P.k1);
-        camera_ray(P.s.camera, W, P.s.height, w, h, smp.x, smp.y, o, d);
+        pixel = (long long)P.pix0 + j / P.spp;
+        s = j % P.spp;
     }
+    const int W = S->width;
+    const int w = (int)(pixel % W), h = (int)(pixel / W);
+    const float2 smp = pixel_sample(s, spp, gd, square, pixel, k0, k1);
+    float3 o, d;
+    camera_ray(S->camera, W, S->height, w, h, smp.x, smp.y, o, d);
     P.ray_o[0][j] = make_float4(o.x, o.y, o.z, __int_as_float(j));
     P.ray_d[0][j] = make_float4(d.x, d.y, d.z, FLT_MAX);
     P.beta[j] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     P.L[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     P.pflags[j] = PFL_LE;
+    if (P.dls) {
+        // the film drops NaN samples (pt_resolve), so they receive no gradient
+        const long long px = (long long)P.pix0 + j / P.spp;
+        const float4 lt = P.Lt[j];
+        const bool nan = lt.x != lt.x || lt.y != lt.y || lt.z != lt.z;
+        P.dls[j] = nan ? make_float4(0.0f, 0.0f, 0.0f, 0.0f)
+                       : make_float4(P.dfilm[3 * px + 2], P.dfilm[3 * px + 1], P.dfilm[3 * px + 0], 0.0f);
+    }
 }
 
 __global__ void pt_reset(PtLaunch P, int bounce) {
@@ -152,10 +211,11 @@ __global__ void __launch_bounds__(TRACE_THREADS) pt_extend(PtLaunch P, int bounc
     }
 }
 
-template <int MODE>
+template <int MODE, bool ADJ = false>
 __global__ void __launch_bounds__(TRACE_THREADS) pt_shadow(PtLaunch P) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
     TraceStats st{0, 0};
+    float acc_sigma = 0.0f, acc_g = 0.0f;  // adjoint: score-weighted contributions
     auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
         const float4 o4 = P.sh_o[i];
         const float4 d4 = P.sh_d[i];
@@ -171,10 +231,28 @@ __global__ void __launch_bounds__(TRACE_THREADS) pt_shadow(PtLaunch P) {
             float4 l = P.L[slot];
             l.x += c.x; l.y += c.y; l.z += c.z;
             P.L[slot] = l;
+            if (ADJ) {
+                // this NEE term alone carries the shadow ray's transmittance decision
+                // and (in a medium) the phase function's value at the light direction
+                const float4 dl = P.dls[slot];
+                const float dterm = dl.x * c.x + dl.y * c.y + dl.z * c.z;
+                const float2 sc = P.sh_s[i];
+                acc_sigma += sc.x * dterm;
+                acc_g += sc.y * dterm;
+            }
         }
     };
     traverse_queue<MODE, true, STACK_SMEM, false>(P.s, P.cnt[C_SHADOW], &P.cnt[C_FETCH_SH], P.refill_min,
                                                   stack + threadIdx.x, TRACE_THREADS, fetch, finish, st);
+    if (ADJ) {
+        __syncwarp();
+        acc_sigma = warp_sum(acc_sigma);
+        acc_g = warp_sum(acc_g);
+        if ((threadIdx.x & 31) == 0 && (acc_sigma != 0.0f || acc_g != 0.0f)) {
+            for (int k = 0; k < 6; ++k) atomicAdd(&P.g_medium[k], acc_sigma);
+            atomicAdd(&P.g_medium[GM_G], acc_g);
+        }
+    }
 }
 
 // Multi-scene batches: the warp-batch traversal with each ray's own scene.
@@ -232,6 +310,18 @@ RUMI_D bool nee_setup(const LightSample &ls, float3 p, float3 &wi, float &dist, 
     return true;
 }
 
+// ADJ: the replay pass of the path-replay adjoint (pt_backward).  Every path is traced a
+// second time on the same random numbers; at each of its events the part of the path's
+// radiance that the event influences -- Lt (the first pass's total) minus the terms
+// already accumulated -- is weighted with dLoss/dradiance and with the event's score:
+//   triangle albedo at a Lambertian vertex: d log / d rho = 1 / rho (per channel)
+//   medium segment passed through:         log P = -avg(sigma_t) * s_max
+//   medium scatter at distance s:          log p = log avg(sigma_t) - avg(sigma_t) s
+//                                                  + log(1 - avg(sigma_a / sigma_t)),
+//                                          weight sigma_s / sigma_t (per channel)
+//   phase direction (applied at the next vertex) and NEE phase value: d log HG / d g
+//   binary shadow transmittance (applied by the shadow kernel to that NEE term alone).
+template <bool ADJ>
 __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce) {
     const int cur = bounce & 1, nxt = cur ^ 1;
     const int n = P.cnt[cur];
@@ -245,6 +335,15 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
     float sh_tmax = 0.0f;
     int slot = 0;
     float3 beta = mk3(0, 0, 0);
+    float pend_g = 0.0f;                     // adjoint: score of the phase direction sampled here
+    float2 sh_score = make_float2(0.0f, 0.0f);
+    float gm[GM_NUM];
+    int alb_key = -1;
+    float3 alb_grad = mk3(0.0f, 0.0f, 0.0f);
+    if (ADJ) {
+#pragma unroll
+        for (int k = 0; k < GM_NUM; ++k) gm[k] = 0.0f;
+    }
 
     if (active) {
         const float4 o4 = P.ray_o[cur][i];
@@ -268,7 +367,18 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
         const int code = __float_as_int(hv.y);
         const unsigned fl = P.pflags[slot];
         const bool le = (fl & PFL_LE) != 0, inobj = (fl & PFL_IN) != 0;
-        beta = f4xyz(P.beta[slot]);
+        const float4 beta4 = P.beta[slot];
+        beta = f4xyz(beta4);
+        // adjoint: radiance of the terms from this vertex on, and its loss weights
+        float3 Lo = mk3(0.0f, 0.0f, 0.0f), dl = mk3(0.0f, 0.0f, 0.0f);
+        float D = 0.0f;
+        if (ADJ) {
+            const float4 lt = P.Lt[slot], la = P.L[slot], d4 = P.dls[slot];
+            Lo = mk3(lt.x - la.x, lt.y - la.y, lt.z - la.z);
+            dl = f4xyz(d4);
+            D = dot3(dl, Lo);
+            gm[GM_G] += beta4.w * D;  // the direction sampled at the previous (medium) vertex
+        }
         const Uniform4 U0 = path_uniforms(path, bounce, 0, k0, k1);
         const Uniform4 U1 = path_uniforms(path, bounce, 1, k0, k1);
         const bool last = bounce + 1 >= P.max_depth;
@@ -283,6 +393,28 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
             if (volume_intersect(V, o, d, thit, tn, tf)) {
                 const float smax = volume_max_distance(thit, tn, tf);
                 const DistSample ds = distance_sample(V.sigma_t, V.avg_sigma_t, V.absorb, smax, U1.u[2], U1.u[3]);
+                if (ADJ) {
+                    const float third = 0.33333333333f;
+                    if (ds.outcome == 0) {
+                        const float c = -smax * third * D;
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) gm[k] += c;
+                    } else if (ds.outcome == 1) {
+                        const float base = (third / V.avg_sigma_t - ds.s * third) * D;
+                        const float inv1a = 1.0f / (1.0f - V.absorb);
+                        const float ss[3] = {V.sigma_s.x, V.sigma_s.y, V.sigma_s.z};
+                        const float sa[3] = {V.sigma_a.x, V.sigma_a.y, V.sigma_a.z};
+                        const float st[3] = {V.sigma_t.x, V.sigma_t.y, V.sigma_t.z};
+                        const float q[3] = {dl.x * Lo.x, dl.y * Lo.y, dl.z * Lo.z};
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const float t2 = 3.0f * st[c] * st[c];
+                            const float ws = ss[c] > 0.0f ? 1.0f / ss[c] - 1.0f / st[c] : 0.0f;
+                            gm[GM_SIGMA_S + c] += base + sa[c] / t2 * inv1a * D + ws * q[c];
+                            gm[GM_SIGMA_A + c] += base - ss[c] / t2 * inv1a * D - q[c] / st[c];
+                        }
+                    }
+                }
                 if (ds.outcome == 2) {
                     done = true;  // absorbed (pathtracer.cpp:164-167)
                 } else if (ds.outcome == 1) {
@@ -295,8 +427,10 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                         float dist, G;
                         if (nee_setup(ls, p, wi, dist, G)) {
                             const Uniform4 U2 = path_uniforms(path, bounce, 2, k0, k1);
-                            const float tr = volume_shadow_tr(V, p, wi, dist, U2.u[2]);
+                            float smax_sh = 0.0f;
+                            const float tr = volume_shadow_tr(V, p, wi, dist, U2.u[2], &smax_sh);
                             if (tr > 0.0f) {
+                                if (ADJ) sh_score = make_float2(-smax_sh * 0.33333333333f, hg_dlog_dg(dot3(d, wi), V.g));
                                 const float fp = V.g == 0.0f ? 1.0f / (4.0f * RUMI_PI_F) : hg_eval(dot3(d, wi), V.g);
                                 const float3 direct = ls.Li * tr * V.sigma_s * fp * G * (1.0f / ls.pdf);
                                 want_sh = true;
@@ -321,6 +455,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                         fp_over_pdf = V.sigma_s;
                     }
                     beta = beta * vol * fp_over_pdf;
+                    if (ADJ) pend_g = hg_dlog_dg(dot3(d, w), V.g);
                     nx_o = p;
                     nx_d = w;
                     nx_flags = 0;  // le = false, in_object = false
@@ -346,6 +481,13 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                 nrm = f4xyz(n0) * (1.0f - u - v) + f4xyz(n1) * u + f4xyz(n2) * v;  // triangle.cpp:111 (Q3)
                 if (back && material_opaque(m)) nrm = -nrm;
                 if (S.tri_albedo) albedo = f4xyz(__ldg(&S.tri_albedo[id]));
+                if (ADJ && P.g_albedo && S.tri_albedo && m.type == MAT_MATTE) {
+                    // every term from this vertex on carries the factor albedo (per channel)
+                    alb_key = id;
+                    alb_grad = mk3(albedo.x > 0.0f ? dl.x * Lo.x / albedo.x : 0.0f,
+                                   albedo.y > 0.0f ? dl.y * Lo.y / albedo.y : 0.0f,
+                                   albedo.z > 0.0f ? dl.z * Lo.z / albedo.z : 0.0f);
+                }
             } else if (id < S.n_tris + S.n_rects) {
                 const int r = id - S.n_tris;
                 nrm = normalize_ref(cross3(f4xyz(S.rects[3 * r + 1]), f4xyz(S.rects[3 * r + 2])));
@@ -409,7 +551,9 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                             float tr = 1.0f;
                             if (V.present) {
                                 const Uniform4 U2 = path_uniforms(path, bounce, 2, k0, k1);
-                                tr = volume_shadow_tr(V, p, wi, dist, U2.u[2]);
+                                float smax_sh = 0.0f;
+                                tr = volume_shadow_tr(V, p, wi, dist, U2.u[2], &smax_sh);
+                                if (ADJ) sh_score = make_float2(-smax_sh * 0.33333333333f, 0.0f);
                             }
                             if (tr > 0.0f) {
                                 want_sh = true;
@@ -444,13 +588,31 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
         P.ray_o[nxt][kn] = make_float4(nx_o.x, nx_o.y, nx_o.z,
                                        __int_as_float(slot | ((nx_flags & PFL_IN) ? (int)0x80000000 : 0)));
         P.ray_d[nxt][kn] = make_float4(nx_d.x, nx_d.y, nx_d.z, FLT_MAX);
-        P.beta[slot] = make_float4(beta.x, beta.y, beta.z, 0.0f);
+        P.beta[slot] = make_float4(beta.x, beta.y, beta.z, pend_g);
         P.pflags[slot] = nx_flags;
     }
     if (want_sh) {
         P.sh_o[ks] = make_float4(sh_o.x, sh_o.y, sh_o.z, __int_as_float(slot));
         P.sh_d[ks] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
         P.sh_c[ks] = make_float4(sh_c.x, sh_c.y, sh_c.z, 0.0f);
+        if (ADJ) P.sh_s[ks] = sh_score;
+    }
+    if (ADJ) {
+        warp_add3_by_key(P.g_albedo, alb_key, alb_grad);
+        // medium: warp sums, then one atomic per parameter per block
+        __shared__ float red[SHADE_THREADS / 32][GM_NUM];
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+        for (int k = 0; k < GM_NUM; ++k) {
+            const float v = warp_sum(gm[k]);
+            if (lane == 0) red[warp][k] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < GM_NUM) {
+            float v = 0.0f;
+            for (int w = 0; w < SHADE_THREADS / 32; ++w) v += red[w][threadIdx.x];
+            if (v != 0.0f) atomicAdd(&P.g_medium[threadIdx.x], v);
+        }
     }
 }
 
@@ -496,6 +658,29 @@ __global__ void pt_resolve(PtLaunch P) {
 }
 
 static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+static inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Carves the wave state for Wp paths out of ws (pt_workspace_bytes(Wp) bytes) and clears
+// every optional field; returns the first byte after it.
+static char *carve_wave(PtLaunch &L, void *ws, size_t Wp) {
+    memset(&L, 0, sizeof(L));
+    const size_t f4 = align256(Wp * sizeof(float4));
+    char *w = (char *)ws;
+    L.ray_o[0] = (float4 *)w; w += f4;
+    L.ray_o[1] = (float4 *)w; w += f4;
+    L.ray_d[0] = (float4 *)w; w += f4;
+    L.ray_d[1] = (float4 *)w; w += f4;
+    L.hit = (float4 *)w; w += f4;
+    L.sh_o = (float4 *)w; w += f4;
+    L.sh_d = (float4 *)w; w += f4;
+    L.sh_c = (float4 *)w; w += f4;
+    L.beta = (float4 *)w; w += f4;
+    L.L = (float4 *)w; w += f4;
+    L.pflags = (unsigned *)w; w += align256(Wp * sizeof(unsigned));
+    L.cnt = (int *)w; w += align256(C_NUM * sizeof(int));
+    L.stats = (unsigned long long *)w; w += align256(S_NUM * sizeof(unsigned long long));
+    return w;
+}
 
 // Device bytes of the wave state for `paths` paths in flight (queues, path state,
 // counters): 164 bytes per path plus alignment and counters.
@@ -531,10 +716,8 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     const int spp = p->spp;
     const long long total_pix = (long long)W * H;
     const size_t Wp = (size_t)(pix_per_wave * spp);
-    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t f4 = al(Wp * sizeof(float4));
-    char *w = (char *)ws;
     PtLaunch L;
+    carve_wave(L, ws, Wp);
     L.s = sc->dev;
     L.spp = spp;
     L.max_depth = p->max_depth;
@@ -544,26 +727,7 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     while ((d + 1) * (d + 1) <= spp) ++d;
     L.grid_d = d;
     L.square = d * d == spp;
-    L.ray_o[0] = (float4 *)w; w += f4;
-    L.ray_o[1] = (float4 *)w; w += f4;
-    L.ray_d[0] = (float4 *)w; w += f4;
-    L.ray_d[1] = (float4 *)w; w += f4;
-    L.hit = (float4 *)w; w += f4;
-    L.sh_o = (float4 *)w; w += f4;
-    L.sh_d = (float4 *)w; w += f4;
-    L.sh_c = (float4 *)w; w += f4;
-    L.beta = (float4 *)w; w += f4;
-    L.L = (float4 *)w; w += f4;
-    L.pflags = (unsigned *)w; w += al(Wp * sizeof(unsigned));
-    L.cnt = (int *)w; w += al(C_NUM * sizeof(int));
-    L.stats = (unsigned long long *)w; w += al(S_NUM * sizeof(unsigned long long));
     L.film = film_dev;
-    L.scenes = nullptr;
-    L.scene_path0 = L.scene_pix0 = nullptr;
-    L.scene_key = nullptr;
-    L.scene_spp = nullptr;
-    L.n_scenes = 0;
-    L.slot_scene = nullptr;
     cudaMemsetAsync(L.cnt, 0, C_NUM * sizeof(int), stream);
     cudaMemsetAsync(L.stats, 0, S_NUM * sizeof(unsigned long long), stream);
 
@@ -573,13 +737,13 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     int occ = 0, occ_sh = 0;
     if (mode == 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<0, false>, TRACE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<0>, TRACE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<0, false>, TRACE_THREADS, 0);
     } else if (mode == 1) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<1, false>, TRACE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<1>, TRACE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<1, false>, TRACE_THREADS, 0);
     } else {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<2, false>, TRACE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<2>, TRACE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<2, false>, TRACE_THREADS, 0);
     }
     if (occ < 1) occ = 1;
     if (occ_sh < 1) occ_sh = 1;
@@ -624,15 +788,15 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
                 pt_extend<2, false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
             if (timing) { mark(); ext_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
-            pt_shade<<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
+            pt_shade<false><<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
             if (timing) { mark(); shade_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
             if (mode == 0)
-                pt_shadow<0><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
+                pt_shadow<0, false><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
             else if (mode == 1)
-                pt_shadow<1><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
+                pt_shadow<1, false><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
             else
-                pt_shadow<2><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
+                pt_shadow<2, false><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
             if (timing) { mark(); sh_ev.push_back({e0, e0 + 1}); }
         }
         pt_finish<<<1, 1, 0, stream>>>(L);
@@ -673,6 +837,141 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     return RUMI_OK;
 }
 
+// ---------------------------------------------------------------- path-replay adjoint
+// Device bytes of the adjoint's wave state: the rendering wave state plus, per path, the
+// first pass's radiance, the loss weights and the shadow-ray scores.
+size_t pt_adjoint_workspace_bytes(long long paths) {
+    const size_t Wp = (size_t)paths;
+    return pt_workspace_bytes(paths) + 2 * align256(Wp * sizeof(float4)) + align256(Wp * sizeof(float2));
+}
+
+// Gradients of <dfilm, film> for the frame rumi_render produces with the same parameters:
+// g_albedo (n_tris * 3, RGB; may be null) and g_medium (GM_NUM; may be null) are
+// overwritten.  Each wave is traced twice: pass 1 records every path's radiance, pass 2
+// replays the same random numbers with the scores of pt_shade<true> / pt_shadow<0, true>.
+rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float *dfilm_dev, float *g_albedo,
+                        float *g_medium, rumi_render_stats *stats, cudaStream_t stream) {
+    const int W = sc->dev.width, H = sc->dev.height;
+    const int spp = p->spp;
+    const long long total_pix = (long long)W * H;
+    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 22);
+    long long pix_per_wave = wave / spp;
+    if (pix_per_wave < 1) pix_per_wave = 1;
+    if (pix_per_wave > total_pix) pix_per_wave = total_pix;
+    const size_t Wp = (size_t)(pix_per_wave * spp);
+    if (Wp > 0x7fffffffULL) {
+        set_error("wave_paths too large");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    rumi_status st = ensure_workspace(sc, pt_adjoint_workspace_bytes((long long)Wp));
+    if (st != RUMI_OK) return st;
+    float *gm_scratch = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (!g_medium) {
+        e = dalloc((void **)&gm_scratch, GM_NUM * sizeof(float), stream);
+        if (e != cudaSuccess) return cuda_status(e, "adjoint scratch");
+        g_medium = gm_scratch;
+    }
+    PtLaunch A;
+    char *w = carve_wave(A, sc->ws, Wp);
+    A.s = sc->dev;
+    A.spp = spp;
+    A.max_depth = p->max_depth;
+    A.k0 = (uint32_t)p->seed;
+    A.k1 = (uint32_t)(p->seed >> 32) ^ 0x5851F42Du;
+    int d = 0;
+    while ((d + 1) * (d + 1) <= spp) ++d;
+    A.grid_d = d;
+    A.square = d * d == spp;
+    A.refill_min = 8;
+    PtLaunch B = A;
+    float4 *Lt = (float4 *)w; w += align256(Wp * sizeof(float4));
+    B.Lt = Lt;
+    B.dls = (float4 *)w; w += align256(Wp * sizeof(float4));
+    B.sh_s = (float2 *)w;
+    B.dfilm = dfilm_dev;
+    B.g_albedo = g_albedo;
+    B.g_medium = g_medium;
+    cudaMemsetAsync(A.cnt, 0, C_NUM * sizeof(int), stream);
+    cudaMemsetAsync(A.stats, 0, S_NUM * sizeof(unsigned long long), stream);
+    cudaMemsetAsync(g_medium, 0, GM_NUM * sizeof(float), stream);
+    if (g_albedo) cudaMemsetAsync(g_albedo, 0, sizeof(float) * 3 * (size_t)sc->dev.n_tris, stream);
+
+    int occ = 0, occ_sh = 0, occ_sh_adj = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<0, false>, TRACE_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<0, false>, TRACE_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh_adj, pt_shadow<0, true>, TRACE_THREADS, 0);
+    const int grid = sc->num_sms * (occ > 0 ? occ : 1);
+    const int grid_sh = sc->num_sms * (occ_sh > 0 ? occ_sh : 1);
+    const int grid_sh_adj = sc->num_sms * (occ_sh_adj > 0 ? occ_sh_adj : 1);
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (p->flags & RUMI_FLAG_TIMING) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, stream);
+    }
+    long long waves = 0;
+    for (long long pix0 = 0; pix0 < total_pix; pix0 += pix_per_wave) {
+        const long long n_pix = pix0 + pix_per_wave <= total_pix ? pix_per_wave : total_pix - pix0;
+        for (PtLaunch *L : {&A, &B}) {
+            L->pix0 = (int)pix0;
+            L->n_pix = (int)n_pix;
+            L->n_paths = (int)(n_pix * spp);
+            L->path0 = pix0 * spp;
+        }
+        // pass 1: radiance of every path
+        pt_generate<<<cdiv(A.n_paths, 256), 256, 0, stream>>>(A);
+        for (int b = 0; b < p->max_depth; ++b) {
+            pt_reset<<<1, 1, 0, stream>>>(A, b);
+            pt_extend<0, false><<<grid, TRACE_THREADS, 0, stream>>>(A, b);
+            pt_shade<false><<<cdiv(A.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(A, b);
+            pt_shadow<0, false><<<grid_sh, TRACE_THREADS, 0, stream>>>(A);
+        }
+        pt_finish<<<1, 1, 0, stream>>>(A);
+        cudaMemcpyAsync(Lt, A.L, sizeof(float4) * (size_t)A.n_paths, cudaMemcpyDeviceToDevice, stream);
+        // pass 2: replay with the scores
+        pt_generate<<<cdiv(B.n_paths, 256), 256, 0, stream>>>(B);
+        for (int b = 0; b < p->max_depth; ++b) {
+            pt_reset<<<1, 1, 0, stream>>>(B, b);
+            pt_extend<0, false><<<grid, TRACE_THREADS, 0, stream>>>(B, b);
+            pt_shade<true><<<cdiv(B.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(B, b);
+            pt_shadow<0, true><<<grid_sh_adj, TRACE_THREADS, 0, stream>>>(B);
+        }
+        pt_finish<<<1, 1, 0, stream>>>(B);
+        ++waves;
+    }
+    if (e1) cudaEventRecord(e1, stream);
+    e = cudaGetLastError();
+    unsigned long long h_stats[S_NUM];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_stats, A.stats, sizeof(h_stats), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    dfree(gm_scratch, stream);
+    if (e != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        return cuda_status(e, "pt_backward");
+    }
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->paths = total_pix * spp;
+        stats->nan_samples = (int64_t)h_stats[S_NAN];
+        stats->rays_extend = (int64_t)h_stats[S_RAYS_EXT];
+        stats->rays_shadow = (int64_t)h_stats[S_RAYS_SH];
+        stats->extend_launches = 2 * waves * p->max_depth;
+        stats->shade_launches = stats->extend_launches;
+        stats->shadow_launches = stats->extend_launches;
+        if (e0) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            stats->total_ms = ms;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return RUMI_OK;
+}
+
 // ---------------------------------------------------------------- scene batches
 // Device bytes of a multi-scene wave: the single-scene wave state plus each slot's scene.
 size_t pt_batch_workspace_bytes(long long wave_paths) {
@@ -684,27 +983,9 @@ size_t pt_batch_workspace_bytes(long long wave_paths) {
 // be captured into a CUDA graph: waves over the batch's global pixel / path index space,
 // every stage serving all scenes from shared queues.
 rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaStream_t stream, int num_sms) {
-    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t Wp = (size_t)F.wave_paths;
-    const size_t f4 = al(Wp * sizeof(float4));
-    char *w = (char *)ws;
     PtLaunch L;
-    memset(&L, 0, sizeof(L));
+    L.slot_scene = (int *)carve_wave(L, ws, (size_t)F.wave_paths);
     L.max_depth = F.max_depth;
-    L.ray_o[0] = (float4 *)w; w += f4;
-    L.ray_o[1] = (float4 *)w; w += f4;
-    L.ray_d[0] = (float4 *)w; w += f4;
-    L.ray_d[1] = (float4 *)w; w += f4;
-    L.hit = (float4 *)w; w += f4;
-    L.sh_o = (float4 *)w; w += f4;
-    L.sh_d = (float4 *)w; w += f4;
-    L.sh_c = (float4 *)w; w += f4;
-    L.beta = (float4 *)w; w += f4;
-    L.L = (float4 *)w; w += f4;
-    L.pflags = (unsigned *)w; w += al(Wp * sizeof(unsigned));
-    L.cnt = (int *)w; w += al(C_NUM * sizeof(int));
-    L.stats = (unsigned long long *)w; w += al(S_NUM * sizeof(unsigned long long));
-    L.slot_scene = (int *)w;
     L.film = films;
     L.scenes = F.scenes;
     L.scene_path0 = F.scene_path0;
@@ -734,7 +1015,7 @@ rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaSt
         for (int b = 0; b < F.max_depth; ++b) {
             pt_reset<<<1, 1, 0, stream>>>(L, b);
             pt_trace_multi<false><<<num_sms * occ, TRACE_THREADS, 0, stream>>>(L, b);
-            pt_shade<<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
+            pt_shade<false><<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
             pt_trace_multi<true><<<num_sms * occ_sh, TRACE_THREADS, 0, stream>>>(L, b);
         }
         pt_finish<<<1, 1, 0, stream>>>(L);

@@ -49,11 +49,16 @@ struct BatchFrame {
     std::vector<BatchWave> waves;
 };
 
+size_t pt_adjoint_workspace_bytes(long long paths);
+rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float *dfilm_dev, float *g_albedo,
+                        float *g_medium, rumi_render_stats *stats, cudaStream_t stream);
 size_t pt_batch_workspace_bytes(long long wave_paths);
 rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaStream_t stream, int num_sms);
 unsigned long long *pt_batch_stats_ptr(void *ws, long long wave_paths);
 
 void set_error(const std::string &msg);
+void fill_dev_volume(DevVolume &dv, const rumi_volume &v);
+void pack_albedo(const float *a_dev, int n, float4 *out, cudaStream_t s);
 rumi_status cuda_status(cudaError_t e, const char *what);
 
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,

@@ -463,10 +463,13 @@ RUMI_D DistSample distance_sample(float3 sigma_t, float avg_sigma_t, float absor
 
 // HomogeneousVolume::ShadowRayTr: binary transmittance of an unblocked shadow ray of
 // length tmax.  Returns 0 (scattered away) or 1.
-RUMI_D float volume_shadow_tr(const DevVolume &v, float3 o, float3 d, float tmax, float xi) {
+// smax_out (optional): the length of the ray inside the medium (0 when it misses it).
+RUMI_D float volume_shadow_tr(const DevVolume &v, float3 o, float3 d, float tmax, float xi,
+                              float *smax_out = nullptr) {
     float tn, tf;
     if (!volume_intersect(v, o, d, 0.0f, tn, tf)) return 1.0f;
     const float smax = volume_max_distance(tmax, tn, tf);
+    if (smax_out) *smax_out = smax;
     if (xi < 1.0f - expf(v.avg_sigma_t * -smax)) return 0.0f;
     return 1.0f;
 }

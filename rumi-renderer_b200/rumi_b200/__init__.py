@@ -134,6 +134,79 @@ class GpuScene:
                     "rumi_render")
         return film, st.as_dict()
 
+    def _pt_params(self, spp, seed, max_depth=None, wave_paths=0, timing=False, stream=None):
+        p = _capi.rumi_render_params()
+        p.integrator = PATH_TRACER
+        p.max_depth = int(max_depth if max_depth is not None else self.flat.tracer.max_depth)
+        p.spp = int(spp if spp is not None else self.flat.image.n_samples)
+        p.seed = int(seed)
+        p.wave_paths = int(wave_paths)
+        p.flags = 1 if timing else 0
+        p.stream = stream
+        return p
+
+    def forward(self, spp: int = None, seed: int = 1, max_depth: int = None, wave_paths: int = 0,
+                film_device_ptr: int = None, stream: int = None, timing: bool = False):
+        """rumi_forward: the path-traced film that backward() differentiates."""
+        p = self._pt_params(spp, seed, max_depth, wave_paths, timing, stream)
+        st = _capi.rumi_render_stats()
+        if film_device_ptr is not None:
+            _capi.check(self.lib.rumi_forward(self.h, C.byref(p), C.c_void_p(film_device_ptr), 1, C.byref(st)),
+                        "rumi_forward")
+            return None, st.as_dict()
+        film = np.zeros((self.height, self.width, 3), np.float32)
+        _capi.check(self.lib.rumi_forward(self.h, C.byref(p), film.ctypes.data_as(C.c_void_p), 0, C.byref(st)),
+                    "rumi_forward")
+        return film, st.as_dict()
+
+    def backward(self, d_film, spp: int = None, seed: int = 1, max_depth: int = None, albedo: bool = True,
+                 volume: bool = True, wave_paths: int = 0, timing: bool = False):
+        """rumi_backward with host buffers: d_film (H, W, 3) in the film's B,G,R layout.
+        Returns (grad_albedo (n_tris, 3) r,g,b or None, grad_volume (7,) or None, stats)."""
+        p = self._pt_params(spp, seed, max_depth, wave_paths, timing)
+        df = np.ascontiguousarray(d_film, np.float32)
+        assert df.size == self.height * self.width * 3
+        ga = np.zeros((self.flat.tri_vertices.shape[0], 3), np.float32) if albedo else None
+        gv = np.zeros(7, np.float32) if volume else None
+        st = _capi.rumi_render_stats()
+        _capi.check(self.lib.rumi_backward(self.h, C.byref(p), df.ctypes.data_as(C.c_void_p),
+                                           None if ga is None else ga.ctypes.data_as(C.c_void_p),
+                                           None if gv is None else gv.ctypes.data_as(C.c_void_p), 0, C.byref(st)),
+                    "rumi_backward")
+        return ga, gv, st.as_dict()
+
+    def backward_device(self, d_film_ptr: int, grad_albedo_ptr, grad_volume_ptr, spp: int = None, seed: int = 1,
+                        max_depth: int = None, wave_paths: int = 0, stream: int = None, timing: bool = False):
+        """rumi_backward with device buffers (pointers as ints; gradient pointers may be None)."""
+        p = self._pt_params(spp, seed, max_depth, wave_paths, timing, stream)
+        st = _capi.rumi_render_stats()
+        _capi.check(self.lib.rumi_backward(self.h, C.byref(p), C.c_void_p(d_film_ptr),
+                                           None if grad_albedo_ptr is None else C.c_void_p(grad_albedo_ptr),
+                                           None if grad_volume_ptr is None else C.c_void_p(grad_volume_ptr), 1,
+                                           C.byref(st)), "rumi_backward")
+        return st.as_dict()
+
+    def set_albedo(self, albedo=None, device_ptr: int = None):
+        """Replaces the per-triangle albedo ((n_tris, 3) r,g,b host array, or a device pointer)."""
+        if device_ptr is not None:
+            _capi.check(self.lib.rumi_scene_set_albedo(self.h, C.c_void_p(device_ptr), 1), "rumi_scene_set_albedo")
+            return
+        a = np.ascontiguousarray(albedo, np.float32)
+        assert a.size == self.flat.tri_vertices.shape[0] * 3
+        _capi.check(self.lib.rumi_scene_set_albedo(self.h, a.ctypes.data_as(C.c_void_p), 0), "rumi_scene_set_albedo")
+
+    def set_volume(self, sigma_s, sigma_a, g: float, pmin=None, pmax=None):
+        """Replaces the medium's coefficients (and optionally its box)."""
+        v = _capi.rumi_volume()
+        cur = self.flat.volume
+        v.present = 1
+        v.pmin = _capi.f3(*(pmin if pmin is not None else cur.pmin))
+        v.pmax = _capi.f3(*(pmax if pmax is not None else cur.pmax))
+        v.sigma_s = _capi.f3(*[float(x) for x in sigma_s])
+        v.sigma_a = _capi.f3(*[float(x) for x in sigma_a])
+        v.g = float(g)
+        _capi.check(self.lib.rumi_scene_set_volume(self.h, C.byref(v)), "rumi_scene_set_volume")
+
     def trace(self, rays: np.ndarray, anyhit: bool = False, in_object=None):
         """rays (n, 7) o, d, tmax (or (n, 8) in the C-ABI layout).  Returns (t, prim,
         node_visits, prim_tests)."""

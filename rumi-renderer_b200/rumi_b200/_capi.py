@@ -83,7 +83,7 @@ class rumi_bvh_info(C.Structure):
 # every symbol include/rumi_b200.h and include/rumi_b200_test.h declare
 EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "rumi_render", "rumi_render_noalloc",
            "rumi_trace_rays", "rumi_batch_create", "rumi_batch_destroy", "rumi_batch_film_floats",
-           "rumi_render_batch",
+           "rumi_render_batch", "rumi_forward", "rumi_backward", "rumi_scene_set_albedo", "rumi_scene_set_volume",
            "rumi_last_error_string", "rumi_version",
            "rumi_test_philox", "rumi_test_material_sample", "rumi_test_material_fr", "rumi_test_distance_sample",
            "rumi_test_phase_sample", "rumi_test_camera_rays", "rumi_test_pixel_samples"]
@@ -123,6 +123,16 @@ def load(path: str = LIB_PATH):
     L.rumi_render_batch.restype = C.c_int
     L.rumi_render_batch.argtypes = [C.c_void_p, C.POINTER(rumi_batch_params), C.c_void_p, C.c_int32,
                                     C.POINTER(rumi_render_stats)]
+    L.rumi_forward.restype = C.c_int
+    L.rumi_forward.argtypes = [C.c_void_p, C.POINTER(rumi_render_params), C.c_void_p, C.c_int32,
+                               C.POINTER(rumi_render_stats)]
+    L.rumi_backward.restype = C.c_int
+    L.rumi_backward.argtypes = [C.c_void_p, C.POINTER(rumi_render_params), C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_int32, C.POINTER(rumi_render_stats)]
+    L.rumi_scene_set_albedo.restype = C.c_int
+    L.rumi_scene_set_albedo.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    L.rumi_scene_set_volume.restype = C.c_int
+    L.rumi_scene_set_volume.argtypes = [C.c_void_p, C.POINTER(rumi_volume)]
     vp = C.c_void_p
     L.rumi_test_philox.argtypes = [C.c_int64, vp, vp, vp]
     L.rumi_test_material_sample.argtypes = [C.POINTER(rumi_material), C.c_int64, vp, vp, vp, vp]

@@ -278,3 +278,30 @@ def batch_scene(i: int, max_depth: int = 8, res: int = None, spp: int = None, n_
     sc.image = Film(res, res, spp)
     sc.tracer = PathTracer(max_depth)
     return sc
+
+
+# Inverse-rendering workload: hidden parameters of the target image.
+INVERSE_TARGET_MEDIUM = dict(sigma_s=(0.45, 0.35, 0.25), sigma_a=(0.04, 0.06, 0.09), g=0.35)
+INVERSE_START_MEDIUM = dict(sigma_s=(0.3, 0.3, 0.3), sigma_a=(0.05, 0.05, 0.05), g=0.1)
+
+
+def inverse_rendering(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8, levels: int = 7,
+                      albedo=None, medium: dict = None, albedo_seed: int = 23) -> Scene:
+    """Differentiable inverse rendering: the Cornell box holding a seeded displaced sphere of
+    4 * 4**levels triangles (levels=7: 65,536) with per-triangle RGB albedo, the whole box
+    filled with a homogeneous medium (sigma_s, sigma_a RGB, Henyey-Greenstein g).
+    albedo: (n_mesh, 3) or None for the hidden target albedo (uniform in [0.2, 0.8]^3,
+    seeded by albedo_seed); medium: dict(sigma_s, sigma_a, g), default the hidden target."""
+    sc = Scene()
+    add_cornell_box(sc)
+    tris = displaced_sphere(levels, (0.5, 0.35, 0.5), 0.25, 0.05, 11)
+    if albedo is None:
+        albedo = random_albedo(tris.shape[0], albedo_seed)
+    sc.add(Model(tris, albedo=np.asarray(albedo, np.float32)), Matte(1.0, WHITE))
+    m = medium or INVERSE_TARGET_MEDIUM
+    sc.volume = HomogeneousVolume((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), tuple(m["sigma_s"]), tuple(m["sigma_a"]),
+                                  float(m["g"]))
+    sc.camera = cornell_camera()
+    sc.image = Film(width, height, spp)
+    sc.tracer = PathTracer(max_depth)
+    return sc

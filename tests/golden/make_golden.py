@@ -204,7 +204,59 @@ def image_fixture(path, size=32, spp=16, depth=8, seeds=64, scene=None):
     print(path, "mean", mean.reshape(-1, 3).mean(0))
 
 
+ADJOINT_MEDIUM = dict(sigma_s=(0.45, 0.35, 0.25), sigma_a=(0.04, 0.06, 0.09), g=0.0)
+
+
+def adjoint_delta():
+    """Positive loss weights (a weighted image sum), seeded."""
+    return (0.5 + np.random.default_rng(77).random((32, 32, 3))).astype(F32)
+
+
+def _adjoint_fd_seed(s, h):
+    alb0 = scenes.random_albedo(4 * 4 ** 3, 23)
+    d64 = adjoint_delta().astype(np.float64)
+    row = []
+    for c in range(3):
+        ap, am = alb0.copy(), alb0.copy()
+        ap[:, c] += F32(h)
+        am[:, c] -= F32(h)
+        sums = []
+        for a in (ap, am):
+            sc = scenes.inverse_rendering(32, 32, 16, 4, levels=3, albedo=a, medium=ADJOINT_MEDIUM)
+            rs = refimpl.RefScene(sc, seed=1000 + s)
+            film, _ = rs.render(7000 + s)
+            rs.close()
+            sums.append((d64 * film).sum())
+        row.append((sums[0] - sums[1]) / (2.0 * h))
+    return row
+
+
+def adjoint_fixture(path, seeds=960, h=1e-3):
+    """The reference renderer's own finite-difference gradient for the albedo adjoint: the
+    inverse-rendering scene at 32x32, 16 spp, depth 4, with a 256-triangle mesh and the
+    reference's isotropic medium.  For each colour channel c the whole mesh's albedo is
+    moved by +-h in c and the frame is re-rendered with the same srand seed (albedo drives
+    no sampling decision of the reference, so the two frames share every random number);
+    fd[seed, c] = (<delta, film+> - <delta, film->) / 2h with seeded positive weights
+    delta (adjoint_delta)."""
+    base = scenes.inverse_rendering(32, 32, 16, 4, levels=3, medium=ADJOINT_MEDIUM)
+    alb0 = scenes.random_albedo(4 * 4 ** 3, 23)
+    assert np.array_equal(base.flatten().tri_albedo[-alb0.shape[0]:], alb0)
+    delta = adjoint_delta()
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 32)) as pool:
+        rows = pool.starmap(_adjoint_fd_seed, [(s, h) for s in range(seeds)])
+    fd = np.array(rows)
+    np.savez_compressed(path, delta=delta, fd=fd, mean=fd.mean(0), stderr=fd.std(0, ddof=1) / np.sqrt(seeds),
+                        h=h, seeds=seeds, sigma_s=np.array(ADJOINT_MEDIUM["sigma_s"], F32),
+                        sigma_a=np.array(ADJOINT_MEDIUM["sigma_a"], F32))
+    print(path, "fd mean", fd.mean(0), "stderr", fd.std(0, ddof=1) / np.sqrt(seeds))
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "adjoint":
+        adjoint_fixture(os.path.join(HERE, "adjoint_fd_ref32.npz"))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "media":
         sc = scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)
         sc.tracer = scenes.PathTracer(8)
