@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--wave-paths", type=int, default=0)
     ap.add_argument("--small", action="store_true", help="256x256 at 16 spp (profiling runs)")
-    ap.add_argument("--workload", default="bvh_bound", choices=["bvh_bound", "batched", "adjoint"],
+    ap.add_argument("--workload", default="bvh_bound", choices=["bvh_bound", "batched", "adjoint", "bdpt_caustic"],
                     help="batched: 256 seeded scenes as one frame vs the per-scene loop; "
                          "adjoint: inverse rendering with the path-replay adjoint")
     ap.add_argument("--adam-steps", type=int, default=200, help="adjoint workload: optimisation steps")
@@ -598,6 +598,65 @@ def adjoint_arm(args):
     return 0
 
 
+def bdpt_arm(args):
+    """BDPT with MIS on the volumetric caustic: glass sphere (IOR 1.5, r 0.3) in a
+    homogeneous medium (sigma_a 0.05, sigma_s 0.4, HG g 0.7) lit by a 30-degree spot of
+    intensity 50; 512x512, 32 spp, max path length 12 (6 light + 7 eye vertices).
+    One step = one frame; value = camera samples (full bidirectional paths) per second.
+    cpu_baseline: the reference's BidirectionalPathTracer on the variant it can express
+    (isotropic medium, small area light in place of the spot), a bounded row sample."""
+    import torch
+    import rumi_b200
+    from rumi_b200 import scenes
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    W, H, spp, nL, nE = 512, 512, 32, 6, 7
+    gs = rumi_b200.GpuScene(scenes.volumetric_caustic(W, H, spp, nL, nE))
+    stream = torch.cuda.current_stream().cuda_stream
+    film = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    for s in range(args.warmup):
+        gs.render(seed=s, film_device_ptr=film.data_ptr(), stream=stream)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    launches = 0
+    for s in range(args.steps):
+        _, st = gs.render(seed=100 + s, film_device_ptr=film.data_ptr(), stream=stream)
+        launches += st["extend_launches"] + 1  # per wave: bdpt_kernel + bdpt_write_film; + add_light_film
+    ev1.record()
+    torch.cuda.synchronize()
+    clocks_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    paths = W * H * spp
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import refimpl
+        sc = scenes.volumetric_caustic(W, H, spp, nL, nE, parity=True)
+        rs = refimpl.RefScene(sc, seed=1)
+        t0 = time.perf_counter()
+        rows = 2
+        rs.render_rows(5, 0, rows)
+        sec = time.perf_counter() - t0
+        n = rows * W * rs.spp
+        cpu = dict(value=n / sec, unit="paths/s", cores=1, kind="reference",
+                   sample=f"{n} camera samples = {rows} rows x {W} px x {rs.spp} spp of the area-light, isotropic "
+                          "variant (the reference has no spot light or HG phase; it truncates spp to a square), "
+                          "BidirectionalPathTracer(6, 7), one thread", seconds=sec)
+        rs.close()
+    gs.close()
+    line = dict(metric="path samples/sec (BDPT camera samples)", value=args.steps * paths / (ms / 1000.0),
+                unit="paths/s", n_gpus=1, steps=args.steps, warmup=args.warmup, ms_per_step=ms / args.steps,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                data="synthetic (analytic scene)",
+                config=dict(workload="volumetric caustic BDPT: glass sphere in HG medium, 30-degree spot", width=W,
+                            height=H, spp=spp, n_light=nL, n_eye=nE, max_path_length=nL + nE - 1),
+                cpu_baseline=cpu, gpu_launches=launches, clocks=clocks_info)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -606,6 +665,8 @@ def main():
         return batched_arm(args)
     if args.workload == "adjoint":
         return adjoint_arm(args)
+    if args.workload == "bdpt_caustic":
+        return bdpt_arm(args)
     return our_arm(args)
 
 

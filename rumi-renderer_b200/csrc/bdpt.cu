@@ -71,6 +71,25 @@ struct BdLaunch {
 
 RUMI_D float3 c3(float v) { return mk3(v, v, v); }
 
+// Spot lights (not in the reference): a point at `position` emitting intensity I (per
+// steradian) uniformly inside the cone of half-angle acos(cos_cone) about `direction`.
+// As the light vertex of a subpath it is a delta position: no eye subpath can hit it,
+// its "emission" is I, it has no cosine of its own, and its emission directions are
+// drawn uniformly from the cone.
+RUMI_D float3 light_emission(const DevLight &l) { return l.type == LIGHT_SPOT ? l.intensity : l.le; }
+
+RUMI_D float spot_pdf_dir(const DevLight &l) { return 1.0f / (2.0f * RUMI_PI_F * (1.0f - l.cos_cone)); }
+
+RUMI_D float3 spot_sample_dir(const DevLight &l, float u1, float u2) {
+    float3 u, w;
+    onb_ref(l.direction, u, w);
+    const float ct = 1.0f - u2 * (1.0f - l.cos_cone);
+    const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+    float sphi, cphi;
+    sincosf(u1 * 2.0f * RUMI_PI_F, &sphi, &cphi);
+    return normalize_ref(frame_dir(u, l.direction, w, st * sphi, ct, st * cphi));
+}
+
 // HomogeneousVolume::Tr over [0, s] (homogeneousvolume.cpp:46-54)
 RUMI_D float3 vol_tr(const DevVolume &V, float s) {
     return mk3(expf(V.sigma_t.x * -s), expf(V.sigma_t.y * -s), expf(V.sigma_t.z * -s));
@@ -311,7 +330,7 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
                     const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
                     a = a * (We / avg3(start.pdf_fwd) * G);
                 } else {
-                    a = a * (light.le / start.pdf_fwd * G);  // Light::L / pick pdf
+                    a = a * (light_emission(light) / start.pdf_fwd * G);  // Light::L / pick pdf
                 }
             } else {
                 const float3 fr = EYE ? vert_fr(S, start, start.n, d, prev_w) : vert_fr(S, start, start.n, prev_w, d);
@@ -360,7 +379,7 @@ RUMI_D float camera_pdfw(const DevCamera &c, float3 w) {
 // ns / nt: vertices used on the light / eye side; VL / VE the subpaths, segL / segE
 // their segment directions.
 RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, const BVert *VE, const float3 *segE,
-                        int ns, int nt, float3 connect_wi, float3 connect_wo, float3 light_n) {
+                        int ns, int nt, float3 connect_wi, float3 connect_wo, float3 light_n, const DevLight &light) {
     if (ns + nt <= 2) return 1.0f;
     const DevScene &S = P.s;
     const DevVolume &vol = S.volume;
@@ -460,7 +479,7 @@ RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, 
             float pw;
             if (s_connect->onsurface)
                 pw = ns > 1 ? material_pdfw(S.materials[s_connect->mat], s_connect->xi, s_connect->n, s_wi, connect_wo)
-                            : light_pdfw(connect_wo, light_n);
+                            : (light.type == LIGHT_SPOT ? spot_pdf_dir(light) : light_pdfw(connect_wo, light_n));
             else
                 pw = phase_value(vol, s_wi, connect_wo);
             tb[nt - 1] = pdf_s * (pw * dwda);
@@ -620,15 +639,28 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
         VE[0].pdf_fwd = c3(1.0f);
     }
     const int nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
-    // light subpath start
-    const LobeSample emit = lambert_sample(light_n, UD.u[0], UD.u[1]);
+    // light subpath start: cosine-weighted emission from an area light
+    // (AreaLight::SolidAngleSampling), uniform in the cone from a spot
+    const bool spot = light.type == LIGHT_SPOT;
     bvert_clear(VL[0]);
     VL[0].p = ls.P;
     VL[0].n = light_n;
-    VL[0].pdf_dir = emit.pdf;
-    VL[0].cos_a = dot3(emit.wi, light_n);
     VL[0].pdf_fwd = c3(ls.pdf);
-    const int nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit.wi, VL, segL, aL, light, light_n, stk, st);
+    float3 emit_w;
+    if (spot) {
+        emit_w = spot_sample_dir(light, UD.u[0], UD.u[1]);
+        VL[0].pdf_dir = spot_pdf_dir(light);
+        VL[0].cos_a = 1.0f;
+    } else {
+        const LobeSample emit = lambert_sample(light_n, UD.u[0], UD.u[1]);
+        emit_w = emit.wi;
+        VL[0].pdf_dir = emit.pdf;
+        VL[0].cos_a = dot3(emit.wi, light_n);
+    }
+    const int nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit_w, VL, segL, aL, light, light_n, stk, st);
+    // a delta position: the strategies in which the eye subpath reaches the light carry
+    // no weight (the MIS sums skip a dirac first light vertex)
+    if (spot) VL[0].dirac = true;
 
     float3 L = mk3(0, 0, 0);
     const int max_len = nE + nLv - 1;
@@ -641,7 +673,7 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 t_wo = -segE[t - 1];
                 if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
                     if (len == nE - 1) {
-                        const float w = mis_weight(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n);
+                        const float w = mis_weight(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
                         L = L + aE[t + 1] * w;
                     }
                     break;
@@ -664,7 +696,11 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
             const float3 cwo = normalize_ref(tc.p - sc.p);
             const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
             if (ci < 1e-4f) continue;
-            const float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
+            float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
+            if (s == 0 && spot) {
+                if (dot3(cwo, light.direction) < light.cos_cone) continue;  // outside the cone
+                co = 1.0f;                                                 // no cosine at a point
+            }
             if (co < 1e-4f) continue;
             const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
             if (dist <= 0.0f) continue;
@@ -682,7 +718,7 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
             }
             if (s == 0) {
-                cL = light.le / sc.pdf_fwd;
+                cL = light_emission(light) / sc.pdf_fwd;
             } else if (sc.onsurface) {
                 cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
             } else {
@@ -694,14 +730,14 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 if (wi == W || hi == H) continue;
                 if (wi < 0 || hi < 0 || wi > W || hi > H) continue;
                 float3 lo = aE[t] * cE * G * cL * aL[s];
-                lo = lo * mis_weight(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n);
+                lo = lo * mis_weight(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n, light);
                 float *dst = P.light_film + ((size_t)hi * W + wi) * 3;
                 atomicAdd(dst + 0, lo.z);
                 atomicAdd(dst + 1, lo.y);
                 atomicAdd(dst + 2, lo.x);
             } else {
                 float3 lo = aE[t] * cE * G * cL * aL[s];
-                lo = lo * mis_weight(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n);
+                lo = lo * mis_weight(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
                 L = L + lo;
             }
         }
