@@ -93,6 +93,7 @@ void free_scene(rumi_scene *sc) {
     if (!sc) return;
     cudaStream_t s = sc->stream;
     dfree(sc->nodes, s);
+    dfree(sc->nodes4, s);
     dfree(sc->leaf_prims, s);
     dfree(sc->tri_shade, s);
     dfree(sc->tri_albedo, s);
@@ -378,6 +379,40 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     cudaEventRecord(e0, s);
     int rc = bvh_build(d_tri_v, nT, sc->rects, d_rect_em, nR, sc->spheres, nS, sc->nodes, sc->leaf_prims, scratch, s,
                        &sc->info);
+    if (rc != 0) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc > 0) return fail(cuda_status((cudaError_t)rc, "bvh_build"));
+        set_error("bvh_build: internal limit reached");
+        return fail(RUMI_ERR_INTERNAL);
+    }
+    if (RUMI_BVH_WIDE) {
+        // four-wide tree: collapse into a worst-case array, then keep an exact copy
+        const int cap4 = bvh4_node_capacity(N);
+        Bvh4Node *tmp4 = nullptr;
+        void *scratch4 = nullptr;
+        e = dalloc((void **)&tmp4, sizeof(Bvh4Node) * (size_t)cap4, s);
+        if (e == cudaSuccess) e = dalloc(&scratch4, bvh4_scratch_bytes(N), s);
+        int n4 = -1;
+        if (e == cudaSuccess) n4 = bvh4_collapse(sc->nodes, sc->n_nodes, tmp4, cap4, scratch4, s);
+        if (e == cudaSuccess && n4 > 0) e = dalloc((void **)&sc->nodes4, sizeof(Bvh4Node) * (size_t)n4, s);
+        if (e == cudaSuccess && n4 > 0)
+            e = cudaMemcpyAsync(sc->nodes4, tmp4, sizeof(Bvh4Node) * (size_t)n4, cudaMemcpyDeviceToDevice, s);
+        dfree(tmp4, s);
+        dfree(scratch4, s);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return fail(cuda_status(e, "four-wide BVH"));
+        }
+        if (n4 <= 0) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            set_error("four-wide BVH collapse failed");
+            return fail(RUMI_ERR_INTERNAL);
+        }
+        sc->n_nodes4 = n4;
+    }
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0.0f;
@@ -385,11 +420,6 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     sc->build_ms = ms;
-    if (rc != 0) {
-        if (rc > 0) return fail(cuda_status((cudaError_t)rc, "bvh_build"));
-        set_error("bvh_build: internal limit reached");
-        return fail(RUMI_ERR_INTERNAL);
-    }
     dfree(d_tri_v, s);
     dfree(d_tri_n, s);
     dfree(d_tri_m, s);
@@ -400,6 +430,8 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     d_rect_em = d_tri_m = nullptr;
     scratch = nullptr;
     ds.nodes = sc->nodes;
+    ds.nodes4 = sc->nodes4;
+    ds.n_nodes4 = sc->n_nodes4;
     ds.leaf_prims = sc->leaf_prims;
     ds.tri_shade = sc->tri_shade;
     ds.tri_albedo = sc->tri_albedo;

@@ -19,4 +19,10 @@ int bvh_build(const float *d_tri_v, int n_tris, const float4 *d_rects, const int
               const float4 *d_spheres, int n_spheres, BvhNode *nodes, float4 *leaf_prims, void *scratch,
               cudaStream_t stream, BvhBuildInfo *info);
 
+// Four-wide tree collapsed from the binary one (bvh4.cu).
+int bvh4_node_capacity(int n_prims);
+size_t bvh4_scratch_bytes(int n_prims);
+int bvh4_collapse(const BvhNode *nodes2, int n_nodes2, Bvh4Node *nodes4, int cap4, void *scratch,
+                  cudaStream_t stream);
+
 }  // namespace rumi

@@ -11,6 +11,8 @@ struct rumi_scene {
     DevScene dev;
     // owned device allocations
     BvhNode *nodes = nullptr;
+    Bvh4Node *nodes4 = nullptr;
+    int n_nodes4 = 0;
     float4 *leaf_prims = nullptr;
     float4 *tri_shade = nullptr;
     float4 *tri_albedo = nullptr;

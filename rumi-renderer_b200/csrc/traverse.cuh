@@ -14,6 +14,7 @@
 // near-first with the far one pushed.  The stack keeps its top STACK_SMEM entries in
 // shared memory (one column per thread) and spills deeper entries to a local array.
 #pragma once
+#include <cfloat>
 #include "scene.cuh"
 
 #define RUMI_MAX_BVH_DEPTH 64
@@ -115,6 +116,17 @@ RUMI_D bool isect_sphere(float3 o, float3 d, float tmax, float tbest, float4 A, 
 }
 
 // ---------------------------------------------------------------------- node test
+// Reciprocal direction for the node slabs.  A zero component would give an infinite
+// reciprocal, (lo - o) * inf = NaN slab ends and -- since fminf/fmaxf drop NaNs -- no
+// culling on that axis: an axis-aligned ray would visit most of the tree.  Zero (and
+// tiny) components are replaced by 2^-80 with their sign, which keeps every slab finite
+// and the test conservative (the ray drifts by < 1e-23 per unit length on that axis).
+RUMI_D float safe_rcp(float x) {
+    const float eps = 8.2718061e-25f;  // 2^-80
+    return 1.0f / (fabsf(x) > eps ? x : copysignf(eps, x));
+}
+RUMI_D float3 safe_inv(float3 d) { return mk3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z)); }
+
 RUMI_D bool slab(float4 a, float4 b, float3 inv, float3 oinv, float tlimit, float &tnear) {
     // t = lo * inv - o * inv; conservative for zero direction components (NaN lanes are
     // dropped by fminf/fmaxf).
@@ -164,19 +176,19 @@ RUMI_D bool leaf_isect(const DevScene &s, int first, int count, float3 o, float3
     return ANYHIT && h.t > 0.0f;
 }
 
-// Closest-hit (ANYHIT=false) or occlusion (ANYHIT=true) query.
+// Closest-hit (ANYHIT=false) or occlusion (ANYHIT=true) query over the binary tree.
 // smem_stack: this thread's first shared-memory stack slot; consecutive slots are
 // `stride` ints apart.
 template <bool ANYHIT, int STACK_SMEM, bool STATS>
-RUMI_D HitRec trace_ray(const DevScene &s, float3 o, float3 d, float tmax, bool in_object, int *smem_stack,
-                        int stride, TraceStats &st) {
+RUMI_D HitRec trace_ray_bin(const DevScene &s, float3 o, float3 d, float tmax, bool in_object, int *smem_stack,
+                            int stride, TraceStats &st) {
     HitRec h;
     h.t = 0.0f;
     h.id = -1;
     h.u = h.v = 0.0f;
     h.back = 0;
     if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) return h;  // bvh.cpp:161-162
-    const float3 inv = mk3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const float3 inv = safe_inv(d);
     const float3 oinv = mk3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
     int spill[RUMI_MAX_BVH_DEPTH - STACK_SMEM > 0 ? RUMI_MAX_BVH_DEPTH - STACK_SMEM : 1];
     int sp = 0;
@@ -252,6 +264,144 @@ RUMI_D HitRec trace_ray(const DevScene &s, float3 o, float3 d, float tmax, bool 
     return h;
 }
 
+// ------------------------------------------------------------ four-wide traversal
+// Stack entries: at most three pushes per four-wide level.
+#define RUMI_STACK4 (3 * RUMI_MAX_BVH_DEPTH)
+
+RUMI_D bool slab_s(float lx, float ly, float lz, float hx, float hy, float hz, float3 inv, float3 oinv, float tlimit,
+                   float &tnear) {
+    const float tx0 = fmaf(lx, inv.x, -oinv.x), tx1 = fmaf(hx, inv.x, -oinv.x);
+    const float ty0 = fmaf(ly, inv.y, -oinv.y), ty1 = fmaf(hy, inv.y, -oinv.y);
+    const float tz0 = fmaf(lz, inv.z, -oinv.z), tz1 = fmaf(hz, inv.z, -oinv.z);
+    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
+    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+    tnear = tn;
+    return tn <= tf && tf >= 0.0f && tn <= tlimit;
+}
+
+RUMI_D int sel4(int4 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
+
+#define RUMI_CSWAP(ka, sa, kb, sb)                  \
+    if (kb < ka) {                                  \
+        const float tk_ = ka; ka = kb; kb = tk_;    \
+        const int ts_ = sa; sa = sb; sb = ts_;      \
+    }
+
+// The same query over the four-wide tree: a node's four child boxes are tested together
+// and visited nearest first (leaves intersected at once, interior children: the nearest
+// next, the others pushed farthest first).
+template <bool ANYHIT, int STACK_SMEM, bool STATS>
+RUMI_D HitRec trace_ray_wide(const DevScene &s, float3 o, float3 d, float tmax, bool in_object, int *smem_stack,
+                             int stride, TraceStats &st) {
+    HitRec h;
+    h.t = 0.0f;
+    h.id = -1;
+    h.u = h.v = 0.0f;
+    h.back = 0;
+    if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) return h;  // bvh.cpp:161-162
+    if (s.n_nodes4 <= 0) return h;
+    const float3 inv = safe_inv(d);
+    const float3 oinv = mk3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+    int spill[RUMI_STACK4 - STACK_SMEM > 0 ? RUMI_STACK4 - STACK_SMEM : 1];
+    int sp = 0;
+    int cur = 0;
+    // every node is visited at most once per ray, so the bound is never reached by a
+    // well-formed tree; it keeps a malformed one from looping
+    for (int guard = 0; guard < s.n_nodes4; ++guard) {
+        const float4 *np = reinterpret_cast<const float4 *>(s.nodes4 + cur);
+        const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+        const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+        const int4 ch = __ldg(reinterpret_cast<const int4 *>(np + 6));
+        const int4 cn = __ldg(reinterpret_cast<const int4 *>(np + 7));
+        if (STATS) st.nodes += 4;  // counted in 32-byte units
+        const float lim = h.t > 0.0f ? fminf(h.t, tmax) : tmax;
+        float k0, k1, k2, k3;
+        if (!(cn.x >= 0 && slab_s(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, inv, oinv, lim, k0))) k0 = FLT_MAX;
+        if (!(cn.y >= 0 && slab_s(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, inv, oinv, lim, k1))) k1 = FLT_MAX;
+        if (!(cn.z >= 0 && slab_s(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, inv, oinv, lim, k2))) k2 = FLT_MAX;
+        if (!(cn.w >= 0 && slab_s(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, inv, oinv, lim, k3))) k3 = FLT_MAX;
+        int s0 = 0, s1 = 1, s2 = 2, s3 = 3;
+        if (!ANYHIT) {  // near-first order; occlusion queries take any order
+            RUMI_CSWAP(k0, s0, k1, s1);
+            RUMI_CSWAP(k2, s2, k3, s3);
+            RUMI_CSWAP(k0, s0, k2, s2);
+            RUMI_CSWAP(k1, s1, k3, s3);
+            RUMI_CSWAP(k1, s1, k2, s2);
+        }
+        // split the hit children (in that order) into leaves and interior nodes
+        int lf0 = 0, lf1 = 0, lf2 = 0, lf3 = 0, lc0 = 0, lc1 = 0, lc2 = 0, lc3 = 0, nl = 0;
+        float lk0 = 0.0f, lk1 = 0.0f, lk2 = 0.0f, lk3 = 0.0f;
+        int c0 = -1, c1 = -1, c2 = -1, c3 = -1, ni = 0;
+        float ck0 = 0.0f, ck1 = 0.0f, ck2 = 0.0f, ck3 = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float kj = j == 0 ? k0 : (j == 1 ? k1 : (j == 2 ? k2 : k3));
+            const int sj = j == 0 ? s0 : (j == 1 ? s1 : (j == 2 ? s2 : s3));
+            if (kj == FLT_MAX) continue;
+            const int child = sel4(ch, sj), count = sel4(cn, sj);
+            if (count > 0) {
+                if (nl == 0) { lf0 = child; lc0 = count; lk0 = kj; }
+                else if (nl == 1) { lf1 = child; lc1 = count; lk1 = kj; }
+                else if (nl == 2) { lf2 = child; lc2 = count; lk2 = kj; }
+                else { lf3 = child; lc3 = count; lk3 = kj; }
+                ++nl;
+            } else {
+                if (ni == 0) { c0 = child; ck0 = kj; }
+                else if (ni == 1) { c1 = child; ck1 = kj; }
+                else if (ni == 2) { c2 = child; ck2 = kj; }
+                else { c3 = child; ck3 = kj; }
+                ++ni;
+            }
+        }
+        // leaves now, nearest first (one copy of the primitive loop)
+#pragma unroll 1
+        for (int q = 0; q < nl; ++q) {
+            const float lk = q == 0 ? lk0 : (q == 1 ? lk1 : (q == 2 ? lk2 : lk3));
+            if (!ANYHIT && h.t > 0.0f && lk > h.t) break;
+            const int lf = q == 0 ? lf0 : (q == 1 ? lf1 : (q == 2 ? lf2 : lf3));
+            const int lc = q == 0 ? lc0 : (q == 1 ? lc1 : (q == 2 ? lc2 : lc3));
+            if (leaf_isect<ANYHIT, STATS>(s, lf, lc, o, d, tmax, in_object, h, st)) return h;
+        }
+        // interior children beyond the closest hit so far are culled
+        if (!ANYHIT && h.t > 0.0f) {
+            if (ni > 3 && ck3 > h.t) ni = 3;
+            if (ni > 2 && ck2 > h.t) ni = 2;
+            if (ni > 1 && ck1 > h.t) ni = 1;
+            if (ni > 0 && ck0 > h.t) ni = 0;
+        }
+        int next;
+        if (ni == 0) {
+            if (sp == 0) break;
+            --sp;
+            next = sp < STACK_SMEM ? smem_stack[sp * stride] : spill[sp - STACK_SMEM];
+        } else {
+            next = c0;
+            // push the others farthest first, so the nearest of them is popped first
+            for (int k = ni - 1; k >= 1; --k) {
+                const int c = k == 3 ? c3 : (k == 2 ? c2 : c1);
+                if (sp < STACK_SMEM)
+                    smem_stack[sp * stride] = c;
+                else if (sp < RUMI_STACK4)
+                    spill[sp - STACK_SMEM] = c;
+                if (sp < RUMI_STACK4) ++sp;  // three per level of a depth-limited tree: always holds
+            }
+        }
+        if ((unsigned)next >= (unsigned)s.n_nodes4) break;  // malformed tree guard
+        cur = next;
+    }
+    return h;
+}
+
+template <bool ANYHIT, int STACK_SMEM, bool STATS>
+RUMI_D HitRec trace_ray(const DevScene &s, float3 o, float3 d, float tmax, bool in_object, int *smem_stack,
+                        int stride, TraceStats &st) {
+#if RUMI_BVH_WIDE
+    return trace_ray_wide<ANYHIT, STACK_SMEM, STATS>(s, o, d, tmax, in_object, smem_stack, stride, st);
+#else
+    return trace_ray_bin<ANYHIT, STACK_SMEM, STATS>(s, o, d, tmax, in_object, smem_stack, stride, st);
+#endif
+}
+
 // ------------------------------------------------------------ resumable form
 // The same traversal split into single node-pair steps, so a warp can refill a lane with
 // a new ray as soon as that lane's ray finishes (dynamic fetch) instead of waiting for
@@ -279,7 +429,7 @@ RUMI_D void trav_begin(const DevScene &s, TravState &T, float3 o, float3 d, floa
     T.h.back = 0;
     T.cur = -2;
     if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) return;  // bvh.cpp:161-162
-    T.inv = mk3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    T.inv = safe_inv(d);
     T.oinv = mk3(o.x * T.inv.x, o.y * T.inv.y, o.z * T.inv.z);
     const float4 *rp = reinterpret_cast<const float4 *>(s.nodes);
     const float4 a = __ldg(rp), b = __ldg(rp + 1);

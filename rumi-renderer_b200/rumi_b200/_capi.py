@@ -8,7 +8,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "librumi_b200.so")
+LIB_PATH = os.environ.get("RUMI_B200_LIB") or os.path.join(os.path.dirname(HERE), "lib", "librumi_b200.so")
 
 f3 = C.c_float * 3
 f16 = C.c_float * 16
