@@ -287,7 +287,8 @@ def our_arm(args):
     paths_per_frame = w["width"] * w["height"] * w["spp"]
     film = torch.empty((w["height"], w["width"], 3), dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    seed0 = 1000 * rank
+    from rumi_b200 import shard
+    seed0 = shard.replica_seed(0, rank)  # each rank renders an independent spp shard
 
     # algorithmic bytes per closest-hit ray, from an instrumented (untimed) frame
     _, st0 = gs.render(seed=seed0 + 999, film_device_ptr=film.data_ptr(), stream=stream, count_stats=True,
@@ -434,7 +435,8 @@ def batched_arm(args):
 
     depth = 8
     # scenes are sharded across ranks (scene i on rank i % world); no exchange
-    ids = [i for i in range(args.scenes) if i % world == rank]
+    from rumi_b200 import shard
+    ids = shard.scene_shard(args.scenes, rank, world)
     t0 = time.perf_counter()
     gss = [rumi_b200.GpuScene(scenes.batch_scene(i, depth)) for i in ids]
     setup_s = time.perf_counter() - t0

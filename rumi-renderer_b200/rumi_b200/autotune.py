@@ -43,12 +43,14 @@ def tune(gs, spp: int, key: str, space: dict = None, repeats: int = 2, film_ptr=
     cur = dict(DEFAULTS)
     cur_ms = measure(gs, cur, spp, repeats=repeats, film_ptr=film_ptr)
     history = [(dict(cur), cur_ms)]
+    seen = {tuple(sorted(cur.items()))}
     for knob in ("trace_mode", "blocks_per_sm", "refill_min", "wave_paths"):
         for v in space[knob]:
-            if v == cur[knob]:
-                continue
             cand = dict(cur)
             cand[knob] = v
+            if tuple(sorted(cand.items())) in seen:
+                continue
+            seen.add(tuple(sorted(cand.items())))
             ms = measure(gs, cand, spp, repeats=repeats, film_ptr=film_ptr)
             history.append((dict(cand), ms))
             if log:
@@ -57,6 +59,31 @@ def tune(gs, spp: int, key: str, space: dict = None, repeats: int = 2, film_ptr=
                 cur, cur_ms = cand, ms
     result = dict(params=cur, ms=cur_ms, gpu=gpu_name(), key=key, when=time.strftime("%Y-%m-%dT%H:%M:%S"),
                   history=[dict(params=p, ms=m) for p, m in history])
+    save(key, result, cache_path)
+    return result
+
+
+BATCH_WAVES = [1 << 21, 1 << 22, 1 << 23]
+
+
+def tune_batch(batch, spp, seeds, max_depth: int, key: str, waves=None, repeats: int = 2, log=None,
+               cache_path: str = CACHE) -> dict:
+    """Queue capacity (paths in flight per wave) of a multi-scene batch: each candidate
+    renders the batch eagerly (no graph) and is timed on the device; the best is cached
+    and is the capacity to capture the frame's CUDA graph with."""
+    best, best_ms, history = None, float("inf"), []
+    for w in waves or BATCH_WAVES:
+        ms = float("inf")
+        for r in range(repeats):
+            _, st = batch.render(spp, seeds, max_depth, graph=False, timing=True, wave_paths=w)
+            ms = min(ms, st["total_ms"])
+        history.append(dict(params=dict(wave_paths=w), ms=ms))
+        if log:
+            log(f"batch wave_paths={w}: {ms:.2f} ms")
+        if ms < best_ms:
+            best, best_ms = w, ms
+    result = dict(params=dict(wave_paths=best), ms=best_ms, gpu=gpu_name(), key=key,
+                  when=time.strftime("%Y-%m-%dT%H:%M:%S"), history=history)
     save(key, result, cache_path)
     return result
 
