@@ -145,9 +145,10 @@ typedef struct {
     void *stream;          /* cudaStream_t, NULL = the library's own stream */
     /* launch tuning (0 = library default; chosen by rumi_b200.autotune) */
     int32_t trace_mode;    /* 1: a warp traces 32 rays to completion; 2: per-lane ray refill;
-                              3: per-lane refill with leaves intersected warp-wide */
+                              3: per-lane refill with leaves intersected warp-wide;
+                              4: speculative while-while walk with per-lane refill */
     int32_t blocks_per_sm; /* persistent traversal blocks (128 threads) per SM, capped by occupancy */
-    int32_t refill_min;    /* idle lanes that trigger a refill (modes 2, 3) */
+    int32_t refill_min;    /* idle lanes that trigger a refill (modes 2, 3, 4) */
 } rumi_render_params;
 
 typedef struct {

@@ -261,42 +261,45 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) pt_shado
     }
 }
 
-// Multi-scene batches: the warp-batch traversal with each ray's own scene.
+// Multi-scene batches: the default traversal scheme (speculative while-while, the walk
+// rumi_render uses) with each ray's own scene, so a batched scene resolves exact-distance
+// ties exactly as its single-scene render does.
 template <bool ANYHIT>
-__global__ void __launch_bounds__(TRACE_THREADS) pt_trace_multi(PtLaunch P, int bounce) {
+__global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) pt_trace_multi(PtLaunch P, int bounce) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
     const int cur = bounce & 1;
     const int n = ANYHIT ? P.cnt[C_SHADOW] : P.cnt[cur];
     int *counter = ANYHIT ? &P.cnt[C_FETCH_SH] : &P.cnt[C_FETCH_EXT];
-    const int lane = threadIdx.x & 31;
     TraceStats st{0, 0};
-    for (;;) {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(counter, 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const int i = base + lane;
-        if (i < n) {
-            const float4 o4 = ANYHIT ? P.sh_o[i] : P.ray_o[cur][i];
-            const float4 d4 = ANYHIT ? P.sh_d[i] : P.ray_d[cur][i];
-            const int slot = __float_as_int(o4.w) & 0x7fffffff;
-            const DevScene &S = P.scenes[P.slot_scene[slot]];
-            const bool in_obj = !ANYHIT && (__float_as_uint(o4.w) >> 31) != 0;
-            const HitRec h = trace_ray<ANYHIT, STACK_SMEM, false>(S, f4xyz(o4), f4xyz(d4), d4.w, in_obj,
-                                                                 stack + threadIdx.x, TRACE_THREADS, st);
-            if (ANYHIT) {
-                if (h.t == 0.0f) {
-                    const float4 c = P.sh_c[i];
-                    float4 l = P.L[slot];
-                    l.x += c.x; l.y += c.y; l.z += c.z;
-                    P.L[slot] = l;
-                }
-            } else {
-                const int code = h.t > 0.0f ? (h.id | (h.back ? (int)0x80000000 : 0)) : -1;
-                P.hit[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
+    auto scene_of = [&](int i) -> const DevScene * {
+        if (i < 0) return &P.scenes[0];
+        const float4 o4 = ANYHIT ? P.sh_o[i] : P.ray_o[cur][i];
+        return &P.scenes[P.slot_scene[__float_as_int(o4.w) & 0x7fffffff]];
+    };
+    auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
+        const float4 o4 = ANYHIT ? P.sh_o[i] : P.ray_o[cur][i];
+        const float4 d4 = ANYHIT ? P.sh_d[i] : P.ray_d[cur][i];
+        o = f4xyz(o4);
+        d = f4xyz(d4);
+        tmax = d4.w;
+        in_obj = !ANYHIT && (__float_as_uint(o4.w) >> 31) != 0;
+    };
+    auto finish = [&](int i, const HitRec &h) {
+        if (ANYHIT) {
+            if (h.t == 0.0f) {
+                const int slot = __float_as_int(P.sh_o[i].w);
+                const float4 c = P.sh_c[i];
+                float4 l = P.L[slot];
+                l.x += c.x; l.y += c.y; l.z += c.z;
+                P.L[slot] = l;
             }
+        } else {
+            const int code = h.t > 0.0f ? (h.id | (h.back ? (int)0x80000000 : 0)) : -1;
+            P.hit[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
         }
-    }
+    };
+    traverse_queue_ww<ANYHIT, STACK_SMEM, false>(scene_of, n, counter, P.refill_min, stack + threadIdx.x,
+                                                 TRACE_THREADS, fetch, finish, st);
 }
 
 // Next-event estimation toward one light sample from p.  Returns false when the light
@@ -666,6 +669,67 @@ __global__ void pt_resolve(PtLaunch P) {
 static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 static inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// Traversal scheme index (traverse_queue MODE) from rumi_render_params.trace_mode:
+// 1..4 select modes 0..3, 0 selects the default, the speculative while-while walk (mode 3),
+// which measured fastest on the BVH-bound workload (238 vs 302 ms per 1024x1024x64 frame
+// for mode 0).
+static inline int trace_scheme(int trace_mode) { return trace_mode >= 1 && trace_mode <= 4 ? trace_mode - 1 : 3; }
+
+template <bool STATS>
+static void launch_extend(int mode, int grid, cudaStream_t st, const PtLaunch &L, int b) {
+    switch (mode) {
+        case 0: pt_extend<0, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
+        case 1: pt_extend<1, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
+        case 2: pt_extend<2, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
+        default: pt_extend<3, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
+    }
+}
+
+template <bool ADJ>
+static void launch_shadow(int mode, int grid, cudaStream_t st, const PtLaunch &L) {
+    switch (mode) {
+        case 0: pt_shadow<0, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
+        case 1: pt_shadow<1, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
+        case 2: pt_shadow<2, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
+        default: pt_shadow<3, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
+    }
+}
+
+// Persistent grids: blocks per SM at the kernels' occupancy (capped by blocks_per_sm > 0).
+static void trace_grids(int mode, int num_sms, int blocks_per_sm, bool adj, int &grid, int &grid_sh) {
+    int occ = 0, occ_sh = 0;
+    switch (mode) {
+        case 0:
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<0, false>, TRACE_THREADS, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<0, true> : pt_shadow<0, false>,
+                                                          TRACE_THREADS, 0);
+            break;
+        case 1:
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<1, false>, TRACE_THREADS, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<1, true> : pt_shadow<1, false>,
+                                                          TRACE_THREADS, 0);
+            break;
+        case 2:
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<2, false>, TRACE_THREADS, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<2, true> : pt_shadow<2, false>,
+                                                          TRACE_THREADS, 0);
+            break;
+        default:
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<3, false>, TRACE_THREADS, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<3, true> : pt_shadow<3, false>,
+                                                          TRACE_THREADS, 0);
+            break;
+    }
+    if (occ < 1) occ = 1;
+    if (occ_sh < 1) occ_sh = 1;
+    if (blocks_per_sm > 0) {
+        occ = blocks_per_sm < occ ? blocks_per_sm : occ;
+        occ_sh = blocks_per_sm < occ_sh ? blocks_per_sm : occ_sh;
+    }
+    grid = num_sms * occ;
+    grid_sh = num_sms * occ_sh;
+}
+
 // Carves the wave state for Wp paths out of ws (pt_workspace_bytes(Wp) bytes) and clears
 // every optional field; returns the first byte after it.
 static char *carve_wave(PtLaunch &L, void *ws, size_t Wp) {
@@ -738,27 +802,10 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     cudaMemsetAsync(L.stats, 0, S_NUM * sizeof(unsigned long long), stream);
 
     // traversal scheme and persistent grid (autotuner knobs; 0 = defaults)
-    const int mode = p->trace_mode >= 1 && p->trace_mode <= 3 ? p->trace_mode - 1 : 0;
+    const int mode = trace_scheme(p->trace_mode);
     L.refill_min = p->refill_min > 0 ? p->refill_min : 8;
-    int occ = 0, occ_sh = 0;
-    if (mode == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<0, false>, TRACE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<0, false>, TRACE_THREADS, 0);
-    } else if (mode == 1) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<1, false>, TRACE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<1, false>, TRACE_THREADS, 0);
-    } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<2, false>, TRACE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<2, false>, TRACE_THREADS, 0);
-    }
-    if (occ < 1) occ = 1;
-    if (occ_sh < 1) occ_sh = 1;
-    if (p->blocks_per_sm > 0) {
-        occ = p->blocks_per_sm < occ ? p->blocks_per_sm : occ;
-        occ_sh = p->blocks_per_sm < occ_sh ? p->blocks_per_sm : occ_sh;
-    }
-    const int trace_grid = sc->num_sms * occ;
-    const int shadow_grid = sc->num_sms * occ_sh;
+    int trace_grid = 0, shadow_grid = 0;
+    trace_grids(mode, sc->num_sms, p->blocks_per_sm, false, trace_grid, shadow_grid);
 
     const bool timing = (p->flags & RUMI_FLAG_TIMING) != 0;
     const bool count_stats = (p->flags & RUMI_FLAG_STATS) != 0;
@@ -785,24 +832,15 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
             int e0 = 0;
             if (timing) { e0 = (int)evs.size(); mark(); }
             if (count_stats)
-                pt_extend<0, true><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
-            else if (mode == 0)
-                pt_extend<0, false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
-            else if (mode == 1)
-                pt_extend<1, false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
+                launch_extend<true>(mode, trace_grid, stream, L, b);
             else
-                pt_extend<2, false><<<trace_grid, TRACE_THREADS, 0, stream>>>(L, b);
+                launch_extend<false>(mode, trace_grid, stream, L, b);
             if (timing) { mark(); ext_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
             pt_shade<false><<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
             if (timing) { mark(); shade_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
-            if (mode == 0)
-                pt_shadow<0, false><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
-            else if (mode == 1)
-                pt_shadow<1, false><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
-            else
-                pt_shadow<2, false><<<shadow_grid, TRACE_THREADS, 0, stream>>>(L);
+            launch_shadow<false>(mode, shadow_grid, stream, L);
             if (timing) { mark(); sh_ev.push_back({e0, e0 + 1}); }
         }
         pt_finish<<<1, 1, 0, stream>>>(L);
@@ -903,13 +941,13 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
     cudaMemsetAsync(g_medium, 0, GM_NUM * sizeof(float), stream);
     if (g_albedo) cudaMemsetAsync(g_albedo, 0, sizeof(float) * 3 * (size_t)sc->dev.n_tris, stream);
 
-    int occ = 0, occ_sh = 0, occ_sh_adj = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<0, false>, TRACE_THREADS, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, pt_shadow<0, false>, TRACE_THREADS, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh_adj, pt_shadow<0, true>, TRACE_THREADS, 0);
-    const int grid = sc->num_sms * (occ > 0 ? occ : 1);
-    const int grid_sh = sc->num_sms * (occ_sh > 0 ? occ_sh : 1);
-    const int grid_sh_adj = sc->num_sms * (occ_sh_adj > 0 ? occ_sh_adj : 1);
+    // the same traversal scheme as rumi_render, so both passes and the forward frame
+    // resolve exact-distance ties alike
+    const int mode = trace_scheme(p->trace_mode);
+    A.refill_min = B.refill_min = p->refill_min > 0 ? p->refill_min : 8;
+    int grid = 0, grid_sh = 0, grid_dummy = 0, grid_sh_adj = 0;
+    trace_grids(mode, sc->num_sms, p->blocks_per_sm, false, grid, grid_sh);
+    trace_grids(mode, sc->num_sms, p->blocks_per_sm, true, grid_dummy, grid_sh_adj);
 
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (p->flags & RUMI_FLAG_TIMING) {
@@ -930,9 +968,9 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
         pt_generate<<<cdiv(A.n_paths, 256), 256, 0, stream>>>(A);
         for (int b = 0; b < p->max_depth; ++b) {
             pt_reset<<<1, 1, 0, stream>>>(A, b);
-            pt_extend<0, false><<<grid, TRACE_THREADS, 0, stream>>>(A, b);
+            launch_extend<false>(mode, grid, stream, A, b);
             pt_shade<false><<<cdiv(A.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(A, b);
-            pt_shadow<0, false><<<grid_sh, TRACE_THREADS, 0, stream>>>(A);
+            launch_shadow<false>(mode, grid_sh, stream, A);
         }
         pt_finish<<<1, 1, 0, stream>>>(A);
         cudaMemcpyAsync(Lt, A.L, sizeof(float4) * (size_t)A.n_paths, cudaMemcpyDeviceToDevice, stream);
@@ -940,9 +978,9 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
         pt_generate<<<cdiv(B.n_paths, 256), 256, 0, stream>>>(B);
         for (int b = 0; b < p->max_depth; ++b) {
             pt_reset<<<1, 1, 0, stream>>>(B, b);
-            pt_extend<0, false><<<grid, TRACE_THREADS, 0, stream>>>(B, b);
+            launch_extend<false>(mode, grid, stream, B, b);
             pt_shade<true><<<cdiv(B.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(B, b);
-            pt_shadow<0, true><<<grid_sh_adj, TRACE_THREADS, 0, stream>>>(B);
+            launch_shadow<true>(mode, grid_sh_adj, stream, B);
         }
         pt_finish<<<1, 1, 0, stream>>>(B);
         ++waves;

@@ -586,17 +586,173 @@ RUMI_D bool run_pending(const DevScene &s, TravState &T, PendingLeaves &pl, Trac
     return found;
 }
 
+// Speculative while-while traversal with per-lane refill (Aila & Laine, "Understanding
+// the efficiency of ray traversal on GPUs", HPG 2009; Aila, Laine & Karras 2012): each
+// lane walks interior node pairs until it holds a postponed leaf, and keeps walking
+// (speculatively) until every lane of the warp holds one; then the warp intersects the
+// postponed leaves together.  Rounds repeat until a lane's ray is finished, and finished
+// lanes are refilled from the queue in warp-aggregated batches.
+//   cur >= 0: a node pair to test; cur < 0, != WW_DONE: the leaf node -(cur + 1);
+//   WW_DONE: the stack is empty.
+#define WW_DONE (-0x7fffffff - 1)
+
+// scene_of(i): the scene ray i is traced in (one scene, or per ray in a multi-scene batch).
+template <bool ANYHIT, int STACK_SMEM, bool STATS, typename SceneOf, typename Fetch, typename Finish>
+RUMI_D void traverse_queue_ww(SceneOf scene_of, int n, int *counter, int refill_min, int *smem_stack, int stride,
+                              Fetch fetch, Finish finish, TraceStats &st) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int spill[RUMI_MAX_BVH_DEPTH - STACK_SMEM > 0 ? RUMI_MAX_BVH_DEPTH - STACK_SMEM : 1];
+    const DevScene *sp_scene = scene_of(-1);
+    const float4 *nodes = reinterpret_cast<const float4 *>(sp_scene->nodes);
+    float3 o = mk3(0, 0, 0), d = mk3(0, 0, 0), inv = mk3(0, 0, 0), oinv = mk3(0, 0, 0);
+    float tmax = 0.0f;
+    bool in_obj = false;
+    HitRec h;
+    h.t = 0.0f;
+    h.id = -1;
+    h.u = h.v = 0.0f;
+    h.back = 0;
+    int ray = -1, cur = WW_DONE, sp = 0, lf_first = 0, lf_count = 0, steps = 0;
+    bool exhausted = false;
+    auto pop = [&]() -> int {
+        if (sp == 0) return WW_DONE;
+        --sp;
+        return sp < STACK_SMEM ? smem_stack[sp * stride] : spill[sp - STACK_SMEM];
+    };
+    auto push = [&](int v) {
+        if (sp < STACK_SMEM)
+            smem_stack[sp * stride] = v;
+        else if (sp < RUMI_MAX_BVH_DEPTH)
+            spill[sp - STACK_SMEM] = v;
+        if (sp < RUMI_MAX_BVH_DEPTH) ++sp;  // the build caps depth at 63: always holds
+    };
+    // leaf node -> pending leaf range (a range check keeps a malformed tree harmless)
+    auto take_leaf = [&](int node) {
+        if ((unsigned)node >= (unsigned)sp_scene->n_nodes) {
+            lf_count = 0;
+            return;
+        }
+        const float4 b = __ldg(nodes + 2 * node + 1);
+        lf_first = __float_as_int(b.z);
+        lf_count = __float_as_int(b.w);
+    };
+    for (;;) {
+        // finished rays -> results; idle lanes -> new rays
+        if (ray >= 0 && cur == WW_DONE && lf_count == 0) {
+            finish(ray, h);
+            ray = -1;
+        }
+        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
+        if (!exhausted && idle && (__popc(idle) >= refill_min || idle == 0xffffffffu)) {
+            int base = 0;
+            const int leader = __ffs(idle) - 1;
+            if (lane == leader) base = atomicAdd(counter, __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= n) exhausted = true;
+            if (ray < 0) {
+                const int r = base + __popc(idle & lt);
+                if (r < n) {
+                    ray = r;
+                    fetch(r, o, d, tmax, in_obj);
+                    sp_scene = scene_of(r);
+                    nodes = reinterpret_cast<const float4 *>(sp_scene->nodes);
+                    h.t = 0.0f;
+                    h.id = -1;
+                    h.u = h.v = 0.0f;
+                    h.back = 0;
+                    sp = 0;
+                    steps = 0;
+                    cur = WW_DONE;
+                    lf_count = 0;
+                    if (!(d.x == 0.0f && d.y == 0.0f && d.z == 0.0f)) {  // bvh.cpp:161-162
+                        inv = safe_inv(d);
+                        oinv = mk3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+                        const float4 a = __ldg(nodes), b = __ldg(nodes + 1);
+                        if (STATS) st.nodes++;
+                        float tn;
+                        if (slab(a, b, inv, oinv, tmax, tn)) {
+                            const int first = __float_as_int(b.z), count = __float_as_int(b.w);
+                            if (count > 0) {
+                                lf_first = first;
+                                lf_count = count;
+                            } else if ((unsigned)first < (unsigned)(sp_scene->n_nodes - 1)) {
+                                cur = first;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, ray >= 0) == 0) break;
+        // interior node pairs, speculatively past the first leaf
+        while (cur >= 0) {
+            if ((unsigned)cur >= (unsigned)(sp_scene->n_nodes - 1) || ++steps > sp_scene->n_nodes) {  // malformed tree guard
+                cur = WW_DONE;
+                lf_count = 0;
+                break;
+            }
+            const float4 a0 = __ldg(nodes + 2 * cur), b0 = __ldg(nodes + 2 * cur + 1);
+            const float4 a1 = __ldg(nodes + 2 * cur + 2), b1 = __ldg(nodes + 2 * cur + 3);
+            if (STATS) st.nodes += 2;
+            const float lim = h.t > 0.0f ? fminf(h.t, tmax) : tmax;
+            float tn0, tn1;
+            const bool h0 = slab(a0, b0, inv, oinv, lim, tn0);
+            const bool h1 = slab(a1, b1, inv, oinv, lim, tn1);
+            const int c0 = __float_as_int(b0.w), c1 = __float_as_int(b1.w);
+            const bool v0 = h0 && c0 >= 0, v1 = h1 && c1 >= 0;
+            const int e0 = c0 > 0 ? -(cur + 1) : __float_as_int(b0.z);
+            const int e1 = c1 > 0 ? -(cur + 2) : __float_as_int(b1.z);
+            if (v0 && v1) {
+                const bool sw = tn1 < tn0;
+                cur = sw ? e1 : e0;
+                push(sw ? e0 : e1);
+            } else if (v0) {
+                cur = e0;
+            } else if (v1) {
+                cur = e1;
+            } else {
+                cur = pop();
+            }
+            if (cur < 0 && cur != WW_DONE && lf_count == 0) {  // postpone the leaf, keep walking
+                take_leaf(-cur - 1);
+                cur = pop();
+            }
+            if (!__any_sync(__activemask(), lf_count == 0 && cur >= 0)) break;
+        }
+        // the postponed leaves, then any leaf the walk stopped at
+        while (lf_count > 0) {
+            if (leaf_isect<ANYHIT, STATS>(*sp_scene, lf_first, lf_count, o, d, tmax, in_obj, h, st)) {
+                cur = WW_DONE;
+                lf_count = 0;
+                break;
+            }
+            lf_count = 0;
+            if (cur < 0 && cur != WW_DONE) {
+                take_leaf(-cur - 1);
+                cur = pop();
+            }
+        }
+    }
+}
+
 // Persistent queue traversal shared by every ray kernel.
 //   MODE 0: a warp takes 32 rays and traces each to completion.
 //   MODE 1: per-lane refill; every iteration advances each ray by one node pair.
 //   MODE 2: per-lane refill; interior node pairs until every busy lane holds postponed
 //           leaves, then the warp intersects those leaves together.
+//   MODE 3: speculative while-while with per-lane refill (traverse_queue_ww).
 // fetch(i, o, d, tmax, in_obj) loads ray i; finish(i, hit) consumes its result.
 template <int MODE, bool ANYHIT, int STACK_SMEM, bool STATS, typename Fetch, typename Finish>
 RUMI_D void traverse_queue(const DevScene &s, int n, int *counter, int refill_min, int *smem_stack, int stride,
                            Fetch fetch, Finish finish, TraceStats &st) {
     const int lane = threadIdx.x & 31;
     int spill[RUMI_MAX_BVH_DEPTH - STACK_SMEM > 0 ? RUMI_MAX_BVH_DEPTH - STACK_SMEM : 1];
+    if (MODE == 3) {
+        traverse_queue_ww<ANYHIT, STACK_SMEM, STATS>([&](int) { return &s; }, n, counter, refill_min, smem_stack,
+                                                      stride, fetch, finish, st);
+        return;
+    }
     if (MODE == 0) {
         for (;;) {
             int base = 0;
