@@ -28,10 +28,20 @@ static constexpr int NBINS = 32;
 static constexpr int CHUNK = 2048;
 static constexpr int BIN_THREADS = 256;
 static constexpr int SMALL_MAX = 256;
-static constexpr int LEAF_MAX = 8;
+// Leaf size cap and SAH traversal cost (relative to one primitive test).  Measured on the
+// 1024x1024x64 BVH-bound frame (ms): cap 8 / C_TRAV 1: 239; cap 16 / 1: 239; 16 / 1.5: 250;
+// 16, 24 or 32 / 2: 225.5; 16 / 3: 231; 8 / 2: 250 (larger leaves pay only when the cap
+// lets the SAH form them).
+#ifndef RUMI_LEAF_MAX
+#define RUMI_LEAF_MAX 16
+#endif
+static constexpr int LEAF_MAX = RUMI_LEAF_MAX;
 static constexpr int MEDIAN_DEPTH = 40;    // past this depth split at the index median
 static constexpr int MAX_DEPTH = 63;       // deepest node (traversal stack holds 64)
-static constexpr float C_TRAV = 1.0f;
+#ifndef RUMI_SAH_CTRAV
+#define RUMI_SAH_CTRAV 2.0f
+#endif
+static constexpr float C_TRAV = RUMI_SAH_CTRAV;
 static constexpr float C_ISECT = 1.0f;
 
 struct BuildTask {
