@@ -253,7 +253,45 @@ def adjoint_fixture(path, seeds=960, h=1e-3):
     print(path, "fd mean", fd.mean(0), "stderr", fd.std(0, ddof=1) / np.sqrt(seeds))
 
 
+def _gt_rows(args):
+    size, spp, depth, row0, row1, seed = args
+    sc = scenes.cornell_pt(size, size, spp, depth)
+    rs = refimpl.RefScene(sc, seed=seed)
+    film, _, nans = rs.render_rows(seed, row0, row1)
+    n = rs.spp
+    rs.close()
+    return row0, row1, film[row0:row1] / n, nans
+
+
+def rmse_fixture(path, size=32, depth=8, gt_spp=65536, spp=16, frames=256, procs=8):
+    """Reference ground truth and the reference's own error at matched spp: the Cornell
+    workload at 32x32 rendered by the reference with 65,536 spp per pixel (rows split over
+    processes, each with its own srand seed), and the RMSE against it of 256 independent
+    reference frames at 16 spp."""
+    import multiprocessing as mp
+    rows_per = size // procs
+    jobs = [(size, gt_spp, depth, k * rows_per, (k + 1) * rows_per, 90000 + k) for k in range(procs)]
+    gt = np.zeros((size, size, 3), np.float64)
+    with mp.get_context("spawn").Pool(procs) as pool:
+        for r0, r1, part, nans in pool.map(_gt_rows, jobs):
+            gt[r0:r1] = part
+    sc = scenes.cornell_pt(size, size, spp, depth)
+    rmse = []
+    for s in range(frames):
+        rs = refimpl.RefScene(sc, seed=1000 + s)
+        film, _ = rs.render(7000 + s)
+        img = film.astype(np.float64) / rs.spp
+        rs.close()
+        rmse.append(float(np.sqrt(((img - gt) ** 2).mean())))
+    np.savez_compressed(path, gt=gt.astype(F32), ref_rmse=np.array(rmse), gt_spp=gt_spp, spp=spp, depth=depth,
+                        size=size)
+    print(path, "reference RMSE at", spp, "spp:", np.mean(rmse), "+-", np.std(rmse) / np.sqrt(frames))
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "rmse":
+        rmse_fixture(os.path.join(HERE, "rmse_cornell32.npz"))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "adjoint":
         adjoint_fixture(os.path.join(HERE, "adjoint_fd_ref32.npz"))
         return

@@ -202,3 +202,14 @@ def test_oracle_subsurface_matches_reference_3sigma(golden):
     """Subsurface random walk and a glossy sphere, path traced to depth 12."""
     frames_vs_reference(oracle_frames(scenes.subsurface_cornell(32, 32, 16, 12), 12, 24, 900),
                         golden("image_sss_pt32.npz"))
+
+
+def test_oracle_rmse_at_matched_spp_within_5pct_of_reference(golden):
+    """The oracle's 16-spp frames against the reference's 65,536-spp image: mean RMSE within
+    5% of the reference's own 16-spp RMSE."""
+    g = golden("rmse_cornell32.npz")
+    gt = g["gt"].astype(np.float64)
+    frames = oracle_frames(scenes.cornell_pt(32, 32, 16, 8), 8, 64, 30000)
+    rm = [float(np.sqrt(((f.astype(np.float64) - gt) ** 2).mean())) for f in frames]
+    ratio = float(np.mean(rm) / np.mean(g["ref_rmse"]))
+    assert abs(ratio - 1.0) < 0.05, ratio
