@@ -357,14 +357,14 @@ def test_gpu_bdpt_volumetric_caustic_spot_workload():
 
 def test_gpu_rmse_at_matched_spp_within_5pct_of_reference(golden):
     """RMSE against the reference's own 65,536-spp image of the Cornell workload (32x32,
-    depth 8), at matched spp (16): our mean over 256 frames within 5% of the mean RMSE of
+    depth 8), at matched spp (16): our mean over 1024 frames within 5% of the mean RMSE of
     256 reference frames (tests/golden/rmse_cornell32.npz)."""
     g = golden("rmse_cornell32.npz")
     gt = g["gt"].astype(np.float64)
     gs = rumi_b200.GpuScene(scenes.cornell_pt(32, 32, 16, 8))
     try:
         rm = []
-        for s in range(256):
+        for s in range(1024):
             film, st = gs.render(seed=20000 + s)
             rm.append(float(np.sqrt(((film.astype(np.float64) / 16.0 - gt) ** 2).mean())))
         ratio = float(np.mean(rm) / np.mean(g["ref_rmse"]))
