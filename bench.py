@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ray-sets", action="store_true", help="skip the primary / secondary / shadow ray-set rates")
     ap.add_argument("--wave-paths", type=int, default=0)
     ap.add_argument("--small", action="store_true", help="256x256 at 16 spp (profiling runs)")
     ap.add_argument("--workload", default="bvh_bound", choices=["bvh_bound", "batched", "adjoint", "bdpt_caustic"],
@@ -140,6 +141,12 @@ def _ref_worker(conn, w):
         msg = conn.recv()
         if msg is None:
             break
+        if msg[0] == "trace":  # BVHAccel::Travel over a ray set, one thread
+            _, rays, anyhit = msg
+            t0 = time.perf_counter()
+            rs.trace(rays, anyhit=anyhit)
+            conn.send((rays.shape[0], time.perf_counter() - t0))
+            continue
         seed, rows = msg
         t0 = time.perf_counter()
         paths = 0
@@ -208,6 +215,72 @@ def cpu_baseline_sample(w, procs, rows_per_proc=1):
                        f"of the same workload, reference renderer built from its sources (oracle/_ref), "
                        f"one thread per process, CPU {cpu_model()}",
                 seconds=secs)
+
+
+def make_ray_sets(sc, gs, n, seed=5):
+    """The three ray sets of the BVH-bound workload (host arrays (n, 7): o, d, tmax):
+    primary camera rays through jittered pixels of the 1024x1024 film; secondary rays
+    leaving the primary hits in cosine-distributed directions about the face normal
+    (diffuse bounce); shadow rays from those hits to uniform points on the light."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    fs = sc.flatten()
+    W, H = fs.image.width, fs.image.height
+    cam = sc.camera
+    tan = np.tan(np.radians(cam.fov) * 0.5)
+    px = rng.integers(0, W, n) + rng.random(n)
+    py = rng.integers(0, H, n) + rng.random(n)
+    x = -((px - W / 2) / (W / 2)) * tan
+    y = -((py - H / 2) / (H / 2)) * tan * cam.y_ratio
+    d = np.stack([x, y, np.ones(n)], 1)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    o = np.tile(np.asarray(cam.position, np.float64), (n, 1))
+    big = np.float32(3.0e38)
+    primary = np.concatenate([o, d, np.full((n, 1), big)], 1).astype(np.float32)
+    t, prim, _, _ = gs.trace(primary)
+    hit = (prim >= 0) & (prim < fs.tri_vertices.shape[0])
+    p = (o + d * t[:, None])[hit]
+    tri = fs.tri_vertices[prim[hit]].astype(np.float64)
+    nrm = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    nrm *= -np.sign((nrm * d[hit]).sum(1))[:, None]  # face the incoming ray
+    m = p.shape[0]
+    u1, u2 = rng.random(m), rng.random(m)
+    a = np.where(np.abs(nrm[:, :1]) > 0.9, np.array([[0.0, 1.0, 0.0]]), np.array([[1.0, 0.0, 0.0]]))
+    tu = np.cross(nrm, a)
+    tu /= np.linalg.norm(tu, axis=1, keepdims=True)
+    tv = np.cross(nrm, tu)
+    r, phi = np.sqrt(u1), 2 * np.pi * u2
+    wi = tu * (r * np.cos(phi))[:, None] + tv * (r * np.sin(phi))[:, None] + nrm * np.sqrt(1 - u1)[:, None]
+    secondary = np.concatenate([p, wi, np.full((m, 1), big)], 1).astype(np.float32)
+    lp = np.array([0.375, 0.999, 0.375]) + rng.random((m, 1)) * np.array([0.25, 0, 0]) + \
+        rng.random((m, 1)) * np.array([0, 0, 0.25])
+    sd = lp - p
+    dist = np.linalg.norm(sd, axis=1)
+    shadow = np.concatenate([p, sd / dist[:, None], (dist - 1e-4)[:, None]], 1).astype(np.float32)
+    return dict(primary=primary, secondary=secondary, shadow=shadow)
+
+
+def gpu_rays_per_s(gs, rays, anyhit, repeats=3):
+    """Device time of rumi_trace_rays (plain kernel) over a device-resident ray set."""
+    import numpy as np
+    import torch
+    r8 = np.zeros((rays.shape[0], 8), np.float32)
+    r8[:, 0:3], r8[:, 4:7], r8[:, 7] = rays[:, 0:3], rays[:, 3:6], rays[:, 6]
+    dr = torch.from_numpy(r8).cuda()
+    dt = torch.empty(rays.shape[0], device="cuda")
+    dp = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    best = float("inf")
+    for _ in range(repeats + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        gs.trace_device(rays.shape[0], dr.data_ptr(), dt.data_ptr(), dp.data_ptr(), anyhit=anyhit, stream=stream,
+                        count=False)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return rays.shape[0] / (best / 1000.0)
 
 
 def reference_arm(args):
@@ -379,6 +452,26 @@ def our_arm(args):
         film_np = film_host.numpy()
         assert np.isfinite(film_np).all()
 
+    # closest-hit / any-hit rays/s on the three ray sets, and the reference's BVHAccel::Travel
+    # on a sample of the same rays (one thread)
+    ray_sets = None
+    if rank == 0 and not args.no_ray_sets:
+        sets = make_ray_sets(sc, gs, 1 << 21)
+        ray_sets = {}
+        for name, rays in sets.items():
+            anyhit = name == "shadow"
+            ray_sets[name] = dict(rays=int(rays.shape[0]), anyhit=anyhit,
+                                  gpu_rays_per_s=gpu_rays_per_s(gs, rays, anyhit))
+        if world == 1 and not args.no_cpu_baseline:
+            pool = RefPool(w, 1)
+            for name, rays in sets.items():
+                sample = rays[:20000]
+                pool.conns[0].send(("trace", sample, name == "shadow"))
+                n, sec = pool.conns[0].recv()
+                ray_sets[name]["ref_rays_per_s_1_thread"] = n / sec
+                ray_sets[name]["ref_sample"] = n
+            pool.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(w, ref_procs(limit=16))
@@ -393,7 +486,7 @@ def our_arm(args):
                                 triangles=4 * 4 ** w["levels"], parallelism=f"replicas x{world} (spp shards)",
                                 l2="inputs larger than L2 (scene ~170 MB + wave queues ~690 MB per GPU)",
                                 bvh_build_ms=bvh["build_ms"]),
-                    rays_per_sec=rays_per_s, roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=launches,
+                    rays_per_sec=rays_per_s, ray_sets=ray_sets, roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=launches,
                     clocks=clocks_info)
         print(json.dumps(line), flush=True)
     if dist:

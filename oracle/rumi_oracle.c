@@ -362,7 +362,7 @@ static V3 hg_sample(V3 d, float g, float u1, float u2, float *pdf) {
 
 typedef struct { V3 w; int le, go_in; float xi, pdf_path, cost, pdfw; } Bsdf;
 
-/* Material::BSDFSampling of every material (src/Material/*.cpp) */
+/* Material::BSDFSampling of every material (the src/Material/ sources) */
 static Bsdf mat_sample(const orc_material *m, V3 wo, V3 n, float ulobe, float u1, float u2) {
     Bsdf b;
     memset(&b, 0, sizeof(b));

@@ -1089,32 +1089,57 @@ struct TraceLaunch {
     unsigned long long *counters;  // [0] fetch, [1] nodes, [2] prims
 };
 
-template <bool ANYHIT>
-__global__ void __launch_bounds__(TRACE_THREADS) trace_batch_kernel(TraceLaunch T) {
+// Ray queries: the renderer's default traversal scheme (speculative while-while with
+// per-lane refill) over a caller's ray array, in chunks of at most 2^30 rays.
+template <bool ANYHIT, bool STATS>
+__global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) trace_batch_kernel(TraceLaunch T, long long first,
+                                                                                         int n, int *fetch_counter) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
-    const int lane = threadIdx.x & 31;
     TraceStats st{0, 0};
-    for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(&T.counters[0], 32ull);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= (unsigned long long)T.n) break;
-        const long long i = (long long)base + lane;
-        if (i < T.n) {
-            const float4 o4 = T.rays[2 * i], d4 = T.rays[2 * i + 1];
-            const HitRec h = trace_ray<ANYHIT, STACK_SMEM, true>(T.s, f4xyz(o4), f4xyz(d4), d4.w, o4.w != 0.0f,
-                                                                 stack + threadIdx.x, TRACE_THREADS, st);
-            T.t[i] = h.t;
-            T.prim[i] = ANYHIT ? (h.t > 0.0f ? 1 : 0) : (h.t > 0.0f ? h.id : -1);
-        }
+    auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
+        const long long k = first + i;
+        const float4 o4 = T.rays[2 * k], d4 = T.rays[2 * k + 1];
+        o = f4xyz(o4);
+        d = f4xyz(d4);
+        tmax = d4.w;
+        in_obj = o4.w != 0.0f;
+    };
+    auto finish = [&](int i, const HitRec &h) {
+        const long long k = first + i;
+        T.t[k] = h.t;
+        T.prim[k] = ANYHIT ? (h.t > 0.0f ? 1 : 0) : (h.t > 0.0f ? h.id : -1);
+    };
+    traverse_queue<3, ANYHIT, STACK_SMEM, STATS>(T.s, n, fetch_counter, 8, stack + threadIdx.x, TRACE_THREADS, fetch,
+                                                 finish, st);
+    if (STATS) {
+        atomicAdd(&T.counters[1], (unsigned long long)st.nodes);
+        atomicAdd(&T.counters[2], (unsigned long long)st.prims);
     }
-    atomicAdd(&T.counters[1], (unsigned long long)st.nodes);
-    atomicAdd(&T.counters[2], (unsigned long long)st.prims);
+}
+
+template <bool ANYHIT, bool STATS>
+static void launch_trace_batch(const TraceLaunch &T, int num_sms, cudaStream_t stream) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_batch_kernel<ANYHIT, STATS>, TRACE_THREADS, 0);
+    if (occ < 1) occ = 1;
+    const long long chunk = 1LL << 30;
+    int k = 0;
+    for (long long first = 0; first < T.n; first += chunk, ++k) {
+        const int n = (int)(T.n - first < chunk ? T.n - first : chunk);
+        // one fetch counter per chunk (counters[3 + k]; chunk count is bounded by the caller's n)
+        int *ctr = reinterpret_cast<int *>(T.counters + 3) + k;
+        trace_batch_kernel<ANYHIT, STATS><<<num_sms * occ, TRACE_THREADS, 0, stream>>>(T, first, n, ctr);
+    }
 }
 
 rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, float *t_dev, int32_t *prim_dev,
                        int64_t *node_visits, int64_t *prim_tests, cudaStream_t stream) {
-    rumi_status st = ensure_workspace(sc, 256);
+    const long long chunks = (n + (1LL << 30) - 1) >> 30;
+    if (chunks > 64) {
+        set_error("trace_rays: at most 2^36 rays per call");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    rumi_status st = ensure_workspace(sc, 256 + 3 * sizeof(unsigned long long) + 64 * sizeof(int));
     if (st != RUMI_OK) return st;
     TraceLaunch T;
     T.s = sc->dev;
@@ -1124,23 +1149,20 @@ rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int any
     T.n = n;
     T.anyhit = anyhit;
     T.counters = (unsigned long long *)sc->ws;
-    cudaMemsetAsync(T.counters, 0, 3 * sizeof(unsigned long long), stream);
-    int occ = 0;
-    if (anyhit)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_batch_kernel<true>, TRACE_THREADS, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_batch_kernel<false>, TRACE_THREADS, 0);
-    if (occ < 1) occ = 1;
-    const int grid = sc->num_sms * occ;
+    cudaMemsetAsync(T.counters, 0, 3 * sizeof(unsigned long long) + 64 * sizeof(int), stream);
+    const bool stats = node_visits != nullptr || prim_tests != nullptr;
     if (n > 0) {
         if (anyhit)
-            trace_batch_kernel<true><<<grid, TRACE_THREADS, 0, stream>>>(T);
+            stats ? launch_trace_batch<true, true>(T, sc->num_sms, stream)
+                  : launch_trace_batch<true, false>(T, sc->num_sms, stream);
         else
-            trace_batch_kernel<false><<<grid, TRACE_THREADS, 0, stream>>>(T);
+            stats ? launch_trace_batch<false, true>(T, sc->num_sms, stream)
+                  : launch_trace_batch<false, false>(T, sc->num_sms, stream);
     }
     unsigned long long h[3] = {0, 0, 0};
-    cudaMemcpyAsync(h, T.counters, sizeof(h), cudaMemcpyDeviceToHost, stream);
-    cudaError_t e = cudaStreamSynchronize(stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, T.counters, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_status(e, "trace_rays");
     if (node_visits) *node_visits = (int64_t)h[1];
     if (prim_tests) *prim_tests = (int64_t)h[2];

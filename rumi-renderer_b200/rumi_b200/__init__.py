@@ -229,12 +229,15 @@ class GpuScene:
                                              C.byref(nv), C.byref(pt), None), "rumi_trace_rays")
         return t, prim, nv.value, pt.value
 
-    def trace_device(self, n: int, rays_ptr: int, t_ptr: int, prim_ptr: int, anyhit: bool = False, stream=None):
+    def trace_device(self, n: int, rays_ptr: int, t_ptr: int, prim_ptr: int, anyhit: bool = False, stream=None,
+                     count: bool = True):
+        """rumi_trace_rays on device buffers; count=False skips the node / primitive
+        counters (the plain kernel).  Returns (node_visits, prim_tests) or (None, None)."""
         nv, pt = C.c_int64(), C.c_int64()
         _capi.check(self.lib.rumi_trace_rays(self.h, n, C.c_void_p(rays_ptr), 1 if anyhit else 0, C.c_void_p(t_ptr),
-                                             C.c_void_p(prim_ptr), 1, C.byref(nv), C.byref(pt), stream),
-                    "rumi_trace_rays")
-        return nv.value, pt.value
+                                             C.c_void_p(prim_ptr), 1, C.byref(nv) if count else None,
+                                             C.byref(pt) if count else None, stream), "rumi_trace_rays")
+        return (nv.value, pt.value) if count else (None, None)
 
     def close(self):
         if getattr(self, "h", None):
