@@ -21,6 +21,8 @@ namespace rumi {
 static constexpr int BD_THREADS = 64;
 static constexpr int BD_STACK = 32;
 static constexpr int BD_MAXV = 16;  // vertices per subpath (nE, nL <= 16)
+// The kernel is instantiated for MAXV = 8 and 16: its per-thread subpath arrays live in
+// local memory, and sizing them to the request halves that traffic for nL, nE <= 8.
 
 struct BVert {
     float3 p, n;
@@ -378,12 +380,13 @@ RUMI_D float camera_pdfw(const DevCamera &c, float3 w) {
 // BidirectionalPathTracer::MISWeight (bidirectionalpathtracer.cpp:1096-1586).
 // ns / nt: vertices used on the light / eye side; VL / VE the subpaths, segL / segE
 // their segment directions.
+template <int MAXV>
 RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, const BVert *VE, const float3 *segE,
                         int ns, int nt, float3 connect_wi, float3 connect_wo, float3 light_n, const DevLight &light) {
     if (ns + nt <= 2) return 1.0f;
     const DevScene &S = P.s;
     const DevVolume &vol = S.volume;
-    float3 sb[BD_MAXV], sf[BD_MAXV], tb[BD_MAXV], tf[BD_MAXV];
+    float3 sb[MAXV], sf[MAXV], tb[MAXV], tf[MAXV];
     const BVert *s_connect = nullptr, *s_prev = nullptr, *t_connect = nullptr, *t_prev = nullptr;
     float3 s_wi = mk3(0, 0, 0), t_wo = mk3(0, 0, 0);
     if (ns > 0) {
@@ -598,6 +601,7 @@ RUMI_D bool volumetric_ok(const DevVolume &V, float3 sp, float3 tp, float xi) {
     return !(xi < 1.0f - expf(avg3(V.sigma_t) * -sm));
 }
 
+template <int MAXV>
 __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
     __shared__ int stack[BD_STACK * BD_THREADS];
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -611,8 +615,8 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
     TraceStats st{0, 0};
     int *stk = stack + threadIdx.x;
 
-    BVert VE[BD_MAXV], VL[BD_MAXV];
-    float3 segE[BD_MAXV], segL[BD_MAXV], aE[BD_MAXV + 2], aL[BD_MAXV + 2];
+    BVert VE[MAXV], VL[MAXV];
+    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
     // Scene::LightsUniformSampling + AreaLight::SolidAngleSampling
     const Uniform4 UL = path_uniforms(path, 1000u, 0, P.k0, P.k1);
     const Uniform4 UD = path_uniforms(path, 1000u, 1, P.k0, P.k1);
@@ -673,7 +677,7 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 t_wo = -segE[t - 1];
                 if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
                     if (len == nE - 1) {
-                        const float w = mis_weight(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
+                        const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
                         L = L + aE[t + 1] * w;
                     }
                     break;
@@ -730,14 +734,14 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 if (wi == W || hi == H) continue;
                 if (wi < 0 || hi < 0 || wi > W || hi > H) continue;
                 float3 lo = aE[t] * cE * G * cL * aL[s];
-                lo = lo * mis_weight(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n, light);
+                lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n, light);
                 float *dst = P.light_film + ((size_t)hi * W + wi) * 3;
                 atomicAdd(dst + 0, lo.z);
                 atomicAdd(dst + 1, lo.y);
                 atomicAdd(dst + 2, lo.x);
             } else {
                 float3 lo = aE[t] * cE * G * cL * aL[s];
-                lo = lo * mis_weight(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
+                lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
                 L = L + lo;
             }
         }
@@ -826,7 +830,11 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
         B.pix0 = (int)pix0;
         B.n_paths = (int)(n_pix * spp);
         B.path0 = pix0 * spp;
-        bdpt_kernel<<<(B.n_paths + BD_THREADS - 1) / BD_THREADS, BD_THREADS, 0, stream>>>(B);
+        const int blocks = (B.n_paths + BD_THREADS - 1) / BD_THREADS;
+        if (p->n_light <= 8 && p->n_eye <= 8)
+            bdpt_kernel<8><<<blocks, BD_THREADS, 0, stream>>>(B);
+        else
+            bdpt_kernel<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B);
         bdpt_write_film<<<(int)((n_pix + 255) / 256), 256, 0, stream>>>(B, (int)n_pix, film_dev, nan_count);
         launches += 2;
     }
