@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--no-ray-sets", action="store_true", help="skip the primary / secondary / shadow ray-set rates")
     ap.add_argument("--wave-paths", type=int, default=0)
     ap.add_argument("--small", action="store_true", help="256x256 at 16 spp (profiling runs)")
-    ap.add_argument("--workload", default="bvh_bound", choices=["bvh_bound", "batched", "adjoint", "bdpt_caustic"],
+    ap.add_argument("--workload", default="bvh_bound", choices=["bvh_bound", "batched", "adjoint", "bdpt_caustic", "cornell"],
                     help="batched: 256 seeded scenes as one frame vs the per-scene loop; "
                          "adjoint: inverse rendering with the path-replay adjoint")
     ap.add_argument("--adam-steps", type=int, default=200, help="adjoint workload: optimisation steps")
@@ -752,6 +752,61 @@ def bdpt_arm(args):
     return 0
 
 
+def cornell_arm(args):
+    """The plain path-tracer Cornell workload, the reference's own CPU-runnable case:
+    5 walls, area light, a Lambertian and a mirror sphere; 256x256, 16 spp, depth 8
+    (1,048,576 paths per frame).  value = paths/s on the device; cpu_baseline = the
+    reference renderer itself on a row sample of the same frame, one thread."""
+    import torch
+    import rumi_b200
+    from rumi_b200 import scenes
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    W, H, spp, depth = 256, 256, 16, 8
+    sc = scenes.cornell_pt(W, H, spp, depth)
+    gs = rumi_b200.GpuScene(sc)
+    stream = torch.cuda.current_stream().cuda_stream
+    film = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    steps = max(args.steps, 20)
+    for s in range(args.warmup):
+        gs.render(seed=s, film_device_ptr=film.data_ptr(), stream=stream)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    launches = 0
+    for s in range(steps):
+        _, st = gs.render(seed=100 + s, film_device_ptr=film.data_ptr(), stream=stream)
+        launches += (st["extend_launches"] // depth) * (3 + 4 * depth)
+    ev1.record()
+    torch.cuda.synchronize()
+    clocks_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import refimpl
+        rs = refimpl.RefScene(sc, seed=1)
+        rows = 16
+        t0 = time.perf_counter()
+        rs.render_rows(5, 0, rows)
+        sec = time.perf_counter() - t0
+        n = rows * W * rs.spp
+        cpu = dict(value=n / sec, unit="paths/s", cores=1, kind="reference",
+                   sample=f"{n} paths = {rows} rows x {W} px x {rs.spp} spp of the same frame, PathTracer(8), "
+                          f"one thread, CPU {cpu_model()}", seconds=sec)
+        rs.close()
+    gs.close()
+    line = dict(metric="path samples/sec", value=steps * W * H * spp / (ms / 1000.0), unit="paths/s", n_gpus=1,
+                steps=steps, warmup=args.warmup, ms_per_step=ms / steps, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f32", data="synthetic (analytic scene)",
+                config=dict(workload="cornell_pt: plain path tracer, Cornell box", width=W, height=H, spp=spp,
+                            max_depth=depth),
+                cpu_baseline=cpu, gpu_launches=launches, clocks=clocks_info)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -762,6 +817,8 @@ def main():
         return adjoint_arm(args)
     if args.workload == "bdpt_caustic":
         return bdpt_arm(args)
+    if args.workload == "cornell":
+        return cornell_arm(args)
     return our_arm(args)
 
 
