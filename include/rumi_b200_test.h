@@ -46,6 +46,11 @@ rumi_status rumi_test_camera_rays(const rumi_camera *cam, int32_t width, int32_t
 rumi_status rumi_test_pixel_samples(int64_t n, const int32_t *s, int32_t spp, const int64_t *pixel, uint64_t seed,
                                     float *out);
 
+/* Device time (ms, CUDA events on `stream`) of one launch that reads the device buffer
+ * `passes` times (float4 loads, cached in L2 only).  A buffer smaller than L2 measures L2
+ * read bandwidth: bytes * passes / ms. */
+rumi_status rumi_test_read_bandwidth(const void *buf_dev, int64_t bytes, int32_t passes, void *stream, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

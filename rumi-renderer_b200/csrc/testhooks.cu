@@ -125,7 +125,45 @@ __global__ void k_pixel_samples(int64_t n, const int32_t *s, int spp, int grid_d
 
 }  // namespace
 
+// Read bandwidth of a device buffer re-read `passes` times in one launch (a buffer
+// smaller than the 126 MB L2 measures L2; a larger one measures HBM).  Each thread
+// streams float4 elements grid-stride and folds them into one value so the loads stay.
+__global__ void k_read_bw(const float4 *__restrict__ buf, size_t n4, int passes, float *out) {
+    float acc = 0.0f;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (int p = 0; p < passes; ++p)
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+            const float4 v = __ldcg(buf + i);
+            acc += v.x + v.y + v.z + v.w;
+        }
+    if (acc == 12345.678f) out[0] = acc;  // practically never: keeps the loads live
+}
+
 extern "C" {
+
+rumi_status rumi_test_read_bandwidth(const void *buf_dev, int64_t bytes, int32_t passes, void *stream, double *ms) {
+    if (!buf_dev || bytes < 16 || passes < 1 || !ms) return set_error("rumi_test_read_bandwidth: bad argument"), RUMI_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const size_t n4 = (size_t)bytes / 16;
+    k_read_bw<<<sms * 8, 256, 0, s>>>((const float4 *)buf_dev, n4, 1, (float *)buf_dev);  // warm
+    cudaEventRecord(e0, s);
+    k_read_bw<<<sms * 8, 256, 0, s>>>((const float4 *)buf_dev, n4, passes, (float *)buf_dev);
+    cudaEventRecord(e1, s);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float t = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_status(e, "rumi_test_read_bandwidth");
+    *ms = t;
+    return RUMI_OK;
+}
 
 rumi_status rumi_test_philox(int64_t n, const uint32_t *ctr, const uint32_t *key, uint32_t *out) {
     if (n < 0 || (n > 0 && (!ctr || !key || !out))) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
