@@ -26,7 +26,7 @@ rumi_status cuda_status(cudaError_t e, const char *what) {
 // Device allocations of scenes and render workspaces come from the device's default
 // stream-ordered memory pool.  The pool keeps up to POOL_KEEP_BYTES of freed memory for
 // reuse within this process, so creating a scene after destroying one does not go back
-// to the driver.
+// to the CUDA driver.
 static constexpr unsigned long long POOL_KEEP_BYTES = 16ull << 30;
 
 void configure_pool(int device) {

@@ -2,7 +2,7 @@
 //
 // The reference builds an object-median BVH on the host (src/Acceleration/bvh.cpp:48-148:
 // longest axis, shell sort, split at the middle index, leaves of <= 6).  Only the hits a
-// BVH produces are observable, so this build uses the surface area heuristic instead,
+// BVH produces are observable, so this builder uses the surface area heuristic instead,
 // entirely on the GPU and deterministically (same input -> same tree):
 //
 //  large phase (tasks with > SMALL_MAX primitives), one level per iteration:
