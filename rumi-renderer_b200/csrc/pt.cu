@@ -298,8 +298,8 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) pt_trace
             P.hit[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
         }
     };
-    traverse_queue_ww<ANYHIT, STACK_SMEM, false>(scene_of, n, counter, P.refill_min, stack + threadIdx.x,
-                                                 TRACE_THREADS, fetch, finish, st);
+    traverse_queue_walk<ANYHIT, STACK_SMEM, false>(scene_of, n, counter, P.refill_min, stack + threadIdx.x,
+                                                   TRACE_THREADS, fetch, finish, st);
 }
 
 // Next-event estimation toward one light sample from p.  Returns false when the light

@@ -44,12 +44,13 @@ struct __align__(128) Bvh4Node {
     int count[4];
 };
 
-// The four-wide walk visits ~2.7x fewer nodes per ray than the binary one (34.6 vs 47.7
-// 32-byte node units per camera ray and fewer primitive tests on the 1M-triangle mesh),
-// but each step costs more issue slots (four slabs, a sorting network, classification),
-// and on B200 the closest-hit frame measured slower (extend 178 vs 143 ms per
-// 1024x1024x64 frame; shadow rays on par, 119 vs 118 ms), so the binary walk is the
-// default and the four-wide tree is built only when this is set to 1.
+// The four-wide tree halves the node steps per ray (34.6 vs 47.7 node units of 32 bytes per
+// camera ray on the 1M-triangle mesh, fewer primitive tests), but each step costs more issue
+// slots (four slabs, a sorting network, classification).  Measured per 1024x1024x64 frame on
+// B200: warp-batch walk, binary 143 / four-wide 178 ms of closest-hit; speculative while-while
+// walk (the default scheme), binary 100 / four-wide 130 ms (any-hit 83.5 / 87.8 ms).  So the
+// binary tree is the default and the four-wide tree is built and walked only when this is 1
+// (both walks pass the same hit and image parity tests).
 #ifndef RUMI_BVH_WIDE
 #define RUMI_BVH_WIDE 0  // 1: walk the four-wide tree (nodes4), 0: the binary tree
 #endif

@@ -736,6 +736,166 @@ RUMI_D void traverse_queue_ww(SceneOf scene_of, int n, int *counter, int refill_
     }
 }
 
+// The same speculative while-while walk over the four-wide tree (nodes4): an interior
+// step tests a node's four child boxes, continues with the nearest hit child and pushes
+// the others farthest first; leaf children are stack entries -(1 + 4 * node + slot).
+template <bool ANYHIT, int STACK_SMEM, bool STATS, typename SceneOf, typename Fetch, typename Finish>
+RUMI_D void traverse_queue_ww4(SceneOf scene_of, int n, int *counter, int refill_min, int *smem_stack, int stride,
+                               Fetch fetch, Finish finish, TraceStats &st) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int spill[RUMI_STACK4 - STACK_SMEM > 0 ? RUMI_STACK4 - STACK_SMEM : 1];
+    const DevScene *sp_scene = scene_of(-1);
+    const float4 *nodes = reinterpret_cast<const float4 *>(sp_scene->nodes4);
+    float3 o = mk3(0, 0, 0), d = mk3(0, 0, 0), inv = mk3(0, 0, 0), oinv = mk3(0, 0, 0);
+    float tmax = 0.0f;
+    bool in_obj = false;
+    HitRec h;
+    h.t = 0.0f;
+    h.id = -1;
+    h.u = h.v = 0.0f;
+    h.back = 0;
+    int ray = -1, cur = WW_DONE, sp = 0, lf_first = 0, lf_count = 0, steps = 0;
+    bool exhausted = false;
+    auto pop = [&]() -> int {
+        if (sp == 0) return WW_DONE;
+        --sp;
+        return sp < STACK_SMEM ? smem_stack[sp * stride] : spill[sp - STACK_SMEM];
+    };
+    auto push = [&](int v) {
+        if (sp < STACK_SMEM)
+            smem_stack[sp * stride] = v;
+        else if (sp < RUMI_STACK4)
+            spill[sp - STACK_SMEM] = v;
+        if (sp < RUMI_STACK4) ++sp;  // three per level of a depth-limited tree: always holds
+    };
+    auto take_leaf = [&](int ref) {
+        const int k = -ref - 1, node = k >> 2, slot = k & 3;
+        if ((unsigned)node >= (unsigned)sp_scene->n_nodes4) {
+            lf_count = 0;
+            return;
+        }
+        const int4 ch = __ldg(reinterpret_cast<const int4 *>(nodes + 8 * node + 6));
+        const int4 cn = __ldg(reinterpret_cast<const int4 *>(nodes + 8 * node + 7));
+        lf_first = sel4(ch, slot);
+        lf_count = sel4(cn, slot);
+    };
+    for (;;) {
+        if (ray >= 0 && cur == WW_DONE && lf_count == 0) {
+            finish(ray, h);
+            ray = -1;
+        }
+        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
+        if (!exhausted && idle && (__popc(idle) >= refill_min || idle == 0xffffffffu)) {
+            int base = 0;
+            const int leader = __ffs(idle) - 1;
+            if (lane == leader) base = atomicAdd(counter, __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= n) exhausted = true;
+            if (ray < 0) {
+                const int r = base + __popc(idle & lt);
+                if (r < n) {
+                    ray = r;
+                    fetch(r, o, d, tmax, in_obj);
+                    sp_scene = scene_of(r);
+                    nodes = reinterpret_cast<const float4 *>(sp_scene->nodes4);
+                    h.t = 0.0f;
+                    h.id = -1;
+                    h.u = h.v = 0.0f;
+                    h.back = 0;
+                    sp = 0;
+                    steps = 0;
+                    lf_count = 0;
+                    cur = WW_DONE;
+                    if (!(d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) && sp_scene->n_nodes4 > 0) {  // bvh.cpp:161-162
+                        inv = safe_inv(d);
+                        oinv = mk3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+                        cur = 0;
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, ray >= 0) == 0) break;
+        while (cur >= 0) {
+            if ((unsigned)cur >= (unsigned)sp_scene->n_nodes4 || ++steps > sp_scene->n_nodes4) {  // malformed tree guard
+                cur = WW_DONE;
+                lf_count = 0;
+                break;
+            }
+            const float4 *np = nodes + 8 * cur;
+            const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+            const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+            const int4 ch = __ldg(reinterpret_cast<const int4 *>(np + 6));
+            const int4 cn = __ldg(reinterpret_cast<const int4 *>(np + 7));
+            if (STATS) st.nodes += 4;  // counted in 32-byte units
+            const float lim = h.t > 0.0f ? fminf(h.t, tmax) : tmax;
+            float k0, k1, k2, k3;
+            if (!(cn.x >= 0 && slab_s(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, inv, oinv, lim, k0))) k0 = FLT_MAX;
+            if (!(cn.y >= 0 && slab_s(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, inv, oinv, lim, k1))) k1 = FLT_MAX;
+            if (!(cn.z >= 0 && slab_s(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, inv, oinv, lim, k2))) k2 = FLT_MAX;
+            if (!(cn.w >= 0 && slab_s(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, inv, oinv, lim, k3))) k3 = FLT_MAX;
+            int s0 = 0, s1 = 1, s2 = 2, s3 = 3;
+            if (!ANYHIT) {
+                RUMI_CSWAP(k0, s0, k1, s1);
+                RUMI_CSWAP(k2, s2, k3, s3);
+                RUMI_CSWAP(k0, s0, k2, s2);
+                RUMI_CSWAP(k1, s1, k3, s3);
+                RUMI_CSWAP(k1, s1, k2, s2);
+            }
+            // entries of the hit children in order: node index or leaf reference
+            auto entry = [&](int slot) {
+                return sel4(cn, slot) > 0 ? -(1 + 4 * cur + slot) : sel4(ch, slot);
+            };
+            const int e0 = entry(s0), e1 = entry(s1), e2 = entry(s2), e3 = entry(s3);
+            const int nh = (k0 != FLT_MAX) + (k1 != FLT_MAX) + (k2 != FLT_MAX) + (k3 != FLT_MAX);
+            if (!ANYHIT) {
+                // sorted: the hit children are the first nh
+                if (nh > 3) push(e3);
+                if (nh > 2) push(e2);
+                if (nh > 1) push(e1);
+                cur = nh > 0 ? e0 : pop();
+            } else {
+                int next = WW_DONE;
+                if (k3 != FLT_MAX) next = e3;
+                if (k2 != FLT_MAX) { if (next != WW_DONE) push(next); next = e2; }
+                if (k1 != FLT_MAX) { if (next != WW_DONE) push(next); next = e1; }
+                if (k0 != FLT_MAX) { if (next != WW_DONE) push(next); next = e0; }
+                cur = next != WW_DONE ? next : pop();
+            }
+            if (cur < 0 && cur != WW_DONE && lf_count == 0) {  // postpone the leaf, keep walking
+                take_leaf(cur);
+                cur = pop();
+            }
+            if (!__any_sync(__activemask(), lf_count == 0 && cur >= 0)) break;
+        }
+        while (lf_count > 0) {
+            if (leaf_isect<ANYHIT, STATS>(*sp_scene, lf_first, lf_count, o, d, tmax, in_obj, h, st)) {
+                cur = WW_DONE;
+                lf_count = 0;
+                break;
+            }
+            lf_count = 0;
+            if (cur < 0 && cur != WW_DONE) {
+                take_leaf(cur);
+                cur = pop();
+            }
+        }
+    }
+}
+
+// The default walk: binary or four-wide tree by RUMI_BVH_WIDE.
+template <bool ANYHIT, int STACK_SMEM, bool STATS, typename SceneOf, typename Fetch, typename Finish>
+RUMI_D void traverse_queue_walk(SceneOf scene_of, int n, int *counter, int refill_min, int *smem_stack, int stride,
+                                Fetch fetch, Finish finish, TraceStats &st) {
+#if RUMI_BVH_WIDE
+    traverse_queue_ww4<ANYHIT, STACK_SMEM, STATS>(scene_of, n, counter, refill_min, smem_stack, stride, fetch, finish,
+                                                  st);
+#else
+    traverse_queue_ww<ANYHIT, STACK_SMEM, STATS>(scene_of, n, counter, refill_min, smem_stack, stride, fetch, finish,
+                                                 st);
+#endif
+}
+
 // Persistent queue traversal shared by every ray kernel.
 //   MODE 0: a warp takes 32 rays and traces each to completion.
 //   MODE 1: per-lane refill; every iteration advances each ray by one node pair.
@@ -749,8 +909,8 @@ RUMI_D void traverse_queue(const DevScene &s, int n, int *counter, int refill_mi
     const int lane = threadIdx.x & 31;
     int spill[RUMI_MAX_BVH_DEPTH - STACK_SMEM > 0 ? RUMI_MAX_BVH_DEPTH - STACK_SMEM : 1];
     if (MODE == 3) {
-        traverse_queue_ww<ANYHIT, STACK_SMEM, STATS>([&](int) { return &s; }, n, counter, refill_min, smem_stack,
-                                                      stride, fetch, finish, st);
+        traverse_queue_walk<ANYHIT, STACK_SMEM, STATS>([&](int) { return &s; }, n, counter, refill_min, smem_stack,
+                                                        stride, fetch, finish, st);
         return;
     }
     if (MODE == 0) {
