@@ -508,3 +508,39 @@ extern "C" void ref_camera_params(void *h, float *out) {
     out[0] = rs->scene->_camera->_tanfov;
     out[1] = rs->scene->_camera->_film_area;
 }
+
+#include <fcntl.h>
+#include <unistd.h>
+
+// Model(file, transform) (src/Shape/model.cpp:35-43, 76-343): the triangles the reference
+// loads from an OBJ file.  m16: row-major Mat4x4 (NULL = identity).  Writes up to cap
+// triangles (9 vertex floats and 9 normal floats each) and returns the model's count.
+extern "C" int ref_load_obj(const char *path, const float *m16, int cap, float *v_out, float *n_out) {
+    Mat4x4 m;
+    if (m16)
+        for (int k = 0; k < 16; ++k) m._m[k] = m16[k];
+    int devnull = open("/dev/null", O_WRONLY), saved = dup(1);
+    fflush(stdout);
+    dup2(devnull, 1);  // the loader prints progress
+    Model *model = new Model(path, m);
+    fflush(stdout);
+    dup2(saved, 1);
+    close(saved);
+    close(devnull);
+    const int n = model->_n_triangles;
+    for (int i = 0; i < n && i < cap; ++i) {
+        const Triangle *t = model->_triangles[i];
+        const Point3 *v[3] = {&t->_v0, &t->_v1, &t->_v2};
+        const Vector3 *nn[3] = {&t->_n0, &t->_n1, &t->_n2};
+        for (int k = 0; k < 3; ++k) {
+            v_out[9 * i + 3 * k + 0] = v[k]->_x;
+            v_out[9 * i + 3 * k + 1] = v[k]->_y;
+            v_out[9 * i + 3 * k + 2] = v[k]->_z;
+            n_out[9 * i + 3 * k + 0] = nn[k]->_x;
+            n_out[9 * i + 3 * k + 1] = nn[k]->_y;
+            n_out[9 * i + 3 * k + 2] = nn[k]->_z;
+        }
+    }
+    delete model;
+    return n;
+}

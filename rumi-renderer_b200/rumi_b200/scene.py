@@ -128,6 +128,14 @@ class Model(Shape):
         self.normals = None if normals is None else np.ascontiguousarray(normals, np.float32).reshape(-1, 3, 3)
         self.albedo = None if albedo is None else np.ascontiguousarray(albedo, np.float32).reshape(-1, 3)
 
+    @classmethod
+    def from_obj(cls, path: str, transform=None, albedo=None) -> "Model":
+        """``Model(file, transform)``: an OBJ file read by the reference's rules
+        (rumi_b200.obj); transform is a row-major 4x4 (16 floats), None = identity."""
+        from .obj import load_obj
+        v, n = load_obj(path, transform)
+        return cls(v, normals=n, albedo=albedo)
+
 
 class Rect(Shape):
     """``Rect(p, l, w[, n_samples])``: parallelogram p + a*l + b*w, normal

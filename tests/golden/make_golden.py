@@ -288,7 +288,28 @@ def rmse_fixture(path, size=32, depth=8, gt_spp=65536, spp=16, frames=256, procs
     print(path, "reference RMSE at", spp, "spp:", np.mean(rmse), "+-", np.std(rmse) / np.sqrt(frames))
 
 
+def obj_fixture(path):
+    """The reference's Model(file, transform) on the OBJ texts of tests/obj_cases.py."""
+    import tempfile
+    from obj_cases import CASES, TRANSFORMS
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for case, text in CASES.items():
+            p = os.path.join(d, case + ".obj")
+            with open(p, "wb") as f:
+                f.write(text.encode())
+            for tname, m in TRANSFORMS.items():
+                v, n = refimpl.load_obj(p, m)
+                out[f"{case}__{tname}__v"] = v
+                out[f"{case}__{tname}__n"] = n
+    np.savez_compressed(path, **out)
+    print(path, len(out) // 2, "loads")
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "obj":
+        obj_fixture(os.path.join(HERE, "obj_loader.npz"))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "rmse":
         rmse_fixture(os.path.join(HERE, "rmse_cornell32.npz"))
         return

@@ -225,6 +225,19 @@ class RefScene:
             pass
 
 
+def load_obj(path: str, m16=None, cap: int = 1 << 20):
+    """The reference's Model(path, transform): (vertices (F,3,3), normals (F,3,3))."""
+    L = lib()
+    L.ref_load_obj.restype = C.c_int
+    L.ref_load_obj.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    v = np.zeros((cap, 9), np.float32)
+    n = np.zeros((cap, 9), np.float32)
+    m = None if m16 is None else f32(np.asarray(m16, np.float32).reshape(16))
+    k = L.ref_load_obj(path.encode(), None if m is None else m.ctypes.data_as(C.c_void_p), cap,
+                       v.ctypes.data_as(C.c_void_p), n.ctypes.data_as(C.c_void_p))
+    return v[:k].reshape(-1, 3, 3), n[:k].reshape(-1, 3, 3)
+
+
 def inject(u: np.ndarray):
     """Make the reference's rand() return exactly the uniforms u (each m * 2^-24)."""
     u = f32(u)
