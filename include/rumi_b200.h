@@ -272,6 +272,21 @@ rumi_status rumi_trace_rays(rumi_scene *scene, int64_t n, const float *rays, int
                             int32_t *prim, int32_t on_device, int64_t *node_visits, int64_t *prim_tests,
                             void *stream);
 
+/* Film output.  rumi_film_tonemap restates Film::Save's conversion
+ * (src/Camera/film.cpp:152-203): each of the film's B,G,R pixel sums is divided by the
+ * square of the film's sampling depth ((int)sqrt(n_samples)), raised to 1 / gamma, scaled
+ * by 255, clamped to [0, 255] and truncated; out holds width*height*bytes_per_pixel bytes
+ * (3 or 4; a fourth byte is 0) in the film's row order.  rumi_film_fireflies restates
+ * FirefliesFiltering (src/Scene/scene.cpp:261-432) on such a buffer: a pixel with a
+ * channel at 255 none of whose neighbours is white (all three channels at 255) becomes the
+ * mean of its neighbours, with the reference's border rules (where those rules reach outside the
+ * image, the reference reads outside its buffer; here such reads give 0).  in and out
+ * must be distinct.  on_device: buffers are device pointers; stream may be NULL. */
+rumi_status rumi_film_tonemap(const float *film, int32_t width, int32_t height, int32_t n_samples, float gamma,
+                              int32_t bytes_per_pixel, uint8_t *out, int32_t on_device, void *stream);
+rumi_status rumi_film_fireflies(const uint8_t *in, int32_t width, int32_t height, int32_t bytes_per_pixel,
+                                uint8_t *out, int32_t on_device, void *stream);
+
 /* Text of the calling thread's last error ("" if none). */
 const char *rumi_last_error_string(void);
 

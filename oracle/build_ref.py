@@ -60,6 +60,28 @@ PATCHES = [
      "if (n2._x == 0.0f && n2._y == 0.0f && n2._z == 0.0f)", "Vector3 has no operator=="),
     ("Scene/scene.cpp", "\t_image->OutputBuffer();\n", "",
      "Film::OutputBuffer is declared nowhere and defined nowhere"),
+    ("Kernel/bmp.h", "\tunsigned long file_size;", "\tuint32_t file_size;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long bitmap_data_offset;", "\tuint32_t bitmap_data_offset;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  bitmap_header_size;", "\tuint32_t  bitmap_header_size;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  width;", "\tuint32_t  width;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  height;", "\tuint32_t  height;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  compression;", "\tuint32_t  compression;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  bitmap_data_size;", "\tuint32_t  bitmap_data_size;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  H_resolution;", "\tuint32_t  H_resolution;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  V_resolution;", "\tuint32_t  V_resolution;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  used_colors;", "\tuint32_t  used_colors;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
+    ("Kernel/bmp.h", "\tunsigned long  important_color;", "\tuint32_t  important_color;",
+     "BMP header fields are 32-bit; unsigned long is 64-bit on LP64 and breaks the header"),
 ]
 
 INCLUDE_RE = re.compile(r'^(\s*#\s*include\s*")([^"]+)(")', re.M)

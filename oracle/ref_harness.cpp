@@ -544,3 +544,36 @@ extern "C" int ref_load_obj(const char *path, const float *m16, int cap, float *
     delete model;
     return n;
 }
+
+// Film::Save (src/Camera/film.cpp:152-203) and FirefliesFiltering (src/Scene/scene.cpp:
+// 261-432) on a caller's pixel sums: writes the reference's BMP into `dir`, reads it back
+// with the reference's LoadBmp (tonemapped bytes, W*H*bpp), runs the fireflies filter on
+// that file and reads its output (filtered bytes).
+#include "Kernel/bmp.h"
+extern "C" int ref_film_save_filter(const char *dir, int width, int height, int bpp, int spp, float gamma,
+                                    const float *film, unsigned char *tonemapped, unsigned char *filtered) {
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd)) || chdir(dir) != 0) return -1;
+    int devnull = open("/dev/null", O_WRONLY), saved = dup(1);
+    fflush(stdout);
+    dup2(devnull, 1);
+    Film *f = new Film(width, height, bpp, spp, gamma);
+    memcpy(f->_pixel_buffer, film, sizeof(float) * width * height * 3);
+    f->Save(0.0f);  // "0.000s.bmp"
+    unsigned int w = 0, h = 0, b = 0;
+    char name[] = "0.000s.bmp";
+    unsigned char *t = LoadBmp(name, &w, &h, &b);
+    memcpy(tonemapped, t, (size_t)width * height * bpp);
+    free(t);
+    FirefliesFiltering(name);
+    char out_name[] = "FirefliesFiltering.bmp";
+    unsigned char *g = LoadBmp(out_name, &w, &h, &b);
+    memcpy(filtered, g, (size_t)width * height * bpp);
+    free(g);
+    delete f;
+    fflush(stdout);
+    dup2(saved, 1);
+    close(saved);
+    close(devnull);
+    return chdir(cwd) == 0 ? 0 : -1;
+}

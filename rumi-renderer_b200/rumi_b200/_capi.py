@@ -84,6 +84,7 @@ class rumi_bvh_info(C.Structure):
 EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "rumi_render", "rumi_render_noalloc",
            "rumi_trace_rays", "rumi_batch_create", "rumi_batch_destroy", "rumi_batch_film_floats",
            "rumi_render_batch", "rumi_forward", "rumi_backward", "rumi_scene_set_albedo", "rumi_scene_set_volume",
+           "rumi_film_tonemap", "rumi_film_fireflies",
            "rumi_last_error_string", "rumi_version",
            "rumi_test_philox", "rumi_test_material_sample", "rumi_test_material_fr", "rumi_test_distance_sample",
            "rumi_test_phase_sample", "rumi_test_camera_rays", "rumi_test_pixel_samples",
@@ -142,6 +143,10 @@ def load(path: str = LIB_PATH):
     L.rumi_test_phase_sample.argtypes = [C.c_int64, vp, C.c_float, vp, vp]
     L.rumi_test_camera_rays.argtypes = [C.POINTER(rumi_camera), C.c_int32, C.c_int32, C.c_int64, vp, vp, vp]
     L.rumi_test_pixel_samples.argtypes = [C.c_int64, vp, C.c_int32, vp, C.c_uint64, vp]
+    L.rumi_film_tonemap.restype = C.c_int
+    L.rumi_film_tonemap.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_int32, vp, C.c_int32, vp]
+    L.rumi_film_fireflies.restype = C.c_int
+    L.rumi_film_fireflies.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, vp, C.c_int32, vp]
     L.rumi_test_read_bandwidth.restype = C.c_int
     L.rumi_test_read_bandwidth.argtypes = [vp, C.c_int64, C.c_int32, vp, C.POINTER(C.c_double)]
     L.rumi_last_error_string.restype = C.c_char_p
