@@ -62,6 +62,8 @@ def test_tonemap_and_fireflies_match_the_reference(tmp_path, spp, gamma, bpp):
     # step lower or higher
     diff = np.abs(t.astype(int) - ref_t.astype(int))
     assert diff.max() <= 1 and (diff > 0).mean() < 0.002, ((diff > 0).mean(), diff.max())
-    # the filter on the reference's own bytes: exact
-    np.testing.assert_array_equal(F.fireflies(ref_t), ref_f)
-    assert (ref_f != ref_t).any()  # some fireflies were removed
+    # the filter on the reference's own bytes: exact in B,G,R (the reference leaves a fourth
+    # byte of its output buffer unwritten; here it keeps the input's)
+    got = F.fireflies(ref_t)
+    np.testing.assert_array_equal(got[..., :3], ref_f[..., :3])
+    assert (ref_f[..., :3] != ref_t[..., :3]).any()  # some fireflies were removed
