@@ -96,6 +96,8 @@ typedef struct {
     float basis[16];      /* Pinhole::_basis_transform, row-major */
     float y_ratio;        /* Pinhole y_ratio (1 / Film aspect in the reference presets) */
     float fov_deg;        /* Pinhole::_fov (the reference constructor fixes 20) */
+    float focal_distance; /* Pinhole::DepthOfField (pinhole.cpp:88-94): > 0 turns on the thin lens */
+    float lens_radius;
 } rumi_camera;
 
 typedef struct {

@@ -37,10 +37,11 @@ rumi_status rumi_test_distance_sample(const float *sigma_s, const float *sigma_a
  * Henyey-Greenstein otherwise).  d: n*3, u: n*2.  out n*4: wi.xyz, pdf. */
 rumi_status rumi_test_phase_sample(int64_t n, const float *d, float g, const float *u, float *out);
 
-/* Pinhole::CastViewRay (src/Camera/pinhole.cpp:97-136).  pix: n*2 (w, h), smp: n*2.
- * out n*6: o.xyz, d.xyz. */
+/* Pinhole::CastViewRay (src/Camera/pinhole.cpp:97-136).  pix: n*2 (w, h), smp: n*2,
+ * lens_u: n*2 lens uniforms (radius, angle) used when cam->focal_distance > 0, or NULL
+ * for zeros.  out n*6: o.xyz, d.xyz. */
 rumi_status rumi_test_camera_rays(const rumi_camera *cam, int32_t width, int32_t height, int64_t n, const int32_t *pix,
-                                  const float *smp, float *out);
+                                  const float *smp, const float *lens_u, float *out);
 
 /* The pixel sampler: sample index s of `spp` in pixel `pixel` for `seed`.  out n*2. */
 rumi_status rumi_test_pixel_samples(int64_t n, const int32_t *s, int32_t spp, const int64_t *pixel, uint64_t seed,

@@ -240,6 +240,11 @@ extern "C" void ref_set_camera(void *h, const float *pos, const float *basis16, 
     rs->scene->_camera = cam;
 }
 
+// Pinhole::DepthOfField on the scene's camera (the BDPT constructor turns it off again).
+extern "C" void ref_set_camera_dof(void *h, float focal_distance, float lens_radius) {
+    ((RefScene *)h)->scene->_camera->DepthOfField(focal_distance, lens_radius);
+}
+
 // integrator: 0 PathTracer(max_depth=a), 1 BidirectionalPathTracer(nL=a, nE=b).
 // Sample sets are generated after seeding, as Scene::Build does once per frame.
 extern "C" int ref_finalize(void *h, int integrator, int a, int b, unsigned long long seed) {
@@ -500,6 +505,36 @@ extern "C" void ref_camera_cast(const float *pos, const float *basis16, float y_
     cam.CastViewRay(W, H, w, h, Point2(sx, sy), &o, &d, &cost, &pdf);
     out[0] = o._x; out[1] = o._y; out[2] = o._z; out[3] = d._x; out[4] = d._y; out[5] = d._z;
     out[6] = cost; out[7] = pdf;
+}
+
+// Pinhole::CastViewRay with depth of field: the harness generator is seeded with
+// `seed` before the call (and restored after it), and the two RandomFloat() values the call draws (lens radius, then angle) are
+// drawn again from the same seed and reported.  out[10]: o.xyz, d.xyz, costheta, pdf_w,
+// u1, u2.
+extern "C" void ref_camera_cast_dof(const float *pos, const float *basis16, float y_ratio, float fov_deg,
+                                    float focal_distance, float lens_radius, int W, int H, int w, int h, float sx,
+                                    float sy, unsigned seed, float *out) {
+    Mat4x4 m;
+    for (int i = 0; i < 16; ++i) m._m[i] = basis16[i];
+    Pinhole cam(P3(pos), m, y_ratio);
+    if (fov_deg > 0.0f) {
+        cam._fov = fov_deg;
+        cam._tanfov = tan(PI / 180.f * cam._fov * 0.5f);
+        cam._film_area = (2.0f * cam._tanfov) * (2.0f * cam._tanfov * cam._y_ratio);
+    }
+    cam.DepthOfField(focal_distance, lens_radius);
+    const uint64_t saved = g_rng_state;
+    ref_seed(seed);
+    const float u1 = RandomFloat();
+    const float u2 = RandomFloat();
+    ref_seed(seed);
+    Point3 o;
+    Vector3 d;
+    float cost = 0.0f, pdf = 0.0f;
+    cam.CastViewRay(W, H, w, h, Point2(sx, sy), &o, &d, &cost, &pdf);
+    out[0] = o._x; out[1] = o._y; out[2] = o._z; out[3] = d._x; out[4] = d._y; out[5] = d._z;
+    g_rng_state = saved;
+    out[6] = cost; out[7] = pdf; out[8] = u1; out[9] = u2;
 }
 
 // Reads back Pinhole::_tanfov / _film_area of a scene's camera.  out[2].

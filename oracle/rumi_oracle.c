@@ -96,6 +96,7 @@ typedef struct {
     float position[3];
     float basis[16];
     float y_ratio, fov_deg;
+    float focal_distance, lens_radius;
 } orc_camera;
 
 typedef struct {
@@ -630,8 +631,13 @@ static void pixel_sample(int s, int spp, long long pixel, const uint32_t key[2],
     }
 }
 
-/* Pinhole::CastViewRay, src/Camera/pinhole.cpp:97-136 (constructor values :30-51) */
-static void camera_ray(const orc_camera *c, int W, int H, int w, int h, float sx, float sy, V3 *o, V3 *d) {
+/* Pinhole::CastViewRay, src/Camera/pinhole.cpp:97-136 (constructor values :30-51); with
+ * a focal distance (Pinhole::DepthOfField, :88-95) the origin is a point of the lens disk
+ * drawn from the uniforms lu1 (radius) and lu2 (angle, PI a double literal) and the ray
+ * aims at the pinhole ray's point on the focal plane.  _up and _right are the basis
+ * applied to (0,1,0) and (1,0,0) with its translation column added, like _dir. */
+static void camera_ray(const orc_camera *c, int W, int H, int w, int h, float sx, float sy, float lu1, float lu2,
+                       V3 *o, V3 *d) {
     float fov = c->fov_deg > 0.0f ? c->fov_deg : 20.0f;
     float tanfov = (float)tan(PI_D / 180.f * fov * 0.5f);
     float hw = W * 0.5f, hh = H * 0.5f;
@@ -642,11 +648,40 @@ static void camera_ray(const orc_camera *c, int W, int H, int w, int h, float sx
     *d = v3(m[0] * l.x + m[1] * l.y + m[2] * l.z + m[3], m[4] * l.x + m[5] * l.y + m[6] * l.z + m[7],
             m[8] * l.x + m[9] * l.y + m[10] * l.z + m[11]);
     *o = fv(c->position);
+    if (c->focal_distance > 0.0f) {
+        V3 p = fv(c->position);
+        float t = c->focal_distance / l.z;
+        V3 fp = v3(p.x + d->x * t, p.y + d->y * t, p.z + d->z * t);
+        V3 up = v3(m[1] + m[3], m[5] + m[7], m[9] + m[11]);
+        V3 right = v3(m[0] + m[3], m[4] + m[7], m[8] + m[11]);
+        float r = sqrtf(lu1) * c->lens_radius;
+        float theta = (float)((double)(lu2 * 2.0f) * PI_D);
+        float sn = sinf(theta), cs = cosf(theta);
+        V3 cp = v3(p.x + up.x * r * sn + right.x * r * cs, p.y + up.y * r * sn + right.y * r * cs,
+                   p.z + up.z * r * sn + right.z * r * cs);
+        *o = cp;
+        *d = normalize(v3(fp.x - cp.x, fp.y - cp.y, fp.z - cp.z));
+    }
+}
+
+/* The two lens uniforms of a camera ray: the path's Philox stream at bounce counter
+ * 0x7FFFFFFF, which no vertex uses. */
+static void lens_u(const orc_camera *c, uint64_t path, const uint32_t key[2], float *lu1, float *lu2) {
+    float u[4] = {0, 0, 0, 0};
+    if (c->focal_distance > 0.0f) path_u(path, 0x7FFFFFFFu, 0, key, u);
+    *lu1 = u[0];
+    *lu2 = u[1];
 }
 
 /* ------------------------------------------------------------------ path tracer
  * PathTracer::Trace(w, h, ...) (src/Integrator/pathtracer.cpp:117-354) in forward form:
  * L = sum_k beta_k direct_k, beta_{k+1} = beta_k vol_k fr_k cos_k / Average(pdf_wi_k pdf_path_k). */
+/* Debug record of one path's extension rays (orc_path_rays): o, in_object, d, tmax;
+ * the closest hit's t and primitive. */
+static float *g_dbg_rays, *g_dbg_t;
+static int32_t *g_dbg_prim;
+static int g_dbg_n;
+
 static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, const uint32_t key[2], V3 o, V3 d) {
     V3 beta = v3(1, 1, 1), L = v3(0, 0, 0);
     int le = 1, inobj = 0;
@@ -663,6 +698,14 @@ static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, cons
         Ray ray = {o, d, 3.402823466e+38f, inobj};
         Hit h = closest(s, &ray, 0);
         int hit = h.t > 0.0f;
+        if (g_dbg_rays) {
+            float *q = g_dbg_rays + 8 * g_dbg_n;
+            q[0] = o.x; q[1] = o.y; q[2] = o.z; q[3] = (float)inobj;
+            q[4] = d.x; q[5] = d.y; q[6] = d.z; q[7] = 3.402823466e+38f;
+            g_dbg_t[g_dbg_n] = h.t;
+            g_dbg_prim[g_dbg_n] = hit ? h.id : -1;
+            ++g_dbg_n;
+        }
         int cont = 0;
         V3 nxo = o, nxd = d;
         int nle = 0, nin = 0;
@@ -802,6 +845,27 @@ static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, cons
     return L;
 }
 
+/* One path of orc_render_pt (pixel, sample k): its radiance (out_L[3], r g b) and its
+ * extension rays, written to rays (max_depth * 8), t and prim; returns their count. */
+int orc_path_rays(const orc_scene_desc *s, int max_depth, int spp, uint64_t seed, long long pixel, int k,
+                  float *out_L, float *rays, float *t, int32_t *prim) {
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32) ^ 0x5851F42Du};
+    int W = s->width, H = s->height;
+    int w = (int)(pixel % W), h = (int)(pixel / W);
+    float sx, sy, lu1, lu2;
+    V3 o, d;
+    (void)H;
+    pixel_sample(k, spp, pixel, key, &sx, &sy);
+    lens_u(&s->camera, (uint64_t)(pixel * spp + k), key, &lu1, &lu2);
+    camera_ray(&s->camera, W, s->height, w, h, sx, sy, lu1, lu2, &o, &d);
+    g_dbg_rays = rays; g_dbg_t = t; g_dbg_prim = prim; g_dbg_n = 0;
+    V3 L = trace_path(s, max_depth, (uint64_t)(pixel * spp + k), key, o, d);
+    int n = g_dbg_n;
+    g_dbg_rays = NULL; g_dbg_t = NULL; g_dbg_prim = NULL;
+    out_L[0] = L.x; out_L[1] = L.y; out_L[2] = L.z;
+    return n;
+}
+
 /* Renders rows [row0, row1): film receives B,G,R sums per pixel (Film::_pixel_buffer
  * layout, src/Camera/film.cpp:83-97); NaN samples dropped and counted like
  * Scene::Rendering (src/Scene/scene.cpp:229-241). */
@@ -818,7 +882,9 @@ long long orc_render_pt(const orc_scene_desc *s, int max_depth, int spp, uint64_
                 float sx, sy;
                 pixel_sample(k, spp, pixel, key, &sx, &sy);
                 V3 o, d;
-                camera_ray(&s->camera, W, H, w, h, sx, sy, &o, &d);
+                float lu1, lu2;
+                lens_u(&s->camera, (uint64_t)(pixel * spp + k), key, &lu1, &lu2);
+                camera_ray(&s->camera, W, H, w, h, sx, sy, lu1, lu2, &o, &d);
                 V3 L = trace_path(s, max_depth, (uint64_t)(pixel * spp + k), key, o, d);
                 if (isnan3(L))
                     ++nan;
@@ -869,9 +935,10 @@ void orc_phase_sample(const float *d, float g, float u1, float u2, float *out) {
 float orc_hg_eval(float cos_theta, float g) { return hg_eval(cos_theta, g); }
 
 /* out[6]: o.xyz, d.xyz */
-void orc_camera_ray(const orc_camera *c, int W, int H, int w, int h, float sx, float sy, float *out) {
+void orc_camera_ray(const orc_camera *c, int W, int H, int w, int h, float sx, float sy, float lu1, float lu2,
+                    float *out) {
     V3 o, d;
-    camera_ray(c, W, H, w, h, sx, sy, &o, &d);
+    camera_ray(c, W, H, w, h, sx, sy, lu1, lu2, &o, &d);
     out[0] = o.x; out[1] = o.y; out[2] = o.z; out[3] = d.x; out[4] = d.y; out[5] = d.z;
 }
 

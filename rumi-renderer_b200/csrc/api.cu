@@ -224,6 +224,24 @@ void fill_dev_volume(DevVolume &dv, const rumi_volume &v) {
     dv.g = v.g;
 }
 
+// Pinhole's constructor (src/Camera/pinhole.cpp:30-49) with _fov set, and DepthOfField.
+// _dir, _up and _right are Mat4x4 * Vector3, which adds the matrix's translation column.
+void fill_dev_camera(DevCamera &dc, const rumi_camera &c) {
+    memset(&dc, 0, sizeof(dc));
+    dc.p = make_float3(c.position[0], c.position[1], c.position[2]);
+    for (int k = 0; k < 12; ++k) dc.m[k] = c.basis[k];
+    const float fov = c.fov_deg > 0.0f ? c.fov_deg : 20.0f;
+    dc.tanfov = (float)std::tan(3.14159265358979323846 / 180.f * fov * 0.5f);
+    dc.plane_dist = 1.0f;
+    dc.y_ratio = c.y_ratio;
+    dc.film_area = (2.0f * dc.tanfov) * (2.0f * dc.tanfov * c.y_ratio);
+    dc.dir = make_float3(c.basis[2] + c.basis[3], c.basis[6] + c.basis[7], c.basis[10] + c.basis[11]);
+    dc.up = make_float3(c.basis[1] + c.basis[3], c.basis[5] + c.basis[7], c.basis[9] + c.basis[11]);
+    dc.right = make_float3(c.basis[0] + c.basis[3], c.basis[4] + c.basis[7], c.basis[8] + c.basis[11]);
+    dc.focal_distance = c.focal_distance;
+    dc.lens_radius = c.lens_radius;
+}
+
 void pack_albedo(const float *a_dev, int n, float4 *out, cudaStream_t s) {
     const int grid = n < 256 * 1184 ? (n + 255) / 256 : 1184;
     if (n > 0) pack_albedo_kernel<<<grid, 256, 0, s>>>(a_dev, n, out);
@@ -315,18 +333,7 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     // volume
     if (d->volume.present) fill_dev_volume(ds.volume, d->volume);
     // camera
-    {
-        const rumi_camera &c = d->camera;
-        DevCamera &dc = ds.camera;
-        dc.p = make_float3(c.position[0], c.position[1], c.position[2]);
-        for (int k = 0; k < 12; ++k) dc.m[k] = c.basis[k];
-        const float fov = c.fov_deg > 0.0f ? c.fov_deg : 20.0f;
-        dc.tanfov = (float)std::tan(3.14159265358979323846 / 180.f * fov * 0.5f);
-        dc.plane_dist = 1.0f;
-        dc.y_ratio = c.y_ratio;
-        dc.film_area = (2.0f * dc.tanfov) * (2.0f * dc.tanfov * c.y_ratio);
-        dc.dir = make_float3(c.basis[2] + c.basis[3], c.basis[6] + c.basis[7], c.basis[10] + c.basis[11]);
-    }
+    fill_dev_camera(ds.camera, d->camera);
     // ---- uploads
     float *d_tri_v = nullptr, *d_tri_n = nullptr, *d_alb = nullptr;
     int *d_rect_em = nullptr, *d_tri_m = nullptr;

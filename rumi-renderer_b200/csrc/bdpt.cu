@@ -141,7 +141,7 @@ RUMI_D bool film_plane_pixel(const BdLaunch &P, float3 pos, int &wi, int &hi) {
 
 // Hit -> vertex fields (position, normal, material).
 RUMI_D void record_hit(const DevScene &S, const HitRec &h, float3 o, float3 d, BVert &v) {
-    v.p = o + d * h.t;
+    v.p = rn_madd(o, d, h.t);
     v.prim = h.id;
     v.mat = prim_material(S, h.id);
     v.n = surface_normal(S, h.id, h.back != 0, h.u, h.v, o, v.p, S.materials[v.mat]);
@@ -627,7 +627,13 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
     // eye subpath start (Pinhole::CastViewRay, pinhole.cpp:97-136)
     const float2 smp = pixel_sample(sidx, P.spp, P.grid_d, P.square != 0, pixel, P.k0, P.k1);
     float3 eo, ed;
-    camera_ray(S.camera, W, H, pw_, ph_, smp.x, smp.y, eo, ed);
+    {
+        // the reference's BDPT turns depth of field off when it is constructed
+        // (BidirectionalPathTracer's constructor, bidirectionalpathtracer.cpp:56)
+        DevCamera pin = S.camera;
+        pin.focal_distance = 0.0f;
+        camera_ray(pin, W, H, pw_, ph_, smp.x, smp.y, 0.0f, 0.0f, eo, ed);
+    }
     {
         const DevCamera &c = S.camera;
         const float hw = W * 0.5f, hh = H * 0.5f;

@@ -71,8 +71,13 @@ RUMI_D float2 pixel_sample(int s, int spp, int grid_d, bool square, long long pi
     return r;
 }
 
-// Pinhole::CastViewRay (src/Camera/pinhole.cpp:97-136) without depth of field.
-RUMI_D void camera_ray(const DevCamera &c, int W, int H, int w, int h, float sx, float sy, float3 &o, float3 &d) {
+// Pinhole::CastViewRay (src/Camera/pinhole.cpp:97-136).  With a focal distance set
+// (Pinhole::DepthOfField, pinhole.cpp:88-95) the origin moves to a point of the lens disk,
+// radius sqrt(lu1) * lens_radius and angle lu2 * 2 * PI (the product taken in double as
+// the reference's PI is a double literal), and the ray aims at the point of the focal
+// plane that the pinhole ray reaches.
+RUMI_D void camera_ray(const DevCamera &c, int W, int H, int w, int h, float sx, float sy, float lu1, float lu2,
+                       float3 &o, float3 &d) {
     // correctly rounded operations in the reference's order (no FMA contraction)
     const float half_w = __fmul_rn((float)W, 0.5f), half_h = __fmul_rn((float)H, 0.5f);
     const float x = -__fmul_rn(__fdiv_rn(__fadd_rn(__fsub_rn((float)w, half_w), sx), half_w), c.tanfov);
@@ -86,6 +91,28 @@ RUMI_D void camera_ray(const DevCamera &c, int W, int H, int w, int h, float sx,
     };
     d = mk3(row(0), row(1), row(2));
     o = c.p;
+    if (c.focal_distance > 0.0f) {
+        const float t = __fdiv_rn(c.focal_distance, l.z);
+        const float3 fp = mk3(__fadd_rn(c.p.x, __fmul_rn(d.x, t)), __fadd_rn(c.p.y, __fmul_rn(d.y, t)),
+                              __fadd_rn(c.p.z, __fmul_rn(d.z, t)));
+        const float r = __fmul_rn(__fsqrt_rn(lu1), c.lens_radius);
+        const float theta = (float)__dmul_rn((double)__fmul_rn(lu2, 2.0f), 3.14159265358979323846);
+        const float sn = sinf(theta), cs = cosf(theta);
+        const float3 a = mk3(__fmul_rn(__fmul_rn(c.up.x, r), sn), __fmul_rn(__fmul_rn(c.up.y, r), sn),
+                             __fmul_rn(__fmul_rn(c.up.z, r), sn));
+        const float3 b = mk3(__fmul_rn(__fmul_rn(c.right.x, r), cs), __fmul_rn(__fmul_rn(c.right.y, r), cs),
+                             __fmul_rn(__fmul_rn(c.right.z, r), cs));
+        o = mk3(__fadd_rn(__fadd_rn(c.p.x, a.x), b.x), __fadd_rn(__fadd_rn(c.p.y, a.y), b.y),
+                __fadd_rn(__fadd_rn(c.p.z, a.z), b.z));
+        d = normalize_ref(mk3(__fsub_rn(fp.x, o.x), __fsub_rn(fp.y, o.y), __fsub_rn(fp.z, o.z)));
+    }
+}
+
+// The two lens uniforms of a camera ray: their own Philox stream of the path (bounce
+// counter 0x7FFFFFFF, which no vertex of a path or subpath uses).
+RUMI_D float2 lens_uniforms(uint64_t path, uint32_t k0, uint32_t k1) {
+    const Uniform4 u = path_uniforms(path, 0x7FFFFFFFu, 0u, k0, k1);
+    return make_float2(u.u[0], u.u[1]);
 }
 
 }  // namespace rumi

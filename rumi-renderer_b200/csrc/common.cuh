@@ -60,6 +60,17 @@ RUMI_D float3 rn_madd(float3 o, float3 d, float t) {  // o + d * t, two rounding
                __fadd_rn(o.z, __fmul_rn(d.z, t)));
 }
 
+// n0 (1 - u - v) + n1 u + n2 v, one rounding per operation in that order (the shading
+// normal of Triangle::Intersect, triangle.cpp:111).  The last bit matters: the
+// reference's tangent frame takes a special branch only for normals of exactly
+// (0, +-1, 0), and the two branches mirror the sampled directions about the frame.
+RUMI_D float3 bary_ref(float3 n0, float3 n1, float3 n2, float u, float v) {
+    const float w = __fsub_rn(__fsub_rn(1.0f, u), v);
+    return mk3(__fadd_rn(__fadd_rn(__fmul_rn(n0.x, w), __fmul_rn(n1.x, u)), __fmul_rn(n2.x, v)),
+               __fadd_rn(__fadd_rn(__fmul_rn(n0.y, w), __fmul_rn(n1.y, u)), __fmul_rn(n2.y, v)),
+               __fadd_rn(__fadd_rn(__fmul_rn(n0.z, w), __fmul_rn(n1.z, u)), __fmul_rn(n2.z, v)));
+}
+
 // ------------------------------------------------------------- Philox4x32-10
 // Counter-based generator of Salmon, Moraes, Dror and Shaw, "Parallel random numbers:
 // as easy as 1, 2, 3" (SC 2011): 10 rounds of two 32x32->64 multiplies with a Weyl key

@@ -137,7 +137,7 @@ __global__ void pt_generate(PtLaunch P) {
     // one call site of the sampler and camera for both forms, so a batched scene's rays
     // are bit-identical to the single-scene ones
     const DevScene *S = &P.s;
-    long long pixel;
+    long long pixel, path = P.path0 + j;
     int s, spp = P.spp, gd = P.grid_d;
     bool square = P.square != 0;
     uint32_t k0 = P.k0, k1 = P.k1;
@@ -147,6 +147,7 @@ __global__ void pt_generate(PtLaunch P) {
         S = &P.scenes[k];
         spp = P.scene_spp[k];
         const long long local = g - P.scene_path0[k];
+        path = local;
         pixel = local / spp;
         s = (int)(local % spp);
         gd = isqrt_floor(spp);
@@ -162,7 +163,8 @@ __global__ void pt_generate(PtLaunch P) {
     const int w = (int)(pixel % W), h = (int)(pixel / W);
     const float2 smp = pixel_sample(s, spp, gd, square, pixel, k0, k1);
     float3 o, d;
-    camera_ray(S->camera, W, S->height, w, h, smp.x, smp.y, o, d);
+    const float2 lu = S->camera.focal_distance > 0.0f ? lens_uniforms((uint64_t)path, k0, k1) : make_float2(0.f, 0.f);
+    camera_ray(S->camera, W, S->height, w, h, smp.x, smp.y, lu.x, lu.y, o, d);
     P.ray_o[0][j] = make_float4(o.x, o.y, o.z, __int_as_float(j));
     P.ray_d[0][j] = make_float4(d.x, d.y, d.z, FLT_MAX);
     P.beta[j] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -480,14 +482,14 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
             const bool back = code < 0;
             const int mi = prim_material(S, id);
             const DevMaterial m = S.materials[mi];
-            float3 p = o + d * t;
+            float3 p = rn_madd(o, d, t);
             float3 nrm;
             float3 albedo = m.rgb;
             if (id < S.n_tris) {
                 const float4 n0 = __ldg(&S.tri_shade[3 * id]), n1 = __ldg(&S.tri_shade[3 * id + 1]),
                              n2 = __ldg(&S.tri_shade[3 * id + 2]);
                 const float u = hv.z, v = hv.w;
-                nrm = f4xyz(n0) * (1.0f - u - v) + f4xyz(n1) * u + f4xyz(n2) * v;  // triangle.cpp:111 (Q3)
+                nrm = bary_ref(f4xyz(n0), f4xyz(n1), f4xyz(n2), u, v);  // triangle.cpp:111 (Q3)
                 if (back && material_opaque(m)) nrm = -nrm;
                 if (S.tri_albedo) albedo = f4xyz(__ldg(&S.tri_albedo[id]));
                 if (ADJ && P.g_albedo && S.tri_albedo && m.type == MAT_MATTE) {

@@ -60,6 +60,7 @@ unsigned long long *pt_batch_stats_ptr(void *ws, long long wave_paths);
 
 void set_error(const std::string &msg);
 void fill_dev_volume(DevVolume &dv, const rumi_volume &v);
+void fill_dev_camera(DevCamera &dc, const rumi_camera &c);
 void pack_albedo(const float *a_dev, int n, float4 *out, cudaStream_t s);
 rumi_status cuda_status(cudaError_t e, const char *what);
 

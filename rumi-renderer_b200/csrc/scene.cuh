@@ -95,6 +95,8 @@ struct DevCamera {
     float m[12];              // first three rows of Pinhole::_basis_transform
     float tanfov, y_ratio, film_area, plane_dist;
     float3 dir;               // _basis_transform * (0,0,1)
+    float3 up, right;         // _basis_transform * (0,1,0), * (1,0,0) (translation column added)
+    float focal_distance, lens_radius;  // Pinhole::DepthOfField; focal_distance > 0: thin lens
 };
 
 struct DevScene {

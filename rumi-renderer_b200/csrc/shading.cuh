@@ -506,7 +506,7 @@ RUMI_D float3 surface_normal(const DevScene &S, int id, bool back, float u, floa
     if (id < S.n_tris) {
         const float4 n0 = __ldg(&S.tri_shade[3 * id]), n1 = __ldg(&S.tri_shade[3 * id + 1]),
                      n2 = __ldg(&S.tri_shade[3 * id + 2]);
-        float3 nrm = f4xyz(n0) * (1.0f - u - v) + f4xyz(n1) * u + f4xyz(n2) * v;
+        float3 nrm = bary_ref(f4xyz(n0), f4xyz(n1), f4xyz(n2), u, v);
         if (back && material_opaque(m)) nrm = -nrm;
         return nrm;
     }

@@ -105,11 +105,13 @@ __global__ void k_phase(int64_t n, const float *d, float g, const float *u, floa
     out[4 * i] = w.x; out[4 * i + 1] = w.y; out[4 * i + 2] = w.z; out[4 * i + 3] = pdf;
 }
 
-__global__ void k_camera(DevCamera c, int W, int H, int64_t n, const int32_t *pix, const float *smp, float *out) {
+__global__ void k_camera(DevCamera c, int W, int H, int64_t n, const int32_t *pix, const float *smp, const float *lens_u,
+                         float *out) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     float3 o, d;
-    camera_ray(c, W, H, pix[2 * i], pix[2 * i + 1], smp[2 * i], smp[2 * i + 1], o, d);
+    const float lu1 = lens_u ? lens_u[2 * i] : 0.0f, lu2 = lens_u ? lens_u[2 * i + 1] : 0.0f;
+    camera_ray(c, W, H, pix[2 * i], pix[2 * i + 1], smp[2 * i], smp[2 * i + 1], lu1, lu2, o, d);
     float *q = out + 6 * i;
     q[0] = o.x; q[1] = o.y; q[2] = o.z; q[3] = d.x; q[4] = d.y; q[5] = d.z;
 }
@@ -227,20 +229,18 @@ rumi_status rumi_test_phase_sample(int64_t n, const float *d, float g, const flo
 }
 
 rumi_status rumi_test_camera_rays(const rumi_camera *cam, int32_t width, int32_t height, int64_t n, const int32_t *pix,
-                                  const float *smp, float *out) {
+                                  const float *smp, const float *lens_u, float *out) {
     if (!cam || n < 0 || width <= 0 || height <= 0) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
     DevCamera dc;
-    memset(&dc, 0, sizeof(dc));
-    dc.p = make_float3(cam->position[0], cam->position[1], cam->position[2]);
-    for (int k = 0; k < 12; ++k) dc.m[k] = cam->basis[k];
-    const float fov = cam->fov_deg > 0.0f ? cam->fov_deg : 20.0f;
-    dc.tanfov = (float)std::tan(3.14159265358979323846 / 180.f * fov * 0.5f);
-    dc.plane_dist = 1.0f;
-    dc.y_ratio = cam->y_ratio;
-    DevBuf a, b, o;
+    fill_dev_camera(dc, *cam);
+    DevBuf a, b, l, o;
     rumi_status st;
-    if ((st = to_dev(a, pix, 2 * n)) || (st = to_dev(b, smp, 2 * n)) || (st = to_dev<float>(o, nullptr, 6 * n))) return st;
-    if (n) k_camera<<<blocks(n), 256>>>(dc, width, height, n, (int32_t *)a.p, (float *)b.p, (float *)o.p);
+    if ((st = to_dev(a, pix, 2 * n)) || (st = to_dev(b, smp, 2 * n)) || (st = to_dev(l, lens_u, 2 * n)) ||
+        (st = to_dev<float>(o, nullptr, 6 * n)))
+        return st;
+    if (n)
+        k_camera<<<blocks(n), 256>>>(dc, width, height, n, (int32_t *)a.p, (float *)b.p, (const float *)l.p,
+                                     (float *)o.p);
     return from_dev(out, o, 6 * n);
 }
 

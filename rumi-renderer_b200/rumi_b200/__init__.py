@@ -81,6 +81,8 @@ def build_desc(fs: FlatScene):
     d.camera.basis = _capi.f16(*np.asarray(cam.basis, np.float32).reshape(16))
     d.camera.y_ratio = cam.y_ratio
     d.camera.fov_deg = cam.fov
+    d.camera.focal_distance = float(getattr(cam, "focal_distance", 0.0))
+    d.camera.lens_radius = float(getattr(cam, "lens_radius", 0.0))
     return d, keep
 
 

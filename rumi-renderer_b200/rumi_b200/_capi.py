@@ -30,7 +30,8 @@ class rumi_volume(C.Structure):
 
 
 class rumi_camera(C.Structure):
-    _fields_ = [("position", f3), ("basis", f16), ("y_ratio", C.c_float), ("fov_deg", C.c_float)]
+    _fields_ = [("position", f3), ("basis", f16), ("y_ratio", C.c_float), ("fov_deg", C.c_float),
+                ("focal_distance", C.c_float), ("lens_radius", C.c_float)]
 
 
 FP = C.POINTER(C.c_float)
@@ -141,7 +142,7 @@ def load(path: str = LIB_PATH):
     L.rumi_test_material_fr.argtypes = [C.POINTER(rumi_material), C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.rumi_test_distance_sample.argtypes = [vp, vp, C.c_int64, vp, vp, vp, vp]
     L.rumi_test_phase_sample.argtypes = [C.c_int64, vp, C.c_float, vp, vp]
-    L.rumi_test_camera_rays.argtypes = [C.POINTER(rumi_camera), C.c_int32, C.c_int32, C.c_int64, vp, vp, vp]
+    L.rumi_test_camera_rays.argtypes = [C.POINTER(rumi_camera), C.c_int32, C.c_int32, C.c_int64, vp, vp, vp, vp]
     L.rumi_test_pixel_samples.argtypes = [C.c_int64, vp, C.c_int32, vp, C.c_uint64, vp]
     L.rumi_film_tonemap.restype = C.c_int
     L.rumi_film_tonemap.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_int32, vp, C.c_int32, vp]

@@ -208,11 +208,15 @@ def matmul16(a, b) -> np.ndarray:
 @dataclass
 class Pinhole:
     """``Pinhole(position, basis_transform, y_ratio)``; the reference fixes fov at 20
-    degrees (src/Camera/pinhole.cpp:36) -- ``fov`` sets the same public member."""
+    degrees (src/Camera/pinhole.cpp:36) -- ``fov`` sets the same public member.
+    ``focal_distance`` / ``lens_radius``: ``Pinhole::DepthOfField`` (thin lens when the
+    focal distance is > 0)."""
     position: Sequence[float]
     basis: np.ndarray = field(default_factory=identity16)
     y_ratio: float = 1.0
     fov: float = 20.0
+    focal_distance: float = 0.0
+    lens_radius: float = 0.0
 
 
 @dataclass

@@ -57,6 +57,16 @@ def cornell_camera() -> Pinhole:
     return Pinhole((0.5, 0.5, -1.4), identity16(), 1.0, fov=40.0)
 
 
+def cornell_dof_pt(width: int = 256, height: int = 256, spp: int = 16, max_depth: int = 8,
+                   focal_distance: float = 2.0, lens_radius: float = 0.08) -> Scene:
+    """``cornell_pt`` seen through a thin lens (``Pinhole::DepthOfField``): in focus at the
+    white sphere's depth (z = 0.6), the back wall and the mirror sphere blurred."""
+    sc = cornell_pt(width, height, spp, max_depth)
+    sc.camera.focal_distance = focal_distance
+    sc.camera.lens_radius = lens_radius
+    return sc
+
+
 def cornell_pt(width: int = 256, height: int = 256, spp: int = 16, max_depth: int = 8) -> Scene:
     """Plain path tracer, Cornell box: 10 wall triangles, 0.25 x 0.25 quad light at y=0.999
     with radiance (17,12,4), a white Lambertian sphere r=0.15 at (0.3,0.15,0.6), a mirror

@@ -186,6 +186,36 @@ def camera_fixture(path, rng):
     print(path)
 
 
+def camera_dof_fixture(path, rng):
+    """Thin-lens camera rays of the reference (Pinhole::DepthOfField + CastViewRay) under
+    a rotated basis with a translation column, which the reference also adds to _up and
+    _right; each ray reports the two RandomFloat() values it drew."""
+    L = refimpl.lib()
+    N = 256
+    ax, ay = 0.3, -0.45
+    rx = np.array([[1, 0, 0], [0, np.cos(ax), -np.sin(ax)], [0, np.sin(ax), np.cos(ax)]])
+    ry = np.array([[np.cos(ay), 0, np.sin(ay)], [0, 1, 0], [-np.sin(ay), 0, np.cos(ay)]])
+    basis = np.eye(4)
+    basis[:3, :3] = ry @ rx
+    basis[:3, 3] = (0.02, -0.03, 0.01)
+    basis = refimpl.f32(basis.reshape(16))
+    pos = refimpl.f32([0.4, 0.6, -1.2])
+    W, H = 80, 60
+    pix = np.stack([rng.integers(0, W, N), rng.integers(0, H, N)], 1).astype(np.int32)
+    smp = u24(rng, (N, 2))
+    focal = rng.uniform(0.5, 5.0, N).astype(F32)
+    lens = rng.uniform(0.01, 0.3, N).astype(F32)
+    seeds = rng.integers(1, 1 << 30, N).astype(np.uint32)
+    out = np.zeros((N, 10), F32)
+    for i in range(N):
+        L.ref_camera_cast_dof(refimpl.P(pos), refimpl.P(basis), 0.75, 35.0, float(focal[i]), float(lens[i]), W, H,
+                              int(pix[i, 0]), int(pix[i, 1]), float(smp[i, 0]), float(smp[i, 1]), int(seeds[i]),
+                              refimpl.P(out[i]))
+    np.savez_compressed(path, pos=pos, basis=basis, y_ratio=np.float32(0.75), fov=np.float32(35.0), W=W, H=H,
+                        pix=pix, smp=smp, focal=focal, lens=lens, out=out)
+    print(path)
+
+
 def image_fixture(path, size=32, spp=16, depth=8, seeds=64, scene=None):
     """Reference renders of a workload at a small size: per-pixel mean radiance over
     `seeds` independent frames and its standard error (spread across frames, which
@@ -307,6 +337,10 @@ def obj_fixture(path):
 
 
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "dof":
+        camera_dof_fixture(os.path.join(HERE, "camera_dof.npz"), np.random.default_rng(88))
+        image_fixture(os.path.join(HERE, "image_cornell_dof32.npz"), scene=scenes.cornell_dof_pt(32, 32, 16, 8))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "obj":
         obj_fixture(os.path.join(HERE, "obj_loader.npz"))
         return

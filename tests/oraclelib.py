@@ -35,7 +35,8 @@ def lib():
         L.orc_phase_sample.argtypes = [FP, C.c_float, C.c_float, C.c_float, FP]
         L.orc_hg_eval.restype = C.c_float
         L.orc_hg_eval.argtypes = [C.c_float, C.c_float]
-        L.orc_camera_ray.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, FP]
+        L.orc_camera_ray.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                     C.c_float, FP]
         L.orc_pixel_sample.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_uint64, FP]
         L.orc_perm.restype = C.c_int
         L.orc_perm.argtypes = [C.c_int, C.c_int, C.c_uint32]
@@ -95,7 +96,7 @@ class OracleScene:
                                   self.height if row1 is None else row1, P(film))
         return film, int(nan)
 
-    def camera_ray(self, w, h, sx, sy):
+    def camera_ray(self, w, h, sx, sy, lu1=0.0, lu2=0.0):
         out = np.zeros(6, np.float32)
-        lib().orc_camera_ray(C.byref(self.desc.camera), self.width, self.height, w, h, sx, sy, P(out))
+        lib().orc_camera_ray(C.byref(self.desc.camera), self.width, self.height, w, h, sx, sy, lu1, lu2, P(out))
         return out

@@ -59,6 +59,9 @@ def lib():
         L.ref_camera_cast.argtypes = [fp, fp, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_float, C.c_float, fp]
         L.ref_camera_params.argtypes = [C.c_void_p, fp]
+        L.ref_camera_cast_dof.argtypes = [fp, fp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int,
+                                          C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint, fp]
+        L.ref_set_camera_dof.argtypes = [C.c_void_p, C.c_float, C.c_float]
         _lib = L
     return _lib
 
@@ -174,6 +177,8 @@ class RefScene:
         pos, basis = f32(cam.position), f32(cam.basis)
         self._keep += [pos, basis]
         L.ref_set_camera(self.h, P(pos), P(basis), cam.y_ratio, cam.fov)
+        if getattr(cam, "focal_distance", 0.0) > 0.0:
+            L.ref_set_camera_dof(self.h, cam.focal_distance, cam.lens_radius)
         tr = integrator or scene.tracer
         if isinstance(tr, PathTracer):
             L.ref_finalize(self.h, 0, tr.max_depth, 0, seed)

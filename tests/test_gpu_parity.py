@@ -140,8 +140,44 @@ def test_gpu_medium_phase_camera_match_reference(golden, lib):
     N = c["pix"].shape[0]
     co = np.zeros((N, 6), np.float32)
     assert lib.rumi_test_camera_rays(C.byref(cam), int(c["W"]), int(c["H"]), N, vp(c["pix"].astype(np.int32)),
-                                     vp(c["smp"]), vp(co)) == 0
+                                     vp(c["smp"]), None, vp(co)) == 0
     np.testing.assert_allclose(co, c["out"][:, 0:6], rtol=0, atol=1e-6)
+
+
+def test_gpu_thin_lens_rays_match_reference(lib, golden):
+    """Thin-lens camera rays (Pinhole::DepthOfField) against the reference's own rays for
+    the same lens uniforms; device sinf/cosf differ from the host's by an ulp or two."""
+    from test_oracle_golden import _dof_camera
+    g = golden("camera_dof.npz")
+    N = g["pix"].shape[0]
+    pix = np.ascontiguousarray(g["pix"].astype(np.int32))
+    lens_u = np.ascontiguousarray(g["out"][:, 8:10])
+    for i in range(N):
+        cam = _dof_camera(g, i)
+        out = np.zeros(6, np.float32)
+        assert lib.rumi_test_camera_rays(C.byref(cam), int(g["W"]), int(g["H"]), 1, vp(pix[i]),
+                                         vp(np.ascontiguousarray(g["smp"][i])), vp(lens_u[i]), vp(out)) == 0
+        np.testing.assert_allclose(out, g["out"][i, 0:6], rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("builder", [lambda: scenes.cornell_pt(32, 32, 4, 2), lambda: scenes.cornell_dof_pt(32, 32, 4, 2)])
+def test_gpu_frame_matches_oracle_per_pixel_two_vertices(builder):
+    """With the same Philox streams, paths of two vertices (camera ray, one bounce, light
+    sampling at both) agree with the oracle pixel by pixel to float rounding."""
+    sc = builder()
+    gs = rumi_b200.GpuScene(sc)
+    film, st = gs.render(spp=4, seed=21)
+    gs.close()
+    ofilm, onan = O.OracleScene(sc).render_pt(2, 4, 21)
+    assert st["nan_samples"] == onan == 0
+    rel = np.abs(film - ofilm) / np.maximum(np.abs(ofilm), 1e-3)
+    assert np.mean(rel.max(2) > 1e-3) <= 2.0 / (32 * 32), float(rel.max())
+
+
+def test_gpu_thin_lens_frames_match_reference_3sigma(golden):
+    from test_oracle_golden import frames_vs_reference
+    frames_vs_reference(gpu_frames(scenes.cornell_dof_pt(32, 32, 16, 8), 32, 14000),
+                        golden("image_cornell_dof32.npz"))
 
 
 def test_gpu_hg_phase_matches_oracle(lib):

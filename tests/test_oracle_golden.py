@@ -130,8 +130,41 @@ def test_oracle_camera_rays(golden):
     out = np.zeros(6, np.float32)
     for pix, smp, ref in zip(g["pix"], g["smp"], g["out"]):
         O.lib().orc_camera_ray(C.byref(cam), int(g["W"]), int(g["H"]), int(pix[0]), int(pix[1]), float(smp[0]),
-                               float(smp[1]), O.P(out))
+                               float(smp[1]), 0.0, 0.0, O.P(out))
         np.testing.assert_allclose(out, ref[0:6], rtol=0, atol=1e-6)
+
+
+def _dof_camera(g, i):
+    import rumi_b200._capi as capi
+    cam = capi.rumi_camera()
+    cam.position = capi.f3(*g["pos"])
+    cam.basis = capi.f16(*g["basis"])
+    cam.y_ratio, cam.fov_deg = float(g["y_ratio"]), float(g["fov"])
+    cam.focal_distance, cam.lens_radius = float(g["focal"][i]), float(g["lens"][i])
+    return cam
+
+
+def test_oracle_thin_lens_rays(golden):
+    """Pinhole::DepthOfField + CastViewRay: lens point from sqrt(u1) * radius and angle
+    u2 * 2 PI along _up / _right (the basis applied with its translation column), aimed
+    at the pinhole ray's focal-plane point; the reference's own two RandomFloat() draws
+    fed to the oracle."""
+    import ctypes as C
+    g = golden("camera_dof.npz")
+    out = np.zeros(6, np.float32)
+    for i, (pix, smp, ref) in enumerate(zip(g["pix"], g["smp"], g["out"])):
+        cam = _dof_camera(g, i)
+        O.lib().orc_camera_ray(C.byref(cam), int(g["W"]), int(g["H"]), int(pix[0]), int(pix[1]), float(smp[0]),
+                               float(smp[1]), float(ref[8]), float(ref[9]), O.P(out))
+        np.testing.assert_allclose(out, ref[0:6], rtol=0, atol=1e-6)
+    # the lens moves the origins: the fixture is not the pinhole case
+    assert np.abs(g["out"][:, 0:3] - g["pos"][None]).max() > 0.05
+
+
+def test_oracle_thin_lens_frames_match_reference_3sigma(golden):
+    """Cornell box through a thin lens focused at the white sphere's depth."""
+    frames_vs_reference(oracle_frames(scenes.cornell_dof_pt(32, 32, 16, 8), 8, 24, 800),
+                        golden("image_cornell_dof32.npz"))
 
 
 def test_pixel_sampler_is_a_stratified_permutation():
