@@ -129,15 +129,18 @@ typedef struct {
 
 typedef struct rumi_scene rumi_scene;
 
-enum { RUMI_PATH_TRACER = 0, RUMI_BDPT = 1 };
+/* RUMI_RAY_TRACER: RayTracer(scene, max_depth), the Whitted integrator
+ * (src/Integrator/raytracer.cpp:30-86): mirror and glass chains up to trace depth
+ * max_depth (>= 0), direct lighting at the first other surface. */
+enum { RUMI_PATH_TRACER = 0, RUMI_BDPT = 1, RUMI_RAY_TRACER = 2 };
 enum {
     RUMI_FLAG_TIMING = 1,  /* per-kernel CUDA-event timing into rumi_render_stats */
     RUMI_FLAG_STATS = 2    /* count BVH node fetches and primitive tests of closest-hit rays */
 };
 
 typedef struct {
-    int32_t integrator;    /* RUMI_PATH_TRACER (PathTracer(scene, max_depth)) or RUMI_BDPT */
-    int32_t max_depth;     /* path tracer: vertices per path */
+    int32_t integrator;    /* RUMI_PATH_TRACER (PathTracer(scene, max_depth)), RUMI_BDPT or RUMI_RAY_TRACER */
+    int32_t max_depth;     /* path tracer: vertices per path; ray tracer: largest trace depth */
     int32_t n_light;       /* BDPT nL (light subpath vertices) */
     int32_t n_eye;         /* BDPT nE (eye subpath vertices) */
     int32_t spp;           /* samples per pixel, rendered exactly */

@@ -42,6 +42,7 @@
 #include "Integrator/path.h"
 #include "Integrator/pathtracer.h"
 #include "Integrator/bidirectionalpathtracer.h"
+#include "Integrator/raytracer.h"
 #include "Scene/scene.h"
 
 // ---------------------------------------------------------------------------------
@@ -245,7 +246,8 @@ extern "C" void ref_set_camera_dof(void *h, float focal_distance, float lens_rad
     ((RefScene *)h)->scene->_camera->DepthOfField(focal_distance, lens_radius);
 }
 
-// integrator: 0 PathTracer(max_depth=a), 1 BidirectionalPathTracer(nL=a, nE=b).
+// integrator: 0 PathTracer(max_depth=a), 1 BidirectionalPathTracer(nL=a, nE=b),
+// 2 RayTracer(max_depth=a).
 // Sample sets are generated after seeding, as Scene::Build does once per frame.
 extern "C" int ref_finalize(void *h, int integrator, int a, int b, unsigned long long seed) {
     RefScene *rs = (RefScene *)h;
@@ -263,6 +265,8 @@ extern "C" int ref_finalize(void *h, int integrator, int a, int b, unsigned long
     rs->integrator = integrator;
     if (integrator == 0)
         sc->_tracer_ptr = new PathTracer(sc, a);
+    else if (integrator == 2)
+        sc->_tracer_ptr = new RayTracer(sc, a);
     else
         sc->_tracer_ptr = new BidirectionalPathTracer(sc, a, b);
     return 0;

@@ -845,6 +845,126 @@ static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, cons
     return L;
 }
 
+/* ------------------------------------------------------------------ ray tracer
+ * RayTracer::Trace(ray, depth, le, in_object) (src/Integrator/raytracer.cpp:37-72) in the
+ * reference's recursive form: Specular::GlobalIllumination (specular.cpp:60-75) and
+ * Dielectric::GlobalIllumination (dielectric.cpp:105-159) recurse, every other material
+ * returns its DirectLighting (Matte next-event estimation matte.cpp:54-82; Glossy only
+ * when Intersection::_rand = 1.0 lies on its diffuse lobe, glossy.cpp:92-102; Emissive
+ * emissive.cpp:61-74; Subsurface none).  *t_hit: the traced ray's Ray::_tmin (0 when
+ * nothing was traced or hit), which Dielectric's Beer-Lambert factor reads. */
+static V3 whitted(const orc_scene_desc *s, int max_depth, uint64_t path, const uint32_t key[2], V3 o, V3 d, int depth,
+                  int le, int inobj, float *t_hit) {
+    *t_hit = 0.0f;
+    if (depth > max_depth) return v3(0, 0, 0);
+    Ray ray = {o, d, 3.402823466e+38f, inobj};
+    Hit h = closest(s, &ray, 0);
+    if (!(h.t > 0.0f)) return v3(0, 0, 0);
+    *t_hit = h.t;
+    const orc_material *m = prim_mat(s, h.id);
+    int opaque = m->type != DIELECTRIC && m->type != SUBSURFACE;
+    V3 p = add(o, mul(d, h.t)), n, albedo = fv(m->rgb);
+    if (h.id < s->n_triangles) {
+        const float *q = s->tri_normals + 9 * (size_t)h.id;
+        n = add(add(mul(fv(q), 1.0f - h.u - h.v), mul(fv(q + 3), h.u)), mul(fv(q + 6), h.v));
+        if (h.back && opaque) n = neg(n);
+        if (s->tri_albedo) albedo = fv(s->tri_albedo + 3 * (size_t)h.id);
+    } else if (h.id < s->n_triangles + s->n_rects) {
+        const float *q = s->rects + 9 * (size_t)(h.id - s->n_triangles);
+        n = normalize(cross(fv(q + 3), fv(q + 6)));
+    } else {
+        const float *c = s->spheres + 4 * (size_t)(h.id - s->n_triangles - s->n_rects);
+        if (m->type == EMISSIVE)
+            n = length(sub(o, fv(c))) > c[3] ? normalize(sub(p, fv(c))) : normalize(sub(fv(c), p));
+        else
+            n = normalize(sub(p, fv(c)));
+    }
+    float U0[4], U1[4], U2[4];
+    path_u(path, depth, 0, key, U0);
+    V3 wo = neg(d);
+    if (m->type == SPECULAR) {
+        Bsdf b = mat_sample(m, wo, n, U0[0], U0[1], U0[2]);
+        float tt;
+        V3 Li = whitted(s, max_depth, path, key, p, b.w, depth + 1, 1, 0, &tt);
+        V3 f = mul(albedo, m->kd);
+        return mul(mul(vmul(f, Li), b.cost), 1.0f / b.pdfw);
+    }
+    if (m->type == DIELECTRIC) {
+        Bsdf b = mat_sample(m, wo, n, U0[0], U0[1], U0[2]);
+        float tt, inv;
+        V3 Li = whitted(s, max_depth, path, key, p, b.w, depth + 1, 1, b.go_in, &tt), lo;
+        if (b.xi == 1.0f) {
+            lo = mul(mul(Li, b.pdf_path), 1.0f / b.pdfw);
+            inv = 1.0f / b.pdf_path;
+        } else {
+            float eta = inobj ? m->eta_in / m->eta_out : m->eta_out / m->eta_in;
+            lo = mul(mul(Li, 1.0f / (eta * eta) * b.pdf_path), 1.0f / b.pdfw);
+            inv = 1.0f / b.pdf_path;
+        }
+        if (b.go_in) lo = vmul(lo, v3(expf(-m->rgb[0] * tt), expf(-m->rgb[1] * tt), expf(-m->rgb[2] * tt)));
+        return mul(lo, inv);
+    }
+    if (m->type == EMISSIVE) {
+        if (inobj || !le || -dot(d, n) <= 0.0f) return v3(0, 0, 0);
+        return mat_le(m);
+    }
+    float kd_pdf = m->type == GLOSSY ? m->kd / (m->kd + m->ks) : 1.0f;
+    if (s->n_lights > 0 && (m->type == MATTE || (m->type == GLOSSY && m->kd != 0.0f && 1.0f <= kd_pdf))) {
+        path_u(path, depth, 1, key, U1);
+        path_u(path, depth, 2, key, U2);
+        LSample ls = light_sample(s, U0[3], U1[0], U1[1]);
+        V3 wi;
+        float dist, G;
+        if (!nee_geom(&ls, p, &wi, &dist, &G)) return v3(0, 0, 0);
+        V3 f = mul(mul(albedo, INV_PI_F), m->kd);
+        float c = dot(wi, n);
+        if (c < 0.0f) c = 0.0f;
+        V3 direct = mul(mul(mul(vmul(f, ls.Li), c), G), 1.0f / ls.pdf);
+        if (m->type == GLOSSY) direct = mul(direct, 1.0f / kd_pdf);
+        const orc_volume *V = &s->volume;
+        float tr = 1.0f, stn, stf;
+        if (V->present && vol_isect(V, p, wi, 0.0f, &stn, &stf)) {
+            V3 vs_t = v3(V->sigma_s[0] + V->sigma_a[0], V->sigma_s[1] + V->sigma_a[1], V->sigma_s[2] + V->sigma_a[2]);
+            float sm = vol_smax(dist, stn, stf);
+            if (U2[2] < 1.0f - expf(average(vs_t) * -sm)) tr = 0.0f;
+        }
+        Ray sr = {p, wi, dist, 0};
+        if (tr > 0.0f && closest(s, &sr, 1).t == 0.0f) return direct;
+    }
+    return v3(0, 0, 0);
+}
+
+/* RayTracer::Trace(w, h, camera, film) over rows [row0, row1), film as orc_render_pt. */
+long long orc_render_whitted(const orc_scene_desc *s, int max_depth, int spp, uint64_t seed, int row0, int row1,
+                             float *film) {
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32) ^ 0x5851F42Du};
+    long long nan = 0;
+    int W = s->width, H = s->height;
+    for (int h = row0; h < row1 && h < H; ++h) {
+        for (int w = 0; w < W; ++w) {
+            long long pixel = (long long)h * W + w;
+            V3 acc = v3(0, 0, 0);
+            for (int k = 0; k < spp; ++k) {
+                float sx, sy, lu1, lu2, tt;
+                V3 o, d;
+                uint64_t path = (uint64_t)(pixel * spp + k);
+                pixel_sample(k, spp, pixel, key, &sx, &sy);
+                lens_u(&s->camera, path, key, &lu1, &lu2);
+                camera_ray(&s->camera, W, H, w, h, sx, sy, lu1, lu2, &o, &d);
+                V3 L = whitted(s, max_depth, path, key, o, d, 0, 1, 0, &tt);
+                if (isnan3(L))
+                    ++nan;
+                else
+                    acc = add(acc, L);
+            }
+            film[pixel * 3 + 0] = acc.z;
+            film[pixel * 3 + 1] = acc.y;
+            film[pixel * 3 + 2] = acc.x;
+        }
+    }
+    return nan;
+}
+
 /* One path of orc_render_pt (pixel, sample k): its radiance (out_L[3], r g b) and its
  * extension rays, written to rays (max_depth * 8), t and prim; returns their count. */
 int orc_path_rays(const orc_scene_desc *s, int max_depth, int spp, uint64_t seed, long long pixel, int k,

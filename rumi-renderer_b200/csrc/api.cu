@@ -482,10 +482,11 @@ rumi_status rumi_render(rumi_scene *sc, const rumi_render_params *p, float *film
         film_dev = tmp;
     }
     rumi_status st;
-    if (p->integrator == RUMI_PATH_TRACER) {
-        if (p->max_depth <= 0) {
+    if (p->integrator == RUMI_PATH_TRACER || p->integrator == RUMI_RAY_TRACER) {
+        // a path has at least one vertex; the ray tracer's depth limit may be 0 (camera rays only)
+        if (p->max_depth < (p->integrator == RUMI_PATH_TRACER ? 1 : 0)) {
             dfree(tmp, s);
-            return set_error("max_depth must be positive"), RUMI_ERR_INVALID_ARG;
+            return set_error("max_depth out of range"), RUMI_ERR_INVALID_ARG;
         }
         st = pt_render(sc, p, film_dev, stats, s);
     } else if (p->integrator == RUMI_BDPT) {

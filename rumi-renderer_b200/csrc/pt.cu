@@ -627,6 +627,143 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
     }
 }
 
+// RayTracer::Trace (src/Integrator/raytracer.cpp:37-72), the Whitted integrator, on the
+// same queues as the path tracer.  A vertex at trace depth `bounce` (the camera ray is
+// depth 0; depths up to max_depth are shaded, so the host runs max_depth + 1 bounces):
+//   Specular   -> Specular::GlobalIllumination: mirror ray, weight kr * colour
+//                 (specular.cpp:60-75);
+//   Dielectric -> Dielectric::GlobalIllumination: reflection with probability kr, else
+//                 refraction with weight 1 / eta^2, eta = in_object ? eta_in / eta_out
+//                 : eta_out / eta_in; a ray that goes into the object is attenuated by
+//                 Beer-Lambert over the length it travels, with the absorption of the
+//                 material it entered (dielectric.cpp:105-159);
+//   otherwise  -> the material's DirectLighting and the walk ends: Matte next-event
+//                 estimation (matte.cpp:54-82), Glossy only when its Intersection::_rand
+//                 (1.0 here, nothing samples a lobe) falls on the diffuse lobe
+//                 (glossy.cpp:92-102), Emissive emission when le, outside objects and
+//                 front-facing (emissive.cpp:61-74), Subsurface nothing.
+// No medium event: the RayTracer sends rays through a volume unattenuated; only the
+// shadow ray of next-event estimation sees it (HomogeneousVolume::ShadowRayTr).  beta.w
+// carries the index of the material a refracted ray entered.
+__global__ void __launch_bounds__(SHADE_THREADS) pt_shade_whitted(PtLaunch P, int bounce) {
+    const int cur = bounce & 1, nxt = cur ^ 1;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = P.cnt[cur];
+    const bool active = i < n;
+    bool want_next = false, want_sh = false;
+    float3 nx_o = mk3(0, 0, 0), nx_d = mk3(0, 0, 0);
+    unsigned nx_flags = 0;
+    float3 sh_o = mk3(0, 0, 0), sh_d = mk3(0, 0, 0), sh_c = mk3(0, 0, 0);
+    float sh_tmax = 0.0f;
+    int slot = 0, enter_mat = 0;
+    float3 beta = mk3(0, 0, 0);
+    if (active) {
+        const float4 o4 = P.ray_o[cur][i];
+        const float4 d4 = P.ray_d[cur][i];
+        const float4 hv = P.hit[i];
+        slot = __float_as_int(o4.w) & 0x7fffffff;
+        const DevScene &S = P.s;
+        const uint64_t path = (uint64_t)(P.path0 + slot);
+        const float3 o = f4xyz(o4), d = f4xyz(d4);
+        const float t = hv.x;
+        const int code = __float_as_int(hv.y);
+        const unsigned fl = P.pflags[slot];
+        const bool le = (fl & PFL_LE) != 0, inobj = (fl & PFL_IN) != 0;
+        const float4 beta4 = P.beta[slot];
+        beta = f4xyz(beta4);
+        const bool last = bounce + 1 >= P.max_depth;
+        float3 addL = mk3(0, 0, 0);
+        if (t > 0.0f) {
+            const int id = code & 0x7fffffff;
+            const DevMaterial m = S.materials[prim_material(S, id)];
+            const float3 p = rn_madd(o, d, t);
+            const float3 nrm = surface_normal(S, id, code < 0, hv.z, hv.w, o, p, m);
+            if (inobj) {  // BeerLambertLaw over the segment the previous vertex sent inside
+                const float3 a = S.materials[__float_as_int(beta4.w)].rgb;
+                beta = beta * mk3(expf(-a.x * t), expf(-a.y * t), expf(-a.z * t));
+            }
+            const float3 wo = -d;
+            const Uniform4 U0 = path_uniforms(path, bounce, 0, P.k0, P.k1);
+            if (m.type == MAT_SPECULAR) {
+                nx_d = mirror_dir(wo, nrm);
+                float3 albedo = m.rgb;
+                if (id < S.n_tris && S.tri_albedo) albedo = f4xyz(__ldg(&S.tri_albedo[id]));
+                beta = beta * (albedo * m.kd);
+                nx_o = p;
+                nx_flags = PFL_LE;
+                want_next = !last;
+            } else if (m.type == MAT_DIELECTRIC) {
+                const float kr = fresnel_kr(d, nrm, m.eta_in, m.eta_out);
+                const float kt = 1.0f - kr;
+                float c;
+                bool entering;
+                if (kr != 0.0f && U0.u[0] <= kr) {
+                    nx_d = fresnel_reflect_dir(wo, nrm, c);
+                    entering = c < 0.0f;
+                    beta = beta * (kr * (1.0f / kr));
+                } else {
+                    nx_d = refract_dir(wo, nrm, m.eta_in, m.eta_out, c);
+                    entering = c > 0.0f;
+                    const float eta = inobj ? m.eta_in / m.eta_out : m.eta_out / m.eta_in;
+                    beta = beta * (1.0f / (eta * eta) * kt * (1.0f / kt));
+                }
+                nx_o = p;
+                nx_flags = PFL_LE | (entering ? PFL_IN : 0);
+                enter_mat = prim_material(S, id);
+                want_next = !last;
+            } else if (m.type == MAT_EMISSIVE) {
+                if (le && !inobj && -dot3(d, nrm) > 0.0f) addL = beta * m.le;
+            } else if (S.n_lights > 0 && (m.type == MAT_MATTE || (m.type == MAT_GLOSSY && m.kd != 0.0f &&
+                                                                  1.0f <= m.kd_pdf))) {
+                const Uniform4 U1 = path_uniforms(path, bounce, 1, P.k0, P.k1);
+                const LightSample ls = sample_light(S, U0.u[3], U1.u[0], U1.u[1]);
+                float3 wi;
+                float dist, G;
+                if (nee_setup(ls, p, wi, dist, G)) {
+                    float3 albedo = m.rgb;
+                    if (id < S.n_tris && S.tri_albedo) albedo = f4xyz(__ldg(&S.tri_albedo[id]));
+                    const float3 f = albedo * RUMI_INV_PI_F * m.kd;
+                    const float cost = fmaxf(dot3(wi, nrm), 0.0f);
+                    float3 direct = f * ls.Li * cost * G / ls.pdf;
+                    if (m.type == MAT_GLOSSY) direct = direct * (1.0f / m.kd_pdf);
+                    float tr = 1.0f;
+                    if (S.volume.present) {
+                        const Uniform4 U2 = path_uniforms(path, bounce, 2, P.k0, P.k1);
+                        float smax_sh = 0.0f;
+                        tr = volume_shadow_tr(S.volume, p, wi, dist, U2.u[2], &smax_sh);
+                    }
+                    if (tr > 0.0f) {
+                        want_sh = true;
+                        sh_o = p;
+                        sh_d = wi;
+                        sh_tmax = dist;
+                        sh_c = beta * direct;
+                    }
+                }
+            }
+        }
+        if (addL.x != 0.0f || addL.y != 0.0f || addL.z != 0.0f) {
+            float4 l = P.L[slot];
+            l.x += addL.x; l.y += addL.y; l.z += addL.z;
+            P.L[slot] = l;
+        }
+    }
+    const int kn = warp_push(&P.cnt[nxt], want_next);
+    const int ks = warp_push(&P.cnt[C_SHADOW], want_sh);
+    if (want_next) {
+        P.ray_o[nxt][kn] = make_float4(nx_o.x, nx_o.y, nx_o.z,
+                                       __int_as_float(slot | ((nx_flags & PFL_IN) ? (int)0x80000000 : 0)));
+        P.ray_d[nxt][kn] = make_float4(nx_d.x, nx_d.y, nx_d.z, FLT_MAX);
+        P.beta[slot] = make_float4(beta.x, beta.y, beta.z, __int_as_float(enter_mat));
+        P.pflags[slot] = nx_flags;
+    }
+    if (want_sh) {
+        P.sh_o[ks] = make_float4(sh_o.x, sh_o.y, sh_o.z, __int_as_float(slot));
+        P.sh_d[ks] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
+        P.sh_c[ks] = make_float4(sh_c.x, sh_c.y, sh_c.z, 0.0f);
+    }
+}
+
 // One warp per pixel: the pixel's samples are summed in sample order by lane 0 after
 // a coalesced load of up to 32 samples at a time.
 __global__ void pt_resolve(PtLaunch P) {
@@ -792,7 +929,10 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     carve_wave(L, ws, Wp);
     L.s = sc->dev;
     L.spp = spp;
-    L.max_depth = p->max_depth;
+    // RayTracer::Trace shades trace depths 0..max_depth (raytracer.cpp:41-42)
+    const bool whitted = p->integrator == RUMI_RAY_TRACER;
+    const int bounces = whitted ? p->max_depth + 1 : p->max_depth;
+    L.max_depth = bounces;
     L.k0 = (uint32_t)p->seed;
     L.k1 = (uint32_t)(p->seed >> 32) ^ 0x5851F42Du;
     int d = 0;
@@ -829,7 +969,7 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
         L.n_paths = (int)(n_pix * spp);
         L.path0 = pix0 * spp;
         pt_generate<<<cdiv(L.n_paths, 256), 256, 0, stream>>>(L);
-        for (int b = 0; b < p->max_depth; ++b) {
+        for (int b = 0; b < bounces; ++b) {
             pt_reset<<<1, 1, 0, stream>>>(L, b);
             int e0 = 0;
             if (timing) { e0 = (int)evs.size(); mark(); }
@@ -839,7 +979,10 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
                 launch_extend<false>(mode, trace_grid, stream, L, b);
             if (timing) { mark(); ext_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
-            pt_shade<false><<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
+            if (whitted)
+                pt_shade_whitted<<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
+            else
+                pt_shade<false><<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
             if (timing) { mark(); shade_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
             launch_shadow<false>(mode, shadow_grid, stream, L);
@@ -867,7 +1010,7 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
         stats->rays_shadow = (int64_t)h_stats[S_RAYS_SH];
         stats->extend_node_fetches = (int64_t)h_stats[S_NODES];
         stats->extend_prim_tests = (int64_t)h_stats[S_PRIMS];
-        stats->extend_launches = (int64_t)waves * p->max_depth;
+        stats->extend_launches = (int64_t)waves * bounces;
         stats->shade_launches = stats->extend_launches;
         stats->shadow_launches = stats->extend_launches;
         if (timing) {

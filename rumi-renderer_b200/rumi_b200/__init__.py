@@ -10,7 +10,8 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
-from .scene import (Scene, FlatScene, PathTracer, BidirectionalPathTracer, PATH_TRACER, BDPT, LIGHT_AREA, LIGHT_SPOT)
+from .scene import (Scene, FlatScene, PathTracer, BidirectionalPathTracer, RayTracer, PATH_TRACER, BDPT, RAY_TRACER,
+                    LIGHT_AREA, LIGHT_SPOT)
 
 __all__ = ["GpuScene", "render", "Scene"]
 
@@ -113,6 +114,8 @@ class GpuScene:
         if isinstance(tr, BidirectionalPathTracer):
             p.integrator, p.n_light, p.n_eye = BDPT, tr.nL, tr.nE
             p.max_depth = tr.nL + tr.nE
+        elif isinstance(tr, RayTracer):
+            p.integrator, p.max_depth = RAY_TRACER, tr.max_depth
         else:
             p.integrator, p.max_depth = PATH_TRACER, tr.max_depth
         p.spp = int(spp if spp is not None else self.flat.image.n_samples)

@@ -29,7 +29,7 @@ SHAPE_TRIANGLE, SHAPE_RECT, SHAPE_SPHERE = range(3)
 # light kinds
 LIGHT_AREA, LIGHT_SPOT = range(2)
 # integrators
-PATH_TRACER, BDPT = range(2)
+PATH_TRACER, BDPT, RAY_TRACER = range(3)
 
 
 def _v3(x) -> np.ndarray:
@@ -246,6 +246,14 @@ class BidirectionalPathTracer:
     """``BidirectionalPathTracer(scene, nL, nE)`` (src/Integrator/bidirectionalpathtracer.cpp:43-96)."""
     nL: int
     nE: int
+
+
+@dataclass
+class RayTracer:
+    """``RayTracer(scene, max_depth)`` (src/Integrator/raytracer.cpp:30-86): the Whitted
+    integrator -- mirror and glass chains up to trace depth ``max_depth``, direct lighting
+    at the first other surface."""
+    max_depth: int
 
 
 class Scene:

@@ -15,7 +15,7 @@ import numpy as np
 
 from .scene import (Scene, Rect, Sphere, Model, Matte, Specular, Emissive, Dielectric, Glossy, Subsurface, AreaLight,
                     SpotLight, HomogeneousVolume, Pinhole, Film, PathTracer, BidirectionalPathTracer,
-                    identity16)
+                    RayTracer, identity16)
 
 F32 = np.float32
 
@@ -55,6 +55,13 @@ def add_cornell_box(sc: Scene, light_samples: int = 256) -> Rect:
 
 def cornell_camera() -> Pinhole:
     return Pinhole((0.5, 0.5, -1.4), identity16(), 1.0, fov=40.0)
+
+
+def whitted(sc: Scene, max_depth: int = 10) -> Scene:
+    """The scene rendered by ``RayTracer(scene, max_depth)`` (the reference's scene presets
+    construct it with depth 10)."""
+    sc.tracer = RayTracer(max_depth)
+    return sc
 
 
 def cornell_dof_pt(width: int = 256, height: int = 256, spp: int = 16, max_depth: int = 8,

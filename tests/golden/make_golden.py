@@ -230,7 +230,11 @@ def image_fixture(path, size=32, spp=16, depth=8, seeds=64, scene=None):
     fr = np.stack(frames).astype(np.float64)
     mean = fr.mean(0).astype(F32)
     stderr = (fr.std(0, ddof=1) / np.sqrt(seeds)).astype(F32)
-    np.savez_compressed(path, mean=mean, stderr=stderr, seeds=seeds, spp=spp, depth=depth, size=size)
+    # per-frame image means: the reference's frames share sample sets across pixels, so the
+    # image mean's spread is not the per-pixel spreads added in quadrature
+    frame_means = fr.mean((1, 2, 3)).astype(np.float64)
+    np.savez_compressed(path, mean=mean, stderr=stderr, seeds=seeds, spp=spp, depth=depth, size=size,
+                        frame_means=frame_means)
     print(path, "mean", mean.reshape(-1, 3).mean(0))
 
 
@@ -337,6 +341,12 @@ def obj_fixture(path):
 
 
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "whitted":
+        image_fixture(os.path.join(HERE, "image_whitted_cornell32.npz"),
+                      scene=scenes.whitted(scenes.cornell_pt(32, 32, 16, 8)))
+        image_fixture(os.path.join(HERE, "image_whitted_caustic32.npz"),
+                      scene=scenes.whitted(scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "dof":
         camera_dof_fixture(os.path.join(HERE, "camera_dof.npz"), np.random.default_rng(88))
         image_fixture(os.path.join(HERE, "image_cornell_dof32.npz"), scene=scenes.cornell_dof_pt(32, 32, 16, 8))

@@ -27,6 +27,8 @@ def lib():
         L.orc_trace.argtypes = [C.c_void_p, C.c_int64, FP, C.c_int, FP, C.POINTER(C.c_int32)]
         L.orc_render_pt.restype = C.c_longlong
         L.orc_render_pt.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, FP]
+        L.orc_render_whitted.restype = C.c_longlong
+        L.orc_render_whitted.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, FP]
         L.orc_material_sample.argtypes = [C.c_void_p, FP, FP, FP, FP]
         L.orc_material_fr.argtypes = [C.c_void_p, FP, FP, FP, C.c_int, C.c_float, C.c_float, C.c_float, FP, FP]
         L.orc_fresnel.restype = C.c_float
@@ -94,6 +96,13 @@ class OracleScene:
         film = np.zeros((self.height, self.width, 3), np.float32)
         nan = lib().orc_render_pt(C.byref(self.desc), max_depth, spp, seed, row0,
                                   self.height if row1 is None else row1, P(film))
+        return film, int(nan)
+
+    def render_whitted(self, max_depth, spp, seed, row0=0, row1=None):
+        """RayTracer(scene, max_depth) frame: film (H, W, 3) B,G,R sums and NaN count."""
+        film = np.zeros((self.height, self.width, 3), np.float32)
+        nan = lib().orc_render_whitted(C.byref(self.desc), max_depth, spp, seed, row0,
+                                       self.height if row1 is None else row1, P(film))
         return film, int(nan)
 
     def camera_ray(self, w, h, sx, sy, lu1=0.0, lu2=0.0):

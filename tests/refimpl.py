@@ -106,7 +106,7 @@ class RefScene:
 
     def __init__(self, scene, seed: int = 1, integrator=None, presort_over: int = 200000):
         from rumi_b200.scene import (Triangle, Model, Rect, Sphere, AreaLight, PathTracer,
-                                     BidirectionalPathTracer, MATTE)
+                                     BidirectionalPathTracer, RayTracer, MATTE)
         L = lib()
         self._keep = []
         img = scene.image
@@ -184,6 +184,8 @@ class RefScene:
             L.ref_finalize(self.h, 0, tr.max_depth, 0, seed)
         elif isinstance(tr, BidirectionalPathTracer):
             L.ref_finalize(self.h, 1, tr.nL, tr.nE, seed)
+        elif isinstance(tr, RayTracer):
+            L.ref_finalize(self.h, 2, tr.max_depth, 0, seed)
         else:
             L.ref_finalize(self.h, 0, 1, 0, seed)
 

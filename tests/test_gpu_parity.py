@@ -174,6 +174,41 @@ def test_gpu_frame_matches_oracle_per_pixel_two_vertices(builder):
     assert np.mean(rel.max(2) > 1e-3) <= 2.0 / (32 * 32), float(rel.max())
 
 
+@pytest.mark.parametrize("fixture,builder", __import__("test_oracle_golden").WHITTED_CASES)
+def test_gpu_whitted_matches_reference_3sigma(golden, fixture, builder):
+    from test_oracle_golden import frames_vs_reference
+    frames_vs_reference(gpu_frames(builder(), 32, 15000), golden(fixture))
+
+
+@pytest.mark.parametrize("fixture,builder", __import__("test_oracle_golden").WHITTED_CASES)
+def test_gpu_whitted_matches_oracle_per_pixel(fixture, builder):
+    """No hemisphere sampling on the Whitted path: with the same Philox streams the GPU's
+    frame equals the oracle's pixel by pixel, up to float rounding; a glass lobe or
+    medium-shadow decision that lands within an ulp of its threshold may flip."""
+    sc = builder()
+    gs = rumi_b200.GpuScene(sc)
+    film, st = gs.render(spp=4, seed=31)
+    gs.close()
+    ofilm, onan = O.OracleScene(sc).render_whitted(sc.tracer.max_depth, 4, 31)
+    assert st["nan_samples"] == onan == 0
+    rel = np.abs(film - ofilm) / np.maximum(np.abs(ofilm), 1e-3)
+    assert np.mean(rel.max(2) > 1e-3) <= 0.01, float(np.mean(rel.max(2) > 1e-3))
+    assert abs(film.sum() / ofilm.sum() - 1.0) < 5e-3
+
+
+def test_gpu_whitted_depth_zero_is_direct_lighting_only():
+    """max_depth 0: camera rays only; a mirror seen directly is black, the walls carry
+    next-event estimation, the light its emission."""
+    sc = scenes.whitted(scenes.cornell_pt(32, 32, 4, 8), max_depth=0)
+    gs = rumi_b200.GpuScene(sc)
+    film, _ = gs.render(spp=4, seed=5)
+    gs.close()
+    ofilm, _ = O.OracleScene(sc).render_whitted(0, 4, 5)
+    rel = np.abs(film - ofilm) / np.maximum(np.abs(ofilm), 1e-3)
+    assert rel.max() < 1e-3
+    assert (ofilm.reshape(-1, 3).sum(1) == 0).any()
+
+
 def test_gpu_thin_lens_frames_match_reference_3sigma(golden):
     from test_oracle_golden import frames_vs_reference
     frames_vs_reference(gpu_frames(scenes.cornell_dof_pt(32, 32, 16, 8), 32, 14000),

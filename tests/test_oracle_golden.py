@@ -203,7 +203,13 @@ def frames_vs_reference(frames, g, max_frac=0.01):
     z = np.abs(m - g["mean"]) / sig
     frac = float(np.mean(z > 3.0))
     ratio = float(m.mean() / g["mean"].mean())
-    rel_sigma = np.sqrt((se ** 2).sum() + (gse ** 2).sum()) / g["mean"].astype(np.float64).sum()
+    if "frame_means" in g.files:
+        # image-mean spread measured frame to frame on both sides (frame-level correlation
+        # of the reference's shared pixel and light sample sets included)
+        fm, gm = fr.mean((1, 2, 3)), g["frame_means"]
+        rel_sigma = np.sqrt(fm.var(ddof=1) / fm.size + gm.var(ddof=1) / gm.size) / float(gm.mean())
+    else:
+        rel_sigma = np.sqrt((se ** 2).sum() + (gse ** 2).sum()) / g["mean"].astype(np.float64).sum()
     assert frac < max_frac, (frac, ratio)
     assert abs(ratio - 1.0) < max(4.0 * rel_sigma, 0.002), (frac, ratio, rel_sigma)
     return frac, ratio
@@ -217,6 +223,26 @@ def oracle_frames(sc, depth, n, seed0):
         assert nan == 0
         frames.append(film / 16.0)
     return frames
+
+
+WHITTED_CASES = [
+    ("image_whitted_cornell32.npz", lambda: scenes.whitted(scenes.cornell_pt(32, 32, 16, 8))),
+    ("image_whitted_caustic32.npz", lambda: scenes.whitted(scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True))),
+]
+
+
+@pytest.mark.parametrize("fixture,builder", WHITTED_CASES)
+def test_oracle_whitted_matches_reference_3sigma(golden, fixture, builder):
+    """RayTracer (Whitted): mirror and glass chains, direct lighting at the first other
+    surface, against the reference's own RayTracer frames."""
+    sc = builder()
+    os_ = O.OracleScene(sc)
+    frames = []
+    for s in range(32):
+        film, nan = os_.render_whitted(sc.tracer.max_depth, 16, seed=900 + s)
+        assert nan == 0
+        frames.append(film / 16.0)
+    frames_vs_reference(frames, golden(fixture))
 
 
 def test_oracle_image_matches_reference_3sigma(golden):
