@@ -70,14 +70,38 @@ typedef struct {
 } rumi_material;
 
 enum { RUMI_SHAPE_TRIANGLE = 0, RUMI_SHAPE_RECT = 1, RUMI_SHAPE_SPHERE = 2 };
-enum { RUMI_LIGHT_AREA = 0, RUMI_LIGHT_SPOT = 1 };
+enum { RUMI_LIGHT_AREA = 0, RUMI_LIGHT_SPOT = 1, RUMI_LIGHT_IBL = 2 };
+
+/* texture kinds (src/Texture/): Texture::Pattern(shape, p) = Pixel(TextureMapping(p)) */
+enum {
+    RUMI_TEX_CHECKER = 0, /* Checker(width, height, c1, c2)                checker.cpp:17-32 */
+    RUMI_TEX_IMAGE = 1,   /* ImageTexture(bmp, gamma): the pixels LoadBmp returns (rows in file
+                             order, bottom row first, B,G,R[,A] bytes, no row padding)
+                                                                    imagetexture.cpp:32-61 */
+    RUMI_TEX_HDR = 2      /* HDRTexture(hdr): the floats LoadHDR returns (top scanline first,
+                             R,G,B)                                 hdrtexture.cpp:30-44 */
+};
+
+typedef struct {
+    int32_t type;
+    float repeat_u, repeat_v;   /* Checker _w, _h */
+    float color1[3], color2[3]; /* Checker _c1, _c2 (r, g, b) */
+    float gamma;                /* ImageTexture _gamma (1 = linear bytes) */
+    int32_t img_width, img_height, bytes_per_pixel;
+    const void *pixels;         /* IMAGE: uint8 img_height*img_width*bytes_per_pixel;
+                                   HDR: float img_height*img_width*3 */
+} rumi_texture;
 
 typedef struct {
     int32_t type;         /* RUMI_LIGHT_AREA: AreaLight(shape) (src/Light/arealight.cpp);
                              RUMI_LIGHT_SPOT: point emitter with a cone (no reference
-                             counterpart) */
-    int32_t shape_type;   /* area light: RUMI_SHAPE_RECT or RUMI_SHAPE_SPHERE */
-    int32_t shape_index;  /* area light: index within that shape array */
+                             counterpart);
+                             RUMI_LIGHT_IBL: ImageBasedLight(sphere, material, texture)
+                             (src/Light/imagebasedlight.cpp): an emissive, textured sphere
+                             around the scene, sampled by cosine-weighted directions about
+                             the shading normal */
+    int32_t shape_type;   /* area light: RUMI_SHAPE_RECT or RUMI_SHAPE_SPHERE; IBL: RUMI_SHAPE_SPHERE */
+    int32_t shape_index;  /* area light / IBL: index within that shape array */
     float position[3];    /* spot */
     float direction[3];   /* spot, unit */
     float cone_deg;       /* spot half-angle */
@@ -125,6 +149,16 @@ typedef struct {
 
     rumi_volume volume;
     rumi_camera camera;
+
+    /* textures (Shape::AddingTexture, src/Shape/shape.cpp:71-84); all may be 0 / NULL */
+    int32_t n_textures;
+    const rumi_texture *textures;
+    const int32_t *tri_texture;    /* n_triangles texture indices, -1 = none (a triangle maps
+                                      every point to (u, v) = (0, 0): Shape::TextureMapping) */
+    const int32_t *rect_texture;   /* n_rects, -1 = none (Rect::TextureMapping, rect.cpp:183-196) */
+    const int32_t *sphere_texture; /* n_spheres, -1 = none (Sphere::TextureMapping, sphere.cpp:172-192) */
+    const float *sphere_frame;     /* n_spheres*9: rows 0-2 of Shape::_transform's upper 3x3, which
+                                      orient a sphere's texture; NULL = identity */
 } rumi_scene_desc;
 
 typedef struct rumi_scene rumi_scene;

@@ -52,6 +52,12 @@ rumi_status rumi_test_pixel_samples(int64_t n, const int32_t *s, int32_t spp, co
  * read bandwidth: bytes * passes / ms. */
 rumi_status rumi_test_read_bandwidth(const void *buf_dev, int64_t bytes, int32_t passes, void *stream, double *ms);
 
+/* Texture::Pattern(shape, p) (src/Texture/texture.cpp:17-23) of a scene's primitives:
+ * prim n canonical primitive ids (triangles, rects, spheres), pts n*3; out n*3 (r, g, b),
+ * 1 where the primitive has no texture. */
+rumi_status rumi_test_texture_pattern(rumi_scene *scene, int64_t n, const int32_t *prim, const float *pts,
+                                      float *out);
+
 #ifdef __cplusplus
 }
 #endif

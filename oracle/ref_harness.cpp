@@ -616,3 +616,80 @@ extern "C" int ref_film_save_filter(const char *dir, int width, int height, int 
     close(devnull);
     return chdir(cwd) == 0 ? 0 : -1;
 }
+
+// ---------------------------------------------------------------------------------
+// Textures and image-based lights.
+#include "Texture/texture.h"
+#include "Texture/checker.h"
+#include "Texture/imagetexture.h"
+#include "Texture/hdrtexture.h"
+#include "Light/imagebasedlight.h"
+#include "Kernel/hdr.h"
+
+// Shape::AddingTexture (Model::AddingTexture hands it to every triangle) of top-level
+// object `object_index`: kind 0 Checker(w, h, c1, c2); 1 ImageTexture(path, gamma);
+// 2 HDRTexture(path).  Colours are (r, g, b).
+extern "C" int ref_add_texture(void *h, int object_index, int kind, float w, float hh, const float *c1,
+                               const float *c2, const char *path, float gamma) {
+    RefScene *rs = (RefScene *)h;
+    Shape *s = rs->objects.at(object_index);
+    Texture *t = nullptr;
+    if (kind == 0)
+        t = new Checker(w, hh, Color(c1[0], c1[1], c1[2]), Color(c2[0], c2[1], c2[2]));
+    else if (kind == 1)
+        t = new ImageTexture((char *)path, gamma);
+    else
+        t = new HDRTexture((char *)path);
+    s->AddingTexture(t);
+    return 0;
+}
+
+// Shape::_transform (public; Sphere::TextureMapping reads its upper 3x3 rows).
+extern "C" void ref_set_shape_transform(void *h, int object_index, const float *m16) {
+    RefScene *rs = (RefScene *)h;
+    Shape *s = rs->objects.at(object_index);
+    for (int i = 0; i < 16; ++i) s->_transform._m[i] = m16[i];
+}
+
+extern "C" int ref_add_ibl_light(void *h, int object_index) {
+    RefScene *rs = (RefScene *)h;
+    Shape *s = rs->objects.at(object_index);
+    rs->lights.push_back(new ImageBasedLight(s, s->MaterialPtr(), s->TexturePtr()));
+    return (int)rs->lights.size() - 1;
+}
+
+// Texture::Pattern(shape, p) of a top-level object's texture at n points (n*3 floats);
+// out n*3 (r, g, b).
+extern "C" void ref_texture_pattern(void *h, int object_index, int n, const float *pts, float *out) {
+    RefScene *rs = (RefScene *)h;
+    Shape *s = rs->objects.at(object_index);
+    Texture *t = s->TexturePtr();
+    for (int i = 0; i < n; ++i) {
+        Color c = t ? t->Pattern(s, P3(pts + 3 * (size_t)i)) : Color(1.0f);
+        out[3 * i] = c._r; out[3 * i + 1] = c._g; out[3 * i + 2] = c._b;
+    }
+}
+
+// LoadHDR into a caller buffer of `cap` floats; returns width * height (0 on failure),
+// dims in wh[2].
+extern "C" int ref_load_hdr(const char *path, int cap, float *out, int *wh) {
+    float *buf = nullptr;
+    int w = 0, hgt = 0;
+    LoadHDR((char *)path, &buf, &w, &hgt);
+    wh[0] = w;
+    wh[1] = hgt;
+    if (!buf) return 0;
+    const long long n = (long long)w * hgt;
+    if (n * 3 <= cap) memcpy(out, buf, sizeof(float) * 3 * (size_t)n);
+    free(buf);
+    return (int)n;
+}
+
+// LoadBmp into a caller buffer of `cap` bytes; returns the byte count, dims in whb[3].
+extern "C" int ref_load_bmp(const char *path, int cap, unsigned char *out, unsigned int *whb) {
+    unsigned char *buf = LoadBmp((char *)path, &whb[0], &whb[1], &whb[2]);
+    const long long n = (long long)whb[0] * whb[1] * whb[2];
+    if (buf && n <= cap) memcpy(out, buf, (size_t)n);
+    free(buf);
+    return (int)n;
+}

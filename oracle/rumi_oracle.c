@@ -100,6 +100,13 @@ typedef struct {
 } orc_camera;
 
 typedef struct {
+    int32_t type;
+    float repeat_u, repeat_v, color1[3], color2[3], gamma;
+    int32_t img_width, img_height, bytes_per_pixel;
+    const void *pixels;
+} orc_texture;
+
+typedef struct {
     int32_t width, height;
     int32_t n_triangles;
     const float *tri_vertices, *tri_normals;
@@ -117,6 +124,10 @@ typedef struct {
     const orc_light *lights;
     orc_volume volume;
     orc_camera camera;
+    int32_t n_textures;
+    const orc_texture *textures;
+    const int32_t *tri_texture, *rect_texture, *sphere_texture;
+    const float *sphere_frame;
 } orc_scene_desc;
 
 enum { MATTE = 0, GLOSSY = 1, SPECULAR = 2, EMISSIVE = 3, DIELECTRIC = 4, SUBSURFACE = 5 };
@@ -184,8 +195,9 @@ static int rect_isect(const Ray *r, V3 p, V3 l, V3 w, int emitting, float tbest,
     return 1;
 }
 
-/* Sphere::Intersect + SolveQuadratic, src/Shape/sphere.cpp:51-132, src/Kernel/clibrary.h:62-87 */
-static int sphere_isect(const Ray *r, V3 c, float rad, int swap, float tbest, float *t_out) {
+/* Sphere::Intersect + SolveQuadratic, src/Shape/sphere.cpp:51-132, src/Kernel/clibrary.h:62-87;
+ * ibl: an emissive, textured sphere, whose roots swap (again) for a ray starting inside */
+static int sphere_isect(const Ray *r, V3 c, float rad, int swap, int ibl, float tbest, float *t_out) {
     V3 roc = sub(r->o, c);
     float A = 1.0f, B = 2.0f * dot(r->d, roc), C = dot(roc, roc) - rad * rad;
     float disc = B * B - 4 * A * C, t0, t1;
@@ -200,6 +212,7 @@ static int sphere_isect(const Ray *r, V3 c, float rad, int swap, float tbest, fl
     }
     if (t0 < 0.0f && t1 < 0.0f) return 0;
     if (swap) { float tmp = t0; t0 = t1; t1 = tmp; }
+    if (ibl && length(roc) < rad) { float tmp = t0; t0 = t1; t1 = tmp; }
     if (t0 < EPS) return 0;
     if (r->tmax - t0 < EPS) return 0;
     if (t0 > tbest && tbest > 0.0f) return 0;
@@ -208,6 +221,12 @@ static int sphere_isect(const Ray *r, V3 c, float rad, int swap, float tbest, fl
 }
 
 typedef struct { float t; int id; float u, v; int back; } Hit;
+
+/* Material::IsLe() and a texture: Sphere::Intersect's image-based-light branch */
+static int sphere_ibl(const orc_scene_desc *s, int i) {
+    return s->materials[s->sphere_material[i]].type == EMISSIVE && s->n_textures > 0 && s->sphere_texture &&
+           s->sphere_texture[i] >= 0;
+}
 
 /* Brute-force stand-in for BVHAccel::Travel (src/Acceleration/bvh.cpp:150-213) over all
  * primitives in canonical order (triangles, rects, spheres), same acceptance rules.
@@ -233,7 +252,7 @@ static Hit closest(const orc_scene_desc *s, const Ray *r, int anyhit) {
     }
     for (int i = 0; i < s->n_spheres; ++i) {
         const float *q = s->spheres + 4 * (size_t)i;
-        if (sphere_isect(r, fv(q), q[3], r->in_object && !anyhit, h.t, &t)) {
+        if (sphere_isect(r, fv(q), q[3], r->in_object && !anyhit, sphere_ibl(s, i), h.t, &t)) {
             h.t = t; h.id = s->n_triangles + s->n_rects + i; h.u = h.v = 0.0f; h.back = 0;
             if (anyhit) return h;
         }
@@ -530,16 +549,126 @@ static int dist_sample(V3 st, float avg_st, float absorb, float smax, float xi, 
 }
 
 /* ------------------------------------------------------------------ lights */
-typedef struct { V3 P, nL, Li; float pdf; int delta; float cos_cone; V3 dir; } LSample;
+typedef struct { V3 P, nL, Li; float pdf; int delta; float cos_cone; V3 dir; int ibl; V3 wi; } LSample;
+
+/* ------------------------------------------------------------------ textures
+ * Checker::Pixel (checker.cpp:24-32), ImageTexture::Pixel (imagetexture.cpp:32-61),
+ * HDRTexture::Pixel (hdrtexture.cpp:46-59). */
+static V3 tex_pixel(const orc_texture *t, float u, float v) {
+    if (t->type == 0) {
+        if ((int)(u * t->repeat_u) % 2 == 0 && (int)(v * t->repeat_v) % 2 == 0) return fv(t->color2);
+        if ((int)(u * t->repeat_u) % 2 != 0 && (int)(v * t->repeat_v) % 2 != 0) return fv(t->color2);
+        return fv(t->color1);
+    }
+    if (t->type == 1) {
+        const unsigned char *b = (const unsigned char *)t->pixels;
+        unsigned H = (unsigned)t->img_height, W = (unsigned)t->img_width, bpp = (unsigned)t->bytes_per_pixel;
+        if (!b) return v3(1, 1, 1);
+        int row = (int)((1.0f - v) * (float)(H - 1));
+        int col = (int)(u * (float)(W - 1));
+        int idx = (int)((H - 1 - (unsigned)row) * W * bpp) + col * (int)bpp;
+        float inv = 1.0f / 255.0f;
+        float cb = (float)b[idx] * inv, cg = (float)b[idx + 1] * inv, cr = (float)b[idx + 2] * inv;
+        if (t->gamma != 1.0f) {
+            cb = powf(cb, t->gamma);
+            cg = powf(cg, t->gamma);
+            cr = powf(cr, t->gamma);
+        }
+        return v3(cr, cg, cb);
+    }
+    const float *h = (const float *)t->pixels;
+    int row = (int)((1.0f - v) * (float)(t->img_height - 1));
+    int col = (int)((1.0f - u) * (float)(t->img_width - 1));
+    int idx = row * t->img_width * 3 + col * 3;
+    return v3(h[idx], h[idx + 1], h[idx + 2]);
+}
+
+/* Shape::TextureMapping (shape.cpp:86-92: (0, 0)), Rect::TextureMapping (rect.cpp:183-196),
+ * Sphere::TextureMapping (sphere.cpp:172-192) */
+static void tex_mapping(const orc_scene_desc *s, int id, V3 p, float *u, float *v) {
+    *u = 0.0f;
+    *v = 0.0f;
+    if (id < s->n_triangles) return;
+    if (id < s->n_triangles + s->n_rects) {
+        const float *q = s->rects + 9 * (size_t)(id - s->n_triangles);
+        V3 l = fv(q + 3), w = fv(q + 6);
+        float len = length(l), wid = length(w);
+        V3 on = sub(p, fv(q));
+        *u = dot(on, l) / (len * len);
+        *v = dot(on, w) / (wid * wid);
+        if (*u >= 1.0f) *u = 1.0f;
+        if (*u <= 0.0f) *u = 0.0f;
+        if (*v >= 1.0f) *v = 1.0f;
+        if (*v <= 0.0f) *v = 0.0f;
+        return;
+    }
+    int k = id - s->n_triangles - s->n_rects;
+    const float *c = s->spheres + 4 * (size_t)k;
+    V3 uu = v3(1, 0, 0), vv = v3(0, 1, 0), ww = v3(0, 0, 1);
+    if (s->sphere_frame) {
+        const float *f = s->sphere_frame + 9 * (size_t)k;
+        uu = fv(f);
+        vv = fv(f + 3);
+        ww = fv(f + 6);
+    }
+    V3 pc = normalize(sub(p, fv(c)));
+    float theta = acosf(dot(pc, vv));
+    V3 pcxz = mul(pc, sinf(theta));
+    float phi = atan2f(dot(pcxz, uu), dot(pcxz, ww));
+    if (phi >= 0.0f)
+        *u = (float)(phi / (2.0f * PI_D));
+    else
+        *u = (float)((phi + 2.0f * PI_D) / (2.0f * PI_D));
+    *v = (float)(1.0f - theta / PI_D);
+}
+
+/* Texture::Pattern (texture.cpp:17-23) of primitive id at p; 1 without a texture */
+static V3 tex_pattern(const orc_scene_desc *s, int id, V3 p) {
+    int t = -1;
+    if (s->n_textures <= 0) return v3(1, 1, 1);
+    if (id < s->n_triangles) t = s->tri_texture ? s->tri_texture[id] : -1;
+    else if (id < s->n_triangles + s->n_rects) t = s->rect_texture ? s->rect_texture[id - s->n_triangles] : -1;
+    else t = s->sphere_texture ? s->sphere_texture[id - s->n_triangles - s->n_rects] : -1;
+    if (t < 0) return v3(1, 1, 1);
+    float u, v;
+    tex_mapping(s, id, p, &u, &v);
+    return tex_pixel(&s->textures[t], u, v);
+}
 
 static float rect_inv_area(const float *r) { return 1.0f / (length(fv(r + 3)) * length(fv(r + 6))); }
 
-static LSample light_sample(const orc_scene_desc *s, float ul, float u1, float u2) {
+/* p, n: the shading point and normal, read by an image-based light
+ * (ImageBasedLight::UniformSampling, imagebasedlight.cpp:38-69) */
+static LSample light_sample(const orc_scene_desc *s, float ul, float u1, float u2, V3 p, V3 n) {
     LSample ls;
     memset(&ls, 0, sizeof(ls));
     int k = (int)(ul * (float)s->n_lights);
     if (k >= s->n_lights) k = s->n_lights - 1;
     const orc_light *L = &s->lights[k];
+    if (L->type == 2) { /* image-based light */
+        V3 uu, ww;
+        onb(n, &uu, &ww);
+        float phi = (float)((double)(u1 * 2.0f) * PI_D);
+        float theta = acosf(sqrtf(1.0f - u2));
+        float st = sinf(theta);
+        float su = st * sinf(phi), sv = cosf(theta), sw = st * cosf(phi);
+        V3 wi = add(add(mul(uu, su), mul(n, sv)), mul(ww, sw));
+        const float *c = s->spheres + 4 * (size_t)L->shape_index;
+        Ray r = {p, wi, 3.402823466e+38f, 0};
+        float t = 0.0f;
+        if (!sphere_isect(&r, fv(c), c[3], 0, sphere_ibl(s, L->shape_index), 0.0f, &t)) t = 0.0f;
+        ls.P = add(p, mul(wi, t));
+        ls.nL = neg(wi);
+        ls.wi = wi;
+        ls.ibl = 1;
+        ls.Li = tex_pattern(s, s->n_triangles + s->n_rects + L->shape_index, ls.P);
+        float cost = dot(wi, n);
+        if (cost <= 0.0f) cost = 1e-4f;
+        float pdf = (float)(0.3183098865475128 * cost);
+        if (pdf <= 0.0f) pdf = 1e-4f;
+        ls.pdf = 1.0f / (float)s->n_lights * pdf;
+        return ls;
+    }
     if (L->type == 1) { /* spot */
         ls.delta = 1;
         ls.P = fv(L->position);
@@ -568,6 +697,12 @@ static LSample light_sample(const orc_scene_desc *s, float ul, float u1, float u
 
 /* Scene::VisibilityTest's geometry + AreaLight::G (scene.cpp:99-123, arealight.cpp:106-112) */
 static int nee_geom(const LSample *ls, V3 p, V3 *wi, float *dist, float *G) {
+    if (ls->ibl) { /* Wi = the sampled direction, G = ImageBasedLight::G = 1 */
+        *wi = ls->wi;
+        *dist = length(sub(ls->P, p));
+        *G = 1.0f;
+        return dot(*wi, ls->nL) < 0.0f;
+    }
     *wi = normalize(sub(ls->P, p));
     *dist = length(sub(p, ls->P));
     if (ls->delta) {
@@ -722,7 +857,7 @@ static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, cons
                     V3 p = add(o, mul(d, tn < 0.0f ? sd : tn + sd));
                     V3 vol = vdiv(tau, pdf);
                     if (s->n_lights > 0) { /* HomogeneousVolume::DirectLighting */
-                        LSample ls = light_sample(s, U0[3], U1[0], U1[1]);
+                        LSample ls = light_sample(s, U0[3], U1[0], U1[1], p, v3(0.0f, 1.0f, 0.0f));
                         V3 wi;
                         float dist, G;
                         if (nee_geom(&ls, p, &wi, &dist, &G)) {
@@ -776,7 +911,7 @@ static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, cons
                     n = normalize(sub(p, fv(c)));
             }
             if (m->type == EMISSIVE) {
-                if (le && !inobj && -dot(d, n) > 0.0f) L = add(L, vmul(beta, mat_le(m)));
+                if (le && !inobj && -dot(d, n) > 0.0f) L = add(L, vmul(vmul(beta, mat_le(m)), tex_pattern(s, h.id, p)));
             } else {
                 V3 wo = neg(d), vol_ratio = v3(1, 1, 1), volw = v3(1, 1, 1);
                 Bsdf bs;
@@ -806,12 +941,14 @@ static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, cons
                 } else {
                     bs = mat_sample(m, wo, n, U0[0], U0[1], U0[2]);
                 }
+                /* Texture::Pattern scales what this vertex returns (pathtracer.cpp:343-344) */
+                beta = vmul(beta, tex_pattern(s, h.id, p));
                 if (!absorbed) {
                     float kd_pdf = m->type == GLOSSY ? m->kd / (m->kd + m->ks) : 1.0f;
                     int nee = s->n_lights > 0 && !walk &&
                               (m->type == MATTE || (m->type == GLOSSY && m->kd != 0.0f && bs.xi <= kd_pdf));
                     if (nee) { /* Matte::DirectLighting, matte.cpp:54-82 */
-                        LSample ls = light_sample(s, U0[3], U1[0], U1[1]);
+                        LSample ls = light_sample(s, U0[3], U1[0], U1[1], p, n);
                         V3 wi;
                         float dist, G;
                         if (nee_geom(&ls, p, &wi, &dist, &G)) {
@@ -882,12 +1019,13 @@ static V3 whitted(const orc_scene_desc *s, int max_depth, uint64_t path, const u
     float U0[4], U1[4], U2[4];
     path_u(path, depth, 0, key, U0);
     V3 wo = neg(d);
+    V3 pat = tex_pattern(s, h.id, p); /* lo *= Texture::Pattern (raytracer.cpp:69-70) */
     if (m->type == SPECULAR) {
         Bsdf b = mat_sample(m, wo, n, U0[0], U0[1], U0[2]);
         float tt;
         V3 Li = whitted(s, max_depth, path, key, p, b.w, depth + 1, 1, 0, &tt);
         V3 f = mul(albedo, m->kd);
-        return mul(mul(vmul(f, Li), b.cost), 1.0f / b.pdfw);
+        return vmul(mul(mul(vmul(f, Li), b.cost), 1.0f / b.pdfw), pat);
     }
     if (m->type == DIELECTRIC) {
         Bsdf b = mat_sample(m, wo, n, U0[0], U0[1], U0[2]);
@@ -902,17 +1040,17 @@ static V3 whitted(const orc_scene_desc *s, int max_depth, uint64_t path, const u
             inv = 1.0f / b.pdf_path;
         }
         if (b.go_in) lo = vmul(lo, v3(expf(-m->rgb[0] * tt), expf(-m->rgb[1] * tt), expf(-m->rgb[2] * tt)));
-        return mul(lo, inv);
+        return vmul(mul(lo, inv), pat);
     }
     if (m->type == EMISSIVE) {
         if (inobj || !le || -dot(d, n) <= 0.0f) return v3(0, 0, 0);
-        return mat_le(m);
+        return vmul(mat_le(m), pat);
     }
     float kd_pdf = m->type == GLOSSY ? m->kd / (m->kd + m->ks) : 1.0f;
     if (s->n_lights > 0 && (m->type == MATTE || (m->type == GLOSSY && m->kd != 0.0f && 1.0f <= kd_pdf))) {
         path_u(path, depth, 1, key, U1);
         path_u(path, depth, 2, key, U2);
-        LSample ls = light_sample(s, U0[3], U1[0], U1[1]);
+        LSample ls = light_sample(s, U0[3], U1[0], U1[1], p, n);
         V3 wi;
         float dist, G;
         if (!nee_geom(&ls, p, &wi, &dist, &G)) return v3(0, 0, 0);
@@ -929,7 +1067,7 @@ static V3 whitted(const orc_scene_desc *s, int max_depth, uint64_t path, const u
             if (U2[2] < 1.0f - expf(average(vs_t) * -sm)) tr = 0.0f;
         }
         Ray sr = {p, wi, dist, 0};
-        if (tr > 0.0f && closest(s, &sr, 1).t == 0.0f) return direct;
+        if (tr > 0.0f && closest(s, &sr, 1).t == 0.0f) return vmul(direct, pat);
     }
     return v3(0, 0, 0);
 }
@@ -1069,3 +1207,11 @@ void orc_pixel_sample(int s, int spp, long long pixel, uint64_t seed, float *out
 }
 
 int orc_perm(int i, int n, uint32_t key) { return perm(i, n, key); }
+
+/* Texture::Pattern of canonical primitives prim[n] at pts (n*3); out n*3 (r, g, b). */
+void orc_texture_pattern(const orc_scene_desc *s, int64_t n, const int32_t *prim, const float *pts, float *out) {
+    for (int64_t i = 0; i < n; ++i) {
+        V3 c = tex_pattern(s, prim[i], fv(pts + 3 * i));
+        out[3 * i] = c.x; out[3 * i + 1] = c.y; out[3 * i + 2] = c.z;
+    }
+}

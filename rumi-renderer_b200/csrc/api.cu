@@ -102,6 +102,10 @@ void free_scene(rumi_scene *sc) {
     dfree(sc->sphere_mat, s);
     dfree(sc->materials, s);
     dfree(sc->lights, s);
+    dfree(sc->textures, s);
+    dfree(sc->prim_tex, s);
+    dfree(sc->sphere_frame, s);
+    for (void *p : sc->tex_pixels) dfree(p, s);
     dfree(sc->ws, s);
     if (s) {
         cudaStreamSynchronize(s);
@@ -144,10 +148,93 @@ rumi_status validate(const rumi_scene_desc *d) {
                 return set_error("light sphere index out of range"), RUMI_ERR_INVALID_ARG;
             if (L.shape_type != RUMI_SHAPE_RECT && L.shape_type != RUMI_SHAPE_SPHERE)
                 return set_error("area lights must be rects or spheres"), RUMI_ERR_INVALID_ARG;
+        } else if (L.type == RUMI_LIGHT_IBL) {
+            if (L.shape_type != RUMI_SHAPE_SPHERE || L.shape_index < 0 || L.shape_index >= d->n_spheres)
+                return set_error("an image-based light needs a sphere index"), RUMI_ERR_INVALID_ARG;
+            // ImageBasedLight reads its radiance from the sphere's texture
+            if (!d->sphere_texture || d->sphere_texture[L.shape_index] < 0)
+                return set_error("the image-based light's sphere has no texture"), RUMI_ERR_INVALID_ARG;
+            // HomogeneousVolume::DirectLighting would sample it about the normal of the
+            // segment's surface hit; not supported
+            if (d->volume.present)
+                return set_error("image-based lights with a medium are not supported"), RUMI_ERR_INVALID_ARG;
         } else if (L.type != RUMI_LIGHT_SPOT) {
             return set_error("unknown light type"), RUMI_ERR_INVALID_ARG;
         }
     }
+    if (d->n_textures < 0 || (d->n_textures > 0 && !d->textures))
+        return set_error("textures missing"), RUMI_ERR_INVALID_ARG;
+    for (int i = 0; i < d->n_textures; ++i) {
+        const rumi_texture &t = d->textures[i];
+        if (t.type == RUMI_TEX_CHECKER) continue;
+        if (t.type != RUMI_TEX_IMAGE && t.type != RUMI_TEX_HDR)
+            return set_error("unknown texture type"), RUMI_ERR_INVALID_ARG;
+        if (t.img_width <= 0 || t.img_height <= 0 || !t.pixels ||
+            (long long)t.img_width * t.img_height > (1LL << 28))
+            return set_error("texture image missing or too large"), RUMI_ERR_INVALID_ARG;
+        if (t.type == RUMI_TEX_IMAGE && (t.bytes_per_pixel < 3 || t.bytes_per_pixel > 4))
+            return set_error("image textures need 3 or 4 bytes per pixel"), RUMI_ERR_INVALID_ARG;
+    }
+    auto check_tex = [&](const int32_t *a, int n) -> bool {
+        if (!a) return true;
+        for (int i = 0; i < n; ++i)
+            if (a[i] < -1 || a[i] >= d->n_textures) return false;
+        return true;
+    };
+    if (!check_tex(d->tri_texture, d->n_triangles) || !check_tex(d->rect_texture, d->n_rects) ||
+        !check_tex(d->sphere_texture, d->n_spheres))
+        return set_error("texture index out of range"), RUMI_ERR_INVALID_ARG;
+    return RUMI_OK;
+}
+
+// Textures: DevTexture table, pixel arrays, per-primitive texture index and sphere frames.
+// Nothing is allocated for a scene without textures.
+static rumi_status upload_textures(rumi_scene *sc, const rumi_scene_desc *d, cudaStream_t s) {
+    const int nT = d->n_triangles, nR = d->n_rects, nS = d->n_spheres;
+    const bool any = d->n_textures > 0 && (d->tri_texture || d->rect_texture || d->sphere_texture);
+    if (!any) return RUMI_OK;
+    std::vector<DevTexture> tex(d->n_textures);
+    for (int i = 0; i < d->n_textures; ++i) {
+        const rumi_texture &t = d->textures[i];
+        DevTexture &dt = tex[i];
+        memset(&dt, 0, sizeof(dt));
+        dt.type = t.type;
+        dt.rep_u = t.repeat_u;
+        dt.rep_v = t.repeat_v;
+        dt.c1 = make_float3(t.color1[0], t.color1[1], t.color1[2]);
+        dt.c2 = make_float3(t.color2[0], t.color2[1], t.color2[2]);
+        dt.gamma = t.gamma;
+        dt.iw = t.img_width;
+        dt.ih = t.img_height;
+        dt.bpp = t.type == RUMI_TEX_HDR ? 3 : t.bytes_per_pixel;
+        if (t.type == RUMI_TEX_CHECKER) continue;
+        const size_t bytes = t.type == RUMI_TEX_HDR ? sizeof(float) * 3 * (size_t)t.img_width * t.img_height
+                                                    : (size_t)t.img_width * t.img_height * t.bytes_per_pixel;
+        void *p = nullptr;
+        rumi_status st = upload(&p, t.pixels, bytes, s);
+        if (p) sc->tex_pixels.push_back(p);
+        if (st != RUMI_OK) return st;
+        if (t.type == RUMI_TEX_HDR)
+            dt.hdr = (const float *)p;
+        else
+            dt.img = (const unsigned char *)p;
+    }
+    std::vector<int> prim_tex((size_t)nT + nR + nS, -1);
+    for (int i = 0; d->tri_texture && i < nT; ++i) prim_tex[i] = d->tri_texture[i];
+    for (int i = 0; d->rect_texture && i < nR; ++i) prim_tex[(size_t)nT + i] = d->rect_texture[i];
+    for (int i = 0; d->sphere_texture && i < nS; ++i) prim_tex[(size_t)nT + nR + i] = d->sphere_texture[i];
+    std::vector<float4> frame((size_t)nS * 3);
+    for (int i = 0; i < nS; ++i) {
+        const float *f = d->sphere_frame ? d->sphere_frame + 9 * (size_t)i : nullptr;
+        for (int r = 0; r < 3; ++r)
+            frame[3 * i + r] = f ? make_float4(f[3 * r], f[3 * r + 1], f[3 * r + 2], 0.0f)
+                                 : make_float4(r == 0, r == 1, r == 2, 0.0f);
+    }
+    rumi_status st;
+    if ((st = upload(&sc->textures, tex.data(), sizeof(DevTexture) * tex.size(), s)) != RUMI_OK) return st;
+    if ((st = upload(&sc->prim_tex, prim_tex.data(), sizeof(int) * prim_tex.size(), s)) != RUMI_OK) return st;
+    if (nS > 0 && (st = upload(&sc->sphere_frame, frame.data(), sizeof(float4) * frame.size(), s)) != RUMI_OK)
+        return st;
     return RUMI_OK;
 }
 
@@ -273,7 +360,7 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     const int N = nT + nR + nS;
     configure_pool(sc->device);
     std::vector<float4> rects((size_t)nR * 3);
-    std::vector<int> rect_emissive(nR);
+    std::vector<int> rect_emissive((size_t)nR + nS);  // prim flags: rects, then spheres
     std::vector<DevMaterial> mats(d->n_materials);
     for (int i = 0; i < d->n_materials; ++i) mats[i] = make_material(d->materials[i]);
     for (int i = 0; i < nR; ++i) {
@@ -289,8 +376,12 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
         rect_emissive[i] = m.type == RUMI_MAT_EMISSIVE && (m.le.x != 0.0f || m.le.y != 0.0f || m.le.z != 0.0f);
     }
     std::vector<float4> spheres(nS);
-    for (int i = 0; i < nS; ++i)
+    for (int i = 0; i < nS; ++i) {
         spheres[i] = make_float4(d->spheres[4 * i], d->spheres[4 * i + 1], d->spheres[4 * i + 2], d->spheres[4 * i + 3]);
+        // Sphere::Intersect's image-based-light branch: Material::IsLe() and a texture
+        rect_emissive[(size_t)nR + i] = mats[d->sphere_material[i]].type == RUMI_MAT_EMISSIVE &&
+                                        d->n_textures > 0 && d->sphere_texture && d->sphere_texture[i] >= 0;
+    }
     std::vector<DevLight> lights(d->n_lights);
     for (int i = 0; i < d->n_lights; ++i) {
         const rumi_light &L = d->lights[i];
@@ -299,7 +390,9 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
         dl.type = L.type;
         dl.shape_type = L.shape_type;
         dl.shape_index = L.shape_index;
-        if (L.type == RUMI_LIGHT_AREA) {
+        if (L.type == RUMI_LIGHT_IBL) {
+            sc->has_ibl = true;
+        } else if (L.type == RUMI_LIGHT_AREA) {
             int mi;
             if (L.shape_type == RUMI_SHAPE_RECT) {
                 const float *r = d->rects + 9 * (size_t)L.shape_index;
@@ -372,6 +465,7 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     if ((st = upload(&sc->sphere_mat, d->sphere_material, sizeof(int) * (size_t)nS, s)) != RUMI_OK) return fail(st);
     if ((st = upload(&sc->materials, mats.data(), sizeof(DevMaterial) * mats.size(), s)) != RUMI_OK) return fail(st);
     if ((st = upload(&sc->lights, lights.data(), sizeof(DevLight) * lights.size(), s)) != RUMI_OK) return fail(st);
+    if ((st = upload_textures(sc, d, s)) != RUMI_OK) return fail(st);
     // ---- BVH
     sc->n_nodes = bvh_node_capacity(N);
     e = dalloc((void **)&sc->nodes, sizeof(BvhNode) * (size_t)sc->n_nodes, s);
@@ -448,6 +542,10 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     ds.materials = sc->materials;
     ds.lights = sc->lights;
     ds.n_nodes = sc->n_nodes;
+    ds.textures = sc->textures;
+    ds.prim_tex = sc->prim_tex;
+    ds.sphere_frame = sc->sphere_frame;
+    ds.n_textures = sc->textures ? d->n_textures : 0;
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(cuda_status(e, "scene upload"));
     *out = sc;

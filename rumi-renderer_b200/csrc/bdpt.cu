@@ -783,6 +783,10 @@ __global__ void add_light_film(float *film, const float *light, size_t n) {
 rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                         cudaStream_t stream) {
     const DevScene &S = sc->dev;
+    if (S.prim_tex || sc->has_ibl) {
+        set_error("BDPT does not support textures or image-based lights");
+        return RUMI_ERR_INVALID_ARG;
+    }
     if (p->n_light < 2 || p->n_eye < 2 || p->n_light > BD_MAXV || p->n_eye > BD_MAXV) {
         set_error("BDPT needs 2 <= n_light, n_eye <= 16");
         return RUMI_ERR_INVALID_ARG;

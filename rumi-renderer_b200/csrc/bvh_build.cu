@@ -89,7 +89,7 @@ __device__ __forceinline__ float3 centroid(float4 lo, float4 hi) {
 // Bounds of every canonical primitive (from the original vertices, so they contain the
 // triangle however its edges round) and its 48-byte intersection record.
 __global__ void prim_prepare_kernel(const float *tri_v, int n_tris, const float4 *rects, int n_rects,
-                                    const float4 *spheres, const int *rect_emissive, int n_spheres,
+                                    const float4 *spheres, const int *prim_flags, int n_spheres,
                                     float4 *aabb_lo, float4 *aabb_hi, float4 *prims) {
     const int N = n_tris + n_rects + n_spheres;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
@@ -114,7 +114,7 @@ __global__ void prim_prepare_kernel(const float *tri_v, int n_tris, const float4
             hi = mk3(fmaxf(fmaxf(p.x, q.x), fmaxf(pl.x, pw.x)), fmaxf(fmaxf(p.y, q.y), fmaxf(pl.y, pw.y)),
                      fmaxf(fmaxf(p.z, q.z), fmaxf(pl.z, pw.z)));
             A = make_float4(p.x, p.y, p.z, __int_as_float(i));
-            B = make_float4(l.x, l.y, l.z, __int_as_float(PRIM_RECT | (rect_emissive[r] ? PRIM_FLAG_EMISSIVE : 0)));
+            B = make_float4(l.x, l.y, l.z, __int_as_float(PRIM_RECT | (prim_flags[r] ? PRIM_FLAG_EMISSIVE : 0)));
             C = make_float4(w.x, w.y, w.z, 0.0f);
         } else {
             const int s = i - n_tris - n_rects;
@@ -122,7 +122,8 @@ __global__ void prim_prepare_kernel(const float *tri_v, int n_tris, const float4
             lo = mk3(c.x - c.w, c.y - c.w, c.z - c.w);
             hi = mk3(c.x + c.w, c.y + c.w, c.z + c.w);
             A = make_float4(c.x, c.y, c.z, __int_as_float(i));
-            B = make_float4(c.w, 0.0f, 0.0f, __int_as_float(PRIM_SPHERE));
+            B = make_float4(c.w, 0.0f, 0.0f,
+                            __int_as_float(PRIM_SPHERE | (prim_flags[n_rects + s] ? PRIM_FLAG_IBL : 0)));
             C = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
         aabb_lo[i] = make_float4(lo.x, lo.y, lo.z, 0.0f);
@@ -910,7 +911,7 @@ size_t bvh_scratch_bytes(int n_prims) {
 // Builds the BVH of the canonical primitives into `nodes` (bvh_node_capacity entries)
 // and `leaf_prims` (3N float4).  scratch must hold bvh_scratch_bytes(N).  Returns 0 on
 // success, else a cudaError_t value (or -1 when the builder's internal bounds were hit).
-int bvh_build(const float *d_tri_v, int n_tris, const float4 *d_rects, const int *d_rect_emissive, int n_rects,
+int bvh_build(const float *d_tri_v, int n_tris, const float4 *d_rects, const int *d_prim_flags, int n_rects,
               const float4 *d_spheres, int n_spheres, BvhNode *nodes, float4 *leaf_prims, void *scratch,
               cudaStream_t stream, BvhBuildInfo *info) {
     const int N = n_tris + n_rects + n_spheres;
@@ -953,7 +954,7 @@ int bvh_build(const float *d_tri_v, int n_tris, const float4 *d_rects, const int
     int pair_base = small_region + 2 * (int)n;
     const int grid_n = cdiv((long long)n, 256) < 148 * 8 ? cdiv((long long)n, 256) : 148 * 8;
     prim_prepare_kernel<<<grid_n > 0 ? grid_n : 1, 256, 0, stream>>>(d_tri_v, n_tris, d_rects, n_rects, d_spheres,
-                                                                     d_rect_emissive, n_spheres, aabb_lo, aabb_hi,
+                                                                     d_prim_flags, n_spheres, aabb_lo, aabb_hi,
                                                                      prims_canon);
     iota_kernel<<<grid_n > 0 ? grid_n : 1, 256, 0, stream>>>(idx, N);
     root_kernel<<<1, 1024, 0, stream>>>(aabb_lo, aabb_hi, N, nodes, tasks[0], n_cur, small, n_small);

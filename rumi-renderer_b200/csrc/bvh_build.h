@@ -15,7 +15,9 @@ struct BvhBuildInfo {
 
 int bvh_node_capacity(int n_prims);
 size_t bvh_scratch_bytes(int n_prims);
-int bvh_build(const float *d_tri_v, int n_tris, const float4 *d_rects, const int *d_rect_emissive, int n_rects,
+// d_prim_flags: n_rects + n_spheres ints -- per rect "emissive" (one-sided test off), then
+// per sphere "image-based light" (far root from inside)
+int bvh_build(const float *d_tri_v, int n_tris, const float4 *d_rects, const int *d_prim_flags, int n_rects,
               const float4 *d_spheres, int n_spheres, BvhNode *nodes, float4 *leaf_prims, void *scratch,
               cudaStream_t stream, BvhBuildInfo *info);
 

@@ -308,6 +308,13 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) pt_trace
 // faces away or lies outside a spot cone (Scene::VisibilityTest's facing test,
 // src/Scene/scene.cpp:99-123).  wi / dist: the shadow ray; G: AreaLight::G.
 RUMI_D bool nee_setup(const LightSample &ls, float3 p, float3 &wi, float &dist, float &G) {
+    if (ls.is_ibl) {  // ImageBasedLight: Wi is the sampled direction, G = 1
+        wi = ls.wi;
+        const float3 dv = rn_sub(ls.P, p);
+        dist = __fsqrt_rn(rn_dot(dv, dv));
+        G = 1.0f;
+        return rn_dot(wi, ls.nL) < 0.0f;
+    }
     const float3 dv = ls.P - p;
     wi = normalize_ref(dv);
     dist = sqrtf(dot3(p - ls.P, p - ls.P));
@@ -513,8 +520,9 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                 }
             }
             if (m.type == MAT_EMISSIVE) {
-                // Emissive::DirectLighting (emissive.cpp:61-74); the path ends here.
-                if (le && !inobj && -dot3(d, nrm) > 0.0f) addL = beta * m.le;
+                // Emissive::DirectLighting (emissive.cpp:61-74) times the texture
+                // (pathtracer.cpp:343-344); the path ends here.
+                if (le && !inobj && -dot3(d, nrm) > 0.0f) addL = beta * m.le * tex_pattern(S, id, p);
             } else {
                 const float3 wo = -d;
                 BsdfSample b;
@@ -544,6 +552,9 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                 } else {
                     b = material_sample(m, wo, nrm, U0.u[0], U0.u[1], U0.u[2]);
                 }
+                // Texture::Pattern scales everything this vertex returns, its light
+                // sample and what comes after it (pathtracer.cpp:343-344)
+                if (S.prim_tex) beta = beta * tex_pattern(S, id, p);
                 if (!absorbed) {
                     // NEE: Matte::DirectLighting (matte.cpp:54-82); Glossy only on its
                     // diffuse lobe, divided by kd_pdf (glossy.cpp:92-102)
@@ -551,7 +562,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce
                                      (m.type == MAT_MATTE ||
                                       (m.type == MAT_GLOSSY && m.kd != 0.0f && b.xi <= m.kd_pdf));
                     if (nee) {
-                        const LightSample ls = sample_light(S, U0.u[3], U1.u[0], U1.u[1]);
+                        const LightSample ls = sample_light(S, U0.u[3], U1.u[0], U1.u[1], p, nrm);
                         float3 wi;
                         float dist, G;
                         if (nee_setup(ls, p, wi, dist, G)) {
@@ -682,6 +693,8 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade_whitted(PtLaunch P, in
                 const float3 a = S.materials[__float_as_int(beta4.w)].rgb;
                 beta = beta * mk3(expf(-a.x * t), expf(-a.y * t), expf(-a.z * t));
             }
+            // Texture::Pattern scales what this vertex returns (raytracer.cpp:69-70)
+            if (S.prim_tex) beta = beta * tex_pattern(S, id, p);
             const float3 wo = -d;
             const Uniform4 U0 = path_uniforms(path, bounce, 0, P.k0, P.k1);
             if (m.type == MAT_SPECULAR) {
@@ -716,7 +729,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade_whitted(PtLaunch P, in
             } else if (S.n_lights > 0 && (m.type == MAT_MATTE || (m.type == MAT_GLOSSY && m.kd != 0.0f &&
                                                                   1.0f <= m.kd_pdf))) {
                 const Uniform4 U1 = path_uniforms(path, bounce, 1, P.k0, P.k1);
-                const LightSample ls = sample_light(S, U0.u[3], U1.u[0], U1.u[1]);
+                const LightSample ls = sample_light(S, U0.u[3], U1.u[0], U1.u[1], p, nrm);
                 float3 wi;
                 float dist, G;
                 if (nee_setup(ls, p, wi, dist, G)) {

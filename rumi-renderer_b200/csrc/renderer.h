@@ -21,6 +21,11 @@ struct rumi_scene {
     int *sphere_mat = nullptr;
     DevMaterial *materials = nullptr;
     DevLight *lights = nullptr;
+    DevTexture *textures = nullptr;
+    int *prim_tex = nullptr;
+    float4 *sphere_frame = nullptr;
+    std::vector<void *> tex_pixels;  // one device array per image texture
+    bool has_ibl = false;
     int n_nodes = 0;
     rumi::BvhBuildInfo info{};
     double build_ms = 0.0;

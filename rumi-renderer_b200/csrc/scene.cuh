@@ -12,15 +12,22 @@
 //   sphere_mat : int[n_spheres]
 //   materials  : DevMaterial[n_materials]
 //   lights     : DevLight[n_lights]
+//   textures   : DevTexture[n_textures] (+ one pixel array each), prim_tex : int[n_prims]
+//                (canonical order, -1 = none), sphere_frame : float4[3 * n_spheres]
+//                (present only when the scene has textures)
 #pragma once
 #include "common.cuh"
 
 // Primitive kinds stored in leaf_prims[3i+1].w (as int bits).
 enum { PRIM_TRI = 0, PRIM_RECT = 1, PRIM_SPHERE = 2 };
 #define PRIM_FLAG_EMISSIVE 0x100
+// an emissive, textured sphere (an image-based light's sphere): a ray that starts inside
+// it takes the far root (Sphere::Intersect, sphere.cpp:85-92)
+#define PRIM_FLAG_IBL 0x200
 
 enum { MAT_MATTE = 0, MAT_GLOSSY = 1, MAT_SPECULAR = 2, MAT_EMISSIVE = 3, MAT_DIELECTRIC = 4, MAT_SUBSURFACE = 5 };
-enum { LIGHT_AREA = 0, LIGHT_SPOT = 1 };
+enum { LIGHT_AREA = 0, LIGHT_SPOT = 1, LIGHT_IBL = 2 };
+enum { TEX_CHECKER = 0, TEX_IMAGE = 1, TEX_HDR = 2 };
 enum { SHAPE_TRI = 0, SHAPE_RECT = 1, SHAPE_SPHERE = 2 };
 
 // 32-byte BVH node.  count > 0: leaf over leaf_prims[first .. first+count).
@@ -67,6 +74,16 @@ struct DevMaterial {
     float kd_pdf;             // Glossy kd / (kd + ks)
     float phong_norm;         // Glossy (e + 1) / (2 pi)
     float3 le;                // Emissive rgb * ls
+};
+
+struct DevTexture {
+    int type;                   // TEX_CHECKER / TEX_IMAGE / TEX_HDR
+    float rep_u, rep_v;         // Checker _w, _h
+    float3 c1, c2;              // Checker colours
+    float gamma;                // ImageTexture gamma
+    int iw, ih, bpp;            // image width, height, bytes per pixel
+    const unsigned char *img;   // ImageTexture: LoadBmp's buffer
+    const float *hdr;           // HDRTexture: LoadHDR's buffer
 };
 
 struct DevLight {
@@ -117,6 +134,11 @@ struct DevScene {
     DevVolume volume;
     DevCamera camera;
     int width, height;
+    // textures (null when the scene has none)
+    const DevTexture *textures;
+    const int *prim_tex;
+    const float4 *sphere_frame;
+    int n_textures;
 };
 
 // Canonical primitive id -> material index.

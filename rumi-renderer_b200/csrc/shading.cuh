@@ -14,6 +14,7 @@
 // sqrt(1-u), cos(acos(x)) = x), equal up to float rounding.
 #pragma once
 #include "scene.cuh"
+#include "traverse.cuh"
 
 // ----------------------------------------------------------------- frames
 RUMI_D void onb_ref(float3 v0, float3 &v1, float3 &v2) {
@@ -328,7 +329,127 @@ struct LightSample {
     bool is_delta;  // spot light: no area pdf, no cosine at the light
     float cos_cone;
     float3 spot_dir;
+    bool is_ibl;    // image-based light: wi sampled about the shading normal, G = 1
+    float3 wi;
 };
+
+// ------------------------------------------------------------------ textures
+// Checker::Pixel (checker.cpp:24-32), ImageTexture::Pixel (imagetexture.cpp:32-61),
+// HDRTexture::Pixel (hdrtexture.cpp:46-59) at (u, v), with the reference's conversions:
+// the index products are float, truncated to int.  Out-of-range indices (only a NaN
+// coordinate produces them) read the first pixel.
+RUMI_D float3 tex_pixel(const DevTexture &t, float u, float v) {
+    if (t.type == TEX_CHECKER) {
+        const int a = (int)(u * t.rep_u) % 2, b = (int)(v * t.rep_v) % 2;
+        if (a == 0 && b == 0) return t.c2;
+        if (a != 0 && b != 0) return t.c2;
+        return t.c1;
+    }
+    if (t.type == TEX_IMAGE) {
+        if (!t.img) return mk3(1.0f, 1.0f, 1.0f);
+        const int row = (int)(__fmul_rn(__fsub_rn(1.0f, v), (float)(unsigned)(t.ih - 1)));
+        const int col = (int)(__fmul_rn(u, (float)(unsigned)(t.iw - 1)));
+        long long idx = (long long)(t.ih - 1 - row) * t.iw * t.bpp + (long long)col * t.bpp;
+        if (idx < 0 || idx + 2 >= (long long)t.iw * t.ih * t.bpp) idx = 0;
+        const float inv = 1.0f / 255.0f;
+        float b = __fmul_rn((float)t.img[idx], inv), g = __fmul_rn((float)t.img[idx + 1], inv),
+              r = __fmul_rn((float)t.img[idx + 2], inv);
+        if (t.gamma != 1.0f) {
+            b = powf(b, t.gamma);
+            g = powf(g, t.gamma);
+            r = powf(r, t.gamma);
+        }
+        return mk3(r, g, b);
+    }
+    const int row = (int)(__fmul_rn(__fsub_rn(1.0f, v), (float)(t.ih - 1)));
+    const int col = (int)(__fmul_rn(__fsub_rn(1.0f, u), (float)(t.iw - 1)));
+    long long idx = (long long)row * t.iw * 3 + (long long)col * 3;
+    if (idx < 0 || idx + 2 >= (long long)t.iw * t.ih * 3) idx = 0;
+    return mk3(t.hdr[idx], t.hdr[idx + 1], t.hdr[idx + 2]);
+}
+
+// Shape::TextureMapping of canonical primitive `id` at p: (0, 0) for triangles
+// (shape.cpp:86-92); Rect::TextureMapping (rect.cpp:183-196); Sphere::TextureMapping
+// (sphere.cpp:172-192), oriented by the rows of the sphere's _transform, with the
+// reference's double-precision divisions by PI.
+RUMI_D void tex_mapping(const DevScene &S, int id, float3 p, float &u, float &v) {
+    u = 0.0f;
+    v = 0.0f;
+    if (id < S.n_tris) return;
+    if (id < S.n_tris + S.n_rects) {
+        const int r = id - S.n_tris;
+        const float3 rp = f4xyz(S.rects[3 * r]), l = f4xyz(S.rects[3 * r + 1]), w = f4xyz(S.rects[3 * r + 2]);
+        const float len = __fsqrt_rn(rn_dot(l, l)), wid = __fsqrt_rn(rn_dot(w, w));
+        const float3 on = rn_sub(p, rp);
+        u = __fdiv_rn(rn_dot(on, l), __fmul_rn(len, len));
+        v = __fdiv_rn(rn_dot(on, w), __fmul_rn(wid, wid));
+        if (u >= 1.0f) u = 1.0f;
+        if (u <= 0.0f) u = 0.0f;
+        if (v >= 1.0f) v = 1.0f;
+        if (v <= 0.0f) v = 0.0f;
+        return;
+    }
+    const int k = id - S.n_tris - S.n_rects;
+    const float3 c = f4xyz(S.spheres[k]);
+    float3 uu = mk3(1.0f, 0.0f, 0.0f), vv = mk3(0.0f, 1.0f, 0.0f), ww = mk3(0.0f, 0.0f, 1.0f);
+    if (S.sphere_frame) {
+        uu = f4xyz(S.sphere_frame[3 * k]);
+        vv = f4xyz(S.sphere_frame[3 * k + 1]);
+        ww = f4xyz(S.sphere_frame[3 * k + 2]);
+    }
+    const float3 pc = normalize_ref(rn_sub(p, c));
+    const float theta = acosf(rn_dot(pc, vv));
+    const float st = sinf(theta);
+    const float3 pcxz = mk3(__fmul_rn(pc.x, st), __fmul_rn(pc.y, st), __fmul_rn(pc.z, st));
+    const float phi = atan2f(rn_dot(pcxz, uu), rn_dot(pcxz, ww));
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    u = phi >= 0.0f ? (float)__ddiv_rn((double)phi, two_pi) : (float)__ddiv_rn(__dadd_rn((double)phi, two_pi), two_pi);
+    v = (float)__dsub_rn(1.0, __ddiv_rn((double)theta, 3.14159265358979323846));
+}
+
+// Texture::Pattern (texture.cpp:17-23): the texture of primitive `id` at p; 1 without one.
+RUMI_D float3 tex_pattern(const DevScene &S, int id, float3 p) {
+    if (!S.prim_tex) return mk3(1.0f, 1.0f, 1.0f);
+    const int t = __ldg(&S.prim_tex[id]);
+    if (t < 0) return mk3(1.0f, 1.0f, 1.0f);
+    float u, v;
+    tex_mapping(S, id, p, u, v);
+    return tex_pixel(S.textures[t], u, v);
+}
+
+// ImageBasedLight::UniformSampling (imagebasedlight.cpp:38-69): a cosine-weighted direction
+// about the shading normal n (first uniform: angle about n, second: elevation), the point
+// where it leaves through the light's sphere (Sphere::Intersect without an Intersection:
+// from inside, the far root), the sphere's texture there as radiance.  A ray that misses
+// the sphere leaves the point at p (Ray::_tmin stays 0).
+RUMI_D void sample_ibl(const DevScene &s, const DevLight &L, float3 p, float3 n, float u1, float u2,
+                       LightSample &ls) {
+    float3 uu, ww;
+    onb_ref(n, uu, ww);
+    const float phi = (float)__dmul_rn((double)__fmul_rn(u1, 2.0f), 3.14159265358979323846);
+    const float theta = acosf(__fsqrt_rn(__fsub_rn(1.0f, u2)));
+    const float st = sinf(theta);
+    const float su = __fmul_rn(st, sinf(phi)), sv = cosf(theta), sw = __fmul_rn(st, cosf(phi));
+    const float3 wi = mk3(__fadd_rn(__fadd_rn(__fmul_rn(uu.x, su), __fmul_rn(n.x, sv)), __fmul_rn(ww.x, sw)),
+                          __fadd_rn(__fadd_rn(__fmul_rn(uu.y, su), __fmul_rn(n.y, sv)), __fmul_rn(ww.y, sw)),
+                          __fadd_rn(__fadd_rn(__fmul_rn(uu.z, su), __fmul_rn(n.z, sv)), __fmul_rn(ww.z, sw)));
+    const float4 c = s.spheres[L.shape_index];
+    float t = 0.0f;
+    if (!isect_sphere(p, wi, FLT_MAX, 0.0f, make_float4(c.x, c.y, c.z, 0.0f), make_float4(c.w, 0.0f, 0.0f, 0.0f),
+                      false, true, t))
+        t = 0.0f;
+    ls.P = rn_madd(p, wi, t);
+    ls.nL = -wi;
+    ls.wi = wi;
+    ls.Li = tex_pattern(s, s.n_tris + s.n_rects + L.shape_index, ls.P);
+    float cost = rn_dot(wi, n);
+    if (cost <= 0.0f) cost = 1e-4f;
+    float pdf = (float)__dmul_rn(0.3183098865475128, (double)cost);  // INV_PI is a double literal
+    if (pdf <= 0.0f) pdf = 1e-4f;
+    ls.pdf = (1.0f / (float)s.n_lights) * pdf;
+    ls.is_ibl = true;
+    ls.is_delta = false;
+}
 
 RUMI_D int pick_light(const DevScene &s, float u) {
     int k = (int)(u * (float)s.n_lights);
@@ -336,11 +457,18 @@ RUMI_D int pick_light(const DevScene &s, float u) {
 }
 
 // Scene::VisibilityTest's light part: pick a light, sample a point on it
-// (AreaLight::Sampling -> Shape::ShapeSampling, uniform over the shape).
-RUMI_D LightSample sample_light(const DevScene &s, float ul, float u1, float u2) {
+// (AreaLight::Sampling -> Shape::ShapeSampling, uniform over the shape; an image-based
+// light samples a direction about the shading normal n at p instead).
+RUMI_D LightSample sample_light(const DevScene &s, float ul, float u1, float u2, float3 p = mk3(0.0f, 0.0f, 0.0f),
+                                float3 n = mk3(0.0f, 1.0f, 0.0f)) {
     LightSample ls;
     const DevLight L = s.lights[pick_light(s, ul)];
     ls.is_delta = false;
+    ls.is_ibl = false;
+    if (L.type == LIGHT_IBL) {
+        sample_ibl(s, L, p, n, u1, u2, ls);
+        return ls;
+    }
     ls.pdf = (1.0f / (float)s.n_lights) * L.inv_area;
     ls.Li = L.le;
     if (L.type == LIGHT_SPOT) {

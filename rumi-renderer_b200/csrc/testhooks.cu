@@ -259,3 +259,26 @@ rumi_status rumi_test_pixel_samples(int64_t n, const int32_t *s, int32_t spp, co
 }
 
 }  // extern "C"
+
+namespace {
+__global__ void k_texture(DevScene S, int64_t n, const int32_t *prim, const float *pts, float *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int id = prim[i];
+    float3 c = mk3(1.0f, 1.0f, 1.0f);
+    if (id >= 0 && id < S.n_prims) c = tex_pattern(S, id, mk3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]));
+    out[3 * i] = c.x;
+    out[3 * i + 1] = c.y;
+    out[3 * i + 2] = c.z;
+}
+}  // namespace
+
+rumi_status rumi_test_texture_pattern(rumi_scene *scene, int64_t n, const int32_t *prim, const float *pts,
+                                      float *out) {
+    if (!scene || n < 0 || (n > 0 && (!prim || !pts || !out))) return set_error("bad argument"), RUMI_ERR_INVALID_ARG;
+    DevBuf a, b, o;
+    rumi_status st;
+    if ((st = to_dev(a, prim, n)) || (st = to_dev(b, pts, 3 * n)) || (st = to_dev<float>(o, nullptr, 3 * n))) return st;
+    if (n) k_texture<<<blocks(n), 256>>>(scene->dev, n, (int32_t *)a.p, (float *)b.p, (float *)o.p);
+    return from_dev(out, o, 3 * n);
+}

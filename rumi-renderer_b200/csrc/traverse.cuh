@@ -87,7 +87,7 @@ RUMI_D bool isect_rect(float3 o, float3 d, float tmax, float tbest, float4 A, fl
     return true;
 }
 
-RUMI_D bool isect_sphere(float3 o, float3 d, float tmax, float tbest, float4 A, float4 B, bool in_object,
+RUMI_D bool isect_sphere(float3 o, float3 d, float tmax, float tbest, float4 A, float4 B, bool in_object, bool ibl,
                          float &t_out) {
     const float3 c = f4xyz(A);
     const float r = B.x;
@@ -106,6 +106,9 @@ RUMI_D bool isect_sphere(float3 o, float3 d, float tmax, float tbest, float4 A, 
     }
     if (t0 < 0.0f && t1 < 0.0f) return false;
     if (in_object) {
+        float tmp = t0; t0 = t1; t1 = tmp;
+    }
+    if (ibl && __fsqrt_rn(rn_dot(roc, roc)) < r) {  // inside an image-based light's sphere
         float tmp = t0; t0 = t1; t1 = tmp;
     }
     if (t0 < RUMI_EPS) return false;
@@ -164,7 +167,7 @@ RUMI_D bool leaf_isect(const DevScene &s, int first, int count, float3 o, float3
         else if (kind == PRIM_RECT)
             ok = isect_rect(o, d, tmax, h.t, A, B, C, (tag & PRIM_FLAG_EMISSIVE) != 0, t);
         else
-            ok = isect_sphere(o, d, tmax, h.t, A, B, in_object && !ANYHIT, t);
+            ok = isect_sphere(o, d, tmax, h.t, A, B, in_object && !ANYHIT, (tag & PRIM_FLAG_IBL) != 0, t);
         if (ok) {
             h.t = t;
             h.id = __float_as_int(A.w);

@@ -11,7 +11,7 @@ import numpy as np
 
 from . import _capi
 from .scene import (Scene, FlatScene, PathTracer, BidirectionalPathTracer, RayTracer, PATH_TRACER, BDPT, RAY_TRACER,
-                    LIGHT_AREA, LIGHT_SPOT)
+                    LIGHT_AREA, LIGHT_SPOT, LIGHT_IBL, TEX_CHECKER, TEX_IMAGE)
 
 __all__ = ["GpuScene", "render", "Scene"]
 
@@ -62,7 +62,7 @@ def build_desc(fs: FlatScene):
     lights = (_capi.rumi_light * max(1, len(fs.lights)))()
     for i, L in enumerate(fs.lights):
         lights[i].type = L["type"]
-        if L["type"] == LIGHT_AREA:
+        if L["type"] in (LIGHT_AREA, LIGHT_IBL):
             lights[i].shape_type, lights[i].shape_index = L["shape_type"], L["shape_index"]
         else:
             lights[i].position = _capi.f3(*L["position"])
@@ -84,6 +84,31 @@ def build_desc(fs: FlatScene):
     d.camera.fov_deg = cam.fov
     d.camera.focal_distance = float(getattr(cam, "focal_distance", 0.0))
     d.camera.lens_radius = float(getattr(cam, "lens_radius", 0.0))
+    texs = getattr(fs, "textures", None) or []
+    if texs:
+        tarr = (_capi.rumi_texture * len(texs))()
+        for i, t in enumerate(texs):
+            tarr[i].type = t.kind
+            if t.kind == TEX_CHECKER:
+                tarr[i].repeat_u, tarr[i].repeat_v = t.width, t.height
+                tarr[i].color1, tarr[i].color2 = _capi.f3(*t.c1), _capi.f3(*t.c2)
+            elif t.kind == TEX_IMAGE:
+                tarr[i].gamma = t.gamma
+                tarr[i].img_height, tarr[i].img_width, tarr[i].bytes_per_pixel = t.pixels.shape
+                tarr[i].pixels = t.pixels.ctypes.data
+                keep.append(t.pixels)
+            else:
+                tarr[i].img_height, tarr[i].img_width = t.data.shape[:2]
+                tarr[i].bytes_per_pixel = 12
+                tarr[i].pixels = t.data.ctypes.data
+                keep.append(t.data)
+        keep.append(tarr)
+        d.n_textures, d.textures = len(texs), C.cast(tarr, C.POINTER(_capi.rumi_texture))
+        tt = arr(fs.tri_texture, np.int32)
+        rt = arr(fs.rect_texture, np.int32)
+        st_ = arr(fs.sphere_texture, np.int32)
+        sf = arr(fs.sphere_frame, np.float32)
+        d.tri_texture, d.rect_texture, d.sphere_texture, d.sphere_frame = _ip(tt), _ip(rt), _ip(st_), _fp(sf)
     return d, keep
 
 

@@ -38,6 +38,12 @@ FP = C.POINTER(C.c_float)
 IP = C.POINTER(C.c_int32)
 
 
+class rumi_texture(C.Structure):
+    _fields_ = [("type", C.c_int32), ("repeat_u", C.c_float), ("repeat_v", C.c_float), ("color1", f3),
+                ("color2", f3), ("gamma", C.c_float), ("img_width", C.c_int32), ("img_height", C.c_int32),
+                ("bytes_per_pixel", C.c_int32), ("pixels", C.c_void_p)]
+
+
 class rumi_scene_desc(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32),
                 ("n_triangles", C.c_int32), ("tri_vertices", FP), ("tri_normals", FP), ("tri_material", IP),
@@ -46,7 +52,9 @@ class rumi_scene_desc(C.Structure):
                 ("n_spheres", C.c_int32), ("spheres", FP), ("sphere_material", IP),
                 ("n_materials", C.c_int32), ("materials", C.POINTER(rumi_material)),
                 ("n_lights", C.c_int32), ("lights", C.POINTER(rumi_light)),
-                ("volume", rumi_volume), ("camera", rumi_camera)]
+                ("volume", rumi_volume), ("camera", rumi_camera),
+                ("n_textures", C.c_int32), ("textures", C.POINTER(rumi_texture)), ("tri_texture", IP),
+                ("rect_texture", IP), ("sphere_texture", IP), ("sphere_frame", FP)]
 
 
 class rumi_render_params(C.Structure):
@@ -89,7 +97,7 @@ EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "ru
            "rumi_last_error_string", "rumi_version",
            "rumi_test_philox", "rumi_test_material_sample", "rumi_test_material_fr", "rumi_test_distance_sample",
            "rumi_test_phase_sample", "rumi_test_camera_rays", "rumi_test_pixel_samples",
-           "rumi_test_read_bandwidth"]
+           "rumi_test_read_bandwidth", "rumi_test_texture_pattern"]
 
 _lib = None
 
@@ -150,6 +158,7 @@ def load(path: str = LIB_PATH):
     L.rumi_film_fireflies.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, vp, C.c_int32, vp]
     L.rumi_test_read_bandwidth.restype = C.c_int
     L.rumi_test_read_bandwidth.argtypes = [vp, C.c_int64, C.c_int32, vp, C.POINTER(C.c_double)]
+    L.rumi_test_texture_pattern.argtypes = [vp, C.c_int64, vp, vp, vp]
     L.rumi_last_error_string.restype = C.c_char_p
     L.rumi_version.restype = C.c_char_p
     _lib = L

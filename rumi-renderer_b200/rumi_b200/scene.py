@@ -30,6 +30,9 @@ SHAPE_TRIANGLE, SHAPE_RECT, SHAPE_SPHERE = range(3)
 LIGHT_AREA, LIGHT_SPOT = range(2)
 # integrators
 PATH_TRACER, BDPT, RAY_TRACER = range(3)
+# light kinds (continued) and texture kinds
+LIGHT_IBL = 2
+TEX_CHECKER, TEX_IMAGE, TEX_HDR = range(3)
 
 
 def _v3(x) -> np.ndarray:
@@ -99,11 +102,76 @@ def Subsurface(eta_in: float, eta_out: float, sigma_s, sigma_a, density: float =
                     density=density)
 
 
+class Texture:
+    """Base of the reference's textures (src/Texture/texture.h): Pattern(shape, p) =
+    Pixel(shape.TextureMapping(p))."""
+    kind: int
+
+
+@dataclass
+class Checker(Texture):
+    """``Checker(width, height, c1, c2)``: c2 where floor(u*width) and floor(v*height) have
+    the same parity, else c1 (src/Texture/checker.cpp:17-32)."""
+    width: float
+    height: float
+    c1: Sequence[float]
+    c2: Sequence[float]
+    kind: int = TEX_CHECKER
+
+
+class ImageTexture(Texture):
+    """``ImageTexture(bmp_file, gamma)`` (src/Texture/imagetexture.cpp:18-61).  ``pixels``:
+    uint8 (height, width, bytes_per_pixel) in the order LoadBmp returns them -- rows as
+    stored in the file (bottom row first), B,G,R[,A]."""
+    kind = TEX_IMAGE
+
+    def __init__(self, pixels, gamma: float = 1.0):
+        self.pixels = np.ascontiguousarray(pixels, dtype=np.uint8)
+        if self.pixels.ndim != 3 or self.pixels.shape[2] not in (3, 4):
+            raise ValueError("image texture pixels must be (height, width, 3 or 4) bytes")
+        self.gamma = float(gamma)
+
+    path: Optional[str] = None
+
+    @classmethod
+    def from_bmp(cls, path: str, gamma: float = 1.0) -> "ImageTexture":
+        from .textures import load_bmp
+        t = cls(load_bmp(path), gamma)
+        t.path = path
+        return t
+
+
+class HDRTexture(Texture):
+    """``HDRTexture(hdr_file)`` (src/Texture/hdrtexture.cpp:22-59).  ``data``: float32
+    (height, width, 3) as LoadHDR returns it -- first scanline first, R,G,B."""
+    kind = TEX_HDR
+
+    def __init__(self, data):
+        self.data = np.ascontiguousarray(data, dtype=np.float32)
+        if self.data.ndim != 3 or self.data.shape[2] != 3:
+            raise ValueError("HDR texture data must be (height, width, 3) floats")
+
+    path: Optional[str] = None
+
+    @classmethod
+    def from_hdr(cls, path: str) -> "HDRTexture":
+        from .textures import load_hdr
+        t = cls(load_hdr(path))
+        t.path = path
+        return t
+
+
 class Shape:
     material: Optional[Material] = None
+    texture: Optional[Texture] = None
 
     def AddingMaterial(self, material: Material) -> bool:
         self.material = material
+        return True
+
+    def AddingTexture(self, texture: Texture) -> bool:
+        """``Shape::AddingTexture`` (src/Shape/shape.cpp:71-84)."""
+        self.texture = texture
         return True
 
 
@@ -147,18 +215,30 @@ class Rect(Shape):
 
 
 class Sphere(Shape):
-    """``Sphere(c, r[, n_samples])`` (src/Shape/sphere.cpp:18-38)."""
+    """``Sphere(c, r[, n_samples])`` (src/Shape/sphere.cpp:18-38).  ``transform``: the public
+    ``Shape::_transform`` (row-major 4x4), whose upper 3x3 rows orient the sphere's texture."""
 
-    def __init__(self, c, r: float, n_samples: int = 0):
+    def __init__(self, c, r: float, n_samples: int = 0, transform=None):
         self.c = _v3(c)
         self.r = float(r)
         self.n_samples = int(n_samples)
+        self.transform = np.eye(4, dtype=np.float32).reshape(16) if transform is None else \
+            np.asarray(transform, np.float32).reshape(16)
 
 
 @dataclass
 class AreaLight:
     """``AreaLight(shape, material)`` over an emissive Rect or Sphere (src/Light/arealight.cpp)."""
     shape: Shape
+
+
+@dataclass
+class ImageBasedLight:
+    """``ImageBasedLight(sphere, material, texture)`` (src/Light/imagebasedlight.cpp): the
+    emissive, textured sphere around the scene as a light, sampled by cosine-weighted
+    directions about the shading normal; radiance = the sphere's texture where the
+    direction leaves it."""
+    sphere: Shape
 
 
 @dataclass
@@ -288,6 +368,18 @@ class Scene:
                 mats.append(m)
             return mat_index[key]
 
+        texs: List[Texture] = []
+        tex_index = {}
+
+        def tid(t: Optional[Texture]) -> int:
+            if t is None:
+                return -1
+            if id(t) not in tex_index:
+                tex_index[id(t)] = len(texs)
+                texs.append(t)
+            return tex_index[id(t)]
+
+        tri_t, rect_t, sphere_t, sphere_f = [], [], [], []
         tri_v, tri_n, tri_m, tri_alb = [], [], [], []
         has_alb = False
         rects, rect_m, spheres, sphere_m = [], [], [], []
@@ -301,6 +393,7 @@ class Scene:
                 tri_n.append(np.asarray(n, np.float32).reshape(1, 3, 3))
                 tri_m.append(np.full(1, mid(s.material), np.int32))
                 tri_alb.append(np.asarray(s.material.rgb, np.float32).reshape(1, 3))
+                tri_t.append(np.full(1, tid(s.texture), np.int32))
                 shape_loc[id(s)] = (SHAPE_TRIANGLE, n_tri)
                 n_tri += 1
             elif isinstance(s, Model):
@@ -316,6 +409,7 @@ class Scene:
                     tri_alb.append(s.albedo)
                 else:
                     tri_alb.append(np.tile(np.asarray(s.material.rgb, np.float32), (k, 1)))
+                tri_t.append(np.full(k, tid(s.texture), np.int32))
                 shape_loc[id(s)] = (SHAPE_TRIANGLE, n_tri)
                 n_tri += k
             elif isinstance(s, Rect):
@@ -323,11 +417,15 @@ class Scene:
                 rects.append(np.concatenate([s.p, s.l, s.w]))
                 rect_m.append(mid(s.material))
                 rect_samples.append(s.n_samples)
+                rect_t.append(tid(s.texture))
             elif isinstance(s, Sphere):
                 shape_loc[id(s)] = (SHAPE_SPHERE, len(spheres))
                 spheres.append(np.array([*s.c, s.r], np.float32))
                 sphere_m.append(mid(s.material))
                 sphere_samples.append(s.n_samples)
+                sphere_t.append(tid(s.texture))
+                tr = np.asarray(getattr(s, "transform", np.eye(4, dtype=np.float32).reshape(16)), np.float32)
+                sphere_f.append(tr.reshape(4, 4)[:3, :3].reshape(9))
             else:
                 raise TypeError(type(s))
         lights = []
@@ -335,6 +433,11 @@ class Scene:
             if isinstance(L, AreaLight):
                 st, si = shape_loc[id(L.shape)]
                 lights.append(dict(type=LIGHT_AREA, shape_type=st, shape_index=si))
+            elif isinstance(L, ImageBasedLight):
+                st, si = shape_loc[id(L.sphere)]
+                if st != SHAPE_SPHERE:
+                    raise TypeError("an image-based light needs a Sphere")
+                lights.append(dict(type=LIGHT_IBL, shape_type=st, shape_index=si))
             elif isinstance(L, SpotLight):
                 lights.append(dict(type=LIGHT_SPOT, position=L.position, direction=L.direction,
                                    cone_deg=L.cone_deg, intensity=L.intensity))
@@ -353,6 +456,14 @@ class Scene:
         fs.sphere_samples = np.asarray(sphere_samples, np.int32)
         fs.materials = mats
         fs.lights = lights
+        fs.textures = texs
+        if texs:
+            fs.tri_texture = np.concatenate(tri_t).astype(np.int32) if tri_t else np.zeros(0, np.int32)
+            fs.rect_texture = np.asarray(rect_t, np.int32)
+            fs.sphere_texture = np.asarray(sphere_t, np.int32)
+            fs.sphere_frame = np.asarray(sphere_f, np.float32).reshape(-1, 9)
+        else:
+            fs.tri_texture = fs.rect_texture = fs.sphere_texture = fs.sphere_frame = None
         fs.volume = self.volume
         fs.camera = self.camera
         fs.image = self.image
@@ -385,6 +496,11 @@ class FlatScene:
     sphere_samples: np.ndarray
     materials: List[Material]
     lights: list
+    textures: list = []
+    tri_texture: Optional[np.ndarray] = None
+    rect_texture: Optional[np.ndarray] = None
+    sphere_texture: Optional[np.ndarray] = None
+    sphere_frame: Optional[np.ndarray] = None
     volume: Optional[HomogeneousVolume]
     camera: Optional[Pinhole]
     image: Optional[Film]

@@ -216,6 +216,15 @@ def camera_dof_fixture(path, rng):
     print(path)
 
 
+def TEXTURE_CASES(img, hdr):
+    """(fixture name, scene) of the texture and image-based-light frames."""
+    import texture_cases as TC
+    return [("image_tex_pt32.npz", TC.textured_cornell(32, 32, 16, 8, img)),
+            ("image_tex_whitted32.npz", scenes.whitted(TC.textured_cornell(32, 32, 16, 8, img))),
+            ("image_ibl_pt32.npz", TC.ibl_scene(32, 32, 16, 8, hdr)),
+            ("image_ibl_whitted32.npz", scenes.whitted(TC.ibl_scene(32, 32, 16, 8, hdr)))]
+
+
 def image_fixture(path, size=32, spp=16, depth=8, seeds=64, scene=None):
     """Reference renders of a workload at a small size: per-pixel mean radiance over
     `seeds` independent frames and its standard error (spread across frames, which
@@ -341,6 +350,14 @@ def obj_fixture(path):
 
 
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "textures":
+        import tempfile
+        import texture_cases as TC
+        with tempfile.TemporaryDirectory() as d:
+            img, hdr = TC.case_files(d)
+            for name, sc in TEXTURE_CASES(img, hdr):
+                image_fixture(os.path.join(HERE, name), scene=sc)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "whitted":
         image_fixture(os.path.join(HERE, "image_whitted_cornell32.npz"),
                       scene=scenes.whitted(scenes.cornell_pt(32, 32, 16, 8)))

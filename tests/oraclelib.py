@@ -27,6 +27,7 @@ def lib():
         L.orc_trace.argtypes = [C.c_void_p, C.c_int64, FP, C.c_int, FP, C.POINTER(C.c_int32)]
         L.orc_render_pt.restype = C.c_longlong
         L.orc_render_pt.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, FP]
+        L.orc_texture_pattern.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, FP, FP]
         L.orc_render_whitted.restype = C.c_longlong
         L.orc_render_whitted.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, FP]
         L.orc_material_sample.argtypes = [C.c_void_p, FP, FP, FP, FP]
@@ -97,6 +98,13 @@ class OracleScene:
         nan = lib().orc_render_pt(C.byref(self.desc), max_depth, spp, seed, row0,
                                   self.height if row1 is None else row1, P(film))
         return film, int(nan)
+
+    def texture_pattern(self, prim, pts):
+        prim = np.ascontiguousarray(prim, np.int32)
+        p = f32(np.asarray(pts).reshape(-1, 3))
+        out = np.zeros_like(p)
+        lib().orc_texture_pattern(C.byref(self.desc), p.shape[0], prim.ctypes.data, P(p), P(out))
+        return out
 
     def render_whitted(self, max_depth, spp, seed, row0=0, row1=None):
         """RayTracer(scene, max_depth) frame: film (H, W, 3) B,G,R sums and NaN count."""

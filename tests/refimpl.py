@@ -62,6 +62,13 @@ def lib():
         L.ref_camera_cast_dof.argtypes = [fp, fp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int,
                                           C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint, fp]
         L.ref_set_camera_dof.argtypes = [C.c_void_p, C.c_float, C.c_float]
+        L.ref_add_texture.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, fp, fp, C.c_char_p,
+                                      C.c_float]
+        L.ref_set_shape_transform.argtypes = [C.c_void_p, C.c_int, fp]
+        L.ref_add_ibl_light.argtypes = [C.c_void_p, C.c_int]
+        L.ref_texture_pattern.argtypes = [C.c_void_p, C.c_int, C.c_int, fp, fp]
+        L.ref_load_hdr.argtypes = [C.c_char_p, C.c_int, fp, C.POINTER(C.c_int)]
+        L.ref_load_bmp.argtypes = [C.c_char_p, C.c_int, C.c_void_p, C.POINTER(C.c_uint)]
         _lib = L
     return _lib
 
@@ -106,7 +113,7 @@ class RefScene:
 
     def __init__(self, scene, seed: int = 1, integrator=None, presort_over: int = 200000):
         from rumi_b200.scene import (Triangle, Model, Rect, Sphere, AreaLight, PathTracer,
-                                     BidirectionalPathTracer, RayTracer, MATTE)
+                                     BidirectionalPathTracer, RayTracer, ImageBasedLight, MATTE)
         L = lib()
         self._keep = []
         img = scene.image
@@ -162,9 +169,22 @@ class RefScene:
                 self._keep.append(c)
                 obj_index[id(s)] = L.ref_add_sphere(self.h, P(c), s.r, s.n_samples, s.material.type, P(mp))
         self.id_map = np.concatenate(id_map).astype(np.int32) if id_map else np.zeros(0, np.int32)
+        self.obj_index = obj_index
+        self._tmpdir = None
+        for s in scene.objects:
+            if isinstance(s, Sphere):
+                tr = f32(getattr(s, "transform", np.eye(4, dtype=np.float32).reshape(16)))
+                self._keep.append(tr)
+                L.ref_set_shape_transform(self.h, obj_index[id(s)], P(tr))
+            t = getattr(s, "texture", None)
+            if t is not None:
+                self._add_texture(obj_index[id(s)], t)
         for light in scene.lights:
+            if isinstance(light, ImageBasedLight):
+                L.ref_add_ibl_light(self.h, obj_index[id(light.sphere)])
+                continue
             if not isinstance(light, AreaLight):
-                raise NotImplementedError("the reference has area lights only")
+                raise NotImplementedError("the reference has area and image-based lights only")
             L.ref_add_area_light(self.h, obj_index[id(light.shape)])
         if scene.volume is not None:
             v = scene.volume
@@ -188,6 +208,36 @@ class RefScene:
             L.ref_finalize(self.h, 2, tr.max_depth, 0, seed)
         else:
             L.ref_finalize(self.h, 0, 1, 0, seed)
+
+    def _add_texture(self, obj, t):
+        """Shape::AddingTexture through the harness; image textures without a file are
+        written to a BMP first (the reference reads textures from files only)."""
+        import tempfile
+        from rumi_b200.scene import TEX_CHECKER, TEX_IMAGE
+        from rumi_b200.film import save_bmp
+        L = lib()
+        if t.kind == TEX_CHECKER:
+            c1, c2 = f32(t.c1), f32(t.c2)
+            self._keep += [c1, c2]
+            L.ref_add_texture(self.h, obj, 0, t.width, t.height, P(c1), P(c2), None, 1.0)
+            return
+        path = getattr(t, "path", None)
+        if path is None:
+            if t.kind != TEX_IMAGE:
+                raise ValueError("an HDR texture for the reference needs its file (HDRTexture.from_hdr)")
+            if self._tmpdir is None:
+                self._tmpdir = tempfile.TemporaryDirectory()
+            path = os.path.join(self._tmpdir.name, "tex%d.bmp" % obj)
+            save_bmp(path, t.pixels)
+        L.ref_add_texture(self.h, obj, 1 if t.kind == TEX_IMAGE else 2, 0.0, 0.0, None, None, path.encode(),
+                          float(getattr(t, "gamma", 1.0)))
+
+    def texture_pattern(self, shape, pts):
+        """Texture::Pattern(shape, p) of the reference at points (n, 3) -> (n, 3) r, g, b."""
+        p = f32(np.asarray(pts).reshape(-1, 3))
+        out = np.zeros_like(p)
+        lib().ref_texture_pattern(self.h, self.obj_index[id(shape)], p.shape[0], P(p), P(out))
+        return out
 
     def render_rows(self, seed: int, row0: int, row1: int):
         """Film pixel sums (H, W, 3) in B,G,R order for rows [row0, row1), the light
