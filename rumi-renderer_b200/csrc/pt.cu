@@ -29,9 +29,17 @@ namespace rumi {
 static constexpr int TRACE_THREADS = 128;
 // Minimum resident traversal blocks per SM: 8 caps the extend / shadow kernels at 64
 // registers (32 warps per SM instead of 28 at their natural 72); measured 5% faster per
-// frame on the 1M-triangle workload.  10 and 12 spill and are slower.
+// frame on the 1M-triangle workload.  10 and 12 spill and are slower.  The any-hit kernel
+// alone (55 registers at 8) measured 83.2 / 84.9 / 122.0 ms per frame at 9 / 10 / 12
+// blocks against 83.6 at 8.
 #ifndef RUMI_TRACE_MIN_BLOCKS
 #define RUMI_TRACE_MIN_BLOCKS 8
+#endif
+#ifndef RUMI_EXTEND_MIN_BLOCKS
+#define RUMI_EXTEND_MIN_BLOCKS RUMI_TRACE_MIN_BLOCKS
+#endif
+#ifndef RUMI_SHADOW_MIN_BLOCKS
+#define RUMI_SHADOW_MIN_BLOCKS RUMI_TRACE_MIN_BLOCKS
 #endif
 static constexpr int STACK_SMEM = 32;
 static constexpr int SHADE_THREADS = 256;
@@ -195,7 +203,7 @@ __global__ void pt_finish(PtLaunch P) { P.stats[S_RAYS_SH] += (unsigned long lon
 // Persistent traversal kernels: every block takes rays from the bounce's queue until it
 // is empty (traverse_queue in traverse.cuh; MODE selects the scheme, see there).
 template <int MODE, bool STATS>
-__global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) pt_extend(PtLaunch P, int bounce) {
+__global__ void __launch_bounds__(TRACE_THREADS, RUMI_EXTEND_MIN_BLOCKS) pt_extend(PtLaunch P, int bounce) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
     const int cur = bounce & 1;
     TraceStats st{0, 0};
@@ -220,7 +228,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) pt_exten
 }
 
 template <int MODE, bool ADJ = false>
-__global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) pt_shadow(PtLaunch P) {
+__global__ void __launch_bounds__(TRACE_THREADS, RUMI_SHADOW_MIN_BLOCKS) pt_shadow(PtLaunch P) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
     TraceStats st{0, 0};
     float acc_sigma = 0.0f, acc_g = 0.0f;  // adjoint: score-weighted contributions
@@ -339,8 +347,16 @@ RUMI_D bool nee_setup(const LightSample &ls, float3 p, float3 &wi, float &dist, 
 //                                          weight sigma_s / sigma_t (per channel)
 //   phase direction (applied at the next vertex) and NEE phase value: d log HG / d g
 //   binary shadow transmittance (applied by the shadow kernel to that NEE term alone).
+// Forward shading is bound by the latency of its scattered per-path loads: three blocks
+// of 256 threads per SM (80 registers, a 120-byte spill to L1) ran the 1024x1024x64
+// BVH-bound frame's shading in 31.0 ms against 37.7 ms at two blocks (118 registers);
+// four blocks (64 registers) gave the same as three.  The adjoint replay keeps its
+// registers.
+#ifndef RUMI_SHADE_MIN_BLOCKS
+#define RUMI_SHADE_MIN_BLOCKS 3
+#endif
 template <bool ADJ>
-__global__ void __launch_bounds__(SHADE_THREADS) pt_shade(PtLaunch P, int bounce) {
+__global__ void __launch_bounds__(SHADE_THREADS, ADJ ? 1 : RUMI_SHADE_MIN_BLOCKS) pt_shade(PtLaunch P, int bounce) {
     const int cur = bounce & 1, nxt = cur ^ 1;
     const int n = P.cnt[cur];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
