@@ -593,12 +593,16 @@ __global__ void __launch_bounds__(SHADE_THREADS, ADJ ? 1 : RUMI_SHADE_MIN_BLOCKS
                                 tr = volume_shadow_tr(V, p, wi, dist, U2.u[2], &smax_sh);
                                 if (ADJ) sh_score = make_float2(-smax_sh * 0.33333333333f, 0.0f);
                             }
-                            if (tr > 0.0f) {
+                            // a shadow ray whose contribution is exactly zero (the light
+                            // below the surface's horizon: cos = 0) cannot change the film
+                            // and is not traced; NaN and inf contributions are
+                            const float3 c = beta * direct;
+                            if (tr > 0.0f && (c.x != 0.0f || c.y != 0.0f || c.z != 0.0f)) {
                                 want_sh = true;
                                 sh_o = p;
                                 sh_d = wi;
                                 sh_tmax = dist;
-                                sh_c = beta * direct;
+                                sh_c = c;
                             }
                         }
                     }
@@ -761,12 +765,13 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade_whitted(PtLaunch P, in
                         float smax_sh = 0.0f;
                         tr = volume_shadow_tr(S.volume, p, wi, dist, U2.u[2], &smax_sh);
                     }
-                    if (tr > 0.0f) {
+                    const float3 c = beta * direct;  // zero contributions are not traced
+                    if (tr > 0.0f && (c.x != 0.0f || c.y != 0.0f || c.z != 0.0f)) {
                         want_sh = true;
                         sh_o = p;
                         sh_d = wi;
                         sh_tmax = dist;
-                        sh_c = beta * direct;
+                        sh_c = c;
                     }
                 }
             }
