@@ -699,9 +699,8 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) continue;
                 if (sc.dirac) continue;
             }
-            if (!visible(S, s + 1, t + 1, sc.p, tc.p, stk, st)) continue;
-            const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
-            if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) continue;
+            // the geometric rejections come before the two visibility tests: they read no
+            // random numbers and change nothing, so the order only saves traversals
             const float3 cwi = normalize_ref(sc.p - tc.p);
             const float3 cwo = normalize_ref(tc.p - sc.p);
             const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
@@ -716,6 +715,15 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
             if (dist <= 0.0f) continue;
             const float G = ci * co / (dist * dist);
             if (G <= 0.0f) continue;
+            int film_w = 0, film_h = 0;
+            if (t == 0) {
+                if (!film_plane_pixel(P, sc.p, film_w, film_h)) continue;
+                if (film_w == W || film_h == H) continue;
+                if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) continue;
+            }
+            if (!visible(S, s + 1, t + 1, sc.p, tc.p, stk, st)) continue;
+            const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
+            if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) continue;
             float3 cE, cL;
             if (t == 0) {
                 const DevCamera &c = S.camera;
@@ -735,13 +743,9 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
             }
             if (t == 0) {
-                int wi, hi;
-                if (!film_plane_pixel(P, sc.p, wi, hi)) continue;
-                if (wi == W || hi == H) continue;
-                if (wi < 0 || hi < 0 || wi > W || hi > H) continue;
                 float3 lo = aE[t] * cE * G * cL * aL[s];
                 lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n, light);
-                float *dst = P.light_film + ((size_t)hi * W + wi) * 3;
+                float *dst = P.light_film + ((size_t)film_h * W + film_w) * 3;
                 atomicAdd(dst + 0, lo.z);
                 atomicAdd(dst + 1, lo.y);
                 atomicAdd(dst + 2, lo.x);
