@@ -183,6 +183,7 @@ rumi_status rumi_render_batch(rumi_batch *b, const rumi_batch_params *p, float *
     if (wave < max_spp) wave = max_spp;
     if (wave > path0.back()) wave = path0.back();
     if (wave < max_spp) wave = max_spp;
+    if (wave > 0x3fffffffLL) return set_error("wave_paths too large"), RUMI_ERR_INVALID_ARG;  // 30-bit slots
     BatchFrame F;
     F.n_scenes = n;
     F.max_depth = p->max_depth;

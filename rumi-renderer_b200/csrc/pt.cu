@@ -45,6 +45,17 @@ static constexpr int STACK_SMEM = 32;
 static constexpr int SHADE_THREADS = 256;
 
 enum { PFL_LE = 1, PFL_IN = 2 };
+// A queued ray's o.w holds its path slot (bits 0-29) and its flags: bit 31 = in_object
+// (read by the traversal), bit 30 = le.  Its throughput travels in the queue too
+// (beta_q, same position), so shading reads and writes path state in queue order.
+RUMI_D float pack_slot(int slot, unsigned fl) {
+    return __int_as_float(slot | ((fl & PFL_IN) ? (int)0x80000000 : 0) | ((fl & PFL_LE) ? 0x40000000 : 0));
+}
+RUMI_D int slot_of(float w) { return __float_as_int(w) & 0x3fffffff; }
+RUMI_D unsigned flags_of(float w) {
+    const unsigned b = __float_as_uint(w);
+    return ((b >> 31) ? PFL_IN : 0u) | (((b >> 30) & 1u) ? PFL_LE : 0u);
+}
 // counters
 enum { C_RAY0 = 0, C_RAY1 = 1, C_SHADOW = 2, C_FETCH_EXT = 3, C_FETCH_SH = 4, C_NUM = 8 };
 // 64-bit device statistics
@@ -59,8 +70,7 @@ struct PtLaunch {
     int n_paths, pix0, n_pix;
     float4 *ray_o[2], *ray_d[2], *hit;
     float4 *sh_o, *sh_d, *sh_c;
-    float4 *beta, *L;
-    unsigned *pflags;
+    float4 *beta_q[2], *L;  // beta_q: throughput (+ one word) in queue order, per ray buffer
     int *cnt;
     unsigned long long *stats;
     float *film;
@@ -173,11 +183,10 @@ __global__ void pt_generate(PtLaunch P) {
     float3 o, d;
     const float2 lu = S->camera.focal_distance > 0.0f ? lens_uniforms((uint64_t)path, k0, k1) : make_float2(0.f, 0.f);
     camera_ray(S->camera, W, S->height, w, h, smp.x, smp.y, lu.x, lu.y, o, d);
-    P.ray_o[0][j] = make_float4(o.x, o.y, o.z, __int_as_float(j));
+    P.ray_o[0][j] = make_float4(o.x, o.y, o.z, pack_slot(j, PFL_LE));
     P.ray_d[0][j] = make_float4(d.x, d.y, d.z, FLT_MAX);
-    P.beta[j] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    P.beta_q[0][j] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     P.L[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    P.pflags[j] = PFL_LE;
     if (P.dls) {
         // the film drops NaN samples (pt_resolve), so they receive no gradient
         const long long px = (long long)P.pix0 + j / P.spp;
@@ -284,7 +293,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) pt_trace
     auto scene_of = [&](int i) -> const DevScene * {
         if (i < 0) return &P.scenes[0];
         const float4 o4 = ANYHIT ? P.sh_o[i] : P.ray_o[cur][i];
-        return &P.scenes[P.slot_scene[__float_as_int(o4.w) & 0x7fffffff]];
+        return &P.scenes[P.slot_scene[ANYHIT ? __float_as_int(o4.w) : slot_of(o4.w)]];
     };
     auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
         const float4 o4 = ANYHIT ? P.sh_o[i] : P.ray_o[cur][i];
@@ -383,7 +392,7 @@ __global__ void __launch_bounds__(SHADE_THREADS, ADJ ? 1 : RUMI_SHADE_MIN_BLOCKS
         const float4 o4 = P.ray_o[cur][i];
         const float4 d4 = P.ray_d[cur][i];
         const float4 hv = P.hit[i];
-        slot = __float_as_int(o4.w) & 0x7fffffff;
+        slot = slot_of(o4.w);
         const DevScene *Sp = &P.s;
         uint32_t k0 = P.k0, k1 = P.k1;
         uint64_t path = (uint64_t)(P.path0 + slot);
@@ -399,9 +408,9 @@ __global__ void __launch_bounds__(SHADE_THREADS, ADJ ? 1 : RUMI_SHADE_MIN_BLOCKS
         const float t = hv.x;
         const bool hit = t > 0.0f;
         const int code = __float_as_int(hv.y);
-        const unsigned fl = P.pflags[slot];
+        const unsigned fl = flags_of(o4.w);
         const bool le = (fl & PFL_LE) != 0, inobj = (fl & PFL_IN) != 0;
-        const float4 beta4 = P.beta[slot];
+        const float4 beta4 = P.beta_q[cur][i];
         beta = f4xyz(beta4);
         // adjoint: radiance of the terms from this vertex on, and its loss weights
         float3 Lo = mk3(0.0f, 0.0f, 0.0f), dl = mk3(0.0f, 0.0f, 0.0f);
@@ -627,11 +636,9 @@ __global__ void __launch_bounds__(SHADE_THREADS, ADJ ? 1 : RUMI_SHADE_MIN_BLOCKS
     const int kn = warp_push(&P.cnt[nxt], want_next);
     const int ks = warp_push(&P.cnt[C_SHADOW], want_sh);
     if (want_next) {
-        P.ray_o[nxt][kn] = make_float4(nx_o.x, nx_o.y, nx_o.z,
-                                       __int_as_float(slot | ((nx_flags & PFL_IN) ? (int)0x80000000 : 0)));
+        P.ray_o[nxt][kn] = make_float4(nx_o.x, nx_o.y, nx_o.z, pack_slot(slot, nx_flags));
         P.ray_d[nxt][kn] = make_float4(nx_d.x, nx_d.y, nx_d.z, FLT_MAX);
-        P.beta[slot] = make_float4(beta.x, beta.y, beta.z, pend_g);
-        P.pflags[slot] = nx_flags;
+        P.beta_q[nxt][kn] = make_float4(beta.x, beta.y, beta.z, pend_g);
     }
     if (want_sh) {
         P.sh_o[ks] = make_float4(sh_o.x, sh_o.y, sh_o.z, __int_as_float(slot));
@@ -692,15 +699,15 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade_whitted(PtLaunch P, in
         const float4 o4 = P.ray_o[cur][i];
         const float4 d4 = P.ray_d[cur][i];
         const float4 hv = P.hit[i];
-        slot = __float_as_int(o4.w) & 0x7fffffff;
+        slot = slot_of(o4.w);
         const DevScene &S = P.s;
         const uint64_t path = (uint64_t)(P.path0 + slot);
         const float3 o = f4xyz(o4), d = f4xyz(d4);
         const float t = hv.x;
         const int code = __float_as_int(hv.y);
-        const unsigned fl = P.pflags[slot];
+        const unsigned fl = flags_of(o4.w);
         const bool le = (fl & PFL_LE) != 0, inobj = (fl & PFL_IN) != 0;
-        const float4 beta4 = P.beta[slot];
+        const float4 beta4 = P.beta_q[cur][i];
         beta = f4xyz(beta4);
         const bool last = bounce + 1 >= P.max_depth;
         float3 addL = mk3(0, 0, 0);
@@ -785,11 +792,9 @@ __global__ void __launch_bounds__(SHADE_THREADS) pt_shade_whitted(PtLaunch P, in
     const int kn = warp_push(&P.cnt[nxt], want_next);
     const int ks = warp_push(&P.cnt[C_SHADOW], want_sh);
     if (want_next) {
-        P.ray_o[nxt][kn] = make_float4(nx_o.x, nx_o.y, nx_o.z,
-                                       __int_as_float(slot | ((nx_flags & PFL_IN) ? (int)0x80000000 : 0)));
+        P.ray_o[nxt][kn] = make_float4(nx_o.x, nx_o.y, nx_o.z, pack_slot(slot, nx_flags));
         P.ray_d[nxt][kn] = make_float4(nx_d.x, nx_d.y, nx_d.z, FLT_MAX);
-        P.beta[slot] = make_float4(beta.x, beta.y, beta.z, __int_as_float(enter_mat));
-        P.pflags[slot] = nx_flags;
+        P.beta_q[nxt][kn] = make_float4(beta.x, beta.y, beta.z, __int_as_float(enter_mat));
     }
     if (want_sh) {
         P.sh_o[ks] = make_float4(sh_o.x, sh_o.y, sh_o.z, __int_as_float(slot));
@@ -917,21 +922,20 @@ static char *carve_wave(PtLaunch &L, void *ws, size_t Wp) {
     L.sh_o = (float4 *)w; w += f4;
     L.sh_d = (float4 *)w; w += f4;
     L.sh_c = (float4 *)w; w += f4;
-    L.beta = (float4 *)w; w += f4;
+    L.beta_q[0] = (float4 *)w; w += f4;
+    L.beta_q[1] = (float4 *)w; w += f4;
     L.L = (float4 *)w; w += f4;
-    L.pflags = (unsigned *)w; w += align256(Wp * sizeof(unsigned));
     L.cnt = (int *)w; w += align256(C_NUM * sizeof(int));
     L.stats = (unsigned long long *)w; w += align256(S_NUM * sizeof(unsigned long long));
     return w;
 }
 
 // Device bytes of the wave state for `paths` paths in flight (queues, path state,
-// counters): 164 bytes per path plus alignment and counters.
+// counters): 176 bytes per path plus alignment and counters.
 size_t pt_workspace_bytes(long long paths) {
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t Wp = (size_t)paths;
-    return 10 * al(Wp * sizeof(float4)) + al(Wp * sizeof(unsigned)) + al(C_NUM * sizeof(int)) +
-           al(S_NUM * sizeof(unsigned long long));
+    return 11 * al(Wp * sizeof(float4)) + al(C_NUM * sizeof(int)) + al(S_NUM * sizeof(unsigned long long));
 }
 
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
@@ -942,7 +946,7 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
     if (pix_per_wave < 1) pix_per_wave = 1;
     if (pix_per_wave > total_pix) pix_per_wave = total_pix;
     const long long n_paths_max = pix_per_wave * p->spp;
-    if (n_paths_max > 0x7fffffffLL) {
+    if (n_paths_max > 0x3fffffffLL) {  // slots are 30-bit (pack_slot)
         set_error("wave_paths too large");
         return RUMI_ERR_INVALID_ARG;
     }
@@ -1082,7 +1086,7 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
     if (pix_per_wave < 1) pix_per_wave = 1;
     if (pix_per_wave > total_pix) pix_per_wave = total_pix;
     const size_t Wp = (size_t)(pix_per_wave * spp);
-    if (Wp > 0x7fffffffULL) {
+    if (Wp > 0x3fffffffULL) {
         set_error("wave_paths too large");
         return RUMI_ERR_INVALID_ARG;
     }
