@@ -337,6 +337,8 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
             } else {
                 const float3 fr = EYE ? vert_fr(S, start, start.n, d, prev_w) : vert_fr(S, start, start.n, prev_w, d);
                 a = a * (fr / (start.pdf_fwd * start.pdf_path) * G);
+                // the surface's texture (bidirectionalpathtracer.cpp:660-661, 971-972)
+                if (S.prim_tex && start.prim >= 0) a = a * tex_pattern(S, start.prim, start.p);
             }
         } else {
             const float fp = EYE ? phase_value(vol, d, prev_w) : phase_value(vol, prev_w, d);
@@ -735,6 +737,10 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
             } else {
                 cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
             }
+            // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
+            // 350-351): a medium vertex takes the texture of the surface its segment was
+            // headed for, evaluated at the medium point; none without such a surface
+            if (t > 0 && S.prim_tex && tc.prim >= 0) cE = cE * tex_pattern(S, tc.prim, tc.p);
             if (s == 0) {
                 cL = light_emission(light) / sc.pdf_fwd;
             } else if (sc.onsurface) {
@@ -742,6 +748,7 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
             } else {
                 cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
             }
+            if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
             if (t == 0) {
                 float3 lo = aE[t] * cE * G * cL * aL[s];
                 lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n, light);
@@ -787,8 +794,8 @@ __global__ void add_light_film(float *film, const float *light, size_t n) {
 rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                         cudaStream_t stream) {
     const DevScene &S = sc->dev;
-    if (S.prim_tex || sc->has_ibl) {
-        set_error("BDPT does not support textures or image-based lights");
+    if (sc->has_ibl) {
+        set_error("BDPT does not support image-based lights");
         return RUMI_ERR_INVALID_ARG;
     }
     if (p->n_light < 2 || p->n_eye < 2 || p->n_light > BD_MAXV || p->n_eye > BD_MAXV) {

@@ -222,7 +222,8 @@ def TEXTURE_CASES(img, hdr):
     return [("image_tex_pt32.npz", TC.textured_cornell(32, 32, 16, 8, img)),
             ("image_tex_whitted32.npz", scenes.whitted(TC.textured_cornell(32, 32, 16, 8, img))),
             ("image_ibl_pt32.npz", TC.ibl_scene(32, 32, 16, 8, hdr)),
-            ("image_ibl_whitted32.npz", scenes.whitted(TC.ibl_scene(32, 32, 16, 8, hdr)))]
+            ("image_ibl_whitted32.npz", scenes.whitted(TC.ibl_scene(32, 32, 16, 8, hdr))),
+            ("image_tex_bdpt32.npz", TC.textured_bdpt(32, 32, 16, img))]
 
 
 def image_fixture(path, size=32, spp=16, depth=8, seeds=64, scene=None):

@@ -192,10 +192,20 @@ def test_gpu_textured_frame_matches_oracle_per_pixel(files, k):
 
 
 @pytest.mark.gpu
-def test_gpu_bdpt_rejects_textures(files):
+def test_gpu_textured_bdpt_matches_reference_3sigma(golden, files):
+    """BDPT with textures: subpath throughputs take each surface vertex's pattern and a
+    connection both connecting vertices' (bidirectionalpathtracer.cpp:350-364, 660-661,
+    971-972), against the reference's BidirectionalPathTracer frames."""
+    from test_gpu_parity import gpu_frames
+    frames_vs_reference(gpu_frames(TC.textured_bdpt(32, 32, 16, files[0]), 32, 17000),
+                        golden("image_tex_bdpt32.npz"))
+
+
+@pytest.mark.gpu
+def test_gpu_bdpt_rejects_image_based_lights(files):
     import rumi_b200
     from rumi_b200 import _capi
-    sc = TC.textured_cornell(8, 8, 1, 2, files[0])
+    sc = TC.ibl_scene(8, 8, 1, 2, files[1])
     gs = rumi_b200.GpuScene(sc)
     with pytest.raises(_capi.RumiError):
         gs.render(spp=1, tracer=BidirectionalPathTracer(3, 3))

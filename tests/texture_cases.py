@@ -68,6 +68,14 @@ def textured_cornell(width: int, height: int, spp: int, max_depth: int, image_pa
     return sc
 
 
+def textured_bdpt(width: int, height: int, spp: int, image_path: str) -> Scene:
+    """textured_cornell under BidirectionalPathTracer(4, 5)."""
+    from rumi_b200.scene import BidirectionalPathTracer
+    sc = textured_cornell(width, height, spp, 8, image_path)
+    sc.tracer = BidirectionalPathTracer(4, 5)
+    return sc
+
+
 def ibl_scene(width: int, height: int, spp: int, max_depth: int, hdr_path: str) -> Scene:
     """An emissive sphere of radius 15 carrying the sky (HDRTexture, turned by RotationY(-PI)
     like the reference's image-based-lighting preset) as the only light, a Matte ball, a
