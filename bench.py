@@ -393,18 +393,18 @@ def our_arm(args):
     barrier()
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ext_ms, ext_launches, rays_ext, rays_sh, launches = 0.0, 0, 0, 0, 0
+    rays_ext, rays_sh, launches = 0, 0, 0
     barrier()
     ev0.record()
+    # the frames as the library renders them: each bounce's shadow rays traced on a second
+    # stream beside the next bounce's closest-hit rays, no per-kernel events
     for s in range(args.steps):
-        _, st = gs.render(seed=seed0 + 100 + s, film_device_ptr=film.data_ptr(), stream=stream, timing=True,
+        _, st = gs.render(seed=seed0 + 100 + s, film_device_ptr=film.data_ptr(), stream=stream,
                           wave_paths=args.wave_paths)
-        ext_ms += st["extend_ms"]
-        ext_launches += st["extend_launches"]
         rays_ext += st["rays_extend"]
         rays_sh += st["rays_shadow"]
         waves = st["extend_launches"] // w["max_depth"]
-        launches += waves * (3 + 4 * w["max_depth"])
+        launches += waves * (3 + 5 * w["max_depth"])
     ev1.record()
     barrier()
     clocks_info = clocks.stop()
@@ -412,9 +412,20 @@ def our_arm(args):
     ms = max_over_ranks(ms)
     value = world * paths_per_frame * args.steps / (ms / 1000.0)
     rays_per_s = world * (rays_ext + rays_sh) / (ms / 1000.0)
-
+    # the same frames with every launch in order on one stream and CUDA events around each
+    # kernel (RUMI_FLAG_SERIAL | RUMI_FLAG_TIMING): each kernel's own device time, for the
+    # roofline of the closest-hit kernel and the per-kernel breakdown
+    ext_ms, ext_launches, ext_rays, kern = 0.0, 0, 0, dict(extend_ms=0.0, shadow_ms=0.0, shade_ms=0.0, total_ms=0.0)
+    for s in range(args.steps):
+        _, st = gs.render(seed=seed0 + 100 + s, film_device_ptr=film.data_ptr(), stream=stream, timing=True,
+                          serial=True, wave_paths=args.wave_paths)
+        ext_ms += st["extend_ms"]
+        ext_launches += st["extend_launches"]
+        ext_rays += st["rays_extend"]
+        for k in kern:
+            kern[k] += st[k] / args.steps
     avg_launch_ms = ext_ms / ext_launches
-    rays_per_launch = rays_ext / ext_launches
+    rays_per_launch = ext_rays / ext_launches
     achieved = bytes_per_ray * rays_per_launch / (avg_launch_ms / 1000.0) / 1e9
     pk, pk_kind = peaks()
     traffic = extend_traffic()
@@ -423,7 +434,10 @@ def our_arm(args):
                     kernel="pt_extend (closest-hit)", peak_kind=pk_kind,
                     algorithmic_bytes_per_ray=bytes_per_ray, nodes_per_ray=nodes_per_ray, prims_per_ray=prims_per_ray,
                     rays_per_launch=rays_per_launch, avg_launch_ms=avg_launch_ms,
-                    closest_hit_rays_per_s=rays_ext / (ext_ms / 1000.0))
+                    closest_hit_rays_per_s=ext_rays / (ext_ms / 1000.0),
+                    measured="CUDA events around every closest-hit launch of --steps frames rendered with "
+                             "RUMI_FLAG_SERIAL (each kernel alone on the GPU), after the timed frames",
+                    per_frame_ms_serial={k: round(v, 2) for k, v in kern.items()})
     # the tree and primitives are served mostly from L2 (see the ncu summary), so the same
     # algorithmic bytes are also set against an L2-resident copy measured here
     l2 = l2_read_gbs()
@@ -466,12 +480,15 @@ def our_arm(args):
         e2e_step(seed0 + 500)
         barrier()
         t0 = time.perf_counter()
+        step_ms = []
         for s in range(args.steps):
+            ts = time.perf_counter()
             e2e_step(seed0 + 600 + s)
+            step_ms.append(round(1000.0 * (time.perf_counter() - ts), 1))
         barrier()
         sec = max_over_ranks(time.perf_counter() - t0)
         e2e = dict(value=world * paths_per_frame * args.steps / sec, unit=UNIT, h2d_bytes_per_step=h2d,
-                   d2h_bytes_per_step=d2h, ms_per_step=1000.0 * sec / args.steps)
+                   d2h_bytes_per_step=d2h, ms_per_step=1000.0 * sec / args.steps, step_ms=step_ms)
         film_np = film_host.numpy()
         assert np.isfinite(film_np).all()
 

@@ -5,6 +5,7 @@
 //   Glossy        src/Material/glossy.cpp:19-25      Subsurface src/Material/subsurface.cpp:21-40
 //   HomogeneousVolume src/Volume/homogeneousvolume.cpp:24-44
 //   Pinhole       src/Camera/pinhole.cpp:30-51
+#include <mutex>
 #include "renderer.h"
 #include <cmath>
 #include <cstring>
@@ -54,12 +55,47 @@ void dfree(void *p, cudaStream_t s) {
     if (p) cudaFreeAsync(p, s);
 }
 
+// One render workspace per device outlives the scene that used it: a scene destroyed
+// hands its workspace here (its stream synchronised, so no work uses it any more) and the
+// next scene on that device takes it if it is large enough.  A program that creates a
+// scene per frame then allocates its ~0.7 GB of wave state once; through the pool alone a
+// fresh 0.7 GB request after many scene-sized ones was measured to stall for up to ~0.7 s.
+static std::mutex g_ws_mutex;
+static void *g_ws_cache[64] = {};
+static size_t g_ws_cache_bytes[64] = {};
+
+static void workspace_release(rumi_scene *sc) {
+    if (!sc->ws) return;
+    void *drop = sc->ws;
+    if (sc->device >= 0 && sc->device < 64) {
+        std::lock_guard<std::mutex> lock(g_ws_mutex);
+        if (g_ws_cache_bytes[sc->device] < sc->ws_bytes) {
+            drop = g_ws_cache[sc->device];
+            g_ws_cache[sc->device] = sc->ws;
+            g_ws_cache_bytes[sc->device] = sc->ws_bytes;
+        }
+    }
+    if (drop) dfree(drop, sc->stream);
+    sc->ws = nullptr;
+    sc->ws_bytes = 0;
+}
+
 rumi_status ensure_workspace(rumi_scene *sc, size_t bytes) {
     if (sc->ws_bytes >= bytes) return RUMI_OK;
     if (sc->ws) {
         dfree(sc->ws, sc->stream);
         sc->ws = nullptr;
         sc->ws_bytes = 0;
+    }
+    if (sc->device >= 0 && sc->device < 64) {
+        std::lock_guard<std::mutex> lock(g_ws_mutex);
+        if (g_ws_cache[sc->device] && g_ws_cache_bytes[sc->device] >= bytes) {
+            sc->ws = g_ws_cache[sc->device];
+            sc->ws_bytes = g_ws_cache_bytes[sc->device];
+            g_ws_cache[sc->device] = nullptr;
+            g_ws_cache_bytes[sc->device] = 0;
+            return RUMI_OK;
+        }
     }
     cudaError_t e = dalloc(&sc->ws, bytes, sc->stream);
     if (e != cudaSuccess) {
@@ -106,7 +142,14 @@ void free_scene(rumi_scene *sc) {
     dfree(sc->prim_tex, s);
     dfree(sc->sphere_frame, s);
     for (void *p : sc->tex_pixels) dfree(p, s);
-    dfree(sc->ws, s);
+    if (sc->aux_stream) {
+        cudaStreamSynchronize(sc->aux_stream);
+        cudaStreamDestroy(sc->aux_stream);
+    }
+    if (sc->ev_fork) cudaEventDestroy(sc->ev_fork);
+    if (sc->ev_join) cudaEventDestroy(sc->ev_join);
+    if (s) cudaStreamSynchronize(s);  // nothing uses the workspace any more
+    workspace_release(sc);
     if (s) {
         cudaStreamSynchronize(s);
         cudaStreamDestroy(s);

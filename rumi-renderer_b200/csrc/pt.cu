@@ -41,6 +41,11 @@ static constexpr int TRACE_THREADS = 128;
 #ifndef RUMI_SHADOW_MIN_BLOCKS
 #define RUMI_SHADOW_MIN_BLOCKS RUMI_TRACE_MIN_BLOCKS
 #endif
+// 1: each bounce's any-hit launch runs on an auxiliary stream beside the next bounce's
+// closest-hit launch (pt_render_in); 0: one stream, launches in order.
+#ifndef RUMI_PT_OVERLAP
+#define RUMI_PT_OVERLAP 1
+#endif
 static constexpr int STACK_SMEM = 32;
 static constexpr int SHADE_THREADS = 256;
 
@@ -208,6 +213,22 @@ __global__ void pt_reset(PtLaunch P, int bounce) {
 }
 
 __global__ void pt_finish(PtLaunch P) { P.stats[S_RAYS_SH] += (unsigned long long)P.cnt[C_SHADOW]; }
+
+// pt_reset in two halves for the overlapped schedule: before a closest-hit launch (its
+// queue into the statistics, its work counter cleared), and before shading, once the
+// previous bounce's shadow rays are traced (their count into the statistics, the queues
+// shading pushes into cleared).
+__global__ void pt_reset_extend(PtLaunch P, int bounce) {
+    P.stats[S_RAYS_EXT] += (unsigned long long)P.cnt[bounce & 1];
+    P.cnt[C_FETCH_EXT] = 0;
+}
+__global__ void pt_reset_shade(PtLaunch P, int bounce) {
+    // (at bounce 0 the count is the previous wave's last bounce, which pt_finish added)
+    if (bounce > 0) P.stats[S_RAYS_SH] += (unsigned long long)P.cnt[C_SHADOW];
+    P.cnt[C_SHADOW] = 0;
+    P.cnt[C_FETCH_SH] = 0;
+    P.cnt[(bounce & 1) ^ 1] = 0;
+}
 
 // Persistent traversal kernels: every block takes rays from the bounce's queue until it
 // is empty (traverse_queue in traverse.cuh; MODE selects the scheme, see there).
@@ -952,13 +973,20 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
     }
     rumi_status st = ensure_workspace(sc, pt_workspace_bytes(n_paths_max));
     if (st != RUMI_OK) return st;
-    return pt_render_in(sc, p, film_dev, stats, stream, sc->ws, pix_per_wave);
+    if (!sc->aux_stream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&sc->aux_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sc->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sc->ev_join, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_status(e, "auxiliary stream");
+    }
+    return pt_render_in(sc, p, film_dev, stats, stream, sc->ws, pix_per_wave,
+                        RUMI_PT_OVERLAP != 0 && !(p->flags & RUMI_FLAG_SERIAL));
 }
 
 // The frame loop over waves of pix_per_wave pixels, with the wave state carved out of
 // `ws` (pt_workspace_bytes(pix_per_wave * spp) bytes).
 rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
-                         cudaStream_t stream, void *ws, long long pix_per_wave) {
+                         cudaStream_t stream, void *ws, long long pix_per_wave, bool overlap) {
     const int W = sc->dev.width, H = sc->dev.height;
     const int spp = p->spp;
     const long long total_pix = (long long)W * H;
@@ -990,12 +1018,13 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
     const bool timing = (p->flags & RUMI_FLAG_TIMING) != 0;
     const bool count_stats = (p->flags & RUMI_FLAG_STATS) != 0;
     std::vector<cudaEvent_t> evs;
-    auto mark = [&]() {
+    auto mark_on = [&](cudaStream_t st_) {
         cudaEvent_t e;
         cudaEventCreate(&e);
-        cudaEventRecord(e, stream);
+        cudaEventRecord(e, st_);
         evs.push_back(e);
     };
+    auto mark = [&]() { mark_on(stream); };
     // event indices of (begin, end) per launch kind
     std::vector<std::pair<int, int>> ext_ev, shade_ev, sh_ev;
     if (timing) mark();
@@ -1007,6 +1036,46 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
         L.n_paths = (int)(n_pix * spp);
         L.path0 = pix0 * spp;
         pt_generate<<<cdiv(L.n_paths, 256), 256, 0, stream>>>(L);
+        if (overlap) {
+            // shadow rays of bounce b are traced on the auxiliary stream while bounce b + 1's
+            // closest-hit rays are traced here: neither reads what the other writes (shadow
+            // queue and per-path radiance vs ray queue and hits); shading of b + 1 waits
+            // for both, as it refills the shadow queue and adds to the radiance
+            // (with timing, a closest-hit launch's events include the time it shares the
+            // GPU with the previous bounce's any-hit launch)
+            for (int b = 0; b < bounces; ++b) {
+                pt_reset_extend<<<1, 1, 0, stream>>>(L, b);
+                int e0 = 0;
+                if (timing) { e0 = (int)evs.size(); mark(); }
+                if (count_stats)
+                    launch_extend<true>(mode, trace_grid, stream, L, b);
+                else
+                    launch_extend<false>(mode, trace_grid, stream, L, b);
+                if (timing) { mark(); ext_ev.push_back({e0, e0 + 1}); }
+                if (b > 0) cudaStreamWaitEvent(stream, sc->ev_join, 0);
+                pt_reset_shade<<<1, 1, 0, stream>>>(L, b);
+                if (timing) { e0 = (int)evs.size(); mark(); }
+                if (whitted)
+                    pt_shade_whitted<<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
+                else
+                    pt_shade<false><<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
+                if (timing) { mark(); shade_ev.push_back({e0, e0 + 1}); }
+                const bool aside = b + 1 < bounces;
+                cudaStream_t ss = aside ? sc->aux_stream : stream;
+                if (aside) {
+                    cudaEventRecord(sc->ev_fork, stream);
+                    cudaStreamWaitEvent(sc->aux_stream, sc->ev_fork, 0);
+                }
+                if (timing) { e0 = (int)evs.size(); mark_on(ss); }
+                launch_shadow<false>(mode, shadow_grid, ss, L);
+                if (timing) { mark_on(ss); sh_ev.push_back({e0, e0 + 1}); }
+                if (aside) cudaEventRecord(sc->ev_join, sc->aux_stream);
+            }
+            pt_finish<<<1, 1, 0, stream>>>(L);
+            pt_resolve<<<cdiv(L.n_pix * 32LL, 256), 256, 0, stream>>>(L);
+            ++waves;
+            continue;
+        }
         for (int b = 0; b < bounces; ++b) {
             pt_reset<<<1, 1, 0, stream>>>(L, b);
             int e0 = 0;

@@ -26,6 +26,9 @@ struct rumi_scene {
     float4 *sphere_frame = nullptr;
     std::vector<void *> tex_pixels;  // one device array per image texture
     bool has_ibl = false;
+    // the any-hit launch of a bounce runs beside the next bounce's closest-hit launch
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int n_nodes = 0;
     rumi::BvhBuildInfo info{};
     double build_ms = 0.0;
@@ -74,8 +77,10 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
 size_t pt_workspace_bytes(long long paths);
 rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                         cudaStream_t stream);
+// overlap: run each bounce's any-hit launch on the scene's auxiliary stream beside the
+// next bounce's closest-hit launch (false: one stream, in order)
 rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
-                         cudaStream_t stream, void *ws, long long pix_per_wave);
+                         cudaStream_t stream, void *ws, long long pix_per_wave, bool overlap = false);
 rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, float *t_dev, int32_t *prim_dev,
                        int64_t *node_visits, int64_t *prim_tests, cudaStream_t stream);
 rumi_status ensure_workspace(rumi_scene *sc, size_t bytes);

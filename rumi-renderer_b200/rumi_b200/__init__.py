@@ -131,7 +131,7 @@ class GpuScene:
 
     def render(self, spp: int = None, seed: int = 1, tracer=None, wave_paths: int = 0, timing: bool = False,
                film_device_ptr: int = None, stream: int = None, count_stats: bool = False, trace_mode: int = 0,
-               blocks_per_sm: int = 0, refill_min: int = 0, tuning: dict = None):
+               blocks_per_sm: int = 0, refill_min: int = 0, tuning: dict = None, serial: bool = False):
         """Renders one frame.  Returns (film (H, W, 3) B,G,R sums, stats dict); with
         film_device_ptr the film stays on the device and the first value is None."""
         tr = tracer or self.flat.tracer
@@ -146,7 +146,7 @@ class GpuScene:
         p.spp = int(spp if spp is not None else self.flat.image.n_samples)
         p.seed = int(seed)
         p.wave_paths = int(wave_paths)
-        p.flags = (1 if timing else 0) | (2 if count_stats else 0)
+        p.flags = (1 if timing else 0) | (2 if count_stats else 0) | (4 if serial else 0)
         p.stream = stream
         t = dict(tuning or {})
         p.trace_mode = int(t.get("trace_mode", trace_mode))

@@ -442,3 +442,21 @@ def test_gpu_rmse_at_matched_spp_within_5pct_of_reference(golden):
         assert abs(ratio - 1.0) < 0.05, (ratio, np.mean(rm), np.mean(g["ref_rmse"]))
     finally:
         gs.close()
+
+
+@pytest.mark.parametrize("builder", [lambda: scenes.cornell_pt(48, 40, 9, 8),
+                                     lambda: scenes.volumetric_caustic(40, 32, 4, 4, 5, parity=True),
+                                     lambda: scenes.whitted(scenes.cornell_pt(32, 32, 4, 8))])
+def test_gpu_overlapped_schedule_equals_serial(builder):
+    """The default schedule traces each bounce's shadow rays on a second stream beside the
+    next bounce's closest-hit rays; the film is bit-identical to the one-stream order
+    (RUMI_FLAG_SERIAL), over several waves."""
+    sc = builder()
+    if not isinstance(sc.tracer, scenes.RayTracer):
+        sc.tracer = scenes.PathTracer(8)
+    gs = rumi_b200.GpuScene(sc)
+    a, sa = gs.render(spp=9, seed=77, wave_paths=4000)
+    b, sb = gs.render(spp=9, seed=77, wave_paths=4000, serial=True)
+    gs.close()
+    np.testing.assert_array_equal(a, b)
+    assert sa["rays_extend"] == sb["rays_extend"] and sa["rays_shadow"] == sb["rays_shadow"]
