@@ -591,7 +591,7 @@ def batched_arm(args):
     def plain(step):
         for g, s, sd, off in zip(gss, spp, seeds(step), offs):
             g.render(spp=s, seed=sd, film_device_ptr=films_plain.data_ptr() + 4 * off, stream=stream)
-        return len(gss) * (3 + 4 * depth)
+        return len(gss) * (3 + 5 * depth)  # rumi_render: per bounce two resets, extend, shade, shadow
 
     def batched(step):
         _, st = batch.render(spp, seeds(step), depth, graph=True, films_device_ptr=films_batch.data_ptr(),
@@ -727,7 +727,7 @@ def adjoint_arm(args):
                 albedo_rmse_start=alb_rmse0, albedo_rmse_end=alb_rmse,
                 medium_end=[float(x) for x in med.detach().cpu()],
                 medium_target=list(t["sigma_s"]) + list(t["sigma_a"]) + [t["g"]],
-                gpu_launches=args.adam_steps * 3 * (3 + 4 * depth), clocks=clocks_info)
+                gpu_launches=args.adam_steps * ((3 + 5 * depth) + 2 * (3 + 4 * depth)), clocks=clocks_info)
     print(json.dumps(line), flush=True)
     g.close()
     return 0
@@ -817,7 +817,7 @@ def cornell_arm(args):
     launches = 0
     for s in range(steps):
         _, st = gs.render(seed=100 + s, film_device_ptr=film.data_ptr(), stream=stream)
-        launches += (st["extend_launches"] // depth) * (3 + 4 * depth)
+        launches += (st["extend_launches"] // depth) * (3 + 5 * depth)
     ev1.record()
     torch.cuda.synchronize()
     clocks_info = clocks.stop()

@@ -1324,10 +1324,9 @@ rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaSt
 
 // Device address of the 64-bit statistics inside a batch workspace.
 unsigned long long *pt_batch_stats_ptr(void *ws, long long wave_paths) {
-    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t Wp = (size_t)wave_paths;
-    const size_t off = 10 * al(Wp * sizeof(float4)) + al(Wp * sizeof(unsigned)) + al(C_NUM * sizeof(int));
-    return (unsigned long long *)((char *)ws + off);
+    PtLaunch L;
+    carve_wave(L, ws, (size_t)wave_paths);  // the same layout pt_enqueue_batch carves
+    return L.stats;
 }
 
 // ---------------------------------------------------------------- ray batches

@@ -25,20 +25,25 @@ def batch_scenes():
         g.close()
 
 
-def singles(gs, seeds, wave_paths=0):
-    return [g.render(spp=s, seed=int(sd), wave_paths=wave_paths)[0]
-            for g, (_, s, _), sd in zip(gs, CASES, seeds)]
+def singles(gs, seeds, wave_paths=0, with_stats=False):
+    out = [g.render(spp=s, seed=int(sd), wave_paths=wave_paths)
+           for g, (_, s, _), sd in zip(gs, CASES, seeds)]
+    return out if with_stats else [f for f, _ in out]
 
 
 @pytest.mark.parametrize("graph", [False, True])
 @pytest.mark.parametrize("wave_paths", [0, 1000, 4099])
 def test_batch_equals_per_scene_renders(batch_scenes, graph, wave_paths):
     seeds = [11 + 7 * i for i in range(len(CASES))]
-    ref = singles(batch_scenes, seeds)
+    ref_st = singles(batch_scenes, seeds, with_stats=True)
+    ref = [f for f, _ in ref_st]
     b = rumi_b200.GpuBatch(batch_scenes)
     try:
         films, st = b.render([c[1] for c in CASES], seeds, DEPTH, graph=graph, wave_paths=wave_paths)
         assert st["paths"] == sum(r * r * s for r, s, _ in CASES)
+        # the frame's ray counts are the scenes' own, read from the batch workspace
+        for k in ("rays_extend", "rays_shadow", "nan_samples"):
+            assert st[k] == sum(x[k] for _, x in ref_st), k
         for k, (f, r) in enumerate(zip(films, ref)):
             assert np.array_equal(f, r), k
             assert f.sum() > 0
