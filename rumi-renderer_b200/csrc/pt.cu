@@ -959,6 +959,16 @@ size_t pt_workspace_bytes(long long paths) {
     return 11 * al(Wp * sizeof(float4)) + al(C_NUM * sizeof(int)) + al(S_NUM * sizeof(unsigned long long));
 }
 
+// The scene's second stream and its fork / join events, made on first use.
+static rumi_status ensure_aux(rumi_scene *sc) {
+    if (sc->aux_stream) return RUMI_OK;
+    cudaError_t e = cudaStreamCreateWithFlags(&sc->aux_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sc->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sc->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_status(e, "auxiliary stream");
+    return RUMI_OK;
+}
+
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                       cudaStream_t stream) {
     const long long total_pix = (long long)sc->dev.width * sc->dev.height;
@@ -973,12 +983,7 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
     }
     rumi_status st = ensure_workspace(sc, pt_workspace_bytes(n_paths_max));
     if (st != RUMI_OK) return st;
-    if (!sc->aux_stream) {
-        cudaError_t e = cudaStreamCreateWithFlags(&sc->aux_stream, cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sc->ev_fork, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sc->ev_join, cudaEventDisableTiming);
-        if (e != cudaSuccess) return cuda_status(e, "auxiliary stream");
-    }
+    if ((st = ensure_aux(sc)) != RUMI_OK) return st;
     return pt_render_in(sc, p, film_dev, stats, stream, sc->ws, pix_per_wave,
                         RUMI_PT_OVERLAP != 0 && !(p->flags & RUMI_FLAG_SERIAL));
 }
@@ -1161,6 +1166,8 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
     }
     rumi_status st = ensure_workspace(sc, pt_adjoint_workspace_bytes((long long)Wp));
     if (st != RUMI_OK) return st;
+    const bool overlap = RUMI_PT_OVERLAP != 0 && !(p->flags & RUMI_FLAG_SERIAL);
+    if (overlap && (st = ensure_aux(sc)) != RUMI_OK) return st;
     float *gm_scratch = nullptr;
     cudaError_t e = cudaSuccess;
     if (!g_medium) {
@@ -1216,25 +1223,38 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
             L->n_paths = (int)(n_pix * spp);
             L->path0 = pix0 * spp;
         }
+        // both passes on the two-stream schedule of pt_render_in: each bounce's shadow rays
+        // beside the next bounce's closest-hit rays, shading after both
+        auto pass = [&](PtLaunch &X, bool adj) {
+            pt_generate<<<cdiv(X.n_paths, 256), 256, 0, stream>>>(X);
+            for (int b = 0; b < p->max_depth; ++b) {
+                pt_reset_extend<<<1, 1, 0, stream>>>(X, b);
+                launch_extend<false>(mode, grid, stream, X, b);
+                if (b > 0 && overlap) cudaStreamWaitEvent(stream, sc->ev_join, 0);
+                pt_reset_shade<<<1, 1, 0, stream>>>(X, b);
+                if (adj)
+                    pt_shade<true><<<cdiv(X.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(X, b);
+                else
+                    pt_shade<false><<<cdiv(X.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(X, b);
+                const bool aside = overlap && b + 1 < p->max_depth;
+                cudaStream_t ss = aside ? sc->aux_stream : stream;
+                if (aside) {
+                    cudaEventRecord(sc->ev_fork, stream);
+                    cudaStreamWaitEvent(sc->aux_stream, sc->ev_fork, 0);
+                }
+                if (adj)
+                    launch_shadow<true>(mode, grid_sh_adj, ss, X);
+                else
+                    launch_shadow<false>(mode, grid_sh, ss, X);
+                if (aside) cudaEventRecord(sc->ev_join, sc->aux_stream);
+            }
+            pt_finish<<<1, 1, 0, stream>>>(X);
+        };
         // pass 1: radiance of every path
-        pt_generate<<<cdiv(A.n_paths, 256), 256, 0, stream>>>(A);
-        for (int b = 0; b < p->max_depth; ++b) {
-            pt_reset<<<1, 1, 0, stream>>>(A, b);
-            launch_extend<false>(mode, grid, stream, A, b);
-            pt_shade<false><<<cdiv(A.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(A, b);
-            launch_shadow<false>(mode, grid_sh, stream, A);
-        }
-        pt_finish<<<1, 1, 0, stream>>>(A);
+        pass(A, false);
         cudaMemcpyAsync(Lt, A.L, sizeof(float4) * (size_t)A.n_paths, cudaMemcpyDeviceToDevice, stream);
         // pass 2: replay with the scores
-        pt_generate<<<cdiv(B.n_paths, 256), 256, 0, stream>>>(B);
-        for (int b = 0; b < p->max_depth; ++b) {
-            pt_reset<<<1, 1, 0, stream>>>(B, b);
-            launch_extend<false>(mode, grid, stream, B, b);
-            pt_shade<true><<<cdiv(B.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(B, b);
-            launch_shadow<true>(mode, grid_sh_adj, stream, B);
-        }
-        pt_finish<<<1, 1, 0, stream>>>(B);
+        pass(B, true);
         ++waves;
     }
     if (e1) cudaEventRecord(e1, stream);

@@ -133,7 +133,9 @@ class GpuScene:
                film_device_ptr: int = None, stream: int = None, count_stats: bool = False, trace_mode: int = 0,
                blocks_per_sm: int = 0, refill_min: int = 0, tuning: dict = None, serial: bool = False):
         """Renders one frame.  Returns (film (H, W, 3) B,G,R sums, stats dict); with
-        film_device_ptr the film stays on the device and the first value is None."""
+        film_device_ptr the film stays on the device and the first value is None.
+        serial=True (RUMI_FLAG_SERIAL) runs every launch in order on one stream, so that
+        timing=True reports each kernel's time alone on the GPU; the film is the same."""
         tr = tracer or self.flat.tracer
         p = _capi.rumi_render_params()
         if isinstance(tr, BidirectionalPathTracer):
