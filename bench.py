@@ -597,7 +597,7 @@ def batched_arm(args):
         _, st = batch.render(spp, seeds(step), depth, graph=True, films_device_ptr=films_batch.data_ptr(),
                              stream=stream)
         waves = st["extend_launches"] // depth
-        return waves * (3 + 4 * depth)
+        return waves * (3 + 5 * depth)
 
     def timed(fn):
         for s in range(args.warmup):

@@ -14,6 +14,8 @@ struct rumi_batch {
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
+    cudaStream_t aux = nullptr;  // second stream of the two-stream schedule
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // device tables
     DevScene *d_scenes = nullptr;
     long long *d_path0 = nullptr, *d_pix0 = nullptr;
@@ -105,6 +107,13 @@ rumi_status rumi_batch_create(rumi_scene *const *scenes, int32_t n, rumi_batch *
         delete b;
         return cuda_status(e, "cudaStreamCreate");
     }
+    e = cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        rumi_batch_destroy(b);
+        return cuda_status(e, "batch auxiliary stream");
+    }
     std::vector<DevScene> table(n);
     b->pix0.assign(n + 1, 0);
     for (int i = 0; i < n; ++i) {
@@ -142,6 +151,12 @@ rumi_status rumi_batch_destroy(rumi_batch *b) {
     dfree(b->d_spp, s);
     dfree(b->ws, s);
     dfree(b->d_films, s);
+    if (b->aux) {
+        cudaStreamSynchronize(b->aux);
+        cudaStreamDestroy(b->aux);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
     if (s) {
         cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
@@ -241,7 +256,7 @@ rumi_status rumi_render_batch(rumi_batch *b, const rumi_batch_params *p, float *
             cudaGraph_t g = nullptr;
             e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
             if (e != cudaSuccess) return cuda_status(e, "cudaStreamBeginCapture");
-            st = pt_enqueue_batch(F, b->ws, films_dev, b->stream, b->num_sms);
+            st = pt_enqueue_batch(F, b->ws, films_dev, b->stream, b->num_sms, b->aux, b->ev_fork, b->ev_join);
             e = cudaStreamEndCapture(b->stream, &g);
             if (st != RUMI_OK) {
                 if (g) cudaGraphDestroy(g);
@@ -265,7 +280,7 @@ rumi_status rumi_render_batch(rumi_batch *b, const rumi_batch_params *p, float *
         if (e != cudaSuccess) return cuda_status(e, "cudaGraphLaunch");
     } else {
         if (e0) cudaEventRecord(e0, s);
-        st = pt_enqueue_batch(F, b->ws, films_dev, s, b->num_sms);
+        st = pt_enqueue_batch(F, b->ws, films_dev, s, b->num_sms, b->aux, b->ev_fork, b->ev_join);
         if (st != RUMI_OK) return st;
     }
     if (e1) cudaEventRecord(e1, s);

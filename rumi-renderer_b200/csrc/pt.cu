@@ -1298,7 +1298,8 @@ size_t pt_batch_workspace_bytes(long long wave_paths) {
 // Enqueues one frame of a multi-scene batch without synchronising, so the sequence can
 // be captured into a CUDA graph: waves over the batch's global pixel / path index space,
 // every stage serving all scenes from shared queues.
-rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaStream_t stream, int num_sms) {
+rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaStream_t stream, int num_sms,
+                             cudaStream_t aux, cudaEvent_t ev_fork, cudaEvent_t ev_join) {
     PtLaunch L;
     L.slot_scene = (int *)carve_wave(L, ws, (size_t)F.wave_paths);
     L.max_depth = F.max_depth;
@@ -1328,11 +1329,21 @@ rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaSt
         L.path0 = wv.path0;
         L.n_paths = (int)(wv.path1 - wv.path0);
         pt_generate<<<cdiv(L.n_paths, 256), 256, 0, stream>>>(L);
+        // the two-stream schedule of pt_render_in (a graph capture takes the auxiliary
+        // stream in through the fork event and every fork is joined before shading)
         for (int b = 0; b < F.max_depth; ++b) {
-            pt_reset<<<1, 1, 0, stream>>>(L, b);
+            pt_reset_extend<<<1, 1, 0, stream>>>(L, b);
             pt_trace_multi<false><<<num_sms * occ, TRACE_THREADS, 0, stream>>>(L, b);
+            if (b > 0 && aux) cudaStreamWaitEvent(stream, ev_join, 0);
+            pt_reset_shade<<<1, 1, 0, stream>>>(L, b);
             pt_shade<false><<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
-            pt_trace_multi<true><<<num_sms * occ_sh, TRACE_THREADS, 0, stream>>>(L, b);
+            const bool aside = aux && b + 1 < F.max_depth;
+            if (aside) {
+                cudaEventRecord(ev_fork, stream);
+                cudaStreamWaitEvent(aux, ev_fork, 0);
+            }
+            pt_trace_multi<true><<<num_sms * occ_sh, TRACE_THREADS, 0, aside ? aux : stream>>>(L, b);
+            if (aside) cudaEventRecord(ev_join, aux);
         }
         pt_finish<<<1, 1, 0, stream>>>(L);
         pt_resolve<<<cdiv(L.n_pix * 32LL, 256), 256, 0, stream>>>(L);

@@ -63,7 +63,10 @@ size_t pt_adjoint_workspace_bytes(long long paths);
 rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float *dfilm_dev, float *g_albedo,
                         float *g_medium, rumi_render_stats *stats, cudaStream_t stream);
 size_t pt_batch_workspace_bytes(long long wave_paths);
-rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaStream_t stream, int num_sms);
+// aux, ev_fork, ev_join: the batch's second stream and its events for the two-stream
+// schedule (aux == nullptr: every launch in order on `stream`)
+rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaStream_t stream, int num_sms,
+                             cudaStream_t aux = nullptr, cudaEvent_t ev_fork = nullptr, cudaEvent_t ev_join = nullptr);
 unsigned long long *pt_batch_stats_ptr(void *ws, long long wave_paths);
 
 void set_error(const std::string &msg);

@@ -142,6 +142,17 @@ RUMI_D bool slab(float4 a, float4 b, float3 inv, float3 oinv, float tlimit, floa
     return tn <= tf && tf >= 0.0f && tn <= tlimit;
 }
 
+// Node culling limit from the best hit so far.  Primitives at exactly the best distance
+// (coplanar neighbours meeting at an edge) are all reached whatever order the leaves are
+// tested in: the limit sits a relative 2^-16 above the best distance, above the rounding
+// of the slab distances, and leaf_isect gives a tie to the larger primitive id (the one an
+// exhaustive scan in canonical order reports last).  The speculative walk tests leaves in
+// an order that depends on the rays sharing the warp, so without this a tie could go
+// either way from run to run.
+RUMI_D float cull_limit(float best_t, float tmax) {
+    return best_t > 0.0f ? fminf(fmaf(fmaxf(best_t, 1.0f), 1.52587890625e-05f, best_t), tmax) : tmax;
+}
+
 struct TraceStats {
     int nodes;   // 32-byte nodes fetched
     int prims;   // primitives tested
@@ -168,6 +179,7 @@ RUMI_D bool leaf_isect(const DevScene &s, int first, int count, float3 o, float3
             ok = isect_rect(o, d, tmax, h.t, A, B, C, (tag & PRIM_FLAG_EMISSIVE) != 0, t);
         else
             ok = isect_sphere(o, d, tmax, h.t, A, B, in_object && !ANYHIT, (tag & PRIM_FLAG_IBL) != 0, t);
+        if (ok && t == h.t && __float_as_int(A.w) < h.id) ok = false;  // a tie: the larger id stays
         if (ok) {
             h.t = t;
             h.id = __float_as_int(A.w);
@@ -217,7 +229,7 @@ RUMI_D HitRec trace_ray_bin(const DevScene &s, float3 o, float3 d, float tmax, b
             const float4 *np = reinterpret_cast<const float4 *>(s.nodes + cur);
             const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
             if (STATS) st.nodes += 2;
-            const float lim = h.t > 0.0f ? fminf(h.t, tmax) : tmax;
+            const float lim = cull_limit(h.t, tmax);
             float tn0, tn1;
             bool h0 = slab(a0, b0, inv, oinv, lim, tn0);
             bool h1 = slab(a1, b1, inv, oinv, lim, tn1);
@@ -317,7 +329,7 @@ RUMI_D HitRec trace_ray_wide(const DevScene &s, float3 o, float3 d, float tmax, 
         const int4 ch = __ldg(reinterpret_cast<const int4 *>(np + 6));
         const int4 cn = __ldg(reinterpret_cast<const int4 *>(np + 7));
         if (STATS) st.nodes += 4;  // counted in 32-byte units
-        const float lim = h.t > 0.0f ? fminf(h.t, tmax) : tmax;
+        const float lim = cull_limit(h.t, tmax);
         float k0, k1, k2, k3;
         if (!(cn.x >= 0 && slab_s(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, inv, oinv, lim, k0))) k0 = FLT_MAX;
         if (!(cn.y >= 0 && slab_s(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, inv, oinv, lim, k1))) k1 = FLT_MAX;
@@ -465,7 +477,7 @@ RUMI_D void trav_step(const DevScene &s, TravState &T, int *smem_stack, int stri
     const float4 *np = reinterpret_cast<const float4 *>(s.nodes + T.cur);
     const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
     if (STATS) st.nodes += 2;
-    const float lim = T.h.t > 0.0f ? fminf(T.h.t, T.tmax) : T.tmax;
+    const float lim = cull_limit(T.h.t, T.tmax);
     float tn0, tn1;
     const bool h0 = slab(a0, b0, T.inv, T.oinv, lim, tn0);
     const bool h1 = slab(a1, b1, T.inv, T.oinv, lim, tn1);
@@ -539,7 +551,7 @@ RUMI_D void trav_step_postpone(const DevScene &s, TravState &T, PendingLeaves &p
     const float4 *np = reinterpret_cast<const float4 *>(s.nodes + T.cur);
     const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
     if (STATS) st.nodes += 2;
-    const float lim = T.h.t > 0.0f ? fminf(T.h.t, T.tmax) : T.tmax;
+    const float lim = cull_limit(T.h.t, T.tmax);
     float tn0, tn1;
     const bool h0 = slab(a0, b0, T.inv, T.oinv, lim, tn0);
     const bool h1 = slab(a1, b1, T.inv, T.oinv, lim, tn1);
@@ -698,7 +710,7 @@ RUMI_D void traverse_queue_ww(SceneOf scene_of, int n, int *counter, int refill_
             const float4 a0 = __ldg(nodes + 2 * cur), b0 = __ldg(nodes + 2 * cur + 1);
             const float4 a1 = __ldg(nodes + 2 * cur + 2), b1 = __ldg(nodes + 2 * cur + 3);
             if (STATS) st.nodes += 2;
-            const float lim = h.t > 0.0f ? fminf(h.t, tmax) : tmax;
+            const float lim = cull_limit(h.t, tmax);
             float tn0, tn1;
             const bool h0 = slab(a0, b0, inv, oinv, lim, tn0);
             const bool h1 = slab(a1, b1, inv, oinv, lim, tn1);
@@ -831,7 +843,7 @@ RUMI_D void traverse_queue_ww4(SceneOf scene_of, int n, int *counter, int refill
             const int4 ch = __ldg(reinterpret_cast<const int4 *>(np + 6));
             const int4 cn = __ldg(reinterpret_cast<const int4 *>(np + 7));
             if (STATS) st.nodes += 4;  // counted in 32-byte units
-            const float lim = h.t > 0.0f ? fminf(h.t, tmax) : tmax;
+            const float lim = cull_limit(h.t, tmax);
             float k0, k1, k2, k3;
             if (!(cn.x >= 0 && slab_s(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, inv, oinv, lim, k0))) k0 = FLT_MAX;
             if (!(cn.y >= 0 && slab_s(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, inv, oinv, lim, k1))) k1 = FLT_MAX;
