@@ -460,3 +460,27 @@ def test_gpu_overlapped_schedule_equals_serial(builder):
     gs.close()
     np.testing.assert_array_equal(a, b)
     assert sa["rays_extend"] == sb["rays_extend"] and sa["rays_shadow"] == sb["rays_shadow"]
+
+
+@pytest.mark.parametrize("fixture,builder", [
+    ("hits_cornell.npz", lambda: scenes.cornell_pt(64, 64, 16, 8)),
+    ("hits_mesh5.npz", lambda: scenes.bvh_bound_pt(64, 64, 4, 10, levels=5, seed=7)),
+])
+def test_gpu_hits_equal_oracle_ties_included_in_any_order(golden, fixture, builder):
+    """A primitive hit at exactly the best distance as another goes to the larger id
+    whatever order the traversal meets them in: the GPU's ids equal the oracle's exhaustive
+    scan (which reports the last tied primitive in canonical order), for the rays in their
+    own order and shuffled (other rays share each warp)."""
+    g = golden(fixture)
+    sc = builder()
+    gs = rumi_b200.GpuScene(sc)
+    rays = np.ascontiguousarray(g["rays"], np.float32)
+    ot, op = O.OracleScene(sc).trace(rays8(rays))
+    t, prim, _, _ = gs.trace(rays)
+    np.testing.assert_array_equal(t, ot)
+    np.testing.assert_array_equal(prim, op)
+    perm = np.random.default_rng(5).permutation(rays.shape[0])
+    t2, prim2, _, _ = gs.trace(np.ascontiguousarray(rays[perm]))
+    np.testing.assert_array_equal(prim2, prim[perm])
+    np.testing.assert_array_equal(t2, t[perm])
+    gs.close()
