@@ -698,6 +698,14 @@ def adjoint_arm(args):
         g.backward(d, seed=7, timing=True)
     fwd_ms = statistics.median(g.forward(seed=8 + i, timing=True)[1]["total_ms"] for i in range(5))
     bwd_ms = statistics.median(g.backward(d, seed=8 + i, timing=True)[2]["total_ms"] for i in range(5))
+    # the same backward right after a forward of the same frame that kept its per-path
+    # radiance (RUMI_FLAG_KEEP_RADIANCE): only the replay pass is traced.  (The optimisation
+    # loop below draws the adjoint's paths with another seed, so it cannot use this.)
+    kept = []
+    for i in range(5):
+        g.forward(seed=8 + i, keep=True)
+        kept.append(g.backward(d, seed=8 + i, timing=True)[2]["total_ms"])
+    bwd_kept_ms = statistics.median(kept)
     alb_rmse0 = float(((mesh.detach() - hidden_t) ** 2).mean().sqrt())
     for it in range(args.warmup):
         step(-1 - it)
@@ -723,6 +731,7 @@ def adjoint_arm(args):
                 config=dict(workload="inverse rendering: 256x256, 64 spp, depth 8, 65,536 triangles in a medium",
                             params=3 * n_mesh + 7, optimiser="Adam lr 1e-2", loss="L2 image"),
                 forward_ms=fwd_ms, backward_ms=bwd_ms, backward_over_forward=bwd_ms / fwd_ms,
+                backward_after_kept_forward_ms=bwd_kept_ms,
                 paths_per_step=size * size * spp, loss_first=losses[0], loss_last=losses[-1],
                 albedo_rmse_start=alb_rmse0, albedo_rmse_end=alb_rmse,
                 medium_end=[float(x) for x in med.detach().cpu()],

@@ -170,10 +170,15 @@ enum { RUMI_PATH_TRACER = 0, RUMI_BDPT = 1, RUMI_RAY_TRACER = 2 };
 enum {
     RUMI_FLAG_TIMING = 1,  /* per-kernel CUDA-event timing into rumi_render_stats */
     RUMI_FLAG_STATS = 2,   /* count BVH node fetches and primitive tests of closest-hit rays */
-    RUMI_FLAG_SERIAL = 4   /* path tracer: every launch in order on the one stream (by default a
+    RUMI_FLAG_SERIAL = 4,  /* path tracer: every launch in order on the one stream (by default a
                               bounce's shadow rays are traced on a second stream of the scene
                               beside the next bounce's closest-hit rays); with TIMING, each
                               kernel's time is then its time alone on the GPU */
+    RUMI_FLAG_KEEP_RADIANCE = 8 /* rumi_forward: keep every path's radiance in a device array of the
+                              scene (16 bytes per path, W*H*spp paths); the next rumi_backward with
+                              the same seed, spp and max_depth, and no rumi_scene_set_albedo /
+                              _set_volume in between, takes the radiance from there instead of
+                              tracing its first pass */
 };
 
 typedef struct {

@@ -14,7 +14,45 @@ rumi_status rumi_forward(rumi_scene *sc, const rumi_render_params *p, float *fil
         set_error("rumi_forward: the adjoint covers the path tracer only");
         return RUMI_ERR_INVALID_ARG;
     }
-    return rumi_render(sc, p, film, film_on_device, stats);
+    if (!sc || !p || !(p->flags & RUMI_FLAG_KEEP_RADIANCE)) {
+        if (sc) sc->kept_valid = false;
+        return rumi_render(sc, p, film, film_on_device, stats);
+    }
+    // RUMI_FLAG_KEEP_RADIANCE: the frame's per-path radiance stays on the device for
+    // rumi_backward (16 bytes per path)
+    sc->kept_valid = false;
+    if (!film || p->spp <= 0 || p->max_depth <= 0) return rumi_render(sc, p, film, film_on_device, stats);
+    cudaStream_t s = p->stream ? (cudaStream_t)p->stream : sc->stream;
+    const long long n = (long long)sc->dev.width * sc->dev.height * p->spp;
+    if (sc->kept_cap < n) {
+        dfree(sc->kept_L, s);
+        sc->kept_L = nullptr;
+        sc->kept_cap = 0;
+        cudaError_t e = dalloc((void **)&sc->kept_L, sizeof(float4) * (size_t)n, s);
+        if (e != cudaSuccess) return cuda_status(e, "rumi_forward: kept radiance");
+        sc->kept_cap = n;
+    }
+    const size_t film_bytes = sizeof(float) * 3 * (size_t)sc->dev.width * sc->dev.height;
+    float *film_dev = film, *tmp = nullptr;
+    if (!film_on_device) {
+        cudaError_t e = dalloc((void **)&tmp, film_bytes, s);
+        if (e != cudaSuccess) return cuda_status(e, "device allocation (film)");
+        film_dev = tmp;
+    }
+    rumi_status st = pt_render(sc, p, film_dev, stats, s, sc->kept_L);
+    if (st == RUMI_OK && !film_on_device) {
+        cudaError_t e = cudaMemcpyAsync(film, film_dev, film_bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_status(e, "film copy");
+    }
+    dfree(tmp, s);
+    if (st == RUMI_OK) {
+        sc->kept_valid = true;
+        sc->kept_seed = p->seed;
+        sc->kept_spp = p->spp;
+        sc->kept_depth = p->max_depth;
+    }
+    return st;
 }
 
 rumi_status rumi_backward(rumi_scene *sc, const rumi_render_params *p, const float *d_film, float *grad_albedo,
@@ -75,6 +113,7 @@ rumi_status rumi_scene_set_albedo(rumi_scene *sc, const float *albedo, int32_t o
         set_error("rumi_scene_set_albedo: NULL argument");
         return RUMI_ERR_INVALID_ARG;
     }
+    sc->kept_valid = false;  // a kept forward radiance no longer describes the scene
     if (!sc->tri_albedo) {
         set_error("rumi_scene_set_albedo: the scene was created without per-triangle albedo");
         return RUMI_ERR_INVALID_ARG;
@@ -98,6 +137,7 @@ rumi_status rumi_scene_set_albedo(rumi_scene *sc, const float *albedo, int32_t o
 }
 
 rumi_status rumi_scene_set_volume(rumi_scene *sc, const rumi_volume *v) {
+    if (sc) sc->kept_valid = false;  // a kept forward radiance no longer describes the scene
     if (!sc || !v) {
         set_error("rumi_scene_set_volume: NULL argument");
         return RUMI_ERR_INVALID_ARG;

@@ -141,6 +141,7 @@ void free_scene(rumi_scene *sc) {
     dfree(sc->textures, s);
     dfree(sc->prim_tex, s);
     dfree(sc->sphere_frame, s);
+    dfree(sc->kept_L, s);
     for (void *p : sc->tex_pixels) dfree(p, s);
     if (sc->aux_stream) {
         cudaStreamSynchronize(sc->aux_stream);

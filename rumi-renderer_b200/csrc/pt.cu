@@ -970,7 +970,7 @@ static rumi_status ensure_aux(rumi_scene *sc) {
 }
 
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, float4 *keep_L) {
     const long long total_pix = (long long)sc->dev.width * sc->dev.height;
     long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 22);
     long long pix_per_wave = wave / p->spp;
@@ -985,13 +985,13 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
     if (st != RUMI_OK) return st;
     if ((st = ensure_aux(sc)) != RUMI_OK) return st;
     return pt_render_in(sc, p, film_dev, stats, stream, sc->ws, pix_per_wave,
-                        RUMI_PT_OVERLAP != 0 && !(p->flags & RUMI_FLAG_SERIAL));
+                        RUMI_PT_OVERLAP != 0 && !(p->flags & RUMI_FLAG_SERIAL), keep_L);
 }
 
 // The frame loop over waves of pix_per_wave pixels, with the wave state carved out of
 // `ws` (pt_workspace_bytes(pix_per_wave * spp) bytes).
 rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
-                         cudaStream_t stream, void *ws, long long pix_per_wave, bool overlap) {
+                         cudaStream_t stream, void *ws, long long pix_per_wave, bool overlap, float4 *keep_L) {
     const int W = sc->dev.width, H = sc->dev.height;
     const int spp = p->spp;
     const long long total_pix = (long long)W * H;
@@ -1078,6 +1078,9 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
             }
             pt_finish<<<1, 1, 0, stream>>>(L);
             pt_resolve<<<cdiv(L.n_pix * 32LL, 256), 256, 0, stream>>>(L);
+            if (keep_L)
+                cudaMemcpyAsync(keep_L + L.path0, L.L, sizeof(float4) * (size_t)L.n_paths, cudaMemcpyDeviceToDevice,
+                                stream);
             ++waves;
             continue;
         }
@@ -1102,6 +1105,9 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
         }
         pt_finish<<<1, 1, 0, stream>>>(L);
         pt_resolve<<<cdiv(L.n_pix * 32LL, 256), 256, 0, stream>>>(L);
+        if (keep_L)
+            cudaMemcpyAsync(keep_L + L.path0, L.L, sizeof(float4) * (size_t)L.n_paths, cudaMemcpyDeviceToDevice,
+                            stream);
         ++waves;
     }
     if (timing) mark();
@@ -1168,6 +1174,9 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
     if (st != RUMI_OK) return st;
     const bool overlap = RUMI_PT_OVERLAP != 0 && !(p->flags & RUMI_FLAG_SERIAL);
     if (overlap && (st = ensure_aux(sc)) != RUMI_OK) return st;
+    // the forward pass of this very frame kept its per-path radiance: pass 1 is not traced
+    const bool reuse = sc->kept_valid && sc->kept_seed == p->seed && sc->kept_spp == spp &&
+                       sc->kept_depth == p->max_depth && sc->kept_cap >= total_pix * spp;
     float *gm_scratch = nullptr;
     cudaError_t e = cudaSuccess;
     if (!g_medium) {
@@ -1250,9 +1259,14 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
             }
             pt_finish<<<1, 1, 0, stream>>>(X);
         };
-        // pass 1: radiance of every path
-        pass(A, false);
-        cudaMemcpyAsync(Lt, A.L, sizeof(float4) * (size_t)A.n_paths, cudaMemcpyDeviceToDevice, stream);
+        // pass 1: radiance of every path (or the radiance rumi_forward kept for this frame)
+        if (reuse) {
+            cudaMemcpyAsync(Lt, sc->kept_L + A.path0, sizeof(float4) * (size_t)A.n_paths, cudaMemcpyDeviceToDevice,
+                            stream);
+        } else {
+            pass(A, false);
+            cudaMemcpyAsync(Lt, A.L, sizeof(float4) * (size_t)A.n_paths, cudaMemcpyDeviceToDevice, stream);
+        }
         // pass 2: replay with the scores
         pass(B, true);
         ++waves;
@@ -1274,7 +1288,7 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
         stats->nan_samples = (int64_t)h_stats[S_NAN];
         stats->rays_extend = (int64_t)h_stats[S_RAYS_EXT];
         stats->rays_shadow = (int64_t)h_stats[S_RAYS_SH];
-        stats->extend_launches = 2 * waves * p->max_depth;
+        stats->extend_launches = (reuse ? 1 : 2) * waves * p->max_depth;
         stats->shade_launches = stats->extend_launches;
         stats->shadow_launches = stats->extend_launches;
         if (e0) {

@@ -29,6 +29,12 @@ struct rumi_scene {
     // the any-hit launch of a bounce runs beside the next bounce's closest-hit launch
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // per-path radiance kept by rumi_forward (RUMI_FLAG_KEEP_RADIANCE) for rumi_backward
+    float4 *kept_L = nullptr;
+    long long kept_cap = 0;
+    bool kept_valid = false;
+    uint64_t kept_seed = 0;
+    int kept_spp = 0, kept_depth = 0;
     int n_nodes = 0;
     rumi::BvhBuildInfo info{};
     double build_ms = 0.0;
@@ -76,14 +82,17 @@ void pack_albedo(const float *a_dev, int n, float4 *out, cudaStream_t s);
 rumi_status cuda_status(cudaError_t e, const char *what);
 
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
-                      cudaStream_t stream);
+                      cudaStream_t stream, float4 *keep_L = nullptr);
 size_t pt_workspace_bytes(long long paths);
 rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                         cudaStream_t stream);
 // overlap: run each bounce's any-hit launch on the scene's auxiliary stream beside the
 // next bounce's closest-hit launch (false: one stream, in order)
+// keep_L: when set, every wave's per-path radiance is copied there at global path index
+// pixel * spp + sample
 rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
-                         cudaStream_t stream, void *ws, long long pix_per_wave, bool overlap = false);
+                         cudaStream_t stream, void *ws, long long pix_per_wave, bool overlap = false,
+                         float4 *keep_L = nullptr);
 rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, float *t_dev, int32_t *prim_dev,
                        int64_t *node_visits, int64_t *prim_tests, cudaStream_t stream);
 rumi_status ensure_workspace(rumi_scene *sc, size_t bytes);

@@ -178,9 +178,14 @@ class GpuScene:
         return p
 
     def forward(self, spp: int = None, seed: int = 1, max_depth: int = None, wave_paths: int = 0,
-                film_device_ptr: int = None, stream: int = None, timing: bool = False):
-        """rumi_forward: the path-traced film that backward() differentiates."""
+                film_device_ptr: int = None, stream: int = None, timing: bool = False, keep: bool = False):
+        """rumi_forward: the path-traced film that backward() differentiates.  keep=True
+        (RUMI_FLAG_KEEP_RADIANCE) keeps every path's radiance on the device (16 bytes per
+        path) so that the next backward() with the same seed, spp and max_depth skips its
+        first pass."""
         p = self._pt_params(spp, seed, max_depth, wave_paths, timing, stream)
+        if keep:
+            p.flags |= 8
         st = _capi.rumi_render_stats()
         if film_device_ptr is not None:
             _capi.check(self.lib.rumi_forward(self.h, C.byref(p), C.c_void_p(film_device_ptr), 1, C.byref(st)),
