@@ -18,7 +18,7 @@ extern "C" {
 /* Philox4x32-10: ctr n*4 words, key 2 words -> out n*4 words. */
 rumi_status rumi_test_philox(int64_t n, const uint32_t *ctr, const uint32_t *key, uint32_t *out);
 
-/* Material::BSDFSampling (src/Material/*.cpp).  wo, nrm: n*3; u: n*3 (lobe, u1, u2).
+/* Material::BSDFSampling (src/Material/, one file per material).  wo, nrm: n*3; u: n*3 (lobe, u1, u2).
  * out n*9: wi.xyz, Le, go_into_object, xi, pdf_path, costheta, pdf_w. */
 rumi_status rumi_test_material_sample(const rumi_material *m, int64_t n, const float *wo, const float *nrm,
                                       const float *u, float *out);

@@ -88,3 +88,58 @@ def test_synthetic_meshes_are_deterministic():
     assert r.min() > 0.19 and r.max() < 0.31
     alb = scenes.random_albedo(1000, 8)
     assert alb.min() >= 0.2 and alb.max() <= 0.8
+
+
+@pytest.mark.parametrize("compiler,std", [("gcc", "-std=c99"), ("g++", "-std=c++11")])
+def test_headers_compile_for_plain_c_and_cxx_hosts(tmp_path, compiler, std):
+    """The boundary headers are what a reference-side host includes: they must compile as
+    plain C99 (cgo / FFI generators) and as C++ without anything from the library's own
+    build (no CUDA headers), with every struct field the ctypes mirror declares."""
+    import shutil
+    import subprocess
+    if shutil.which(compiler) is None:
+        pytest.skip(compiler + " not installed")
+    inc = os.path.join(ROOT, "include")
+    src = tmp_path / ("h.c" if compiler == "gcc" else "h.cpp")
+    src.write_text('#include "rumi_b200.h"\n#include "rumi_b200_test.h"\n'
+                   "int main(void) {\n"
+                   "    rumi_scene_desc d; rumi_render_params p; rumi_texture t;\n"
+                   "    (void)d; (void)p; (void)t;\n"
+                   "    return (int)sizeof(rumi_scene_desc) + RUMI_FLAG_KEEP_RADIANCE + RUMI_LIGHT_IBL + RUMI_TEX_HDR;\n"
+                   "}\n")
+    r = subprocess.run([compiler, std, "-Wall", "-Werror", "-fsyntax-only", "-I", inc, str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_ctypes_structs_match_the_c_layout(tmp_path):
+    """sizeof and field offsets of the C structs equal those of the ctypes mirror in
+    rumi_b200/_capi.py (a mismatch would hand the library misread scene descriptions)."""
+    import ctypes as C
+    import shutil
+    import subprocess
+    from rumi_b200 import _capi
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not installed")
+    structs = ["rumi_material", "rumi_light", "rumi_volume", "rumi_camera", "rumi_texture", "rumi_scene_desc",
+               "rumi_render_params", "rumi_render_stats"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rumi_b200.h"', "int main(void) {"]
+    for sname in structs:
+        cls = getattr(_capi, sname)
+        lines.append('    printf("%s %%zu\\n", sizeof(%s));' % (sname, sname))
+        for fname, _ in cls._fields_:
+            lines.append('    printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (sname, fname, sname, fname))
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    r = subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = dict(line.rsplit(" ", 1) for line in out if line)
+    for sname in structs:
+        cls = getattr(_capi, sname)
+        assert int(got[sname]) == C.sizeof(cls), sname
+        for fname, _ in cls._fields_:
+            assert int(got[f"{sname}.{fname}"]) == getattr(cls, fname).offset, (sname, fname)
