@@ -4,8 +4,8 @@
  * Plain C99, float arithmetic, compiled with -ffp-contract=off so every operation
  * rounds as the reference's x86 build does.  Each routine cites the reference code it
  * restates.  It is pinned to the reference itself (oracle/_ref, built from the
- * reference's sources by oracle/build_ref.py) by tests/test_oracle_vs_reference.py and
- * the golden vectors under tests/golden/.
+ * reference's sources by oracle/build_ref.py) by tests/test_oracle_golden.py and
+ * tests/test_textures.py, and to the golden vectors under tests/golden/.
  *
  * Randomness: the reference draws from a global rand().  The oracle instead consumes
  * the same counter-based Philox4x32-10 stream layout the GPU renderer uses -- counter
@@ -1191,6 +1191,21 @@ void orc_phase_sample(const float *d, float g, float u1, float u2, float *out) {
 }
 
 float orc_hg_eval(float cos_theta, float g) { return hg_eval(cos_theta, g); }
+
+/* Batched forms of the three samplers above for the sample-versus-pdf histogram tests:
+ * `count` draws, u holding 3 (material) or 2 (phase, distance) uniforms per draw, out the
+ * per-draw records of the single-draw entry points. */
+void orc_material_sample_n(const orc_material *m, const float *wo, const float *n, int64_t count, const float *u,
+                           float *out) {
+    for (int64_t i = 0; i < count; ++i) orc_material_sample(m, wo, n, u + 3 * i, out + 9 * i);
+}
+void orc_phase_sample_n(const float *d, float g, int64_t count, const float *u, float *out) {
+    for (int64_t i = 0; i < count; ++i) orc_phase_sample(d, g, u[2 * i], u[2 * i + 1], out + 4 * i);
+}
+void orc_distance_sample_n(const float *sigma_s, const float *sigma_a, float smax, int64_t count, const float *u,
+                           float *out) {
+    for (int64_t i = 0; i < count; ++i) orc_distance_sample(sigma_s, sigma_a, smax, u[2 * i], u[2 * i + 1], out + 9 * i);
+}
 
 /* out[6]: o.xyz, d.xyz */
 void orc_camera_ray(const orc_camera *c, int W, int H, int w, int h, float sx, float sy, float lu1, float lu2,

@@ -16,12 +16,12 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            import importlib.util
-            spec = importlib.util.spec_from_file_location("build_oracle", os.path.join(ROOT, "oracle", "build_oracle.py"))
-            mod = importlib.util.module_from_spec(spec)
-            spec.loader.exec_module(mod)
-            mod.build()
+        # (re)built when missing or older than oracle/rumi_oracle.c
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("build_oracle", os.path.join(ROOT, "oracle", "build_oracle.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
         L = C.CDLL(LIB_PATH)
         L.orc_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.orc_trace.argtypes = [C.c_void_p, C.c_int64, FP, C.c_int, FP, C.POINTER(C.c_int32)]
@@ -36,6 +36,9 @@ def lib():
         L.orc_fresnel.argtypes = [FP, FP, C.c_float, C.c_float]
         L.orc_distance_sample.argtypes = [FP, FP, C.c_float, C.c_float, C.c_float, FP]
         L.orc_phase_sample.argtypes = [FP, C.c_float, C.c_float, C.c_float, FP]
+        L.orc_material_sample_n.argtypes = [C.c_void_p, FP, FP, C.c_int64, FP, FP]
+        L.orc_phase_sample_n.argtypes = [FP, C.c_float, C.c_int64, FP, FP]
+        L.orc_distance_sample_n.argtypes = [FP, FP, C.c_float, C.c_int64, FP, FP]
         L.orc_hg_eval.restype = C.c_float
         L.orc_hg_eval.argtypes = [C.c_float, C.c_float]
         L.orc_camera_ray.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
