@@ -38,6 +38,11 @@
 extern "C" {
 #endif
 
+/* RUMI_ERR_INTERNAL: a device-side consistency check failed (the BVH builder's or the
+ * four-wide collapse's range checks, which record the violation instead of writing).
+ * RUMI_ERR_QUEUE_OVERFLOW and RUMI_ERR_TIMEOUT are reserved and returned by no entry
+ * point: every ray queue is sized to its wave before launch, so no push can overflow,
+ * and no kernel waits on another kernel or on a flag. */
 typedef enum {
     RUMI_OK = 0,
     RUMI_ERR_INVALID_ARG = 1,
