@@ -13,8 +13,11 @@ import json
 import os
 import time
 
-DEFAULTS = dict(trace_mode=1, blocks_per_sm=0, refill_min=8, wave_paths=1 << 22)
-SPACE = dict(trace_mode=[1, 2, 3], blocks_per_sm=[0, 4, 5, 6], refill_min=[4, 8, 16],
+# What the library uses when a knob is 0 (include/rumi_b200.h, rumi_render_params): the
+# speculative while-while walk (trace_mode 4), the occupancy limit of traversal blocks, a
+# refill at 8 idle lanes and 4,194,304 paths per wave.  The search starts there.
+DEFAULTS = dict(trace_mode=4, blocks_per_sm=0, refill_min=8, wave_paths=1 << 22)
+SPACE = dict(trace_mode=[4, 1, 2, 3], blocks_per_sm=[0, 4, 5, 6], refill_min=[4, 8, 16],
              wave_paths=[1 << 21, 1 << 22, 1 << 23])
 CACHE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tuning", "autotune_cache.json")
 

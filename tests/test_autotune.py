@@ -1,5 +1,7 @@
 """The autotuner's search and cache on CPU, against fake render objects with a known
 cost surface (the GPU measurement itself is exercised by bench runs)."""
+import os
+
 from rumi_b200 import autotune
 
 
@@ -13,7 +15,7 @@ class FakeScene:
         self.calls += 1
         t = tuning
         ms = 100.0
-        ms += {1: 10.0, 2: 0.0, 3: 30.0}[t["trace_mode"]]
+        ms += {1: 10.0, 2: 0.0, 3: 30.0, 4: 6.0}[t["trace_mode"]]
         ms += {0: 4.0, 4: 8.0, 5: 0.0, 6: 2.0}[t["blocks_per_sm"]]
         ms += {4: 0.0, 8: 1.0, 16: 3.0}[t["refill_min"]]
         ms += {1 << 21: 5.0, 1 << 22: 2.0, 1 << 23: 0.0}[t["wave_paths"]]
@@ -42,3 +44,14 @@ def test_batch_queue_capacity(tmp_path):
     res = autotune.tune_batch(FakeBatch(), [4], [1], 8, key="batch", repeats=1, cache_path=cache)
     assert res["params"] == dict(wave_paths=1 << 22)
     assert autotune.load("batch", cache_path=cache)["ms"] == 7.0
+
+
+def test_search_starts_from_the_library_defaults():
+    """The starting point is what the library does with every knob at 0 (the speculative
+    walk, trace_mode 4), and every traversal scheme of rumi_render_params is searched."""
+    assert autotune.DEFAULTS["trace_mode"] == 4
+    assert sorted(autotune.SPACE["trace_mode"]) == [1, 2, 3, 4]
+    for k, v in autotune.DEFAULTS.items():
+        assert v in autotune.SPACE[k], k
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "rumi_b200.h")).read()
+    assert "4: speculative while-while walk" in hdr
