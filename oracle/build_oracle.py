@@ -15,13 +15,17 @@ def build(force=False):
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= os.path.getmtime(SRC):
         return LIB
+    # built under a private name and renamed into place, so a process loading the library
+    # while another rebuilds it never sees a partly written file
+    tmp = f"{LIB}.{os.getpid()}.tmp"
     cmd = ["gcc", "-O2", "-std=c99", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", "-Wall",
-           "-Wno-unused-function", "-o", LIB, SRC, "-lm"]
+           "-Wno-unused-function", "-o", tmp, SRC, "-lm"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stderr)
     if r.stderr.strip():
         sys.stderr.write(r.stderr)
+    os.replace(tmp, LIB)
     return LIB
 
 
