@@ -206,6 +206,16 @@ rumi_status validate(const rumi_scene_desc *d) {
             return set_error("unknown light type"), RUMI_ERR_INVALID_ARG;
         }
     }
+    if (d->volume.present) {
+        // the free-flight sampler divides by the mean extinction and the absorption
+        // probability by each channel's (rumi_scene_set_volume applies the same rule)
+        for (int c = 0; c < 3; ++c)
+            if (!(d->volume.sigma_s[c] >= 0.0f) || !(d->volume.sigma_a[c] >= 0.0f) ||
+                !(d->volume.sigma_s[c] + d->volume.sigma_a[c] > 0.0f))
+                return set_error("medium coefficients must be >= 0 with positive extinction"), RUMI_ERR_INVALID_ARG;
+        if (!(d->volume.g > -1.0f && d->volume.g < 1.0f))
+            return set_error("medium g must lie in (-1, 1)"), RUMI_ERR_INVALID_ARG;
+    }
     if (d->n_textures < 0 || (d->n_textures > 0 && !d->textures))
         return set_error("textures missing"), RUMI_ERR_INVALID_ARG;
     for (int i = 0; i < d->n_textures; ++i) {

@@ -58,6 +58,92 @@ def test_invalid_arguments_return_status_without_touching_the_gpu():
     assert L.rumi_trace_rays(None, 1, None, 0, None, None, 0, None, None, None) == 1
 
 
+def _tex_table(*types, pixels=None, bpp=3):
+    t = (_capi.rumi_texture * len(types))()
+    for i, ty in enumerate(types):
+        t[i].type = ty
+        t[i].repeat_u = t[i].repeat_v = 4.0
+        t[i].img_width = t[i].img_height = 2
+        t[i].bytes_per_pixel = bpp
+        t[i].pixels = pixels
+    return t
+
+
+def _set_volume(d, sigma_s=(0.4, 0.4, 0.4), sigma_a=(0.05, 0.05, 0.05), g=0.0):
+    d.volume.present = 1
+    d.volume.pmin = _capi.f3(0, 0, 0)
+    d.volume.pmax = _capi.f3(1, 1, 1)
+    d.volume.sigma_s = _capi.f3(*sigma_s)
+    d.volume.sigma_a = _capi.f3(*sigma_a)
+    d.volume.g = g
+
+
+def _ibl(d, keep, with_texture=True):
+    d.lights[0].type, d.lights[0].shape_type, d.lights[0].shape_index = 2, 2, 0
+    if with_texture:
+        keep.append(_tex_table(0))
+        d.n_textures, d.textures = 1, C.cast(keep[-1], C.POINTER(_capi.rumi_texture))
+        keep.append(np.array([0, -1], np.int32))
+        d.sphere_texture = keep[-1].ctypes.data_as(_capi.IP)
+
+
+# (what is wrong, how to make it, text of the error): every rejection of rumi_scene_create's
+# descriptor check, reached before any device call
+DESC_FAULTS = [
+    ("negative count", lambda d, k: setattr(d, "n_lights", -1), "negative count"),
+    ("too many primitives", lambda d, k: setattr(d, "n_triangles", 0x3FFFFFFF), "too many primitives"),
+    ("no triangle vertices", lambda d, k: setattr(d, "tri_vertices", None), "triangle arrays missing"),
+    ("no rect materials", lambda d, k: setattr(d, "rect_material", None), "rect arrays missing"),
+    ("no sphere array", lambda d, k: setattr(d, "spheres", None), "sphere arrays missing"),
+    ("no materials", lambda d, k: setattr(d, "materials", None), "materials missing"),
+    ("no lights", lambda d, k: setattr(d, "lights", None), "lights missing"),
+    ("unknown material", lambda d, k: setattr(d.materials[0], "type", 9), "unknown material type"),
+    ("light on a missing rect", lambda d, k: setattr(d.lights[0], "shape_index", 7), "light rect index"),
+    ("light on a missing sphere", lambda d, k: (setattr(d.lights[0], "shape_type", 2),
+                                                setattr(d.lights[0], "shape_index", 5)), "light sphere index"),
+    ("triangle area light", lambda d, k: setattr(d.lights[0], "shape_type", 0), "rects or spheres"),
+    ("image light on a rect", lambda d, k: (_ibl(d, k), setattr(d.lights[0], "shape_type", 1)), "sphere index"),
+    ("image light without texture", lambda d, k: _ibl(d, k, with_texture=False), "has no texture"),
+    ("image light in a medium", lambda d, k: (_ibl(d, k), _set_volume(d)), "with a medium"),
+    ("unknown light", lambda d, k: setattr(d.lights[0], "type", 7), "unknown light type"),
+    ("no texture table", lambda d, k: setattr(d, "n_textures", 1), "textures missing"),
+    ("unknown texture", lambda d, k: (k.append(_tex_table(5)), setattr(d, "n_textures", 1),
+                                      setattr(d, "textures", C.cast(k[-1], C.POINTER(_capi.rumi_texture)))),
+     "unknown texture type"),
+    ("image texture without pixels", lambda d, k: (k.append(_tex_table(1)), setattr(d, "n_textures", 1),
+                                                   setattr(d, "textures", C.cast(k[-1], C.POINTER(_capi.rumi_texture)))),
+     "texture image missing"),
+    ("two bytes per pixel", lambda d, k: (k.append(np.zeros(16, np.uint8)),
+                                          k.append(_tex_table(1, pixels=k[-1].ctypes.data, bpp=2)),
+                                          setattr(d, "n_textures", 1),
+                                          setattr(d, "textures", C.cast(k[-1], C.POINTER(_capi.rumi_texture)))),
+     "3 or 4 bytes per pixel"),
+    ("texture index past the table", lambda d, k: (k.append(_tex_table(0)), setattr(d, "n_textures", 1),
+                                                   setattr(d, "textures", C.cast(k[-1], C.POINTER(_capi.rumi_texture))),
+                                                   k.append(np.full(d.n_triangles, 1, np.int32)),
+                                                   setattr(d, "tri_texture", k[-1].ctypes.data_as(_capi.IP))),
+     "texture index out of range"),
+    ("negative scattering", lambda d, k: _set_volume(d, sigma_s=(-0.1, 0.4, 0.4)), "positive extinction"),
+    ("a clear channel", lambda d, k: _set_volume(d, sigma_s=(0.4, 0.0, 0.4), sigma_a=(0.05, 0.0, 0.05)),
+     "positive extinction"),
+    ("NaN absorption", lambda d, k: _set_volume(d, sigma_a=(float("nan"), 0.05, 0.05)), "positive extinction"),
+    ("g of one", lambda d, k: _set_volume(d, g=1.0), "medium g"),
+]
+
+
+@pytest.mark.parametrize("what,fault,message", DESC_FAULTS, ids=[f[0] for f in DESC_FAULTS])
+def test_scene_descriptor_faults_are_rejected_before_the_device(what, fault, message):
+    """Host-side fault injection: a descriptor broken in one way returns
+    RUMI_ERR_INVALID_ARG with its reason and no scene, without a GPU."""
+    L = _capi.load()
+    desc, keep = rumi_b200.build_desc(scenes.cornell_pt(8, 8, 1, 2).flatten())
+    fault(desc, keep)
+    h = C.c_void_p()
+    assert L.rumi_scene_create(C.byref(desc), C.byref(h)) == 1
+    assert h.value is None
+    assert message.encode() in L.rumi_last_error_string(), L.rumi_last_error_string()
+
+
 def test_flatten_canonical_order_and_lights():
     sc = Scene()
     r = sc.add(Rect((0, 1, 0), (1, 0, 0), (0, 0, 1)), Emissive(2.0, (1, 1, 1)))
