@@ -144,6 +144,33 @@ def test_scene_descriptor_faults_are_rejected_before_the_device(what, fault, mes
     assert message.encode() in L.rumi_last_error_string(), L.rumi_last_error_string()
 
 
+def test_every_entry_point_rejects_null_handles_without_a_gpu():
+    """NULL scenes, batches, parameter blocks and buffers: RUMI_ERR_INVALID_ARG from every
+    entry point that takes them, a no-op from the destroy calls (as free(NULL))."""
+    L = _capi.load()
+    p = _capi.rumi_render_params()
+    p.integrator, p.max_depth, p.spp = 0, 2, 1
+    buf = np.zeros(16, np.float32)
+    ptr = buf.ctypes.data_as(C.c_void_p)
+    out = C.c_void_p()
+    assert L.rumi_scene_destroy(None) == 0
+    assert L.rumi_batch_destroy(None) == 0
+    assert L.rumi_batch_film_floats(None) == 0
+    assert L.rumi_scene_bvh_info(None, None) == 1
+    assert L.rumi_render_noalloc(None, C.byref(p), ptr, None) == 1
+    assert L.rumi_forward(None, C.byref(p), ptr, 0, None) == 1
+    assert L.rumi_forward(None, None, ptr, 0, None) == 1
+    assert L.rumi_backward(None, C.byref(p), ptr, ptr, ptr, 0, None) == 1
+    assert L.rumi_scene_set_albedo(None, ptr, 0) == 1
+    assert L.rumi_scene_set_volume(None, None) == 1
+    assert L.rumi_batch_create(None, 0, C.byref(out)) == 1 and out.value is None
+    arr = (C.c_void_p * 2)(None, None)
+    assert L.rumi_batch_create(arr, 0, C.byref(out)) == 1
+    assert b"empty batch" in L.rumi_last_error_string()
+    bp = _capi.rumi_batch_params()
+    assert L.rumi_render_batch(None, C.byref(bp), ptr, 0, None) == 1
+
+
 def test_flatten_canonical_order_and_lights():
     sc = Scene()
     r = sc.add(Rect((0, 1, 0), (1, 0, 0), (0, 0, 1)), Emissive(2.0, (1, 1, 1)))
