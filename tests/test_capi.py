@@ -32,6 +32,33 @@ def test_library_exports_every_declared_symbol():
     assert L.rumi_version().decode().startswith("rumi_b200")
 
 
+def _prototypes():
+    """{name: number of parameters} of every function declared in the two headers."""
+    out = {}
+    for h in ("rumi_b200.h", "rumi_b200_test.h"):
+        text = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", h)).read(), flags=re.S)
+        for name, args in re.findall(r"\b(rumi_\w+)\s*\(([^;{]*?)\)\s*;", text, re.S):
+            args = args.strip()
+            out[name] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_ctypes_bindings_take_the_declared_parameters():
+    """Every entry point the ctypes layer binds has as many argtypes as the header's
+    prototype has parameters (a missing or extra argument would shift every later one)."""
+    L = _capi.load()
+    protos = _prototypes()
+    assert "rumi_render" in protos and "rumi_trace_rays" in protos
+    bound = 0
+    for name, n in protos.items():
+        fn = getattr(L, name)
+        if fn.argtypes is None:
+            continue
+        bound += 1
+        assert len(fn.argtypes) == n, (name, len(fn.argtypes), n)
+    assert bound >= 15
+
+
 def test_invalid_arguments_return_status_without_touching_the_gpu():
     L = _capi.load()
     h = C.c_void_p()
