@@ -324,8 +324,8 @@ def reference_arm(args):
 # ----------------------------------------------------------------- our arm
 def peaks():
     """({"hbm_gbs": copy bandwidth}, "measured" | "fallback"): the measured copy bandwidth of
-    MEASURED_PEAKS.json (its `hbm_gbs`, at the top level or one level down), else the
-    fallback 6650 GB/s measured earlier on the same pool of GPUs."""
+    MEASURED_PEAKS.json (its `hbm_gbs`, at the top level or one level down), else a
+    fallback copy bandwidth of 6650 GB/s measured earlier on B200s of the same kind."""
     try:
         d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         cands = [d] + [v for v in d.values() if isinstance(v, dict)]
