@@ -244,15 +244,16 @@ rumi_status rumi_render(rumi_scene *scene, const rumi_render_params *params, flo
 
 /* Renders one path-traced frame like rumi_render, but allocates no device memory: the
  * wave state lives in a fixed 16 MiB device array inside the library (held on every GPU
- * that loads it until exit), so frames render in waves of about 100k paths.  For callers
- * that may not allocate once running -- an application that owns a fixed device-memory
- * budget, a real-time loop that cannot take cudaMalloc's device-wide synchronisation, or
- * work issued while a stream is being captured.  The scene is created beforehand with
- * rumi_scene_create.  film: device pointer, H*W*3 floats.  Path tracer only; spp or
- * wave_paths beyond the array's capacity and RUMI_FLAG_TIMING are rejected with
- * RUMI_ERR_INVALID_ARG.  The first call on a device looks up the array's device address
- * (do it before any stream capture).  All calls share the array: calls that overlap on
- * the GPU race and must be serialised by the caller.  No counterpart in the reference. */
+ * that loads it until exit), so frames render in waves of about 95k paths (176 bytes per
+ * path).  For callers that may not allocate once running -- an application that owns a
+ * fixed device-memory budget, or a real-time loop that cannot take cudaMalloc's
+ * device-wide synchronisation.  The scene is created beforehand with rumi_scene_create.
+ * film: device pointer, H*W*3 floats.  Path tracer only; spp or wave_paths beyond the
+ * array's capacity and RUMI_FLAG_TIMING are rejected with RUMI_ERR_INVALID_ARG.  The
+ * first call on a device looks up the array's device address and caches it (make that
+ * call before any stream capture; the cache does not survive cudaDeviceReset).  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  No counterpart in the reference. */
 rumi_status rumi_render_noalloc(rumi_scene *scene, const rumi_render_params *params, float *film,
                                 rumi_render_stats *stats);
 

@@ -5,8 +5,9 @@ baseline.  Test infrastructure: nothing in the product links or loads it.
 
 What this script does (and nothing more):
 
-1. copies ``src/**/*.{cpp,h}`` of the reference checkout (default
-   ``/root/reference``) into ``oracle/_ref/src`` (git-ignored, never committed);
+1. copies ``src/**/*.{cpp,h}`` of the reference checkout (``--ref``, else the
+   ``RUMI_REFERENCE`` environment variable, else ``DEFAULT_REF``) into
+   ``oracle/_ref/src`` (git-ignored, never committed);
 2. applies portability-only patches so that the MSVC-dialect sources build with g++ on
    LP64 Linux.  None of them changes rendering logic; each is listed in ``PATCHES``;
 3. compiles every reference ``.cpp`` except ``main.cpp`` together with
@@ -31,6 +32,14 @@ OUT = os.path.join(HERE, "_ref")
 SRC_OUT = os.path.join(OUT, "src")
 OBJ_OUT = os.path.join(OUT, "obj")
 LIB = os.path.join(OUT, "librumi_ref.so")
+# Where the read-only reference checkout is mounted in the container that builds the
+# checker; machines without it use the prebuilt oracle/_ref.
+DEFAULT_REF = "/root/reference"
+
+
+def reference_dir():
+    """The reference checkout to build from: $RUMI_REFERENCE, else DEFAULT_REF."""
+    return os.environ.get("RUMI_REFERENCE") or DEFAULT_REF
 
 # (file, old text, new text, reason) -- applied after CRLF -> LF normalisation.
 PATCHES = [
@@ -152,21 +161,60 @@ def compile_all(cpp_files, jobs):
 
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         objs = list(ex.map(run, jobs_list))
-    cmd = ["g++", "-shared", "-o", LIB] + objs + ["-lm"]
+    cmd = ["g++", "-shared", "-Wl,-soname,librumi_ref.so", "-o", LIB] + objs + ["-lm"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n" + r.stderr[-4000:])
     return LIB
 
 
+REPO = os.path.dirname(HERE)
+ADAPTER = os.path.join(REPO, "rumi-renderer_b200", "adapter")
+PRODUCT_LIB_DIR = os.path.join(REPO, "rumi-renderer_b200", "lib")
+GPU_HOST_LIB = os.path.join(OUT, "librumi_ref_gpuhost.so")
+
+
+def build_gpu_host():
+    """oracle/_ref/librumi_ref_gpuhost.so: the reference-side adapter
+    (rumi-renderer_b200/adapter/rumi_gpu_integrators.cpp, compiled against the reference's
+    headers like any reference source) plus the test host oracle/ref_gpu_host.cpp, linked
+    with the reference build and librumi_b200.so.  Skipped while librumi_b200.so is not
+    built."""
+    if not os.path.exists(os.path.join(PRODUCT_LIB_DIR, "librumi_b200.so")):
+        return None
+    flags = ["g++", "-O2", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-variable", "-fno-strict-aliasing",
+             "-include", os.path.join(HERE, "ref_shim.h"), "-I", SRC_OUT, "-I", ADAPTER,
+             "-I", os.path.join(REPO, "include")]
+    objs = []
+    for src in (os.path.join(ADAPTER, "rumi_gpu_integrators.cpp"), os.path.join(HERE, "ref_gpu_host.cpp")):
+        obj = os.path.join(OBJ_OUT, "gpuhost_" + os.path.basename(src).replace(".cpp", ".o"))
+        r = subprocess.run(flags + ["-c", src, "-o", obj], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("compile failed: " + src + "\n" + r.stderr[-4000:])
+        objs.append(obj)
+    tmp = GPU_HOST_LIB + ".tmp"
+    rel_lib = os.path.relpath(PRODUCT_LIB_DIR, OUT)
+    cmd = ["g++", "-shared", "-o", tmp] + objs + [
+        "-L", OUT, "-lrumi_ref", "-L", PRODUCT_LIB_DIR, "-lrumi_b200",
+        "-Wl,-rpath,$ORIGIN", "-Wl,-rpath,$ORIGIN/" + rel_lib]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("link failed:\n" + r.stderr[-4000:])
+    os.replace(tmp, GPU_HOST_LIB)
+    return GPU_HOST_LIB
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("RUMI_REFERENCE", "/root/reference"))
+    ap.add_argument("--ref", default=reference_dir())
     ap.add_argument("-j", type=int, default=os.cpu_count() or 4)
     a = ap.parse_args(argv)
     cpp = copy_and_patch(a.ref)
     lib = compile_all(cpp, a.j)
     print(lib)
+    host = build_gpu_host()
+    if host:
+        print(host)
     return 0
 
 

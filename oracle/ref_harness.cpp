@@ -693,3 +693,7 @@ extern "C" int ref_load_bmp(const char *path, int cap, unsigned char *out, unsig
     free(buf);
     return (int)n;
 }
+
+// The reference Scene a harness handle wraps (the GPU-integrator host library,
+// oracle/ref_gpu_host.cpp, installs its integrators on it).
+extern "C" void *ref_scene_ptr(void *h) { return ((RefScene *)h)->scene; }

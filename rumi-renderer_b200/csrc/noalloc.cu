@@ -4,21 +4,23 @@
 //
 // Who needs it: callers that may not allocate device memory once they are running --
 // an embedding application that owns a fixed device-memory budget and forbids
-// allocation after start-up, a real-time loop that cannot afford the device-wide
-// synchronisation cudaMalloc/cudaFree imply, or code that renders while a CUDA stream is
-// being captured, where allocation calls are not allowed.  Such a caller creates its
-// scene once at set-up time (rumi_scene_create allocates) and then renders frames into a
-// device film it owns.
+// allocation after start-up, or a real-time loop that cannot afford the device-wide
+// synchronisation cudaMalloc/cudaFree imply.  Such a caller creates its scene once at
+// set-up time (rumi_scene_create allocates) and then renders frames into a device film
+// it owns.
 //
 // Limits and rules:
 //  - The array holds RUMI_NOALLOC_SCRATCH_BYTES (16 MiB) on every GPU that loads the
-//    library, for the life of the process.  At 164 bytes per path in flight that is
-//    about 100k paths per wave; a frame is rendered in as many waves as it needs.  A
-//    request whose single pixel (spp paths) does not fit, or whose wave_paths exceeds the
-//    capacity, is rejected with RUMI_ERR_INVALID_ARG before anything is launched.
+//    library, for the life of the process.  At 176 bytes per path in flight (eleven
+//    float4 per path, pt_workspace_bytes) that is about 95k paths per wave; a frame is
+//    rendered in as many waves as it needs.  A request whose single pixel (spp paths)
+//    does not fit, or whose wave_paths exceeds the capacity, is rejected with
+//    RUMI_ERR_INVALID_ARG before anything is launched.
 //  - Host code cannot use the array's name as a device address.  The first call on a
 //    device (with that device current) looks the address up with cudaGetSymbolAddress
-//    and caches it per device; make that first call before any stream capture.
+//    and caches it per device index; make that first call before any stream capture.
+//    The cache does not survive cudaDeviceReset (the module, and with it the array, may
+//    be reloaded at another address): do not call this entry point after a reset.
 //  - Every call shares the one array and its counters are cleared at the start of each
 //    call; calls whose work overlaps on the GPU (different streams, other threads) race
 //    on it and must be serialised by the caller.

@@ -332,6 +332,44 @@ def rmse_fixture(path, size=32, depth=8, gt_spp=65536, spp=16, frames=256, procs
     print(path, "reference RMSE at", spp, "spp:", np.mean(rmse), "+-", np.std(rmse) / np.sqrt(frames))
 
 
+C2_ROWS = (64, 192, 320, 448, 576, 704, 832, 960)
+
+
+def _c2_worker(args):
+    seeds, rows = args
+    sc = scenes.bvh_bound_pt(1024, 1024, 64, 10, levels=9, seed=7)
+    rs = refimpl.RefScene(sc, seed=1)
+    out = []
+    for s in seeds:
+        strip = np.zeros((len(rows), 1024, 3), np.float64)
+        for k, r in enumerate(rows):
+            film, light, nans = rs.render_rows(50000 + 97 * s + k, r, r + 1)
+            strip[k] = (film[r] + light[r]) / rs.spp
+        out.append(strip)
+    spp = rs.spp
+    rs.close()
+    return out, spp
+
+
+def c2_strip_fixture(path, seeds=48, procs=8):
+    """The headline BVH-bound workload itself (Cornell box + 1,048,576-triangle displaced
+    sphere with per-triangle albedo, 1024x1024, 64 spp, depth 10, NEE) rendered by the
+    reference on eight full image rows: per-pixel mean and standard error over `seeds`
+    independent frames of those rows, and the per-frame strip means."""
+    import multiprocessing as mp
+    jobs = [(list(range(k, seeds, procs)), C2_ROWS) for k in range(procs)]
+    frames = []
+    with mp.get_context("spawn").Pool(procs) as pool:
+        for out, spp in pool.map(_c2_worker, jobs):
+            frames += out
+    fr = np.stack(frames)
+    mean = fr.mean(0).astype(F32)
+    stderr = (fr.std(0, ddof=1) / np.sqrt(seeds)).astype(F32)
+    np.savez_compressed(path, mean=mean, stderr=stderr, rows=np.array(C2_ROWS, np.int32), seeds=seeds, spp=spp,
+                        depth=10, frame_means=fr.mean((1, 2, 3)))
+    print(path, "strip mean", mean.reshape(-1, 3).mean(0), "frames", len(frames))
+
+
 def obj_fixture(path):
     """The reference's Model(file, transform) on the OBJ texts of tests/obj_cases.py."""
     import tempfile
@@ -368,6 +406,9 @@ def main():
     if len(sys.argv) > 1 and sys.argv[1] == "dof":
         camera_dof_fixture(os.path.join(HERE, "camera_dof.npz"), np.random.default_rng(88))
         image_fixture(os.path.join(HERE, "image_cornell_dof32.npz"), scene=scenes.cornell_dof_pt(32, 32, 16, 8))
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == "c2":
+        c2_strip_fixture(os.path.join(HERE, "image_bvh_bound_rows.npz"))
         return
     if len(sys.argv) > 1 and sys.argv[1] == "obj":
         obj_fixture(os.path.join(HERE, "obj_loader.npz"))
