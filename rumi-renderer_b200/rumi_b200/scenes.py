@@ -88,6 +88,46 @@ def cornell_pt(width: int = 256, height: int = 256, spp: int = 16, max_depth: in
     return sc
 
 
+def cornell_sphere_light_pt(width: int = 32, height: int = 32, spp: int = 16, max_depth: int = 8) -> Scene:
+    """The Cornell walls lit by a spherical emitter instead of the quad: an Emissive sphere
+    of radius 0.06 under the ceiling with a 4096-point sample set and an AreaLight over it
+    (the arrangement the reference's "RGB Sphere" preset keeps as its alternative light,
+    Sphere(c, r, 4096) + Emissive; its points come from Sphere::ShapeSampling,
+    src/Shape/sphere.cpp:152-170), a white Lambertian sphere and a glossy sphere."""
+    sc = Scene()
+    for tris, alb in cornell_walls():
+        sc.add(Model(tris), Matte(1.0, alb))
+    light = Sphere((0.5, 0.86, 0.5), 0.06, 4096)
+    sc.add(light, Emissive(1.0, (60.0, 48.0, 30.0)))
+    sc.lights.append(AreaLight(light))
+    sc.add(Sphere((0.3, 0.15, 0.6), 0.15), Matte(1.0, WHITE))
+    sc.add(Sphere((0.72, 0.12, 0.38), 0.12), Glossy(0.6, 0.4, 25.0, (0.8, 0.75, 0.7)))
+    sc.camera = cornell_camera()
+    sc.image = Film(width, height, spp)
+    sc.tracer = PathTracer(max_depth)
+    return sc
+
+
+def cornell_two_lights_pt(width: int = 32, height: int = 32, spp: int = 16, max_depth: int = 8) -> Scene:
+    """The Cornell box with two area lights of different size and colour under the ceiling:
+    next-event estimation picks one of them uniformly per sample (Scene::
+    LightsUniformSampling, src/Scene/scene.cpp:91-97, pdf = (1/n) / area)."""
+    sc = Scene()
+    for tris, alb in cornell_walls():
+        sc.add(Model(tris), Matte(1.0, alb))
+    a = Rect((0.15, 0.999, 0.55), (0.2, 0.0, 0.0), (0.0, 0.0, 0.3), 256)
+    b = Rect((0.7, 0.999, 0.2), (0.12, 0.0, 0.0), (0.0, 0.0, 0.12), 64)
+    sc.add(a, Emissive(1.0, (14.0, 10.0, 6.0)))
+    sc.add(b, Emissive(1.0, (6.0, 12.0, 24.0)))
+    sc.lights += [AreaLight(a), AreaLight(b)]
+    sc.add(Sphere((0.3, 0.15, 0.6), 0.15), Matte(1.0, WHITE))
+    sc.add(Sphere((0.7, 0.1, 0.4), 0.1), Specular(1.0, (0.9, 0.9, 0.9)))
+    sc.camera = cornell_camera()
+    sc.image = Film(width, height, spp)
+    sc.tracer = PathTracer(max_depth)
+    return sc
+
+
 # ----------------------------------------------------------------------------- meshes
 def _hash3(ix, iy, iz, seed):
     """32-bit integer hash of lattice coordinates -> float32 in [-1, 1)."""

@@ -332,6 +332,19 @@ def rmse_fixture(path, size=32, depth=8, gt_spp=65536, spp=16, frames=256, procs
     print(path, "reference RMSE at", spp, "spp:", np.mean(rmse), "+-", np.std(rmse) / np.sqrt(frames))
 
 
+def LIGHT_CASES():
+    """A spherical area light and two area lights, path traced and under BDPT (4, 5)."""
+    from rumi_b200.scene import BidirectionalPathTracer
+
+    def bdpt(sc):
+        sc.tracer = BidirectionalPathTracer(4, 5)
+        return sc
+    return [("image_sphere_light_pt32.npz", scenes.cornell_sphere_light_pt(32, 32, 16, 8)),
+            ("image_two_lights_pt32.npz", scenes.cornell_two_lights_pt(32, 32, 16, 8)),
+            ("image_sphere_light_bdpt32.npz", bdpt(scenes.cornell_sphere_light_pt(32, 32, 16, 8))),
+            ("image_two_lights_bdpt32.npz", bdpt(scenes.cornell_two_lights_pt(32, 32, 16, 8)))]
+
+
 C2_ROWS = (64, 192, 320, 448, 576, 704, 832, 960)
 
 
@@ -406,6 +419,10 @@ def main():
     if len(sys.argv) > 1 and sys.argv[1] == "dof":
         camera_dof_fixture(os.path.join(HERE, "camera_dof.npz"), np.random.default_rng(88))
         image_fixture(os.path.join(HERE, "image_cornell_dof32.npz"), scene=scenes.cornell_dof_pt(32, 32, 16, 8))
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == "lights":
+        for name, sc in LIGHT_CASES():
+            image_fixture(os.path.join(HERE, name), scene=sc)
         return
     if len(sys.argv) > 1 and sys.argv[1] == "c2":
         c2_strip_fixture(os.path.join(HERE, "image_bvh_bound_rows.npz"))

@@ -398,6 +398,26 @@ def test_gpu_bdpt_matches_reference_3sigma(golden, fixture, builder):
     frames_vs_reference(gpu_frames(builder(), 32, 13000), golden(fixture))
 
 
+def _bdpt45(sc):
+    sc.tracer = scenes.BidirectionalPathTracer(4, 5)
+    return sc
+
+
+@pytest.mark.parametrize("fixture,builder", [
+    ("image_sphere_light_pt32.npz", lambda: scenes.cornell_sphere_light_pt(32, 32, 16, 8)),
+    ("image_two_lights_pt32.npz", lambda: scenes.cornell_two_lights_pt(32, 32, 16, 8)),
+    ("image_sphere_light_bdpt32.npz", lambda: _bdpt45(scenes.cornell_sphere_light_pt(32, 32, 16, 8))),
+    ("image_two_lights_bdpt32.npz", lambda: _bdpt45(scenes.cornell_two_lights_pt(32, 32, 16, 8))),
+])
+def test_gpu_sphere_and_multiple_area_lights_match_reference_3sigma(golden, fixture, builder):
+    """An emissive sphere as the area light (points from Sphere::ShapeSampling,
+    src/Shape/sphere.cpp:152-170, pdf 1 / (4 pi r^2); BDPT emission about Sphere::Normal)
+    and two area lights picked uniformly (Scene::LightsUniformSampling,
+    src/Scene/scene.cpp:91-97), path tracer and BDPT, against the reference's frames."""
+    from test_oracle_golden import frames_vs_reference
+    frames_vs_reference(gpu_frames(builder(), 32, 14000), golden(fixture))
+
+
 def _floor_scene(light, size=48, spp=64):
     """A single Lambertian plane under one light: every path is direct illumination."""
     from rumi_b200.scene import (Scene, Model, Matte, Rect, Emissive, AreaLight, SpotLight, Pinhole, Film,

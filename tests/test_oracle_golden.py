@@ -257,6 +257,16 @@ def test_oracle_medium_and_glass_match_reference_3sigma(golden):
     frames_vs_reference(oracle_frames(sc, 8, 24, 700), golden("image_caustic_pt32.npz"))
 
 
+@pytest.mark.parametrize("fixture,builder", [
+    ("image_sphere_light_pt32.npz", lambda: scenes.cornell_sphere_light_pt(32, 32, 16, 8)),
+    ("image_two_lights_pt32.npz", lambda: scenes.cornell_two_lights_pt(32, 32, 16, 8)),
+])
+def test_oracle_sphere_and_multiple_area_lights_match_reference_3sigma(golden, fixture, builder):
+    """Next-event estimation toward a spherical area light (uniform points on the sphere,
+    pdf 1 / (4 pi r^2)) and toward one of two area lights picked uniformly."""
+    frames_vs_reference(oracle_frames(builder(), 8, 24, 1300), golden(fixture))
+
+
 def test_oracle_subsurface_matches_reference_3sigma(golden):
     """Subsurface random walk and a glossy sphere, path traced to depth 12."""
     frames_vs_reference(oracle_frames(scenes.subsurface_cornell(32, 32, 16, 12), 12, 24, 900),
