@@ -138,8 +138,11 @@ class ClockSampler:
 
 
 # ------------------------------------------------------ reference (CPU) arm
-def _ref_worker(conn, w):
-    """One host process: builds the reference scene once, then renders the rows it is sent."""
+def _ref_worker(conn, w, pin=None):
+    """One host process: builds the reference scene once, then renders the rows it is sent.
+    pin: a host core the process is bound to (like `taskset -c <core>`)."""
+    if pin is not None:
+        os.sched_setaffinity(0, {pin})
     sys.path.insert(0, os.path.join(ROOT, "rumi-renderer_b200"))
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import refimpl
@@ -169,13 +172,13 @@ def _ref_worker(conn, w):
 
 
 class RefPool:
-    def __init__(self, w, n_procs):
+    def __init__(self, w, n_procs, pin=None):
         ctx = mp.get_context("spawn")
         self.w = w
         self.conns, self.procs = [], []
         for _ in range(n_procs):
             a, b = ctx.Pipe()
-            p = ctx.Process(target=_ref_worker, args=(b, w), daemon=True)
+            p = ctx.Process(target=_ref_worker, args=(b, w, pin), daemon=True)
             p.start()
             self.conns.append(a)
             self.procs.append(p)
@@ -217,6 +220,22 @@ def ref_procs(limit=None):
     return max(1, min(n, limit or n))
 
 
+def single_core_sample(w):
+    """The reference renderer single-threaded on one pinned host core (taskset -c 0, or the
+    lowest core this process may use): one full row of the workload (1024 px at the
+    workload's spp)."""
+    allowed = os.sched_getaffinity(0)
+    core = 0 if 0 in allowed else min(allowed)
+    pool = RefPool(w, 1, pin=core)
+    paths, secs = pool.step(seed=5, rows_per_proc=1, offset=w["height"] // 2)
+    pool.close()
+    return dict(value=paths / secs, unit=UNIT, cores=1, pinned_core=core, kind="reference",
+                sample=f"{paths} paths = 1 row of {w['width']} px x {pool.spp} spp of the same workload, one "
+                       f"process pinned to host core {core}, reference renderer built from its sources "
+                       f"(oracle/_ref), CPU {cpu_model()}",
+                seconds=secs)
+
+
 def cpu_baseline_sample(w, procs, rows_per_proc=1):
     pool = RefPool(w, procs)
     paths, secs = pool.step(seed=3, rows_per_proc=rows_per_proc, offset=0)
@@ -225,7 +244,7 @@ def cpu_baseline_sample(w, procs, rows_per_proc=1):
                 sample=f"{paths} paths = {procs} processes x {rows_per_proc} row(s) of 1024 px x {pool.spp} spp "
                        f"of the same workload, reference renderer built from its sources (oracle/_ref), "
                        f"one thread per process, CPU {cpu_model()}",
-                seconds=secs)
+                seconds=secs, single_core=single_core_sample(w))
 
 
 def make_ray_sets(sc, gs, n, seed=5):

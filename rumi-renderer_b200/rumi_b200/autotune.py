@@ -19,7 +19,16 @@ import time
 DEFAULTS = dict(trace_mode=4, blocks_per_sm=0, refill_min=8, wave_paths=1 << 22)
 SPACE = dict(trace_mode=[4, 1, 2, 3], blocks_per_sm=[0, 4, 5, 6], refill_min=[4, 8, 16],
              wave_paths=[1 << 21, 1 << 22, 1 << 23])
-CACHE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tuning", "autotune_cache.json")
+def default_cache_path() -> str:
+    """$RUMI_TUNING_CACHE, else autotune_cache.json under the user's cache directory
+    ($XDG_CACHE_HOME or ~/.cache)/rumi_b200 -- never inside the package tree."""
+    if os.environ.get("RUMI_TUNING_CACHE"):
+        return os.environ["RUMI_TUNING_CACHE"]
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return os.path.join(base, "rumi_b200", "autotune_cache.json")
+
+
+CACHE = default_cache_path()
 
 
 def gpu_name() -> str:

@@ -2,6 +2,8 @@
 cost surface (the GPU measurement itself is exercised by bench runs)."""
 import os
 
+import pytest
+
 from rumi_b200 import autotune
 
 
@@ -55,3 +57,35 @@ def test_search_starts_from_the_library_defaults():
         assert v in autotune.SPACE[k], k
     hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "rumi_b200.h")).read()
     assert "4: speculative while-while walk" in hdr
+
+
+def test_cache_lives_outside_the_package(monkeypatch, tmp_path):
+    monkeypatch.delenv("RUMI_TUNING_CACHE", raising=False)
+    monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
+    assert autotune.default_cache_path() == str(tmp_path / "rumi_b200" / "autotune_cache.json")
+    monkeypatch.setenv("RUMI_TUNING_CACHE", str(tmp_path / "x.json"))
+    assert autotune.default_cache_path() == str(tmp_path / "x.json")
+    pkg = os.path.dirname(os.path.abspath(autotune.__file__))
+    assert not autotune.CACHE.startswith(os.path.dirname(pkg))
+
+
+@pytest.mark.gpu
+def test_gpu_tune_on_a_small_scene_keeps_the_film(tmp_path):
+    """tune() on the device over a small scene: it measures every candidate, caches the
+    best, and the chosen launch parameters render the film the defaults render (launch
+    parameters change the schedule, never a result)."""
+    import numpy as np
+    import torch
+    import rumi_b200
+    from rumi_b200 import scenes
+    torch.cuda.set_device(0)
+    gs = rumi_b200.GpuScene(scenes.bvh_bound_pt(64, 64, 4, 6, levels=5, seed=7))
+    space = dict(trace_mode=[autotune.DEFAULTS["trace_mode"], 1], blocks_per_sm=[0, 4], refill_min=[8, 16],
+                 wave_paths=[1 << 22, 1 << 14])
+    res = autotune.tune(gs, spp=4, key="small", space=space, repeats=1, cache_path=str(tmp_path / "c.json"))
+    assert len(res["history"]) == 1 + 4 and all(h["ms"] > 0 for h in res["history"])
+    assert autotune.load("small", cache_path=str(tmp_path / "c.json"))["params"] == res["params"]
+    want, _ = gs.render(spp=4, seed=77)
+    got, _ = gs.render(spp=4, seed=77, tuning=res["params"])
+    np.testing.assert_array_equal(got, want)
+    gs.close()
