@@ -197,9 +197,12 @@ typedef struct {
     int32_t flags;         /* RUMI_FLAG_* */
     void *stream;          /* cudaStream_t, NULL = the library's own stream */
     /* launch tuning (0 = library default; chosen by rumi_b200.autotune) */
-    int32_t trace_mode;    /* 1: a warp traces 32 rays to completion; 2: per-lane ray refill;
-                              3: per-lane refill with leaves intersected warp-wide;
-                              4: speculative while-while walk with per-lane refill */
+    int32_t trace_mode;    /* traversal scheme.  Binary tree -- 1: a warp traces 32 rays to
+                              completion; 2: per-lane ray refill; 3: per-lane refill with
+                              leaves intersected warp-wide; 4: speculative while-while walk
+                              with per-lane refill.  5: the same walk over the compressed
+                              eight-wide tree.  0: the library default.  Every scheme gives
+                              the same hits and films */
     int32_t blocks_per_sm; /* persistent traversal blocks (128 threads) per SM, capped by occupancy */
     int32_t refill_min;    /* idle lanes that trigger a refill (modes 2, 3, 4) */
 } rumi_render_params;
@@ -216,7 +219,8 @@ typedef struct {
     double total_ms;             /* device time of the whole render (TIMING) */
     int64_t rays_extend;         /* closest-hit rays traced */
     int64_t rays_shadow;         /* shadow rays traced */
-    int64_t extend_node_fetches; /* 32-byte nodes fetched by closest-hit rays (STATS) */
+    int64_t extend_node_fetches; /* node bytes fetched by closest-hit rays / 32 (STATS): a binary
+                                    node counts 1, a compressed eight-wide node 2.5 */
     int64_t extend_prim_tests;   /* primitives tested by closest-hit rays (STATS) */
 } rumi_render_stats;
 
@@ -321,7 +325,7 @@ rumi_status rumi_scene_set_volume(rumi_scene *scene, const rumi_volume *volume);
  * Ray::_tmin after Travel) and prim (canonical primitive id, -1 = miss).  anyhit = 1:
  * occlusion -> prim 1 when something lies in [1e-4, tmax - 1e-4], else 0.
  * on_device != 0: all pointers are device pointers.  node_visits / prim_tests (may be
- * NULL): summed 32-byte node fetches and primitive tests over the batch. */
+ * NULL): summed node bytes fetched / 32 and primitive tests over the batch. */
 rumi_status rumi_trace_rays(rumi_scene *scene, int64_t n, const float *rays, int32_t anyhit, float *t,
                             int32_t *prim, int32_t on_device, int64_t *node_visits, int64_t *prim_tests,
                             void *stream);

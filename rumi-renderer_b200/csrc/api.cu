@@ -130,6 +130,8 @@ void free_scene(rumi_scene *sc) {
     cudaStream_t s = sc->stream;
     dfree(sc->nodes, s);
     dfree(sc->nodes4, s);
+    dfree(sc->nodes8, s);
+    dfree(sc->prims8, s);
     dfree(sc->leaf_prims, s);
     dfree(sc->tri_shade, s);
     dfree(sc->tri_albedo, s);
@@ -568,6 +570,36 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
         }
         sc->n_nodes4 = n4;
     }
+    {
+        // compressed eight-wide tree: collapse into a worst-case array, then keep an exact copy
+        const int cap8 = bvh8_node_capacity(N);
+        Bvh8Node *tmp8 = nullptr;
+        void *scratch8 = nullptr;
+        e = dalloc((void **)&tmp8, sizeof(Bvh8Node) * (size_t)cap8, s);
+        if (e == cudaSuccess) e = dalloc((void **)&sc->prims8, sizeof(float4) * 3 * (size_t)(N > 0 ? N : 1), s);
+        if (e == cudaSuccess) e = dalloc(&scratch8, bvh8_scratch_bytes(N), s);
+        int n8 = -1;
+        if (e == cudaSuccess)
+            n8 = bvh8_collapse(sc->nodes, sc->n_nodes, sc->leaf_prims, N, tmp8, cap8, sc->prims8, scratch8, s);
+        if (e == cudaSuccess && n8 > 0) e = dalloc((void **)&sc->nodes8, sizeof(Bvh8Node) * (size_t)n8, s);
+        if (e == cudaSuccess && n8 > 0)
+            e = cudaMemcpyAsync(sc->nodes8, tmp8, sizeof(Bvh8Node) * (size_t)n8, cudaMemcpyDeviceToDevice, s);
+        dfree(tmp8, s);
+        dfree(scratch8, s);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return fail(cuda_status(e, "eight-wide BVH"));
+        }
+        // stack entries hold node << 8: fewer than 2^24 nodes
+        if (n8 < 0 || n8 >= (1 << 24)) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            set_error("eight-wide BVH collapse failed");
+            return fail(RUMI_ERR_INTERNAL);
+        }
+        sc->n_nodes8 = n8;
+    }
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0.0f;
@@ -587,6 +619,9 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     ds.nodes = sc->nodes;
     ds.nodes4 = sc->nodes4;
     ds.n_nodes4 = sc->n_nodes4;
+    ds.nodes8 = sc->nodes8;
+    ds.prims8 = sc->prims8;
+    ds.n_nodes8 = sc->n_nodes8;
     ds.leaf_prims = sc->leaf_prims;
     ds.tri_shade = sc->tri_shade;
     ds.tri_albedo = sc->tri_albedo;

@@ -27,4 +27,11 @@ size_t bvh4_scratch_bytes(int n_prims);
 int bvh4_collapse(const BvhNode *nodes2, int n_nodes2, Bvh4Node *nodes4, int cap4, void *scratch,
                   cudaStream_t stream);
 
+// Compressed eight-wide tree collapsed from the binary one (bvh8.cu); prims8 receives the
+// leaf primitives in its order.  Returns the node count, 0 without primitives, -1 on error.
+int bvh8_node_capacity(int n_prims);
+size_t bvh8_scratch_bytes(int n_prims);
+int bvh8_collapse(const BvhNode *nodes2, int n_nodes2, const float4 *prims2, int n_prims, Bvh8Node *nodes8, int cap8,
+                  float4 *prims8, void *scratch, cudaStream_t stream);
+
 }  // namespace rumi

@@ -872,7 +872,10 @@ static inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // 1..4 select modes 0..3, 0 selects the default, the speculative while-while walk (mode 3),
 // which measured fastest on the BVH-bound workload (238 vs 302 ms per 1024x1024x64 frame
 // for mode 0).
-static inline int trace_scheme(int trace_mode) { return trace_mode >= 1 && trace_mode <= 4 ? trace_mode - 1 : 3; }
+static constexpr int DEFAULT_WALK_MODE = RUMI_WALK8 ? 4 : 3;
+static inline int trace_scheme(int trace_mode) {
+    return trace_mode >= 1 && trace_mode <= 5 ? trace_mode - 1 : DEFAULT_WALK_MODE;
+}
 
 template <bool STATS>
 static void launch_extend(int mode, int grid, cudaStream_t st, const PtLaunch &L, int b) {
@@ -880,7 +883,8 @@ static void launch_extend(int mode, int grid, cudaStream_t st, const PtLaunch &L
         case 0: pt_extend<0, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
         case 1: pt_extend<1, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
         case 2: pt_extend<2, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
-        default: pt_extend<3, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
+        case 3: pt_extend<3, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
+        default: pt_extend<4, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
     }
 }
 
@@ -890,7 +894,8 @@ static void launch_shadow(int mode, int grid, cudaStream_t st, const PtLaunch &L
         case 0: pt_shadow<0, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
         case 1: pt_shadow<1, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
         case 2: pt_shadow<2, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
-        default: pt_shadow<3, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
+        case 3: pt_shadow<3, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
+        default: pt_shadow<4, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
     }
 }
 
@@ -913,9 +918,14 @@ static void trace_grids(int mode, int num_sms, int blocks_per_sm, bool adj, int 
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<2, true> : pt_shadow<2, false>,
                                                           TRACE_THREADS, 0);
             break;
-        default:
+        case 3:
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<3, false>, TRACE_THREADS, 0);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<3, true> : pt_shadow<3, false>,
+                                                          TRACE_THREADS, 0);
+            break;
+        default:
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<4, false>, TRACE_THREADS, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<4, true> : pt_shadow<4, false>,
                                                           TRACE_THREADS, 0);
             break;
     }
@@ -1126,7 +1136,7 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
         stats->nan_samples = (int64_t)h_stats[S_NAN];
         stats->rays_extend = (int64_t)h_stats[S_RAYS_EXT];
         stats->rays_shadow = (int64_t)h_stats[S_RAYS_SH];
-        stats->extend_node_fetches = (int64_t)h_stats[S_NODES];
+        stats->extend_node_fetches = (int64_t)(h_stats[S_NODES] / 2);  // 16-byte units -> 32-byte nodes
         stats->extend_prim_tests = (int64_t)h_stats[S_PRIMS];
         stats->extend_launches = (int64_t)waves * bounces;
         stats->shade_launches = stats->extend_launches;
@@ -1405,8 +1415,8 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) trace_ba
         T.t[k] = h.t;
         T.prim[k] = ANYHIT ? (h.t > 0.0f ? 1 : 0) : (h.t > 0.0f ? h.id : -1);
     };
-    traverse_queue<3, ANYHIT, STACK_SMEM, STATS>(T.s, n, fetch_counter, 8, stack + threadIdx.x, TRACE_THREADS, fetch,
-                                                 finish, st);
+    traverse_queue<DEFAULT_WALK_MODE, ANYHIT, STACK_SMEM, STATS>(T.s, n, fetch_counter, 8, stack + threadIdx.x,
+                                                                 TRACE_THREADS, fetch, finish, st);
     if (STATS) {
         atomicAdd(&T.counters[1], (unsigned long long)st.nodes);
         atomicAdd(&T.counters[2], (unsigned long long)st.prims);
@@ -1460,7 +1470,7 @@ rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int any
     if (e == cudaSuccess) e = cudaMemcpyAsync(h, T.counters, sizeof(h), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_status(e, "trace_rays");
-    if (node_visits) *node_visits = (int64_t)h[1];
+    if (node_visits) *node_visits = (int64_t)(h[1] / 2);  // 16-byte units -> 32-byte nodes
     if (prim_tests) *prim_tests = (int64_t)h[2];
     return RUMI_OK;
 }

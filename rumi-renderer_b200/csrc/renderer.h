@@ -13,6 +13,9 @@ struct rumi_scene {
     BvhNode *nodes = nullptr;
     Bvh4Node *nodes4 = nullptr;
     int n_nodes4 = 0;
+    Bvh8Node *nodes8 = nullptr;
+    float4 *prims8 = nullptr;
+    int n_nodes8 = 0;
     float4 *leaf_prims = nullptr;
     float4 *tri_shade = nullptr;
     float4 *tri_albedo = nullptr;

@@ -3,6 +3,10 @@
 // HBM layout (all arrays cudaMalloc'd by rumi_scene_create, 256-byte aligned):
 //   nodes      : BvhNode[n_nodes]        32 B each; siblings adjacent, pairs 64-B aligned
 //   nodes4     : Bvh4Node[n_nodes4]      128 B each, collapsed from `nodes`; siblings adjacent
+//   nodes8     : Bvh8Node[n_nodes8]      80 B each, compressed eight-wide tree collapsed from
+//                                        `nodes`; a node's interior children are adjacent
+//   prims8     : float4[3 * n_prims]     the leaf primitives re-laid out for nodes8: the leaf
+//                                        children of one node are adjacent, in slot order
 //   leaf_prims : float4[3 * n_prims]     48 B per primitive, in BVH leaf order
 //   tri_shade  : float4[3 * n_tris]      shading normals n0,n1,n2 (canonical order);
 //                                        .w of the first holds the material index
@@ -61,6 +65,36 @@ struct __align__(128) Bvh4Node {
 #ifndef RUMI_BVH_WIDE
 #define RUMI_BVH_WIDE 0  // 1: walk the four-wide tree (nodes4), 0: the binary tree
 #endif
+
+// 80-byte compressed eight-wide node (five float4 loads), collapsed from the binary tree by
+// bvh8.cu.  Child boxes are stored as 8-bit multiples of a per-axis power-of-two quantum
+// 2^e relative to the origin (ox, oy, oz), rounded strictly outward by at least one
+// quantum, so every child box contains its exact box: culling stays conservative and hit
+// results equal the binary tree's.  Slot k of a node:
+//   - interior child when bit k of imask is set: node child_base + popc(imask & ((1<<k)-1));
+//   - leaf child when its count byte c_k (cnt_lo / cnt_hi) is > 0: primitives
+//     prims8[prim_base + c_0 + ... + c_{k-1} .. + c_k);
+//   - empty otherwise.
+// Children are assigned to slots by octant: slot k holds the child that comes first along
+// the diagonal direction (-1)^(k&1), (-1)^(k>>1&1), (-1)^(k>>2&1), so a ray whose direction
+// signs form octant code q (bit a set when component a is negative) visits slots in the
+// order k ^ q for k = 0, 1, ... -- near children first without sorting.
+struct __align__(16) Bvh8Node {
+    // first float4: what taking a child from a node needs
+    unsigned int meta;        // bytes 0-2: e_x, e_y, e_z biased by 127 (the float exponent
+                              // field of the quantum); byte 3: imask
+    int child_base;           // first interior child
+    int prim_base;            // first primitive of the leaf children
+    float ox;                 // quantisation origin (x)
+    // second float4
+    float oy, oz;             // quantisation origin (y, z)
+    unsigned int cnt_lo;      // leaf primitive counts of slots 0-3, one byte each
+    unsigned int cnt_hi;      // slots 4-7
+    // three float4 of child bounds
+    unsigned int qlo_x[2], qlo_y[2], qlo_z[2];  // byte k: child k's low bound in quanta
+    unsigned int qhi_x[2], qhi_y[2], qhi_z[2];  // byte k: high bound
+};
+static_assert(sizeof(Bvh8Node) == 80, "Bvh8Node is five float4");
 
 struct DevMaterial {
     int type;
@@ -131,6 +165,9 @@ struct DevScene {
     int n_nodes;
     const Bvh4Node *nodes4;     // the four-wide tree the traversal kernels walk
     int n_nodes4;
+    const Bvh8Node *nodes8;     // the compressed eight-wide tree (0 nodes: empty scene)
+    const float4 *prims8;       // leaf primitives in nodes8 order
+    int n_nodes8;
     DevVolume volume;
     DevCamera camera;
     int width, height;

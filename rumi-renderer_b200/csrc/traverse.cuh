@@ -19,6 +19,12 @@
 
 #define RUMI_MAX_BVH_DEPTH 64
 
+// 1: the default walk (trace_mode 0, ray queries, batches, per-thread rays) is the
+// compressed eight-wide tree; 0: the binary (or, with RUMI_BVH_WIDE, four-wide) tree.
+#ifndef RUMI_WALK8
+#define RUMI_WALK8 0
+#endif
+
 struct HitRec {
     float t;      // 0 = miss
     int id;       // canonical primitive id, -1 = miss
@@ -154,19 +160,20 @@ RUMI_D float cull_limit(float best_t, float tmax) {
 }
 
 struct TraceStats {
-    int nodes;   // 32-byte nodes fetched
+    int nodes;   // node bytes fetched, in 16-byte units (a binary node is 2, an eight-wide node 5)
     int prims;   // primitives tested
 };
 
-// Intersects every primitive of one leaf.  Returns true when ANYHIT and a hit was found.
+// Intersects every primitive of one leaf (records prims[3*first ...]: the binary tree's
+// leaf_prims or the eight-wide tree's prims8).  Returns true when ANYHIT and a hit was found.
 template <bool ANYHIT, bool STATS>
-RUMI_D bool leaf_isect(const DevScene &s, int first, int count, float3 o, float3 d, float tmax, bool in_object,
-                       HitRec &h, TraceStats &st) {
+RUMI_D bool leaf_isect_in(const DevScene &s, const float4 *__restrict__ prims, int first, int count, float3 o,
+                          float3 d, float tmax, bool in_object, HitRec &h, TraceStats &st) {
     if (first < 0 || count > s.n_prims - first) return false;  // malformed leaf guard
     for (int i = first; i < first + count; ++i) {
-        const float4 A = __ldg(&s.leaf_prims[3 * i + 0]);
-        const float4 B = __ldg(&s.leaf_prims[3 * i + 1]);
-        const float4 C = __ldg(&s.leaf_prims[3 * i + 2]);
+        const float4 A = __ldg(&prims[3 * i + 0]);
+        const float4 B = __ldg(&prims[3 * i + 1]);
+        const float4 C = __ldg(&prims[3 * i + 2]);
         if (STATS) st.prims++;
         const int tag = __float_as_int(B.w);
         const int kind = tag & 0xff;
@@ -191,6 +198,12 @@ RUMI_D bool leaf_isect(const DevScene &s, int first, int count, float3 o, float3
     return ANYHIT && h.t > 0.0f;
 }
 
+template <bool ANYHIT, bool STATS>
+RUMI_D bool leaf_isect(const DevScene &s, int first, int count, float3 o, float3 d, float tmax, bool in_object,
+                       HitRec &h, TraceStats &st) {
+    return leaf_isect_in<ANYHIT, STATS>(s, s.leaf_prims, first, count, o, d, tmax, in_object, h, st);
+}
+
 // Closest-hit (ANYHIT=false) or occlusion (ANYHIT=true) query over the binary tree.
 // smem_stack: this thread's first shared-memory stack slot; consecutive slots are
 // `stride` ints apart.
@@ -212,7 +225,7 @@ RUMI_D HitRec trace_ray_bin(const DevScene &s, float3 o, float3 d, float tmax, b
     {
         const float4 *rp = reinterpret_cast<const float4 *>(s.nodes);
         const float4 a = __ldg(rp), b = __ldg(rp + 1);
-        if (STATS) st.nodes++;
+        if (STATS) st.nodes += 2;
         float tn;
         if (!slab(a, b, inv, oinv, tmax, tn)) return h;
         const int first = __float_as_int(b.z), count = __float_as_int(b.w);
@@ -228,7 +241,7 @@ RUMI_D HitRec trace_ray_bin(const DevScene &s, float3 o, float3 d, float tmax, b
         for (int guard = 0; guard < s.n_nodes; ++guard) {
             const float4 *np = reinterpret_cast<const float4 *>(s.nodes + cur);
             const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
-            if (STATS) st.nodes += 2;
+            if (STATS) st.nodes += 4;
             const float lim = cull_limit(h.t, tmax);
             float tn0, tn1;
             bool h0 = slab(a0, b0, inv, oinv, lim, tn0);
@@ -328,7 +341,7 @@ RUMI_D HitRec trace_ray_wide(const DevScene &s, float3 o, float3 d, float tmax, 
         const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
         const int4 ch = __ldg(reinterpret_cast<const int4 *>(np + 6));
         const int4 cn = __ldg(reinterpret_cast<const int4 *>(np + 7));
-        if (STATS) st.nodes += 4;  // counted in 32-byte units
+        if (STATS) st.nodes += 8;  // counted in 16-byte units
         const float lim = cull_limit(h.t, tmax);
         float k0, k1, k2, k3;
         if (!(cn.x >= 0 && slab_s(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, inv, oinv, lim, k0))) k0 = FLT_MAX;
@@ -408,9 +421,15 @@ RUMI_D HitRec trace_ray_wide(const DevScene &s, float3 o, float3 d, float tmax, 
 }
 
 template <bool ANYHIT, int STACK_SMEM, bool STATS>
+RUMI_D HitRec trace_ray_w8(const DevScene &s, float3 o, float3 d, float tmax, bool in_object, int *smem_stack,
+                           int stride, TraceStats &st);
+
+template <bool ANYHIT, int STACK_SMEM, bool STATS>
 RUMI_D HitRec trace_ray(const DevScene &s, float3 o, float3 d, float tmax, bool in_object, int *smem_stack,
                         int stride, TraceStats &st) {
-#if RUMI_BVH_WIDE
+#if RUMI_WALK8
+    return trace_ray_w8<ANYHIT, STACK_SMEM, STATS>(s, o, d, tmax, in_object, smem_stack, stride, st);
+#elif RUMI_BVH_WIDE
     return trace_ray_wide<ANYHIT, STACK_SMEM, STATS>(s, o, d, tmax, in_object, smem_stack, stride, st);
 #else
     return trace_ray_bin<ANYHIT, STACK_SMEM, STATS>(s, o, d, tmax, in_object, smem_stack, stride, st);
@@ -448,7 +467,7 @@ RUMI_D void trav_begin(const DevScene &s, TravState &T, float3 o, float3 d, floa
     T.oinv = mk3(o.x * T.inv.x, o.y * T.inv.y, o.z * T.inv.z);
     const float4 *rp = reinterpret_cast<const float4 *>(s.nodes);
     const float4 a = __ldg(rp), b = __ldg(rp + 1);
-    if (STATS) st.nodes++;
+    if (STATS) st.nodes += 2;
     float tn;
     if (!slab(a, b, T.inv, T.oinv, tmax, tn)) return;
     const int first = __float_as_int(b.z), count = __float_as_int(b.w);
@@ -476,7 +495,7 @@ RUMI_D void trav_step(const DevScene &s, TravState &T, int *smem_stack, int stri
     }
     const float4 *np = reinterpret_cast<const float4 *>(s.nodes + T.cur);
     const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
-    if (STATS) st.nodes += 2;
+    if (STATS) st.nodes += 4;
     const float lim = cull_limit(T.h.t, T.tmax);
     float tn0, tn1;
     const bool h0 = slab(a0, b0, T.inv, T.oinv, lim, tn0);
@@ -550,7 +569,7 @@ RUMI_D void trav_step_postpone(const DevScene &s, TravState &T, PendingLeaves &p
     }
     const float4 *np = reinterpret_cast<const float4 *>(s.nodes + T.cur);
     const float4 a0 = __ldg(np + 0), b0 = __ldg(np + 1), a1 = __ldg(np + 2), b1 = __ldg(np + 3);
-    if (STATS) st.nodes += 2;
+    if (STATS) st.nodes += 4;
     const float lim = cull_limit(T.h.t, T.tmax);
     float tn0, tn1;
     const bool h0 = slab(a0, b0, T.inv, T.oinv, lim, tn0);
@@ -684,7 +703,7 @@ RUMI_D void traverse_queue_ww(SceneOf scene_of, int n, int *counter, int refill_
                         inv = safe_inv(d);
                         oinv = mk3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
                         const float4 a = __ldg(nodes), b = __ldg(nodes + 1);
-                        if (STATS) st.nodes++;
+                        if (STATS) st.nodes += 2;
                         float tn;
                         if (slab(a, b, inv, oinv, tmax, tn)) {
                             const int first = __float_as_int(b.z), count = __float_as_int(b.w);
@@ -709,7 +728,7 @@ RUMI_D void traverse_queue_ww(SceneOf scene_of, int n, int *counter, int refill_
             }
             const float4 a0 = __ldg(nodes + 2 * cur), b0 = __ldg(nodes + 2 * cur + 1);
             const float4 a1 = __ldg(nodes + 2 * cur + 2), b1 = __ldg(nodes + 2 * cur + 3);
-            if (STATS) st.nodes += 2;
+            if (STATS) st.nodes += 4;
             const float lim = cull_limit(h.t, tmax);
             float tn0, tn1;
             const bool h0 = slab(a0, b0, inv, oinv, lim, tn0);
@@ -842,7 +861,7 @@ RUMI_D void traverse_queue_ww4(SceneOf scene_of, int n, int *counter, int refill
             const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
             const int4 ch = __ldg(reinterpret_cast<const int4 *>(np + 6));
             const int4 cn = __ldg(reinterpret_cast<const int4 *>(np + 7));
-            if (STATS) st.nodes += 4;  // counted in 32-byte units
+            if (STATS) st.nodes += 8;  // counted in 16-byte units
             const float lim = cull_limit(h.t, tmax);
             float k0, k1, k2, k3;
             if (!(cn.x >= 0 && slab_s(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, inv, oinv, lim, k0))) k0 = FLT_MAX;
@@ -898,11 +917,322 @@ RUMI_D void traverse_queue_ww4(SceneOf scene_of, int n, int *counter, int refill
     }
 }
 
-// The default walk: binary or four-wide tree by RUMI_BVH_WIDE.
+// ------------------------------------------------ compressed eight-wide traversal
+// Walk over nodes8 (Bvh8Node, scene.cuh).  A node visit loads its 80 bytes and tests the
+// eight quantised child boxes at once; the hit children form a group (node, hit slots in
+// visiting order) that is taken apart one child at a time: an interior child is visited
+// next (the rest of the group is pushed as one 32-bit stack entry, node << 8 | slots), a
+// leaf child becomes the lane's postponed leaf.  Children are visited in the octant order
+// the build arranged (slot k ^ oct for the k-th visit), so nothing is sorted.
+
+// Depth of the eight-wide tree <= the binary tree's (63): one stack entry per level.
+#define RUMI_STACK8 64
+
+// Ray constants of the node test.
+struct Ray8 {
+    float3 inv, oinv;  // safe reciprocal direction and origin * inv
+    unsigned int oct;  // bit a set when direction component a is negative
+};
+
+RUMI_D Ray8 make_ray8(float3 o, float3 d) {
+    Ray8 r;
+    r.inv = safe_inv(d);
+    r.oinv = mk3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
+    r.oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    return r;
+}
+
+// Byte b of w as a float, exactly: the bits of 2^23 + byte, minus 2^23.
+RUMI_D float q8(unsigned int w, int b) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (unsigned)b)) - 8388608.0f;
+}
+
+// Slot bits (bit k = slot k) -> visiting order (bit k ^ oct).
+RUMI_D unsigned int oct_order(unsigned int m, unsigned int oct) {
+    if (oct & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+    if (oct & 2u) m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+    if (oct & 4u) m = ((m & 0x0Fu) << 4) | ((m >> 4) & 0x0Fu);
+    return m;
+}
+
+// Bit k set where byte k of (lo, hi) is non-zero.
+RUMI_D unsigned int nonzero_bytes(unsigned int lo, unsigned int hi) {
+    const unsigned int a = __vcmpne4(lo, 0u) & 0x08040201u, b = __vcmpne4(hi, 0u) & 0x80402010u;
+    return (a | b) * 0x01010101u >> 24;
+}
+
+// What taking a child from a node needs: the node's first two float4.
+struct Group8 {
+    unsigned int imask;
+    int child_base, prim_base;
+    unsigned int cnt_lo, cnt_hi;
+};
+
+RUMI_D Group8 group_of(float4 a, float4 b) {
+    Group8 g;
+    g.imask = __float_as_uint(a.x) >> 24;
+    g.child_base = __float_as_int(a.y);
+    g.prim_base = __float_as_int(a.z);
+    g.cnt_lo = __float_as_uint(b.z);
+    g.cnt_hi = __float_as_uint(b.w);
+    return g;
+}
+
+// Tests node n's children; returns the hit slots in visiting order and the node's group.
+template <bool STATS>
+RUMI_D unsigned int visit8(const float4 *__restrict__ nodes, int n, const Ray8 &r, float lim, Group8 &g,
+                           TraceStats &st) {
+    const float4 *np = nodes + 5 * n;
+    const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), d = __ldg(np + 3), e = __ldg(np + 4);
+    if (STATS) st.nodes += 5;
+    g = group_of(a, b);
+    const unsigned int meta = __float_as_uint(a.x);
+    // the quantum 2^e per axis straight from its biased exponent; the grid's map to ray t
+    const float ax = __uint_as_float((meta & 0xFFu) << 23) * r.inv.x;
+    const float ay = __uint_as_float(((meta >> 8) & 0xFFu) << 23) * r.inv.y;
+    const float az = __uint_as_float(((meta >> 16) & 0xFFu) << 23) * r.inv.z;
+    const float bx = fmaf(a.w, r.inv.x, -r.oinv.x);
+    const float by = fmaf(b.x, r.inv.y, -r.oinv.y);
+    const float bz = fmaf(b.y, r.inv.z, -r.oinv.z);
+    // near / far planes by the direction's signs
+    const bool sx = r.oct & 1u, sy = r.oct & 2u, sz = r.oct & 4u;
+    const unsigned int lx0 = __float_as_uint(c.x), lx1 = __float_as_uint(c.y);
+    const unsigned int ly0 = __float_as_uint(c.z), ly1 = __float_as_uint(c.w);
+    const unsigned int lz0 = __float_as_uint(d.x), lz1 = __float_as_uint(d.y);
+    const unsigned int hx0 = __float_as_uint(d.z), hx1 = __float_as_uint(d.w);
+    const unsigned int hy0 = __float_as_uint(e.x), hy1 = __float_as_uint(e.y);
+    const unsigned int hz0 = __float_as_uint(e.z), hz1 = __float_as_uint(e.w);
+    const unsigned int nx[2] = {sx ? hx0 : lx0, sx ? hx1 : lx1}, fx[2] = {sx ? lx0 : hx0, sx ? lx1 : hx1};
+    const unsigned int ny[2] = {sy ? hy0 : ly0, sy ? hy1 : ly1}, fy[2] = {sy ? ly0 : hy0, sy ? ly1 : hy1};
+    const unsigned int nz[2] = {sz ? hz0 : lz0, sz ? hz1 : lz1}, fz[2] = {sz ? lz0 : hz0, sz ? lz1 : hz1};
+    unsigned int hits = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int w = k >> 2, bb = k & 3;
+        const float tnx = fmaf(q8(nx[w], bb), ax, bx), tfx = fmaf(q8(fx[w], bb), ax, bx);
+        const float tny = fmaf(q8(ny[w], bb), ay, by), tfy = fmaf(q8(fy[w], bb), ay, by);
+        const float tnz = fmaf(q8(nz[w], bb), az, bz), tfz = fmaf(q8(fz[w], bb), az, bz);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, lim));
+        hits |= (tn <= tf ? 1u : 0u) << k;
+    }
+    hits &= g.imask | nonzero_bytes(g.cnt_lo, g.cnt_hi);  // empty slots never hit
+    return oct_order(hits, r.oct);
+}
+
+// Primitive range of leaf slot k of a group: prim_base + the counts of slots 0..k-1.
+RUMI_D void leaf_of(const Group8 &g, int k, int &first, int &count) {
+    const unsigned long long cnt = ((unsigned long long)g.cnt_hi << 32) | g.cnt_lo;
+    const unsigned long long below = cnt & ((1ull << (8 * k)) - 1ull);
+    // bytes -> four 16-bit pair sums (each <= 510) -> their total in the top 16 bits
+    const unsigned long long s16 = (below & 0x00FF00FF00FF00FFull) + ((below >> 8) & 0x00FF00FF00FF00FFull);
+    first = g.prim_base + (int)((s16 * 0x0001000100010001ull) >> 48);
+    count = (int)((cnt >> (8 * k)) & 0xFFull);
+}
+
+// Speculative while-while walk with per-lane refill (as traverse_queue_ww) over nodes8.
+template <bool ANYHIT, int STACK_SMEM, bool STATS, typename SceneOf, typename Fetch, typename Finish>
+RUMI_D void traverse_queue_ww8(SceneOf scene_of, int n, int *counter, int refill_min, int *smem_stack, int stride,
+                               Fetch fetch, Finish finish, TraceStats &st) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned int spill[RUMI_STACK8 - STACK_SMEM > 0 ? RUMI_STACK8 - STACK_SMEM : 1];
+    const DevScene *sp_scene = scene_of(-1);
+    const float4 *nodes = reinterpret_cast<const float4 *>(sp_scene->nodes8);
+    const float4 *prims = sp_scene->prims8;
+    float3 o = mk3(0, 0, 0), d = mk3(0, 0, 0);
+    Ray8 r;
+    r.inv = r.oinv = mk3(0, 0, 0);
+    r.oct = 0;
+    float tmax = 0.0f;
+    bool in_obj = false;
+    HitRec h;
+    h.t = 0.0f;
+    h.id = -1;
+    h.u = h.v = 0.0f;
+    h.back = 0;
+    Group8 g;
+    g.imask = 0;
+    g.child_base = g.prim_base = 0;
+    g.cnt_lo = g.cnt_hi = 0;
+    int ray = -1, gnode = 0, sp = 0, lf_first = 0, lf_count = 0, steps = 0;
+    unsigned int ghits = 0;
+    bool exhausted = false;
+    auto push = [&](unsigned int v) {
+        if (sp < STACK_SMEM)
+            smem_stack[sp * stride] = (int)v;
+        else if (sp < RUMI_STACK8)
+            spill[sp - STACK_SMEM] = v;
+        if (sp < RUMI_STACK8) ++sp;  // one entry per level of a depth-limited tree: always holds
+    };
+    // the next group from the stack (its node's first two float4 give the group's decode)
+    auto pop = [&]() {
+        --sp;
+        const unsigned int v = sp < STACK_SMEM ? (unsigned int)smem_stack[sp * stride] : spill[sp - STACK_SMEM];
+        gnode = (int)(v >> 8);
+        ghits = v & 0xFFu;
+        if ((unsigned)gnode >= (unsigned)sp_scene->n_nodes8) {  // malformed stack entry guard
+            ghits = 0;
+            sp = 0;
+            return;
+        }
+        const float4 *np = nodes + 5 * gnode;
+        g = group_of(__ldg(np), __ldg(np + 1));
+        if (STATS) st.nodes += 2;
+    };
+    for (;;) {
+        // finished rays -> results; idle lanes -> new rays
+        if (ray >= 0 && ghits == 0 && sp == 0 && lf_count == 0) {
+            finish(ray, h);
+            ray = -1;
+        }
+        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
+        if (!exhausted && idle && (__popc(idle) >= refill_min || idle == 0xffffffffu)) {
+            int base = 0;
+            const int leader = __ffs(idle) - 1;
+            if (lane == leader) base = atomicAdd(counter, __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= n) exhausted = true;
+            if (ray < 0) {
+                const int rr = base + __popc(idle & lt);
+                if (rr < n) {
+                    ray = rr;
+                    fetch(rr, o, d, tmax, in_obj);
+                    sp_scene = scene_of(rr);
+                    nodes = reinterpret_cast<const float4 *>(sp_scene->nodes8);
+                    prims = sp_scene->prims8;
+                    h.t = 0.0f;
+                    h.id = -1;
+                    h.u = h.v = 0.0f;
+                    h.back = 0;
+                    sp = 0;
+                    steps = 0;
+                    lf_count = 0;
+                    ghits = 0;
+                    if (!(d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) && sp_scene->n_nodes8 > 0) {  // bvh.cpp:161-162
+                        r = make_ray8(o, d);
+                        gnode = 0;
+                        ghits = visit8<STATS>(nodes, 0, r, tmax, g, st);
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, ray >= 0) == 0) break;
+        // interior steps, speculatively past the first postponed leaf; a lane stops when it
+        // meets a second leaf (kept in its group) or runs out of work
+        bool blocked = false;
+        while (ray >= 0 && !blocked && (ghits != 0 || sp != 0)) {
+            if (ghits == 0) pop();
+            if (ghits != 0) {
+                const int kslot = (__ffs(ghits) - 1) ^ (int)r.oct;
+                if ((g.imask >> kslot) & 1u) {
+                    ghits &= ghits - 1u;
+                    const int child = g.child_base + __popc(g.imask & ((1u << kslot) - 1u));
+                    if ((unsigned)child >= (unsigned)sp_scene->n_nodes8 || ++steps > sp_scene->n_nodes8) {
+                        ghits = 0;  // malformed tree guard
+                        sp = 0;
+                    } else {
+                        if (ghits != 0) push(((unsigned int)gnode << 8) | ghits);
+                        gnode = child;
+                        ghits = visit8<STATS>(nodes, child, r, cull_limit(h.t, tmax), g, st);
+                    }
+                } else if (lf_count == 0) {
+                    ghits &= ghits - 1u;
+                    leaf_of(g, kslot, lf_first, lf_count);
+                } else {
+                    blocked = true;
+                }
+            }
+            if (!__any_sync(__activemask(), lf_count == 0 && (ghits != 0 || sp != 0))) break;
+        }
+        // the postponed leaf, then the leaf the walk stopped at
+        if (ray >= 0 && lf_count > 0) {
+            for (int rep = 0; rep < 2 && lf_count > 0; ++rep) {
+                const bool any =
+                    leaf_isect_in<ANYHIT, STATS>(*sp_scene, prims, lf_first, lf_count, o, d, tmax, in_obj, h, st);
+                lf_count = 0;
+                if (any) {
+                    ghits = 0;
+                    sp = 0;
+                    break;
+                }
+                if (ghits != 0) {
+                    const int kslot = (__ffs(ghits) - 1) ^ (int)r.oct;
+                    if (!((g.imask >> kslot) & 1u)) {
+                        ghits &= ghits - 1u;
+                        leaf_of(g, kslot, lf_first, lf_count);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// One ray to completion over nodes8 (the per-thread form, for integrators that trace one
+// ray at a time).  smem_stack: this thread's first shared-memory stack slot.
+template <bool ANYHIT, int STACK_SMEM, bool STATS>
+RUMI_D HitRec trace_ray_w8(const DevScene &s, float3 o, float3 d, float tmax, bool in_object, int *smem_stack,
+                           int stride, TraceStats &st) {
+    HitRec h;
+    h.t = 0.0f;
+    h.id = -1;
+    h.u = h.v = 0.0f;
+    h.back = 0;
+    if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) return h;  // bvh.cpp:161-162
+    if (s.n_nodes8 <= 0) return h;
+    const float4 *nodes = reinterpret_cast<const float4 *>(s.nodes8);
+    unsigned int spill[RUMI_STACK8 - STACK_SMEM > 0 ? RUMI_STACK8 - STACK_SMEM : 1];
+    const Ray8 r = make_ray8(o, d);
+    Group8 g;
+    int gnode = 0, sp = 0;
+    unsigned int ghits = visit8<STATS>(nodes, 0, r, tmax, g, st);
+    // every node is visited at most once per ray: the bound only stops a malformed tree
+    for (int guard = 0; guard <= s.n_nodes8;) {
+        if (ghits == 0) {
+            if (sp == 0) break;
+            --sp;
+            const unsigned int v = sp < STACK_SMEM ? (unsigned int)smem_stack[sp * stride] : spill[sp - STACK_SMEM];
+            gnode = (int)(v >> 8);
+            ghits = v & 0xFFu;
+            if ((unsigned)gnode >= (unsigned)s.n_nodes8) break;  // malformed stack entry guard
+            const float4 *np = nodes + 5 * gnode;
+            g = group_of(__ldg(np), __ldg(np + 1));
+            if (STATS) st.nodes += 2;
+        }
+        const int kslot = (__ffs(ghits) - 1) ^ (int)r.oct;
+        ghits &= ghits - 1u;
+        if ((g.imask >> kslot) & 1u) {
+            const int child = g.child_base + __popc(g.imask & ((1u << kslot) - 1u));
+            if ((unsigned)child >= (unsigned)s.n_nodes8) break;  // malformed tree guard
+            ++guard;
+            if (ghits != 0) {
+                const unsigned int v = ((unsigned int)gnode << 8) | ghits;
+                if (sp < STACK_SMEM)
+                    smem_stack[sp * stride] = (int)v;
+                else if (sp < RUMI_STACK8)
+                    spill[sp - STACK_SMEM] = v;
+                if (sp < RUMI_STACK8) ++sp;
+            }
+            gnode = child;
+            ghits = visit8<STATS>(nodes, child, r, cull_limit(h.t, tmax), g, st);
+        } else {
+            int first, count;
+            leaf_of(g, kslot, first, count);
+            if (leaf_isect_in<ANYHIT, STATS>(s, s.prims8, first, count, o, d, tmax, in_object, h, st)) return h;
+        }
+    }
+    return h;
+}
+
+// The default walk: the compressed eight-wide tree (RUMI_WALK8), else the binary or the
+// four-wide tree by RUMI_BVH_WIDE.
 template <bool ANYHIT, int STACK_SMEM, bool STATS, typename SceneOf, typename Fetch, typename Finish>
 RUMI_D void traverse_queue_walk(SceneOf scene_of, int n, int *counter, int refill_min, int *smem_stack, int stride,
                                 Fetch fetch, Finish finish, TraceStats &st) {
-#if RUMI_BVH_WIDE
+#if RUMI_WALK8
+    traverse_queue_ww8<ANYHIT, STACK_SMEM, STATS>(scene_of, n, counter, refill_min, smem_stack, stride, fetch, finish,
+                                                  st);
+#elif RUMI_BVH_WIDE
     traverse_queue_ww4<ANYHIT, STACK_SMEM, STATS>(scene_of, n, counter, refill_min, smem_stack, stride, fetch, finish,
                                                   st);
 #else
@@ -917,6 +1247,7 @@ RUMI_D void traverse_queue_walk(SceneOf scene_of, int n, int *counter, int refil
 //   MODE 2: per-lane refill; interior node pairs until every busy lane holds postponed
 //           leaves, then the warp intersects those leaves together.
 //   MODE 3: speculative while-while with per-lane refill (traverse_queue_ww).
+//   MODE 4: the same walk over the compressed eight-wide tree (traverse_queue_ww8).
 // fetch(i, o, d, tmax, in_obj) loads ray i; finish(i, hit) consumes its result.
 template <int MODE, bool ANYHIT, int STACK_SMEM, bool STATS, typename Fetch, typename Finish>
 RUMI_D void traverse_queue(const DevScene &s, int n, int *counter, int refill_min, int *smem_stack, int stride,
@@ -924,8 +1255,18 @@ RUMI_D void traverse_queue(const DevScene &s, int n, int *counter, int refill_mi
     const int lane = threadIdx.x & 31;
     int spill[RUMI_MAX_BVH_DEPTH - STACK_SMEM > 0 ? RUMI_MAX_BVH_DEPTH - STACK_SMEM : 1];
     if (MODE == 3) {
-        traverse_queue_walk<ANYHIT, STACK_SMEM, STATS>([&](int) { return &s; }, n, counter, refill_min, smem_stack,
-                                                        stride, fetch, finish, st);
+#if RUMI_BVH_WIDE
+        traverse_queue_ww4<ANYHIT, STACK_SMEM, STATS>([&](int) { return &s; }, n, counter, refill_min, smem_stack,
+                                                      stride, fetch, finish, st);
+#else
+        traverse_queue_ww<ANYHIT, STACK_SMEM, STATS>([&](int) { return &s; }, n, counter, refill_min, smem_stack,
+                                                     stride, fetch, finish, st);
+#endif
+        return;
+    }
+    if (MODE == 4) {
+        traverse_queue_ww8<ANYHIT, STACK_SMEM, STATS>([&](int) { return &s; }, n, counter, refill_min, smem_stack,
+                                                      stride, fetch, finish, st);
         return;
     }
     if (MODE == 0) {

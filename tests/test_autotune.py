@@ -17,7 +17,7 @@ class FakeScene:
         self.calls += 1
         t = tuning
         ms = 100.0
-        ms += {1: 10.0, 2: 0.0, 3: 30.0, 4: 6.0}[t["trace_mode"]]
+        ms += {1: 10.0, 2: 0.0, 3: 30.0, 4: 6.0, 5: 7.0}[t["trace_mode"]]
         ms += {0: 4.0, 4: 8.0, 5: 0.0, 6: 2.0}[t["blocks_per_sm"]]
         ms += {4: 0.0, 8: 1.0, 16: 3.0}[t["refill_min"]]
         ms += {1 << 21: 5.0, 1 << 22: 2.0, 1 << 23: 0.0}[t["wave_paths"]]
@@ -52,7 +52,7 @@ def test_search_starts_from_the_library_defaults():
     """The starting point is what the library does with every knob at 0 (the speculative
     walk, trace_mode 4), and every traversal scheme of rumi_render_params is searched."""
     assert autotune.DEFAULTS["trace_mode"] == 4
-    assert sorted(autotune.SPACE["trace_mode"]) == [1, 2, 3, 4]
+    assert sorted(autotune.SPACE["trace_mode"]) == [1, 2, 3, 4, 5]
     for k, v in autotune.DEFAULTS.items():
         assert v in autotune.SPACE[k], k
     hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "rumi_b200.h")).read()
