@@ -48,3 +48,32 @@ def render(albedo, medium, gscene, spp, seed, grad_seed=None):
     """Differentiable render; grad_seed defaults to a seed decorrelated from `seed`."""
     return PathTracedFilm.apply(albedo, medium, gscene, spp, seed,
                                 seed + 0x5BD1E995 if grad_seed is None else grad_seed)
+
+
+def visible_triangles(gscene, scene, first_mesh, n_mesh, sub=4, min_pixels=1.0):
+    """Mesh triangles the camera sees: closest hits of sub x sub rays per pixel through the
+    pinhole (Pinhole::CastViewRay's pixel grid, src/Camera/pinhole.cpp:97-136) counted per
+    triangle; a triangle covering at least `min_pixels` pixels is visible.  first_mesh:
+    canonical id of the mesh's first triangle.  Returns a boolean mask (n_mesh,)."""
+    import numpy as np
+    cam, img = scene.camera, scene.image
+    W, H = img.width, img.height
+    tan = np.tan(np.radians(cam.fov) * 0.5)
+    xs = (np.arange(W * sub) + 0.5) / sub
+    ys = (np.arange(H * sub) + 0.5) / sub
+    X, Y = np.meshgrid(xs, ys)
+    dx = -(X - W / 2) / (W / 2) * tan
+    dy = -(Y - H / 2) / (H / 2) * tan * cam.y_ratio
+    d = np.stack([dx, dy, np.ones_like(dx)], -1).reshape(-1, 3)
+    m = np.asarray(cam.basis, np.float64).reshape(4, 4)[:3, :3]
+    d = d @ m.T
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((d.shape[0], 7), np.float32)
+    rays[:, 0:3] = np.asarray(cam.position, np.float32)
+    rays[:, 3:6] = d
+    rays[:, 6] = 3.4e38
+    _, prim, _, _ = gscene.trace(rays)
+    k = prim - first_mesh
+    k = k[(prim >= 0) & (k >= 0) & (k < n_mesh)]
+    cover = np.bincount(k, minlength=n_mesh) / float(sub * sub)
+    return cover >= min_pixels
