@@ -232,9 +232,11 @@ __global__ void pt_reset_shade(PtLaunch P, int bounce) {
 
 // Persistent traversal kernels: every block takes rays from the bounce's queue until it
 // is empty (traverse_queue in traverse.cuh; MODE selects the scheme, see there).
-template <int MODE, bool STATS>
+// SMEM: traversal stack entries per thread kept in shared memory (deeper entries spill to
+// local memory); a smaller stack leaves more of the SM's unified L1/shared storage to L1.
+template <int MODE, bool STATS, int SMEM = STACK_SMEM>
 __global__ void __launch_bounds__(TRACE_THREADS, RUMI_EXTEND_MIN_BLOCKS) pt_extend(PtLaunch P, int bounce) {
-    __shared__ int stack[STACK_SMEM * TRACE_THREADS];
+    __shared__ int stack[SMEM * TRACE_THREADS];
     const int cur = bounce & 1;
     TraceStats st{0, 0};
     auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
@@ -249,17 +251,17 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_EXTEND_MIN_BLOCKS) pt_exte
         const int code = h.t > 0.0f ? (h.id | (h.back ? (int)0x80000000 : 0)) : -1;
         P.hit[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
     };
-    traverse_queue<MODE, false, STACK_SMEM, STATS>(P.s, P.cnt[cur], &P.cnt[C_FETCH_EXT], P.refill_min,
-                                                   stack + threadIdx.x, TRACE_THREADS, fetch, finish, st);
+    traverse_queue<MODE, false, SMEM, STATS>(P.s, P.cnt[cur], &P.cnt[C_FETCH_EXT], P.refill_min,
+                                             stack + threadIdx.x, TRACE_THREADS, fetch, finish, st);
     if (STATS) {
         atomicAdd(&P.stats[S_NODES], (unsigned long long)st.nodes);
         atomicAdd(&P.stats[S_PRIMS], (unsigned long long)st.prims);
     }
 }
 
-template <int MODE, bool ADJ = false>
+template <int MODE, bool ADJ = false, int SMEM = STACK_SMEM>
 __global__ void __launch_bounds__(TRACE_THREADS, RUMI_SHADOW_MIN_BLOCKS) pt_shadow(PtLaunch P) {
-    __shared__ int stack[STACK_SMEM * TRACE_THREADS];
+    __shared__ int stack[SMEM * TRACE_THREADS];
     TraceStats st{0, 0};
     float acc_sigma = 0.0f, acc_g = 0.0f;  // adjoint: score-weighted contributions
     auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
@@ -288,8 +290,8 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_SHADOW_MIN_BLOCKS) pt_shad
             }
         }
     };
-    traverse_queue<MODE, true, STACK_SMEM, false>(P.s, P.cnt[C_SHADOW], &P.cnt[C_FETCH_SH], P.refill_min,
-                                                  stack + threadIdx.x, TRACE_THREADS, fetch, finish, st);
+    traverse_queue<MODE, true, SMEM, false>(P.s, P.cnt[C_SHADOW], &P.cnt[C_FETCH_SH], P.refill_min,
+                                            stack + threadIdx.x, TRACE_THREADS, fetch, finish, st);
     if (ADJ) {
         __syncwarp();
         acc_sigma = warp_sum(acc_sigma);
@@ -877,58 +879,65 @@ static inline int trace_scheme(int trace_mode) {
     return trace_mode >= 1 && trace_mode <= 5 ? trace_mode - 1 : DEFAULT_WALK_MODE;
 }
 
+using ExtendKernel = void (*)(PtLaunch, int);
+using ShadowKernel = void (*)(PtLaunch);
+
+// Shared-memory stack depth from rumi_render_params.stack_depth: 8, 16 or 32 entries per
+// thread (0 = 32).  Only the while-while walks (schemes 3 and 4) come in all three depths.
+static inline int stack_entries(int stack_depth) { return stack_depth == 8 || stack_depth == 16 ? stack_depth : 32; }
+
 template <bool STATS>
-static void launch_extend(int mode, int grid, cudaStream_t st, const PtLaunch &L, int b) {
+static ExtendKernel extend_kernel(int mode, int smem) {
     switch (mode) {
-        case 0: pt_extend<0, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
-        case 1: pt_extend<1, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
-        case 2: pt_extend<2, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
-        case 3: pt_extend<3, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
-        default: pt_extend<4, STATS><<<grid, TRACE_THREADS, 0, st>>>(L, b); break;
+        case 0: return pt_extend<0, STATS>;
+        case 1: return pt_extend<1, STATS>;
+        case 2: return pt_extend<2, STATS>;
+        case 3: return smem == 8 ? pt_extend<3, STATS, 8> : smem == 16 ? pt_extend<3, STATS, 16> : pt_extend<3, STATS>;
+        default: return smem == 8 ? pt_extend<4, STATS, 8> : smem == 16 ? pt_extend<4, STATS, 16> : pt_extend<4, STATS>;
     }
 }
 
 template <bool ADJ>
-static void launch_shadow(int mode, int grid, cudaStream_t st, const PtLaunch &L) {
+static ShadowKernel shadow_kernel(int mode, int smem) {
     switch (mode) {
-        case 0: pt_shadow<0, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
-        case 1: pt_shadow<1, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
-        case 2: pt_shadow<2, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
-        case 3: pt_shadow<3, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
-        default: pt_shadow<4, ADJ><<<grid, TRACE_THREADS, 0, st>>>(L); break;
+        case 0: return pt_shadow<0, ADJ>;
+        case 1: return pt_shadow<1, ADJ>;
+        case 2: return pt_shadow<2, ADJ>;
+        case 3: return smem == 8 ? pt_shadow<3, ADJ, 8> : smem == 16 ? pt_shadow<3, ADJ, 16> : pt_shadow<3, ADJ>;
+        default: return smem == 8 ? pt_shadow<4, ADJ, 8> : smem == 16 ? pt_shadow<4, ADJ, 16> : pt_shadow<4, ADJ>;
     }
 }
 
+template <bool STATS>
+static void launch_extend(int mode, int smem, int grid, cudaStream_t st, const PtLaunch &L, int b) {
+    extend_kernel<STATS>(mode, smem)<<<grid, TRACE_THREADS, 0, st>>>(L, b);
+}
+
+template <bool ADJ>
+static void launch_shadow(int mode, int smem, int grid, cudaStream_t st, const PtLaunch &L) {
+    shadow_kernel<ADJ>(mode, smem)<<<grid, TRACE_THREADS, 0, st>>>(L);
+}
+
+// Asks for just the shared memory the resident blocks' stacks need (RUMI_TRACE_MIN_BLOCKS
+// blocks of smem entries per thread), so the rest of the unified L1 / shared storage stays L1.
+template <typename K>
+static void prefer_l1(K k, int smem) {
+    const int need = RUMI_TRACE_MIN_BLOCKS * smem * TRACE_THREADS * (int)sizeof(int);
+    int pct = (need * 100 + 228 * 1024 - 1) / (228 * 1024);
+    if (pct > 100) pct = 100;
+    cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+}
+
 // Persistent grids: blocks per SM at the kernels' occupancy (capped by blocks_per_sm > 0).
-static void trace_grids(int mode, int num_sms, int blocks_per_sm, bool adj, int &grid, int &grid_sh) {
+static void trace_grids(int mode, int smem, int num_sms, int blocks_per_sm, bool adj, int &grid, int &grid_sh) {
     int occ = 0, occ_sh = 0;
-    switch (mode) {
-        case 0:
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<0, false>, TRACE_THREADS, 0);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<0, true> : pt_shadow<0, false>,
-                                                          TRACE_THREADS, 0);
-            break;
-        case 1:
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<1, false>, TRACE_THREADS, 0);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<1, true> : pt_shadow<1, false>,
-                                                          TRACE_THREADS, 0);
-            break;
-        case 2:
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<2, false>, TRACE_THREADS, 0);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<2, true> : pt_shadow<2, false>,
-                                                          TRACE_THREADS, 0);
-            break;
-        case 3:
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<3, false>, TRACE_THREADS, 0);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<3, true> : pt_shadow<3, false>,
-                                                          TRACE_THREADS, 0);
-            break;
-        default:
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pt_extend<4, false>, TRACE_THREADS, 0);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, adj ? pt_shadow<4, true> : pt_shadow<4, false>,
-                                                          TRACE_THREADS, 0);
-            break;
-    }
+    const ExtendKernel ke = extend_kernel<false>(mode, smem);
+    const ShadowKernel ks = adj ? shadow_kernel<true>(mode, smem) : shadow_kernel<false>(mode, smem);
+    prefer_l1(ke, smem);
+    prefer_l1(extend_kernel<true>(mode, smem), smem);
+    prefer_l1(ks, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ke, TRACE_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, ks, TRACE_THREADS, 0);
     if (occ < 1) occ = 1;
     if (occ_sh < 1) occ_sh = 1;
     if (blocks_per_sm > 0) {
@@ -1026,9 +1035,10 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
 
     // traversal scheme and persistent grid (autotuner knobs; 0 = defaults)
     const int mode = trace_scheme(p->trace_mode);
+    const int smem = stack_entries(p->stack_depth);
     L.refill_min = p->refill_min > 0 ? p->refill_min : 8;
     int trace_grid = 0, shadow_grid = 0;
-    trace_grids(mode, sc->num_sms, p->blocks_per_sm, false, trace_grid, shadow_grid);
+    trace_grids(mode, smem, sc->num_sms, p->blocks_per_sm, false, trace_grid, shadow_grid);
 
     const bool timing = (p->flags & RUMI_FLAG_TIMING) != 0;
     const bool count_stats = (p->flags & RUMI_FLAG_STATS) != 0;
@@ -1063,9 +1073,9 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
                 int e0 = 0;
                 if (timing) { e0 = (int)evs.size(); mark(); }
                 if (count_stats)
-                    launch_extend<true>(mode, trace_grid, stream, L, b);
+                    launch_extend<true>(mode, smem, trace_grid, stream, L, b);
                 else
-                    launch_extend<false>(mode, trace_grid, stream, L, b);
+                    launch_extend<false>(mode, smem, trace_grid, stream, L, b);
                 if (timing) { mark(); ext_ev.push_back({e0, e0 + 1}); }
                 if (b > 0) cudaStreamWaitEvent(stream, sc->ev_join, 0);
                 pt_reset_shade<<<1, 1, 0, stream>>>(L, b);
@@ -1082,7 +1092,7 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
                     cudaStreamWaitEvent(sc->aux_stream, sc->ev_fork, 0);
                 }
                 if (timing) { e0 = (int)evs.size(); mark_on(ss); }
-                launch_shadow<false>(mode, shadow_grid, ss, L);
+                launch_shadow<false>(mode, smem, shadow_grid, ss, L);
                 if (timing) { mark_on(ss); sh_ev.push_back({e0, e0 + 1}); }
                 if (aside) cudaEventRecord(sc->ev_join, sc->aux_stream);
             }
@@ -1099,9 +1109,9 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
             int e0 = 0;
             if (timing) { e0 = (int)evs.size(); mark(); }
             if (count_stats)
-                launch_extend<true>(mode, trace_grid, stream, L, b);
+                launch_extend<true>(mode, smem, trace_grid, stream, L, b);
             else
-                launch_extend<false>(mode, trace_grid, stream, L, b);
+                launch_extend<false>(mode, smem, trace_grid, stream, L, b);
             if (timing) { mark(); ext_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
             if (whitted)
@@ -1110,7 +1120,7 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
                 pt_shade<false><<<cdiv(L.n_paths, SHADE_THREADS), SHADE_THREADS, 0, stream>>>(L, b);
             if (timing) { mark(); shade_ev.push_back({e0, e0 + 1}); }
             if (timing) { e0 = (int)evs.size(); mark(); }
-            launch_shadow<false>(mode, shadow_grid, stream, L);
+            launch_shadow<false>(mode, smem, shadow_grid, stream, L);
             if (timing) { mark(); sh_ev.push_back({e0, e0 + 1}); }
         }
         pt_finish<<<1, 1, 0, stream>>>(L);
@@ -1222,10 +1232,11 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
     // the same traversal scheme as rumi_render, so both passes and the forward frame
     // resolve exact-distance ties alike
     const int mode = trace_scheme(p->trace_mode);
+    const int smem = stack_entries(p->stack_depth);
     A.refill_min = B.refill_min = p->refill_min > 0 ? p->refill_min : 8;
     int grid = 0, grid_sh = 0, grid_dummy = 0, grid_sh_adj = 0;
-    trace_grids(mode, sc->num_sms, p->blocks_per_sm, false, grid, grid_sh);
-    trace_grids(mode, sc->num_sms, p->blocks_per_sm, true, grid_dummy, grid_sh_adj);
+    trace_grids(mode, smem, sc->num_sms, p->blocks_per_sm, false, grid, grid_sh);
+    trace_grids(mode, smem, sc->num_sms, p->blocks_per_sm, true, grid_dummy, grid_sh_adj);
 
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (p->flags & RUMI_FLAG_TIMING) {
@@ -1248,7 +1259,7 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
             pt_generate<<<cdiv(X.n_paths, 256), 256, 0, stream>>>(X);
             for (int b = 0; b < p->max_depth; ++b) {
                 pt_reset_extend<<<1, 1, 0, stream>>>(X, b);
-                launch_extend<false>(mode, grid, stream, X, b);
+                launch_extend<false>(mode, smem, grid, stream, X, b);
                 if (b > 0 && overlap) cudaStreamWaitEvent(stream, sc->ev_join, 0);
                 pt_reset_shade<<<1, 1, 0, stream>>>(X, b);
                 if (adj)
@@ -1262,9 +1273,9 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
                     cudaStreamWaitEvent(sc->aux_stream, sc->ev_fork, 0);
                 }
                 if (adj)
-                    launch_shadow<true>(mode, grid_sh_adj, ss, X);
+                    launch_shadow<true>(mode, smem, grid_sh_adj, ss, X);
                 else
-                    launch_shadow<false>(mode, grid_sh, ss, X);
+                    launch_shadow<false>(mode, smem, grid_sh, ss, X);
                 if (aside) cudaEventRecord(sc->ev_join, sc->aux_stream);
             }
             pt_finish<<<1, 1, 0, stream>>>(X);

@@ -154,6 +154,7 @@ class GpuScene:
         p.trace_mode = int(t.get("trace_mode", trace_mode))
         p.blocks_per_sm = int(t.get("blocks_per_sm", blocks_per_sm))
         p.refill_min = int(t.get("refill_min", refill_min))
+        p.stack_depth = int(t.get("stack_depth", 0))
         if "wave_paths" in t and not wave_paths:
             p.wave_paths = int(t["wave_paths"])
         st = _capi.rumi_render_stats()

@@ -61,7 +61,7 @@ class rumi_render_params(C.Structure):
     _fields_ = [("integrator", C.c_int32), ("max_depth", C.c_int32), ("n_light", C.c_int32), ("n_eye", C.c_int32),
                 ("spp", C.c_int32), ("seed", C.c_uint64), ("wave_paths", C.c_int32), ("flags", C.c_int32),
                 ("stream", C.c_void_p), ("trace_mode", C.c_int32), ("blocks_per_sm", C.c_int32),
-                ("refill_min", C.c_int32)]
+                ("refill_min", C.c_int32), ("stack_depth", C.c_int32)]
 
 
 class rumi_render_stats(C.Structure):

@@ -2,8 +2,9 @@
 
 Knobs (fields of rumi_render_params): ``trace_mode`` (traversal scheme of the persistent
 ray kernels), ``blocks_per_sm`` (persistent traversal blocks per SM, i.e. warps per SM in
-steps of 4), ``refill_min`` (idle lanes that trigger a per-lane refill) and ``wave_paths``
-(queue capacity: paths in flight per wave).  Each candidate renders the given scene and is
+steps of 4), ``refill_min`` (idle lanes that trigger a per-lane refill), ``wave_paths``
+(queue capacity: paths in flight per wave) and ``stack_depth`` (traversal stack entries
+per thread in shared memory).  Each candidate renders the given scene and is
 timed on the device (RUMI_FLAG_TIMING); the search is coordinate descent from the library
 defaults.  Results are cached per GPU model and workload key in a JSON file.
 """
@@ -16,9 +17,9 @@ import time
 # What the library uses when a knob is 0 (include/rumi_b200.h, rumi_render_params): the
 # speculative while-while walk (trace_mode 4), the occupancy limit of traversal blocks, a
 # refill at 8 idle lanes and 4,194,304 paths per wave.  The search starts there.
-DEFAULTS = dict(trace_mode=4, blocks_per_sm=0, refill_min=8, wave_paths=1 << 22)
+DEFAULTS = dict(trace_mode=4, blocks_per_sm=0, refill_min=8, wave_paths=1 << 22, stack_depth=32)
 SPACE = dict(trace_mode=[4, 5, 1, 2, 3], blocks_per_sm=[0, 4, 5, 6], refill_min=[4, 8, 16],
-             wave_paths=[1 << 21, 1 << 22, 1 << 23])
+             wave_paths=[1 << 21, 1 << 22, 1 << 23], stack_depth=[32, 16, 8])
 def default_cache_path() -> str:
     """$RUMI_TUNING_CACHE, else autotune_cache.json under the user's cache directory
     ($XDG_CACHE_HOME or ~/.cache)/rumi_b200 -- never inside the package tree."""
@@ -56,7 +57,7 @@ def tune(gs, spp: int, key: str, space: dict = None, repeats: int = 2, film_ptr=
     cur_ms = measure(gs, cur, spp, repeats=repeats, film_ptr=film_ptr)
     history = [(dict(cur), cur_ms)]
     seen = {tuple(sorted(cur.items()))}
-    for knob in ("trace_mode", "blocks_per_sm", "refill_min", "wave_paths"):
+    for knob in ("trace_mode", "blocks_per_sm", "refill_min", "wave_paths", "stack_depth"):
         for v in space[knob]:
             cand = dict(cur)
             cand[knob] = v

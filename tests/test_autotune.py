@@ -21,6 +21,7 @@ class FakeScene:
         ms += {0: 4.0, 4: 8.0, 5: 0.0, 6: 2.0}[t["blocks_per_sm"]]
         ms += {4: 0.0, 8: 1.0, 16: 3.0}[t["refill_min"]]
         ms += {1 << 21: 5.0, 1 << 22: 2.0, 1 << 23: 0.0}[t["wave_paths"]]
+        ms += {32: 1.0, 16: 0.0, 8: 0.5}[t["stack_depth"]]
         return None, {"total_ms": ms}
 
 
@@ -33,7 +34,7 @@ def test_coordinate_descent_finds_the_optimum_and_caches(tmp_path):
     cache = str(tmp_path / "cache.json")
     g = FakeScene()
     res = autotune.tune(g, spp=4, key="fake", repeats=1, cache_path=cache)
-    assert res["params"] == dict(trace_mode=2, blocks_per_sm=5, refill_min=4, wave_paths=1 << 23)
+    assert res["params"] == dict(trace_mode=2, blocks_per_sm=5, refill_min=4, wave_paths=1 << 23, stack_depth=16)
     assert res["ms"] == 100.0
     # one baseline + every alternative value of every knob
     assert g.calls == 1 + sum(len(v) - 1 for v in autotune.SPACE.values())
@@ -81,9 +82,9 @@ def test_gpu_tune_on_a_small_scene_keeps_the_film(tmp_path):
     torch.cuda.set_device(0)
     gs = rumi_b200.GpuScene(scenes.bvh_bound_pt(64, 64, 4, 6, levels=5, seed=7))
     space = dict(trace_mode=[autotune.DEFAULTS["trace_mode"], 1], blocks_per_sm=[0, 4], refill_min=[8, 16],
-                 wave_paths=[1 << 22, 1 << 14])
+                 wave_paths=[1 << 22, 1 << 14], stack_depth=[32, 8])
     res = autotune.tune(gs, spp=4, key="small", space=space, repeats=1, cache_path=str(tmp_path / "c.json"))
-    assert len(res["history"]) == 1 + 4 and all(h["ms"] > 0 for h in res["history"])
+    assert len(res["history"]) == 1 + 5 and all(h["ms"] > 0 for h in res["history"])
     assert autotune.load("small", cache_path=str(tmp_path / "c.json"))["params"] == res["params"]
     want, _ = gs.render(spp=4, seed=77)
     got, _ = gs.render(spp=4, seed=77, tuning=res["params"])
