@@ -603,23 +603,25 @@ RUMI_D bool volumetric_ok(const DevVolume &V, float3 sp, float3 tp, float xi) {
     return !(xi < 1.0f - expf(avg3(V.sigma_t) * -sm));
 }
 
+// The light a sample picked and its sampled point (Scene::LightsUniformSampling +
+// AreaLight::SolidAngleSampling's position).
+struct BdLight {
+    int li;
+    float3 n;
+};
+
+// Both subpaths of camera sample j (ConstructViewPath / ConstructLightPath with their
+// starts, bidirectionalpathtracer.cpp:121-180).  Returns the light; nE / nLv receive the
+// vertex counts.
 template <int MAXV>
-__global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
-    __shared__ int stack[BD_STACK * BD_THREADS];
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.n_paths) return;
+RUMI_D BdLight build_subpaths(const BdLaunch &P, int j, BVert *VE, float3 *segE, float3 *aE, BVert *VL, float3 *segL,
+                              float3 *aL, int &nE, int &nLv, int *stk, TraceStats &st) {
     const DevScene &S = P.s;
     const uint64_t path = (uint64_t)(P.path0 + j);
     const long long pixel = (long long)P.pix0 + j / P.spp;
     const int sidx = j % P.spp;
     const int W = S.width, H = S.height;
     const int pw_ = (int)(pixel % W), ph_ = (int)(pixel / W);
-    TraceStats st{0, 0};
-    int *stk = stack + threadIdx.x;
-
-    BVert VE[MAXV], VL[MAXV];
-    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
-    // Scene::LightsUniformSampling + AreaLight::SolidAngleSampling
     const Uniform4 UL = path_uniforms(path, 1000u, 0, P.k0, P.k1);
     const Uniform4 UD = path_uniforms(path, 1000u, 1, P.k0, P.k1);
     const int li = pick_light(S, UL.u[0]);
@@ -650,7 +652,7 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
         VE[0].pdf_dir = c.plane_dist * c.plane_dist / (l.z * l.z * l.z * c.film_area);
         VE[0].pdf_fwd = c3(1.0f);
     }
-    const int nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
+    nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
     // light subpath start: cosine-weighted emission from an area light
     // (AreaLight::SolidAngleSampling), uniform in the cone from a spot
     const bool spot = light.type == LIGHT_SPOT;
@@ -669,16 +671,114 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
         VL[0].pdf_dir = emit.pdf;
         VL[0].cos_a = dot3(emit.wi, light_n);
     }
-    const int nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit_w, VL, segL, aL, light, light_n, stk, st);
+    nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit_w, VL, segL, aL, light, light_n, stk, st);
     // a delta position: the strategies in which the eye subpath reaches the light carry
     // no weight (the MIS sums skip a dirac first light vertex)
     if (spot) VL[0].dirac = true;
+    BdLight bl;
+    bl.li = li;
+    bl.n = light_n;
+    return bl;
+}
 
+// ------------------------------------------------------------ staged form
+// The staged form splits a wave of camera samples into
+//   bdpt_subpaths  both subpaths of every sample -> vertex store (SoA, coalesced by sample)
+//   bdpt_connect   every (s, t) strategy: contribution and MIS weight; the strategies that
+//                  need a visibility test become shadow-queue entries, the others are
+//                  written to their result slot at once
+//   bdpt_shadow    the shadow queue through the persistent any-hit walk; an unoccluded
+//                  entry writes its result slot (or splats, t = 0)
+//   bdpt_resolve   per sample, the result slots summed in the reference's strategy order
+// so the sums equal the one-thread form's, and the visibility rays -- most of BDPT's rays
+// -- run through the same traversal kernels as the path tracer's.
+//
+// Vertex store: six float4 per vertex, field f of vertex k of sample j at
+// [(f * MAXV + k) * n + j]:
+//   0: p, xi   1: n, pdf_path   2: pdf_fwd, t_in   3: pdf_bwd, material
+//   4: vtau / vpdf, primitive   5: direction of the segment to the next vertex, flags
+struct BdStore {
+    float4 *ev, *lv;        // eye / light vertices
+    float4 *ea, *la;        // throughputs: [k * n + j], k < MAXV + 2
+    int2 *counts;           // (eye vertices, light vertices)
+    float4 *light;          // (light normal, light index)
+    float4 *result;         // [slot * n + j]: each strategy's contribution (0 when rejected)
+    float4 *q;              // shadow queue: 3 float4 per entry
+    int *q_count;           // entries pushed
+    int *q_fetch;           // the any-hit walk's fetch counter
+    int *overflow;          // set when a push found the queue full
+    int n, slots, q_cap;
+};
+
+enum { BF_DIRAC = 1, BF_SURF = 2, BF_INOBJ = 4 };
+
+template <int MAXV>
+RUMI_D void store_vertex(float4 *base, int n, int j, int k, const BVert &v, float3 seg) {
+    const int flags = (v.dirac ? BF_DIRAC : 0) | (v.onsurface ? BF_SURF : 0) | (v.in_obj ? BF_INOBJ : 0);
+    const float3 ratio = v.vtau / v.vpdf;
+    base[(0 * MAXV + k) * (size_t)n + j] = make_float4(v.p.x, v.p.y, v.p.z, v.xi);
+    base[(1 * MAXV + k) * (size_t)n + j] = make_float4(v.n.x, v.n.y, v.n.z, v.pdf_path);
+    base[(2 * MAXV + k) * (size_t)n + j] = make_float4(v.pdf_fwd.x, v.pdf_fwd.y, v.pdf_fwd.z, v.t_in);
+    base[(3 * MAXV + k) * (size_t)n + j] = make_float4(v.pdf_bwd.x, v.pdf_bwd.y, v.pdf_bwd.z, __int_as_float(v.mat));
+    base[(4 * MAXV + k) * (size_t)n + j] = make_float4(ratio.x, ratio.y, ratio.z, __int_as_float(v.prim));
+    base[(5 * MAXV + k) * (size_t)n + j] = make_float4(seg.x, seg.y, seg.z, __int_as_float(flags));
+}
+
+template <int MAXV>
+RUMI_D void load_vertex(const float4 *base, int n, int j, int k, BVert &v, float3 &seg) {
+    const float4 f0 = base[(0 * MAXV + k) * (size_t)n + j], f1 = base[(1 * MAXV + k) * (size_t)n + j];
+    const float4 f2 = base[(2 * MAXV + k) * (size_t)n + j], f3 = base[(3 * MAXV + k) * (size_t)n + j];
+    const float4 f4 = base[(4 * MAXV + k) * (size_t)n + j], f5 = base[(5 * MAXV + k) * (size_t)n + j];
+    bvert_clear(v);
+    v.p = f4xyz(f0);
+    v.xi = f0.w;
+    v.n = f4xyz(f1);
+    v.pdf_path = f1.w;
+    v.pdf_fwd = f4xyz(f2);
+    v.t_in = f2.w;
+    v.pdf_bwd = f4xyz(f3);
+    v.mat = __float_as_int(f3.w);
+    v.vtau = f4xyz(f4);  // vtau / vpdf, with vpdf 1: Material::Fr reads only the ratio
+    v.vpdf = c3(1.0f);
+    v.prim = __float_as_int(f4.w);
+    seg = f4xyz(f5);
+    const int flags = __float_as_int(f5.w);
+    v.dirac = (flags & BF_DIRAC) != 0;
+    v.onsurface = (flags & BF_SURF) != 0;
+    v.in_obj = (flags & BF_INOBJ) != 0;
+}
+
+// One slot of a warp-aggregated push (the calling lanes are the pushers).
+RUMI_D int bd_push_slot(int *counter) {
+    const unsigned act = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(act) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(act));
+    base = __shfl_sync(act, base, leader);
+    return base + __popc(act & ((1u << lane) - 1u));
+}
+
+// Every (s, t) strategy of one sample (Trace's double loop, bidirectionalpathtracer.cpp:
+// 182-390).  STAGED = false: visibility traced here and the contributions summed into the
+// returned radiance, splats added to the light film.  STAGED = true: contributions go to
+// result slots / the shadow queue of B and the returned value is unused.
+template <int MAXV, bool STAGED>
+RUMI_D float3 connect_strategies(const BdLaunch &P, const BdStore &B, int j, const BVert *VE, const float3 *segE,
+                                 const float3 *aE, int nE, const BVert *VL, const float3 *segL, const float3 *aL,
+                                 int nLv, const BdLight &bl, int *stk, TraceStats &st) {
+    const DevScene &S = P.s;
+    const uint64_t path = (uint64_t)(P.path0 + j);
+    const int W = S.width, H = S.height;
+    const DevLight light = S.lights[bl.li];
+    const float3 light_n = bl.n;
+    const bool spot = light.type == LIGHT_SPOT;
     float3 L = mk3(0, 0, 0);
     const int max_len = nE + nLv - 1;
     for (int len = 1; len <= max_len; ++len) {
         for (int t = 0; t <= len; ++t) {
             if (t >= nE) break;
+            const int slot = (len - 1) * P.nE + t;
             const BVert &tc = VE[t];
             float3 t_wo = mk3(0, 0, 0);
             if (t > 0) {
@@ -686,7 +786,11 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
                     if (len == nE - 1) {
                         const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
-                        L = L + aE[t + 1] * w;
+                        const float3 c = aE[t + 1] * w;
+                        if (STAGED)
+                            B.result[(size_t)slot * B.n + j] = make_float4(c.x, c.y, c.z, 0.0f);
+                        else
+                            L = L + c;
                     }
                     break;
                 }
@@ -723,7 +827,9 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 if (film_w == W || film_h == H) continue;
                 if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) continue;
             }
-            if (!visible(S, s + 1, t + 1, sc.p, tc.p, stk, st)) continue;
+            if (!STAGED && !visible(S, s + 1, t + 1, sc.p, tc.p, stk, st)) continue;
+            // VolumetricTest reads its own uniform, so it may come before the visibility
+            // test the staged form defers
             const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
             if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) continue;
             float3 cE, cL;
@@ -749,19 +855,144 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
                 cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
             }
             if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
-            if (t == 0) {
-                float3 lo = aE[t] * cE * G * cL * aL[s];
-                lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n, light);
+            float3 lo = aE[t] * cE * G * cL * aL[s];
+            lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
+            if (STAGED) {
+                // the shadow ray VisibilityTest would trace (from the eye vertex unless it
+                // is the camera), with what the strategy adds when nothing blocks it
+                float3 o, dir;
+                if (t == 0) {
+                    o = sc.p;
+                    dir = normalize_ref(tc.p - sc.p);
+                } else {
+                    o = tc.p;
+                    dir = normalize_ref(sc.p - tc.p);
+                }
+                const float tmax = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+                const int dest = t == 0 ? -1 - (film_h * W + film_w) : slot * B.n + j;
+                const int qi = bd_push_slot(B.q_count);
+                if (qi < B.q_cap) {
+                    B.q[3 * (size_t)qi + 0] = make_float4(o.x, o.y, o.z, __int_as_float(dest));
+                    B.q[3 * (size_t)qi + 1] = make_float4(dir.x, dir.y, dir.z, tmax);
+                    B.q[3 * (size_t)qi + 2] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+                } else {
+                    atomicExch(B.overflow, 1);
+                }
+            } else if (t == 0) {
                 float *dst = P.light_film + ((size_t)film_h * W + film_w) * 3;
                 atomicAdd(dst + 0, lo.z);
                 atomicAdd(dst + 1, lo.y);
                 atomicAdd(dst + 2, lo.x);
             } else {
-                float3 lo = aE[t] * cE * G * cL * aL[s];
-                lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
                 L = L + lo;
             }
         }
+    }
+    return L;
+}
+
+// One thread renders one camera sample: both subpaths and every strategy.
+template <int MAXV>
+__global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
+    __shared__ int stack[BD_STACK * BD_THREADS];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_paths) return;
+    TraceStats st{0, 0};
+    int *stk = stack + threadIdx.x;
+    BVert VE[MAXV], VL[MAXV];
+    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
+    int nE, nLv;
+    const BdLight bl = build_subpaths<MAXV>(P, j, VE, segE, aE, VL, segL, aL, nE, nLv, stk, st);
+    BdStore none;
+    const float3 L = connect_strategies<MAXV, false>(P, none, j, VE, segE, aE, nE, VL, segL, aL, nLv, bl, stk, st);
+    P.L[j] = make_float4(L.x, L.y, L.z, 0.0f);
+}
+
+template <int MAXV>
+__global__ void __launch_bounds__(BD_THREADS) bdpt_subpaths(BdLaunch P, BdStore B) {
+    __shared__ int stack[BD_STACK * BD_THREADS];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_paths) return;
+    TraceStats st{0, 0};
+    BVert VE[MAXV], VL[MAXV];
+    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
+    int nE, nLv;
+    const BdLight bl = build_subpaths<MAXV>(P, j, VE, segE, aE, VL, segL, aL, nE, nLv, stack + threadIdx.x, st);
+    const int n = B.n;
+    for (int k = 0; k < nE; ++k) store_vertex<MAXV>(B.ev, n, j, k, VE[k], k + 1 < nE ? segE[k] : mk3(0, 0, 0));
+    for (int k = 0; k < nLv; ++k) store_vertex<MAXV>(B.lv, n, j, k, VL[k], k + 1 < nLv ? segL[k] : mk3(0, 0, 0));
+    // throughputs the subpath loops wrote: alpha[0 .. vertices], one more after an emitter hit
+    for (int k = 0; k <= nE && k < MAXV + 2; ++k) B.ea[(size_t)k * n + j] = make_float4(aE[k].x, aE[k].y, aE[k].z, 0.0f);
+    for (int k = 0; k < nLv; ++k) B.la[(size_t)k * n + j] = make_float4(aL[k].x, aL[k].y, aL[k].z, 0.0f);
+    B.counts[j] = make_int2(nE, nLv);
+    B.light[j] = make_float4(bl.n.x, bl.n.y, bl.n.z, __int_as_float(bl.li));
+}
+
+template <int MAXV>
+__global__ void __launch_bounds__(BD_THREADS) bdpt_connect(BdLaunch P, BdStore B) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_paths) return;
+    TraceStats st{0, 0};
+    const int n = B.n;
+    const int2 cnt = B.counts[j];
+    const int nE = cnt.x, nLv = cnt.y;
+    BVert VE[MAXV], VL[MAXV];
+    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
+    for (int k = 0; k < nE; ++k) load_vertex<MAXV>(B.ev, n, j, k, VE[k], segE[k]);
+    for (int k = 0; k < nLv; ++k) load_vertex<MAXV>(B.lv, n, j, k, VL[k], segL[k]);
+    for (int k = 0; k <= nE && k < MAXV + 2; ++k) aE[k] = f4xyz(B.ea[(size_t)k * n + j]);
+    for (int k = 0; k < nLv; ++k) aL[k] = f4xyz(B.la[(size_t)k * n + j]);
+    const float4 l4 = B.light[j];
+    BdLight bl;
+    bl.n = f4xyz(l4);
+    bl.li = __float_as_int(l4.w);
+    connect_strategies<MAXV, true>(P, B, j, VE, segE, aE, nE, VL, segL, aL, nLv, bl, nullptr, st);
+}
+
+// VisibilityTest for the queued strategies: blocked when something lies more than 1e-4
+// before the far vertex (bidirectionalpathtracer.cpp:1018-1050).
+__global__ void __launch_bounds__(128, 8) bdpt_shadow(BdLaunch P, BdStore B) {
+    __shared__ int stack[BD_STACK * 128];
+    TraceStats st{0, 0};
+    const int W = P.s.width;
+    auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
+        const float4 a = B.q[3 * (size_t)i], b = B.q[3 * (size_t)i + 1];
+        o = f4xyz(a);
+        d = f4xyz(b);
+        tmax = b.w;
+        in_obj = false;
+    };
+    auto finish = [&](int i, const HitRec &h) {
+        const float tmax = B.q[3 * (size_t)i + 1].w;
+        if (h.t > 0.0f && tmax - h.t > 1e-4f) return;
+        const int dest = __float_as_int(B.q[3 * (size_t)i].w);
+        const float4 c = B.q[3 * (size_t)i + 2];
+        if (dest >= 0) {
+            B.result[dest] = make_float4(c.x, c.y, c.z, 0.0f);
+        } else {
+            const int px = -1 - dest;
+            float *dst = P.light_film + (size_t)px * 3;
+            (void)W;
+            atomicAdd(dst + 0, c.z);
+            atomicAdd(dst + 1, c.y);
+            atomicAdd(dst + 2, c.x);
+        }
+    };
+    const int n = *B.q_count < B.q_cap ? *B.q_count : B.q_cap;
+    traverse_queue_walk<true, BD_STACK, false>([&](int) { return &P.s; }, n, B.q_fetch, 8, stack + threadIdx.x, 128,
+                                               fetch, finish, st);
+}
+
+// The sample's radiance: its result slots summed in strategy order.
+__global__ void bdpt_resolve(BdLaunch P, BdStore B) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_paths) return;
+    float3 L = mk3(0, 0, 0);
+    for (int k = 0; k < B.slots; ++k) {
+        const float4 c = B.result[(size_t)k * B.n + j];
+        L.x += c.x;
+        L.y += c.y;
+        L.z += c.z;
     }
     P.L[j] = make_float4(L.x, L.y, L.z, 0.0f);
 }
@@ -808,14 +1039,27 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
     }
     const int W = S.width, H = S.height, spp = p->spp;
     const long long total_pix = (long long)W * H;
-    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 20);
+    // trace_mode 1: the one-thread-per-sample kernel; otherwise the staged form
+    const bool staged = p->trace_mode != 1;
+    const int maxv = p->n_light <= 8 && p->n_eye <= 8 ? 8 : BD_MAXV;
+    const int slots = (p->n_eye + p->n_light - 1) * p->n_eye;
+    long long wave = p->wave_paths > 0 ? p->wave_paths : (staged ? (1 << 18) : (1 << 20));
     long long pix_per_wave = wave / spp;
     if (pix_per_wave < 1) pix_per_wave = 1;
     if (pix_per_wave > total_pix) pix_per_wave = total_pix;
     const size_t npaths = (size_t)(pix_per_wave * spp);
+    const size_t q_cap = npaths * (size_t)p->n_eye * (size_t)p->n_light;
+    if (staged && q_cap > (size_t)0x7fffffff / 3) {
+        set_error("BDPT: wave_paths too large for the shadow queue");
+        return RUMI_ERR_INVALID_ARG;
+    }
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t film_bytes = sizeof(float) * 3 * (size_t)total_pix;
-    const size_t bytes = al(npaths * sizeof(float4)) + al(film_bytes) + al(64);
+    size_t bytes = al(npaths * sizeof(float4)) + al(film_bytes) + al(64);
+    if (staged)
+        bytes += 2 * al(6 * (size_t)maxv * npaths * sizeof(float4)) + 2 * al((size_t)(maxv + 2) * npaths * sizeof(float4)) +
+                 al(npaths * sizeof(int2)) + al(npaths * sizeof(float4)) + al((size_t)slots * npaths * sizeof(float4)) +
+                 al(3 * q_cap * sizeof(float4)) + al(64);
     rumi_status st = ensure_workspace(sc, bytes);
     if (st != RUMI_OK) return st;
     char *w = (char *)sc->ws;
@@ -833,6 +1077,25 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
     B.L = (float4 *)w; w += al(npaths * sizeof(float4));
     B.light_film = (float *)w; w += al(film_bytes);
     unsigned long long *nan_count = (unsigned long long *)w;
+    w += al(64);
+    BdStore Q;
+    memset(&Q, 0, sizeof(Q));
+    if (staged) {
+        Q.ev = (float4 *)w; w += al(6 * (size_t)maxv * npaths * sizeof(float4));
+        Q.lv = (float4 *)w; w += al(6 * (size_t)maxv * npaths * sizeof(float4));
+        Q.ea = (float4 *)w; w += al((size_t)(maxv + 2) * npaths * sizeof(float4));
+        Q.la = (float4 *)w; w += al((size_t)(maxv + 2) * npaths * sizeof(float4));
+        Q.counts = (int2 *)w; w += al(npaths * sizeof(int2));
+        Q.light = (float4 *)w; w += al(npaths * sizeof(float4));
+        Q.result = (float4 *)w; w += al((size_t)slots * npaths * sizeof(float4));
+        Q.q = (float4 *)w; w += al(3 * q_cap * sizeof(float4));
+        Q.q_count = (int *)w;
+        Q.q_fetch = Q.q_count + 1;
+        Q.overflow = Q.q_count + 2;
+        Q.slots = slots;
+        Q.q_cap = (int)q_cap;
+        cudaMemsetAsync(Q.overflow, 0, sizeof(int), stream);
+    }
     const DevCamera &c = S.camera;
     B.right = mk3(c.m[0] + c.m[3], c.m[4] + c.m[7], c.m[8] + c.m[11]);
     B.up = mk3(c.m[1] + c.m[3], c.m[5] + c.m[7], c.m[9] + c.m[11]);
@@ -845,6 +1108,12 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
         cudaEventCreate(&e1);
         cudaEventRecord(e0, stream);
     }
+    int shadow_grid = 0;
+    if (staged) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bdpt_shadow, 128, 0);
+        shadow_grid = sc->num_sms * (occ > 0 ? occ : 1);
+    }
     long long launches = 0;
     for (long long pix0 = 0; pix0 < total_pix; pix0 += pix_per_wave) {
         const long long n_pix = pix0 + pix_per_wave <= total_pix ? pix_per_wave : total_pix - pix0;
@@ -852,19 +1121,42 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
         B.n_paths = (int)(n_pix * spp);
         B.path0 = pix0 * spp;
         const int blocks = (B.n_paths + BD_THREADS - 1) / BD_THREADS;
-        if (p->n_light <= 8 && p->n_eye <= 8)
-            bdpt_kernel<8><<<blocks, BD_THREADS, 0, stream>>>(B);
-        else
-            bdpt_kernel<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B);
+        if (staged) {
+            Q.n = (int)npaths;
+            cudaMemsetAsync(Q.q_count, 0, 2 * sizeof(int), stream);
+            cudaMemsetAsync(Q.result, 0, (size_t)slots * npaths * sizeof(float4), stream);
+            if (maxv == 8) {
+                bdpt_subpaths<8><<<blocks, BD_THREADS, 0, stream>>>(B, Q);
+                bdpt_connect<8><<<blocks, BD_THREADS, 0, stream>>>(B, Q);
+            } else {
+                bdpt_subpaths<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B, Q);
+                bdpt_connect<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B, Q);
+            }
+            bdpt_shadow<<<shadow_grid, 128, 0, stream>>>(B, Q);
+            bdpt_resolve<<<(B.n_paths + 255) / 256, 256, 0, stream>>>(B, Q);
+            launches += 4;
+        } else {
+            if (maxv == 8)
+                bdpt_kernel<8><<<blocks, BD_THREADS, 0, stream>>>(B);
+            else
+                bdpt_kernel<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B);
+            launches += 1;
+        }
         bdpt_write_film<<<(int)((n_pix + 255) / 256), 256, 0, stream>>>(B, (int)n_pix, film_dev, nan_count);
-        launches += 2;
+        launches += 1;
     }
     add_light_film<<<sc->num_sms * 4, 256, 0, stream>>>(film_dev, B.light_film, (size_t)total_pix * 3);
     if (timing) cudaEventRecord(e1, stream);
     unsigned long long h_nan = 0;
+    int h_overflow = 0;
     cudaMemcpyAsync(&h_nan, nan_count, sizeof(h_nan), cudaMemcpyDeviceToHost, stream);
+    if (staged) cudaMemcpyAsync(&h_overflow, Q.overflow, sizeof(int), cudaMemcpyDeviceToHost, stream);
     cudaError_t e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_status(e, "bdpt_render");
+    if (h_overflow) {  // cannot happen: the queue holds every strategy of every sample
+        set_error("bdpt_render: shadow queue overflow");
+        return RUMI_ERR_INTERNAL;
+    }
     if (stats) {
         memset(stats, 0, sizeof(*stats));
         stats->paths = total_pix * spp;
