@@ -1122,37 +1122,25 @@ RUMI_D void traverse_queue_ww8(SceneOf scene_of, int n, int *counter, int refill
         // meets a second leaf (kept in its group) or runs out of work
         bool blocked = false;
         while (ray >= 0 && !blocked && (ghits != 0 || sp != 0)) {
-            // the cheap part first -- pops and leaf takes -- up to the next interior child,
-            // so that every iteration's one expensive step (a node visit) is in step
-            // across the lanes
-            int child = -1;
-            for (;;) {
-                if (ghits == 0) {
-                    if (sp == 0) break;
-                    pop();
-                    continue;
-                }
+            if (ghits == 0) pop();
+            if (ghits != 0) {
                 const int kslot = (__ffs(ghits) - 1) ^ (int)r.oct;
                 if ((g.imask >> kslot) & 1u) {
                     ghits &= ghits - 1u;
-                    child = g.child_base + __popc(g.imask & ((1u << kslot) - 1u));
-                    break;
-                }
-                if (lf_count != 0) {
-                    blocked = true;  // a second leaf: keep it in the group for the leaf phase
-                    break;
-                }
-                ghits &= ghits - 1u;
-                leaf_of(g, kslot, lf_first, lf_count);
-            }
-            if (child >= 0) {
-                if ((unsigned)child >= (unsigned)sp_scene->n_nodes8 || ++steps > sp_scene->n_nodes8) {
-                    ghits = 0;  // malformed tree guard
-                    sp = 0;
+                    const int child = g.child_base + __popc(g.imask & ((1u << kslot) - 1u));
+                    if ((unsigned)child >= (unsigned)sp_scene->n_nodes8 || ++steps > sp_scene->n_nodes8) {
+                        ghits = 0;  // malformed tree guard
+                        sp = 0;
+                    } else {
+                        if (ghits != 0) push(((unsigned int)gnode << 8) | ghits);
+                        gnode = child;
+                        ghits = visit8<STATS>(nodes, child, r, cull_limit(h.t, tmax), g, st);
+                    }
+                } else if (lf_count == 0) {
+                    ghits &= ghits - 1u;
+                    leaf_of(g, kslot, lf_first, lf_count);
                 } else {
-                    if (ghits != 0) push(((unsigned int)gnode << 8) | ghits);
-                    gnode = child;
-                    ghits = visit8<STATS>(nodes, child, r, cull_limit(h.t, tmax), g, st);
+                    blocked = true;
                 }
             }
             if (!__any_sync(__activemask(), lf_count == 0 && (ghits != 0 || sp != 0))) break;
