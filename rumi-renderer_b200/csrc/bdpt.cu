@@ -707,8 +707,15 @@ struct BdStore {
     int *q_count;           // entries pushed
     int *q_fetch;           // the any-hit walk's fetch counter
     int *overflow;          // set when a push found the queue full
+    int *err;               // [0]: first failed consistency check (0 = none), [1]: its index
     int n, slots, q_cap;
 };
+
+// Records the first failed consistency check of the staged kernels; the caller then
+// skips the access it guarded.
+RUMI_D void bd_fail(const BdStore &B, int code, int index) {
+    if (atomicCAS(B.err, 0, code) == 0) B.err[1] = index;
+}
 
 enum { BF_DIRAC = 1, BF_SURF = 2, BF_INOBJ = 4 };
 
@@ -787,9 +794,12 @@ RUMI_D float3 connect_strategies(const BdLaunch &P, const BdStore &B, int j, con
                     if (len == nE - 1) {
                         const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
                         const float3 c = aE[t + 1] * w;
-                        if (STAGED)
-                            B.result[(size_t)slot * B.n + j] = make_float4(c.x, c.y, c.z, 0.0f);
-                        else
+                        if (STAGED) {
+                            if (slot < 0 || slot >= B.slots)
+                                bd_fail(B, 5, j);
+                            else
+                                B.result[(size_t)slot * B.n + j] = make_float4(c.x, c.y, c.z, 0.0f);
+                        } else
                             L = L + c;
                     }
                     break;
@@ -870,6 +880,10 @@ RUMI_D float3 connect_strategies(const BdLaunch &P, const BdStore &B, int j, con
                 }
                 const float tmax = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
                 const int dest = t == 0 ? -1 - (film_h * W + film_w) : slot * B.n + j;
+                if (t > 0 && (slot < 0 || slot >= B.slots)) {
+                    bd_fail(B, 6, j);
+                    continue;
+                }
                 const int qi = bd_push_slot(B.q_count);
                 if (qi < B.q_cap) {
                     B.q[3 * (size_t)qi + 0] = make_float4(o.x, o.y, o.z, __int_as_float(dest));
@@ -919,6 +933,11 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_subpaths(BdLaunch P, BdStore 
     int nE, nLv;
     const BdLight bl = build_subpaths<MAXV>(P, j, VE, segE, aE, VL, segL, aL, nE, nLv, stack + threadIdx.x, st);
     const int n = B.n;
+    if (nE < 1 || nE > MAXV || nLv < 1 || nLv > MAXV || bl.li < 0 || bl.li >= P.s.n_lights || j >= n) {
+        bd_fail(B, 1, j);
+        B.counts[j] = make_int2(0, 0);
+        return;
+    }
     for (int k = 0; k < nE; ++k) store_vertex<MAXV>(B.ev, n, j, k, VE[k], k + 1 < nE ? segE[k] : mk3(0, 0, 0));
     for (int k = 0; k < nLv; ++k) store_vertex<MAXV>(B.lv, n, j, k, VL[k], k + 1 < nLv ? segL[k] : mk3(0, 0, 0));
     // throughputs the subpath loops wrote: alpha[0 .. vertices], one more after an emitter hit
@@ -936,16 +955,40 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_connect(BdLaunch P, BdStore B
     const int n = B.n;
     const int2 cnt = B.counts[j];
     const int nE = cnt.x, nLv = cnt.y;
+    if (nE < 1 || nE > MAXV || nLv < 1 || nLv > MAXV) {
+        bd_fail(B, 2, j);
+        return;
+    }
     BVert VE[MAXV], VL[MAXV];
     float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
     for (int k = 0; k < nE; ++k) load_vertex<MAXV>(B.ev, n, j, k, VE[k], segE[k]);
     for (int k = 0; k < nLv; ++k) load_vertex<MAXV>(B.lv, n, j, k, VL[k], segL[k]);
+    // the one-thread form leaves the vertex after the last one cleared (its loop clears
+    // it before the segment that ends the subpath), and MISWeight's "locked" test reads
+    // VE[1] even when the eye subpath is the camera alone
+    for (int k = nE; k < MAXV; ++k) bvert_clear(VE[k]);
+    for (int k = nLv; k < MAXV; ++k) bvert_clear(VL[k]);
+    const int n_mat = P.s.n_materials;
+    for (int k = 1; k < nE; ++k)
+        if (VE[k].onsurface && (VE[k].mat < 0 || VE[k].mat >= n_mat)) {
+            bd_fail(B, 4, j);
+            return;
+        }
+    for (int k = 1; k < nLv; ++k)
+        if (VL[k].onsurface && (VL[k].mat < 0 || VL[k].mat >= n_mat)) {
+            bd_fail(B, 4, j);
+            return;
+        }
     for (int k = 0; k <= nE && k < MAXV + 2; ++k) aE[k] = f4xyz(B.ea[(size_t)k * n + j]);
     for (int k = 0; k < nLv; ++k) aL[k] = f4xyz(B.la[(size_t)k * n + j]);
     const float4 l4 = B.light[j];
     BdLight bl;
     bl.n = f4xyz(l4);
     bl.li = __float_as_int(l4.w);
+    if (bl.li < 0 || bl.li >= P.s.n_lights) {
+        bd_fail(B, 3, j);
+        return;
+    }
     connect_strategies<MAXV, true>(P, B, j, VE, segE, aE, nE, VL, segL, aL, nLv, bl, nullptr, st);
 }
 
@@ -962,15 +1005,28 @@ __global__ void __launch_bounds__(128, 8) bdpt_shadow(BdLaunch P, BdStore B) {
         tmax = b.w;
         in_obj = false;
     };
+    const int n_pix = P.s.width * P.s.height;
     auto finish = [&](int i, const HitRec &h) {
+        if (i < 0 || i >= B.q_cap) {
+            bd_fail(B, 7, i);
+            return;
+        }
         const float tmax = B.q[3 * (size_t)i + 1].w;
         if (h.t > 0.0f && tmax - h.t > 1e-4f) return;
         const int dest = __float_as_int(B.q[3 * (size_t)i].w);
         const float4 c = B.q[3 * (size_t)i + 2];
         if (dest >= 0) {
+            if (dest >= B.slots * B.n) {
+                bd_fail(B, 8, i);
+                return;
+            }
             B.result[dest] = make_float4(c.x, c.y, c.z, 0.0f);
         } else {
             const int px = -1 - dest;
+            if (px >= n_pix) {
+                bd_fail(B, 9, i);
+                return;
+            }
             float *dst = P.light_film + (size_t)px * 3;
             (void)W;
             atomicAdd(dst + 0, c.z);
@@ -1092,9 +1148,10 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
         Q.q_count = (int *)w;
         Q.q_fetch = Q.q_count + 1;
         Q.overflow = Q.q_count + 2;
+        Q.err = Q.q_count + 3;
         Q.slots = slots;
         Q.q_cap = (int)q_cap;
-        cudaMemsetAsync(Q.overflow, 0, sizeof(int), stream);
+        cudaMemsetAsync(Q.overflow, 0, 3 * sizeof(int), stream);
     }
     const DevCamera &c = S.camera;
     B.right = mk3(c.m[0] + c.m[3], c.m[4] + c.m[7], c.m[8] + c.m[11]);
@@ -1148,13 +1205,14 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
     add_light_film<<<sc->num_sms * 4, 256, 0, stream>>>(film_dev, B.light_film, (size_t)total_pix * 3);
     if (timing) cudaEventRecord(e1, stream);
     unsigned long long h_nan = 0;
-    int h_overflow = 0;
+    int h_chk[3] = {0, 0, 0};  // overflow, first failed check, its index
     cudaMemcpyAsync(&h_nan, nan_count, sizeof(h_nan), cudaMemcpyDeviceToHost, stream);
-    if (staged) cudaMemcpyAsync(&h_overflow, Q.overflow, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (staged) cudaMemcpyAsync(h_chk, Q.overflow, sizeof(h_chk), cudaMemcpyDeviceToHost, stream);
     cudaError_t e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_status(e, "bdpt_render");
-    if (h_overflow) {  // cannot happen: the queue holds every strategy of every sample
-        set_error("bdpt_render: shadow queue overflow");
+    if (h_chk[0] || h_chk[1]) {  // neither can happen: the queue holds every strategy of every sample
+        set_error("bdpt_render: staged consistency check " + std::to_string(h_chk[1]) + " failed at " +
+                  std::to_string(h_chk[2]) + (h_chk[0] ? " (shadow queue overflow)" : ""));
         return RUMI_ERR_INTERNAL;
     }
     if (stats) {
