@@ -755,154 +755,198 @@ RUMI_D void load_vertex(const float4 *base, int n, int j, int k, BVert &v, float
     v.in_obj = (flags & BF_INOBJ) != 0;
 }
 
-// One slot of a warp-aggregated push (the calling lanes are the pushers).
-RUMI_D int bd_push_slot(int *counter) {
-    const unsigned act = __activemask();
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(act) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(counter, __popc(act));
-    base = __shfl_sync(act, base, leader);
-    return base + __popc(act & ((1u << lane) - 1u));
-}
+// One strategy of Trace's double loop (bidirectionalpathtracer.cpp:182-390): eye subpath
+// vertex t and light subpath vertex s = len - (t + 1).  Returns
+//   STRAT_NONE   nothing to add (rejected, or a skipped combination);
+//   STRAT_ADD    `lo` is added to the sample as it is (the eye subpath reached a light);
+//   STRAT_SHADOW `lo` counts once the shadow ray (o, dir, tmax) is unoccluded; t == 0 splats
+//                it onto film pixel `px`.
+// *stop: Trace leaves the t loop of this length here (t past the eye subpath, or an eye
+// vertex on a light).  VisibilityTest is the caller's.
+enum { STRAT_NONE = 0, STRAT_ADD = 1, STRAT_SHADOW = 2 };
 
-// Every (s, t) strategy of one sample (Trace's double loop, bidirectionalpathtracer.cpp:
-// 182-390).  STAGED = false: visibility traced here and the contributions summed into the
-// returned radiance, splats added to the light film.  STAGED = true: contributions go to
-// result slots / the shadow queue of B and the returned value is unused.
-template <int MAXV, bool STAGED>
-RUMI_D float3 connect_strategies(const BdLaunch &P, const BdStore &B, int j, const BVert *VE, const float3 *segE,
-                                 const float3 *aE, int nE, const BVert *VL, const float3 *segL, const float3 *aL,
-                                 int nLv, const BdLight &bl, int *stk, TraceStats &st) {
+struct StratOut {
+    float3 lo, o, dir;
+    float tmax;
+    int px;
+};
+
+template <int MAXV>
+RUMI_D int strategy(const BdLaunch &P, int j, int len, int t, const BVert *VE, const float3 *segE, const float3 *aE,
+                    int nE, const BVert *VL, const float3 *segL, const float3 *aL, int nLv, const DevLight &light,
+                    float3 light_n, bool &stop, StratOut &out) {
     const DevScene &S = P.s;
     const uint64_t path = (uint64_t)(P.path0 + j);
     const int W = S.width, H = S.height;
-    const DevLight light = S.lights[bl.li];
-    const float3 light_n = bl.n;
     const bool spot = light.type == LIGHT_SPOT;
+    if (t >= nE) {
+        stop = true;
+        return STRAT_NONE;
+    }
+    const BVert &tc = VE[t];
+    float3 t_wo = mk3(0, 0, 0);
+    if (t > 0) {
+        t_wo = -segE[t - 1];
+        if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
+            stop = true;
+            if (len == nE - 1) {
+                const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
+                out.lo = aE[t + 1] * w;
+                return STRAT_ADD;
+            }
+            return STRAT_NONE;
+        }
+        if (tc.dirac) return STRAT_NONE;
+    }
+    const int s = len - (t + 1);
+    if (s >= nLv || s <= -1) return STRAT_NONE;
+    const BVert &sc = VL[s];
+    float3 s_wi = mk3(0, 0, 0);
+    if (s > 0) {
+        s_wi = -segL[s - 1];
+        if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) return STRAT_NONE;
+        if (sc.dirac) return STRAT_NONE;
+    }
+    // the geometric rejections come before the two visibility tests: they read no random
+    // numbers and change nothing, so the order only saves traversals
+    const float3 cwi = normalize_ref(sc.p - tc.p);
+    const float3 cwo = normalize_ref(tc.p - sc.p);
+    const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
+    if (ci < 1e-4f) return STRAT_NONE;
+    float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
+    if (s == 0 && spot) {
+        if (dot3(cwo, light.direction) < light.cos_cone) return STRAT_NONE;  // outside the cone
+        co = 1.0f;                                                         // no cosine at a point
+    }
+    if (co < 1e-4f) return STRAT_NONE;
+    const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+    if (dist <= 0.0f) return STRAT_NONE;
+    const float G = ci * co / (dist * dist);
+    if (G <= 0.0f) return STRAT_NONE;
+    int film_w = 0, film_h = 0;
+    if (t == 0) {
+        if (!film_plane_pixel(P, sc.p, film_w, film_h)) return STRAT_NONE;
+        if (film_w == W || film_h == H) return STRAT_NONE;
+        if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) return STRAT_NONE;
+    }
+    // VolumetricTest reads its own uniform, so it may come before the visibility test
+    const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
+    if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) return STRAT_NONE;
+    float3 cE, cL;
+    if (t == 0) {
+        const DevCamera &c = S.camera;
+        const float cs = dot3(tc.n, cwi);
+        const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
+        cE = c3(We / avg3(tc.pdf_fwd));
+    } else if (tc.onsurface) {
+        cE = vert_fr(S, tc, tc.n, cwi, t_wo) / (tc.pdf_fwd * tc.pdf_path);
+    } else {
+        cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
+    }
+    // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
+    // 350-351): a medium vertex takes the texture of the surface its segment was headed
+    // for, evaluated at the medium point; none without such a surface
+    if (t > 0 && S.prim_tex && tc.prim >= 0) cE = cE * tex_pattern(S, tc.prim, tc.p);
+    if (s == 0) {
+        cL = light_emission(light) / sc.pdf_fwd;
+    } else if (sc.onsurface) {
+        cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
+    } else {
+        cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
+    }
+    if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
+    const float3 lo = aE[t] * cE * G * cL * aL[s];
+    out.lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
+    // the shadow ray of VisibilityTest (:1018-1050): from the eye vertex unless the eye
+    // vertex is the camera
+    if (t == 0) {
+        out.o = sc.p;
+        out.dir = normalize_ref(tc.p - sc.p);
+    } else {
+        out.o = tc.p;
+        out.dir = normalize_ref(sc.p - tc.p);
+    }
+    out.tmax = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+    out.px = t == 0 ? film_h * W + film_w : -1;
+    return STRAT_SHADOW;
+}
+
+// Every strategy of one sample in Trace's order, visibility traced by this thread; splats
+// go to the light film.  Returns the sample's radiance.
+template <int MAXV>
+RUMI_D float3 connect_strategies(const BdLaunch &P, int j, const BVert *VE, const float3 *segE, const float3 *aE,
+                                 int nE, const BVert *VL, const float3 *segL, const float3 *aL, int nLv,
+                                 const BdLight &bl, int *stk, TraceStats &st) {
+    const DevScene &S = P.s;
+    const DevLight light = S.lights[bl.li];
     float3 L = mk3(0, 0, 0);
     const int max_len = nE + nLv - 1;
     for (int len = 1; len <= max_len; ++len) {
         for (int t = 0; t <= len; ++t) {
-            if (t >= nE) break;
-            const int slot = (len - 1) * P.nE + t;
-            const BVert &tc = VE[t];
-            float3 t_wo = mk3(0, 0, 0);
-            if (t > 0) {
-                t_wo = -segE[t - 1];
-                if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
-                    if (len == nE - 1) {
-                        const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
-                        const float3 c = aE[t + 1] * w;
-                        if (STAGED) {
-                            if (slot < 0 || slot >= B.slots)
-                                bd_fail(B, 5, j);
-                            else
-                                B.result[(size_t)slot * B.n + j] = make_float4(c.x, c.y, c.z, 0.0f);
-                        } else
-                            L = L + c;
+            bool stop = false;
+            StratOut out;
+            const int r = strategy<MAXV>(P, j, len, t, VE, segE, aE, nE, VL, segL, aL, nLv, light, bl.n, stop, out);
+            if (r == STRAT_ADD) {
+                L = L + out.lo;
+            } else if (r == STRAT_SHADOW) {
+                const HitRec h = trace_ray<true, BD_STACK, false>(S, out.o, out.dir, out.tmax, false, stk, BD_THREADS, st);
+                if (!(h.t > 0.0f && out.tmax - h.t > 1e-4f)) {
+                    if (out.px >= 0) {
+                        float *dst = P.light_film + (size_t)out.px * 3;
+                        atomicAdd(dst + 0, out.lo.z);
+                        atomicAdd(dst + 1, out.lo.y);
+                        atomicAdd(dst + 2, out.lo.x);
+                    } else {
+                        L = L + out.lo;
                     }
-                    break;
                 }
-                if (tc.dirac) continue;
             }
-            const int s = len - (t + 1);
-            if (s >= nLv || s <= -1) continue;
-            const BVert &sc = VL[s];
-            float3 s_wi = mk3(0, 0, 0);
-            if (s > 0) {
-                s_wi = -segL[s - 1];
-                if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) continue;
-                if (sc.dirac) continue;
-            }
-            // the geometric rejections come before the two visibility tests: they read no
-            // random numbers and change nothing, so the order only saves traversals
-            const float3 cwi = normalize_ref(sc.p - tc.p);
-            const float3 cwo = normalize_ref(tc.p - sc.p);
-            const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
-            if (ci < 1e-4f) continue;
-            float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
-            if (s == 0 && spot) {
-                if (dot3(cwo, light.direction) < light.cos_cone) continue;  // outside the cone
-                co = 1.0f;                                                 // no cosine at a point
-            }
-            if (co < 1e-4f) continue;
-            const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
-            if (dist <= 0.0f) continue;
-            const float G = ci * co / (dist * dist);
-            if (G <= 0.0f) continue;
-            int film_w = 0, film_h = 0;
-            if (t == 0) {
-                if (!film_plane_pixel(P, sc.p, film_w, film_h)) continue;
-                if (film_w == W || film_h == H) continue;
-                if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) continue;
-            }
-            if (!STAGED && !visible(S, s + 1, t + 1, sc.p, tc.p, stk, st)) continue;
-            // VolumetricTest reads its own uniform, so it may come before the visibility
-            // test the staged form defers
-            const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
-            if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) continue;
-            float3 cE, cL;
-            if (t == 0) {
-                const DevCamera &c = S.camera;
-                const float cs = dot3(tc.n, cwi);
-                const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
-                cE = c3(We / avg3(tc.pdf_fwd));
-            } else if (tc.onsurface) {
-                cE = vert_fr(S, tc, tc.n, cwi, t_wo) / (tc.pdf_fwd * tc.pdf_path);
-            } else {
-                cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
-            }
-            // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
-            // 350-351): a medium vertex takes the texture of the surface its segment was
-            // headed for, evaluated at the medium point; none without such a surface
-            if (t > 0 && S.prim_tex && tc.prim >= 0) cE = cE * tex_pattern(S, tc.prim, tc.p);
-            if (s == 0) {
-                cL = light_emission(light) / sc.pdf_fwd;
-            } else if (sc.onsurface) {
-                cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
-            } else {
-                cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
-            }
-            if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
-            float3 lo = aE[t] * cE * G * cL * aL[s];
-            lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
-            if (STAGED) {
-                // the shadow ray VisibilityTest would trace (from the eye vertex unless it
-                // is the camera), with what the strategy adds when nothing blocks it
-                float3 o, dir;
-                if (t == 0) {
-                    o = sc.p;
-                    dir = normalize_ref(tc.p - sc.p);
-                } else {
-                    o = tc.p;
-                    dir = normalize_ref(sc.p - tc.p);
-                }
-                const float tmax = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
-                const int dest = t == 0 ? -1 - (film_h * W + film_w) : slot * B.n + j;
-                if (t > 0 && (slot < 0 || slot >= B.slots)) {
-                    bd_fail(B, 6, j);
-                    continue;
-                }
-                const int qi = bd_push_slot(B.q_count);
-                if (qi < B.q_cap) {
-                    B.q[3 * (size_t)qi + 0] = make_float4(o.x, o.y, o.z, __int_as_float(dest));
-                    B.q[3 * (size_t)qi + 1] = make_float4(dir.x, dir.y, dir.z, tmax);
-                    B.q[3 * (size_t)qi + 2] = make_float4(lo.x, lo.y, lo.z, 0.0f);
-                } else {
-                    atomicExch(B.overflow, 1);
-                }
-            } else if (t == 0) {
-                float *dst = P.light_film + ((size_t)film_h * W + film_w) * 3;
-                atomicAdd(dst + 0, lo.z);
-                atomicAdd(dst + 1, lo.y);
-                atomicAdd(dst + 2, lo.x);
-            } else {
-                L = L + lo;
-            }
+            if (stop) break;
         }
     }
     return L;
+}
+
+// The staged form of the same loop: the warp walks the (length, t) grid of the largest
+// subpaths in step (lanes past their own subpaths do nothing), so every shadow-queue push
+// happens at one point of the loop for all 32 lanes -- a full-warp ballot hands out the
+// slots.  Added terms go to their result slot (length - 1) * nE + t.
+template <int MAXV>
+RUMI_D void connect_strategies_staged(const BdLaunch &P, const BdStore &B, int j, bool valid, const BVert *VE,
+                                      const float3 *segE, const float3 *aE, int nE, const BVert *VL,
+                                      const float3 *segL, const float3 *aL, int nLv, const BdLight &bl) {
+    const DevScene &S = P.s;
+    const DevLight light = valid ? S.lights[bl.li] : S.lights[0];
+    const int lane = threadIdx.x & 31;
+    const int max_len = P.nE + P.nL - 1;  // the longest any sample can reach
+    for (int len = 1; len <= max_len; ++len) {
+        bool stop = !valid || len > nE + nLv - 1;
+        for (int t = 0; t < P.nE && t <= len; ++t) {
+            int r = STRAT_NONE;
+            StratOut out;
+            if (!stop) r = strategy<MAXV>(P, j, len, t, VE, segE, aE, nE, VL, segL, aL, nLv, light, bl.n, stop, out);
+            const int slot = (len - 1) * P.nE + t;
+            if (r == STRAT_ADD) B.result[(size_t)slot * B.n + j] = make_float4(out.lo.x, out.lo.y, out.lo.z, 0.0f);
+            // every lane of the warp reaches this point in every iteration
+            const bool push = r == STRAT_SHADOW;
+            const unsigned m = __ballot_sync(0xffffffffu, push);
+            if (m == 0u) continue;
+            int base = 0;
+            if (lane == 0) base = atomicAdd(B.q_count, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (push) {
+                const int qi = base + __popc(m & ((1u << lane) - 1u));
+                const int dest = out.px >= 0 ? -1 - out.px : slot * B.n + j;
+                if (qi < B.q_cap) {
+                    B.q[3 * (size_t)qi + 0] = make_float4(out.o.x, out.o.y, out.o.z, __int_as_float(dest));
+                    B.q[3 * (size_t)qi + 1] = make_float4(out.dir.x, out.dir.y, out.dir.z, out.tmax);
+                    B.q[3 * (size_t)qi + 2] = make_float4(out.lo.x, out.lo.y, out.lo.z, 0.0f);
+                } else {
+                    atomicExch(B.overflow, 1);
+                }
+            }
+        }
+    }
 }
 
 // One thread renders one camera sample: both subpaths and every strategy.
@@ -917,8 +961,7 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
     float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
     int nE, nLv;
     const BdLight bl = build_subpaths<MAXV>(P, j, VE, segE, aE, VL, segL, aL, nE, nLv, stk, st);
-    BdStore none;
-    const float3 L = connect_strategies<MAXV, false>(P, none, j, VE, segE, aE, nE, VL, segL, aL, nLv, bl, stk, st);
+    const float3 L = connect_strategies<MAXV>(P, j, VE, segE, aE, nE, VL, segL, aL, nLv, bl, stk, st);
     P.L[j] = make_float4(L.x, L.y, L.z, 0.0f);
 }
 
@@ -947,49 +990,54 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_subpaths(BdLaunch P, BdStore 
     B.light[j] = make_float4(bl.n.x, bl.n.y, bl.n.z, __int_as_float(bl.li));
 }
 
+// Every lane of a warp stays to the end (the staged strategy loop votes with the whole
+// warp); lanes without a sample, or whose sample failed a check, take part without work.
 template <int MAXV>
 __global__ void __launch_bounds__(BD_THREADS) bdpt_connect(BdLaunch P, BdStore B) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.n_paths) return;
-    TraceStats st{0, 0};
+    bool valid = j < P.n_paths;
     const int n = B.n;
-    const int2 cnt = B.counts[j];
-    const int nE = cnt.x, nLv = cnt.y;
-    if (nE < 1 || nE > MAXV || nLv < 1 || nLv > MAXV) {
-        bd_fail(B, 2, j);
-        return;
+    int nE = 1, nLv = 1;
+    if (valid) {
+        const int2 cnt = B.counts[j];
+        nE = cnt.x;
+        nLv = cnt.y;
+        if (nE < 1 || nE > MAXV || nLv < 1 || nLv > MAXV) {
+            bd_fail(B, 2, j);
+            valid = false;
+            nE = nLv = 1;
+        }
     }
     BVert VE[MAXV], VL[MAXV];
     float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
-    for (int k = 0; k < nE; ++k) load_vertex<MAXV>(B.ev, n, j, k, VE[k], segE[k]);
-    for (int k = 0; k < nLv; ++k) load_vertex<MAXV>(B.lv, n, j, k, VL[k], segL[k]);
-    // the one-thread form leaves the vertex after the last one cleared (its loop clears
-    // it before the segment that ends the subpath), and MISWeight's "locked" test reads
-    // VE[1] even when the eye subpath is the camera alone
-    for (int k = nE; k < MAXV; ++k) bvert_clear(VE[k]);
-    for (int k = nLv; k < MAXV; ++k) bvert_clear(VL[k]);
-    const int n_mat = P.s.n_materials;
-    for (int k = 1; k < nE; ++k)
-        if (VE[k].onsurface && (VE[k].mat < 0 || VE[k].mat >= n_mat)) {
-            bd_fail(B, 4, j);
-            return;
-        }
-    for (int k = 1; k < nLv; ++k)
-        if (VL[k].onsurface && (VL[k].mat < 0 || VL[k].mat >= n_mat)) {
-            bd_fail(B, 4, j);
-            return;
-        }
-    for (int k = 0; k <= nE && k < MAXV + 2; ++k) aE[k] = f4xyz(B.ea[(size_t)k * n + j]);
-    for (int k = 0; k < nLv; ++k) aL[k] = f4xyz(B.la[(size_t)k * n + j]);
-    const float4 l4 = B.light[j];
     BdLight bl;
-    bl.n = f4xyz(l4);
-    bl.li = __float_as_int(l4.w);
-    if (bl.li < 0 || bl.li >= P.s.n_lights) {
-        bd_fail(B, 3, j);
-        return;
+    bl.li = 0;
+    bl.n = mk3(0, 0, 0);
+    if (valid) {
+        for (int k = 0; k < nE; ++k) load_vertex<MAXV>(B.ev, n, j, k, VE[k], segE[k]);
+        for (int k = 0; k < nLv; ++k) load_vertex<MAXV>(B.lv, n, j, k, VL[k], segL[k]);
+        // the one-thread form leaves the vertex after the last one cleared (its loop clears
+        // it before the segment that ends the subpath), and MISWeight's "locked" test reads
+        // VE[1] even when the eye subpath is the camera alone
+        for (int k = nE; k < MAXV; ++k) bvert_clear(VE[k]);
+        for (int k = nLv; k < MAXV; ++k) bvert_clear(VL[k]);
+        const int n_mat = P.s.n_materials;
+        for (int k = 1; k < nE; ++k)
+            if (VE[k].onsurface && (VE[k].mat < 0 || VE[k].mat >= n_mat)) valid = false;
+        for (int k = 1; k < nLv; ++k)
+            if (VL[k].onsurface && (VL[k].mat < 0 || VL[k].mat >= n_mat)) valid = false;
+        if (!valid) bd_fail(B, 4, j);
+        for (int k = 0; k <= nE && k < MAXV + 2; ++k) aE[k] = f4xyz(B.ea[(size_t)k * n + j]);
+        for (int k = 0; k < nLv; ++k) aL[k] = f4xyz(B.la[(size_t)k * n + j]);
+        const float4 l4 = B.light[j];
+        bl.n = f4xyz(l4);
+        bl.li = __float_as_int(l4.w);
+        if (valid && (bl.li < 0 || bl.li >= P.s.n_lights)) {
+            bd_fail(B, 3, j);
+            valid = false;
+        }
     }
-    connect_strategies<MAXV, true>(P, B, j, VE, segE, aE, nE, VL, segL, aL, nLv, bl, nullptr, st);
+    connect_strategies_staged<MAXV>(P, B, valid ? j : 0, valid, VE, segE, aE, nE, VL, segL, aL, nLv, bl);
 }
 
 // VisibilityTest for the queued strategies: blocked when something lies more than 1e-4
