@@ -603,25 +603,23 @@ RUMI_D bool volumetric_ok(const DevVolume &V, float3 sp, float3 tp, float xi) {
     return !(xi < 1.0f - expf(avg3(V.sigma_t) * -sm));
 }
 
-// The light a sample picked and its sampled point (Scene::LightsUniformSampling +
-// AreaLight::SolidAngleSampling's position).
-struct BdLight {
-    int li;
-    float3 n;
-};
-
-// Both subpaths of camera sample j (ConstructViewPath / ConstructLightPath with their
-// starts, bidirectionalpathtracer.cpp:121-180).  Returns the light; nE / nLv receive the
-// vertex counts.
 template <int MAXV>
-RUMI_D BdLight build_subpaths(const BdLaunch &P, int j, BVert *VE, float3 *segE, float3 *aE, BVert *VL, float3 *segL,
-                              float3 *aL, int &nE, int &nLv, int *stk, TraceStats &st) {
+__global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
+    __shared__ int stack[BD_STACK * BD_THREADS];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_paths) return;
     const DevScene &S = P.s;
     const uint64_t path = (uint64_t)(P.path0 + j);
     const long long pixel = (long long)P.pix0 + j / P.spp;
     const int sidx = j % P.spp;
     const int W = S.width, H = S.height;
     const int pw_ = (int)(pixel % W), ph_ = (int)(pixel / W);
+    TraceStats st{0, 0};
+    int *stk = stack + threadIdx.x;
+
+    BVert VE[MAXV], VL[MAXV];
+    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
+    // Scene::LightsUniformSampling + AreaLight::SolidAngleSampling
     const Uniform4 UL = path_uniforms(path, 1000u, 0, P.k0, P.k1);
     const Uniform4 UD = path_uniforms(path, 1000u, 1, P.k0, P.k1);
     const int li = pick_light(S, UL.u[0]);
@@ -652,7 +650,7 @@ RUMI_D BdLight build_subpaths(const BdLaunch &P, int j, BVert *VE, float3 *segE,
         VE[0].pdf_dir = c.plane_dist * c.plane_dist / (l.z * l.z * l.z * c.film_area);
         VE[0].pdf_fwd = c3(1.0f);
     }
-    nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
+    const int nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
     // light subpath start: cosine-weighted emission from an area light
     // (AreaLight::SolidAngleSampling), uniform in the cone from a spot
     const bool spot = light.type == LIGHT_SPOT;
@@ -671,432 +669,99 @@ RUMI_D BdLight build_subpaths(const BdLaunch &P, int j, BVert *VE, float3 *segE,
         VL[0].pdf_dir = emit.pdf;
         VL[0].cos_a = dot3(emit.wi, light_n);
     }
-    nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit_w, VL, segL, aL, light, light_n, stk, st);
+    const int nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit_w, VL, segL, aL, light, light_n, stk, st);
     // a delta position: the strategies in which the eye subpath reaches the light carry
     // no weight (the MIS sums skip a dirac first light vertex)
     if (spot) VL[0].dirac = true;
-    BdLight bl;
-    bl.li = li;
-    bl.n = light_n;
-    return bl;
-}
 
-// ------------------------------------------------------------ staged form
-// The staged form splits a wave of camera samples into
-//   bdpt_subpaths  both subpaths of every sample -> vertex store (SoA, coalesced by sample)
-//   bdpt_connect   every (s, t) strategy: contribution and MIS weight; the strategies that
-//                  need a visibility test become shadow-queue entries, the others are
-//                  written to their result slot at once
-//   bdpt_shadow    the shadow queue through the persistent any-hit walk; an unoccluded
-//                  entry writes its result slot (or splats, t = 0)
-//   bdpt_resolve   per sample, the result slots summed in the reference's strategy order
-// so the sums equal the one-thread form's, and the visibility rays -- most of BDPT's rays
-// -- run through the same traversal kernels as the path tracer's.
-//
-// Vertex store: six float4 per vertex, field f of vertex k of sample j at
-// [(f * MAXV + k) * n + j]:
-//   0: p, xi   1: n, pdf_path   2: pdf_fwd, t_in   3: pdf_bwd, material
-//   4: vtau / vpdf, primitive   5: direction of the segment to the next vertex, flags
-struct BdStore {
-    float4 *ev, *lv;        // eye / light vertices
-    float4 *ea, *la;        // throughputs: [k * n + j], k < MAXV + 2
-    int2 *counts;           // (eye vertices, light vertices)
-    float4 *light;          // (light normal, light index)
-    float4 *result;         // [slot * n + j]: each strategy's contribution (0 when rejected)
-    float4 *q;              // shadow queue: 3 float4 per entry
-    int *q_count;           // entries pushed
-    int *q_fetch;           // the any-hit walk's fetch counter
-    int *overflow;          // set when a push found the queue full
-    int *err;               // [0]: first failed consistency check (0 = none), [1]: its index
-    int n, slots, q_cap;
-};
-
-// Records the first failed consistency check of the staged kernels; the caller then
-// skips the access it guarded.
-RUMI_D void bd_fail(const BdStore &B, int code, int index) {
-    if (atomicCAS(B.err, 0, code) == 0) B.err[1] = index;
-}
-
-enum { BF_DIRAC = 1, BF_SURF = 2, BF_INOBJ = 4 };
-
-template <int MAXV>
-RUMI_D void store_vertex(float4 *base, int n, int j, int k, const BVert &v, float3 seg) {
-    const int flags = (v.dirac ? BF_DIRAC : 0) | (v.onsurface ? BF_SURF : 0) | (v.in_obj ? BF_INOBJ : 0);
-    const float3 ratio = v.vtau / v.vpdf;
-    base[(0 * MAXV + k) * (size_t)n + j] = make_float4(v.p.x, v.p.y, v.p.z, v.xi);
-    base[(1 * MAXV + k) * (size_t)n + j] = make_float4(v.n.x, v.n.y, v.n.z, v.pdf_path);
-    base[(2 * MAXV + k) * (size_t)n + j] = make_float4(v.pdf_fwd.x, v.pdf_fwd.y, v.pdf_fwd.z, v.t_in);
-    base[(3 * MAXV + k) * (size_t)n + j] = make_float4(v.pdf_bwd.x, v.pdf_bwd.y, v.pdf_bwd.z, __int_as_float(v.mat));
-    base[(4 * MAXV + k) * (size_t)n + j] = make_float4(ratio.x, ratio.y, ratio.z, __int_as_float(v.prim));
-    base[(5 * MAXV + k) * (size_t)n + j] = make_float4(seg.x, seg.y, seg.z, __int_as_float(flags));
-}
-
-template <int MAXV>
-RUMI_D void load_vertex(const float4 *base, int n, int j, int k, BVert &v, float3 &seg) {
-    const float4 f0 = base[(0 * MAXV + k) * (size_t)n + j], f1 = base[(1 * MAXV + k) * (size_t)n + j];
-    const float4 f2 = base[(2 * MAXV + k) * (size_t)n + j], f3 = base[(3 * MAXV + k) * (size_t)n + j];
-    const float4 f4 = base[(4 * MAXV + k) * (size_t)n + j], f5 = base[(5 * MAXV + k) * (size_t)n + j];
-    bvert_clear(v);
-    v.p = f4xyz(f0);
-    v.xi = f0.w;
-    v.n = f4xyz(f1);
-    v.pdf_path = f1.w;
-    v.pdf_fwd = f4xyz(f2);
-    v.t_in = f2.w;
-    v.pdf_bwd = f4xyz(f3);
-    v.mat = __float_as_int(f3.w);
-    v.vtau = f4xyz(f4);  // vtau / vpdf, with vpdf 1: Material::Fr reads only the ratio
-    v.vpdf = c3(1.0f);
-    v.prim = __float_as_int(f4.w);
-    seg = f4xyz(f5);
-    const int flags = __float_as_int(f5.w);
-    v.dirac = (flags & BF_DIRAC) != 0;
-    v.onsurface = (flags & BF_SURF) != 0;
-    v.in_obj = (flags & BF_INOBJ) != 0;
-}
-
-// One strategy of Trace's double loop (bidirectionalpathtracer.cpp:182-390): eye subpath
-// vertex t and light subpath vertex s = len - (t + 1).  Returns
-//   STRAT_NONE   nothing to add (rejected, or a skipped combination);
-//   STRAT_ADD    `lo` is added to the sample as it is (the eye subpath reached a light);
-//   STRAT_SHADOW `lo` counts once the shadow ray (o, dir, tmax) is unoccluded; t == 0 splats
-//                it onto film pixel `px`.
-// *stop: Trace leaves the t loop of this length here (t past the eye subpath, or an eye
-// vertex on a light).  VisibilityTest is the caller's.
-enum { STRAT_NONE = 0, STRAT_ADD = 1, STRAT_SHADOW = 2 };
-
-struct StratOut {
-    float3 lo, o, dir;
-    float tmax;
-    int px;
-};
-
-template <int MAXV>
-RUMI_D int strategy(const BdLaunch &P, int j, int len, int t, const BVert *VE, const float3 *segE, const float3 *aE,
-                    int nE, const BVert *VL, const float3 *segL, const float3 *aL, int nLv, const DevLight &light,
-                    float3 light_n, bool &stop, StratOut &out) {
-    const DevScene &S = P.s;
-    const uint64_t path = (uint64_t)(P.path0 + j);
-    const int W = S.width, H = S.height;
-    const bool spot = light.type == LIGHT_SPOT;
-    if (t >= nE) {
-        stop = true;
-        return STRAT_NONE;
-    }
-    const BVert &tc = VE[t];
-    float3 t_wo = mk3(0, 0, 0);
-    if (t > 0) {
-        t_wo = -segE[t - 1];
-        if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
-            stop = true;
-            if (len == nE - 1) {
-                const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
-                out.lo = aE[t + 1] * w;
-                return STRAT_ADD;
-            }
-            return STRAT_NONE;
-        }
-        if (tc.dirac) return STRAT_NONE;
-    }
-    const int s = len - (t + 1);
-    if (s >= nLv || s <= -1) return STRAT_NONE;
-    const BVert &sc = VL[s];
-    float3 s_wi = mk3(0, 0, 0);
-    if (s > 0) {
-        s_wi = -segL[s - 1];
-        if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) return STRAT_NONE;
-        if (sc.dirac) return STRAT_NONE;
-    }
-    // the geometric rejections come before the two visibility tests: they read no random
-    // numbers and change nothing, so the order only saves traversals
-    const float3 cwi = normalize_ref(sc.p - tc.p);
-    const float3 cwo = normalize_ref(tc.p - sc.p);
-    const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
-    if (ci < 1e-4f) return STRAT_NONE;
-    float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
-    if (s == 0 && spot) {
-        if (dot3(cwo, light.direction) < light.cos_cone) return STRAT_NONE;  // outside the cone
-        co = 1.0f;                                                         // no cosine at a point
-    }
-    if (co < 1e-4f) return STRAT_NONE;
-    const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
-    if (dist <= 0.0f) return STRAT_NONE;
-    const float G = ci * co / (dist * dist);
-    if (G <= 0.0f) return STRAT_NONE;
-    int film_w = 0, film_h = 0;
-    if (t == 0) {
-        if (!film_plane_pixel(P, sc.p, film_w, film_h)) return STRAT_NONE;
-        if (film_w == W || film_h == H) return STRAT_NONE;
-        if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) return STRAT_NONE;
-    }
-    // VolumetricTest reads its own uniform, so it may come before the visibility test
-    const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
-    if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) return STRAT_NONE;
-    float3 cE, cL;
-    if (t == 0) {
-        const DevCamera &c = S.camera;
-        const float cs = dot3(tc.n, cwi);
-        const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
-        cE = c3(We / avg3(tc.pdf_fwd));
-    } else if (tc.onsurface) {
-        cE = vert_fr(S, tc, tc.n, cwi, t_wo) / (tc.pdf_fwd * tc.pdf_path);
-    } else {
-        cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
-    }
-    // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
-    // 350-351): a medium vertex takes the texture of the surface its segment was headed
-    // for, evaluated at the medium point; none without such a surface
-    if (t > 0 && S.prim_tex && tc.prim >= 0) cE = cE * tex_pattern(S, tc.prim, tc.p);
-    if (s == 0) {
-        cL = light_emission(light) / sc.pdf_fwd;
-    } else if (sc.onsurface) {
-        cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
-    } else {
-        cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
-    }
-    if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
-    const float3 lo = aE[t] * cE * G * cL * aL[s];
-    out.lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
-    // the shadow ray of VisibilityTest (:1018-1050): from the eye vertex unless the eye
-    // vertex is the camera
-    if (t == 0) {
-        out.o = sc.p;
-        out.dir = normalize_ref(tc.p - sc.p);
-    } else {
-        out.o = tc.p;
-        out.dir = normalize_ref(sc.p - tc.p);
-    }
-    out.tmax = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
-    out.px = t == 0 ? film_h * W + film_w : -1;
-    return STRAT_SHADOW;
-}
-
-// Every strategy of one sample in Trace's order, visibility traced by this thread; splats
-// go to the light film.  Returns the sample's radiance.
-template <int MAXV>
-RUMI_D float3 connect_strategies(const BdLaunch &P, int j, const BVert *VE, const float3 *segE, const float3 *aE,
-                                 int nE, const BVert *VL, const float3 *segL, const float3 *aL, int nLv,
-                                 const BdLight &bl, int *stk, TraceStats &st) {
-    const DevScene &S = P.s;
-    const DevLight light = S.lights[bl.li];
     float3 L = mk3(0, 0, 0);
     const int max_len = nE + nLv - 1;
     for (int len = 1; len <= max_len; ++len) {
         for (int t = 0; t <= len; ++t) {
-            bool stop = false;
-            StratOut out;
-            const int r = strategy<MAXV>(P, j, len, t, VE, segE, aE, nE, VL, segL, aL, nLv, light, bl.n, stop, out);
-            if (r == STRAT_ADD) {
-                L = L + out.lo;
-            } else if (r == STRAT_SHADOW) {
-                const HitRec h = trace_ray<true, BD_STACK, false>(S, out.o, out.dir, out.tmax, false, stk, BD_THREADS, st);
-                if (!(h.t > 0.0f && out.tmax - h.t > 1e-4f)) {
-                    if (out.px >= 0) {
-                        float *dst = P.light_film + (size_t)out.px * 3;
-                        atomicAdd(dst + 0, out.lo.z);
-                        atomicAdd(dst + 1, out.lo.y);
-                        atomicAdd(dst + 2, out.lo.x);
-                    } else {
-                        L = L + out.lo;
+            if (t >= nE) break;
+            const BVert &tc = VE[t];
+            float3 t_wo = mk3(0, 0, 0);
+            if (t > 0) {
+                t_wo = -segE[t - 1];
+                if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
+                    if (len == nE - 1) {
+                        const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
+                        L = L + aE[t + 1] * w;
                     }
+                    break;
                 }
+                if (tc.dirac) continue;
             }
-            if (stop) break;
-        }
-    }
-    return L;
-}
-
-// The staged form of the same loop: the warp walks the (length, t) grid of the largest
-// subpaths in step (lanes past their own subpaths do nothing), so every shadow-queue push
-// happens at one point of the loop for all 32 lanes -- a full-warp ballot hands out the
-// slots.  Added terms go to their result slot (length - 1) * nE + t.
-template <int MAXV>
-RUMI_D void connect_strategies_staged(const BdLaunch &P, const BdStore &B, int j, bool valid, const BVert *VE,
-                                      const float3 *segE, const float3 *aE, int nE, const BVert *VL,
-                                      const float3 *segL, const float3 *aL, int nLv, const BdLight &bl) {
-    const DevScene &S = P.s;
-    const DevLight light = valid ? S.lights[bl.li] : S.lights[0];
-    const int lane = threadIdx.x & 31;
-    const int max_len = P.nE + P.nL - 1;  // the longest any sample can reach
-    for (int len = 1; len <= max_len; ++len) {
-        bool stop = !valid || len > nE + nLv - 1;
-        for (int t = 0; t < P.nE && t <= len; ++t) {
-            int r = STRAT_NONE;
-            StratOut out;
-            if (!stop) r = strategy<MAXV>(P, j, len, t, VE, segE, aE, nE, VL, segL, aL, nLv, light, bl.n, stop, out);
-            const int slot = (len - 1) * P.nE + t;
-            if (r == STRAT_ADD) B.result[(size_t)slot * B.n + j] = make_float4(out.lo.x, out.lo.y, out.lo.z, 0.0f);
-            // every lane of the warp reaches this point in every iteration
-            const bool push = r == STRAT_SHADOW;
-            const unsigned m = __ballot_sync(0xffffffffu, push);
-            if (m == 0u) continue;
-            int base = 0;
-            if (lane == 0) base = atomicAdd(B.q_count, __popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (push) {
-                const int qi = base + __popc(m & ((1u << lane) - 1u));
-                const int dest = out.px >= 0 ? -1 - out.px : slot * B.n + j;
-                if (qi < B.q_cap) {
-                    B.q[3 * (size_t)qi + 0] = make_float4(out.o.x, out.o.y, out.o.z, __int_as_float(dest));
-                    B.q[3 * (size_t)qi + 1] = make_float4(out.dir.x, out.dir.y, out.dir.z, out.tmax);
-                    B.q[3 * (size_t)qi + 2] = make_float4(out.lo.x, out.lo.y, out.lo.z, 0.0f);
-                } else {
-                    atomicExch(B.overflow, 1);
-                }
+            const int s = len - (t + 1);
+            if (s >= nLv || s <= -1) continue;
+            const BVert &sc = VL[s];
+            float3 s_wi = mk3(0, 0, 0);
+            if (s > 0) {
+                s_wi = -segL[s - 1];
+                if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) continue;
+                if (sc.dirac) continue;
+            }
+            // the geometric rejections come before the two visibility tests: they read no
+            // random numbers and change nothing, so the order only saves traversals
+            const float3 cwi = normalize_ref(sc.p - tc.p);
+            const float3 cwo = normalize_ref(tc.p - sc.p);
+            const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
+            if (ci < 1e-4f) continue;
+            float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
+            if (s == 0 && spot) {
+                if (dot3(cwo, light.direction) < light.cos_cone) continue;  // outside the cone
+                co = 1.0f;                                                 // no cosine at a point
+            }
+            if (co < 1e-4f) continue;
+            const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+            if (dist <= 0.0f) continue;
+            const float G = ci * co / (dist * dist);
+            if (G <= 0.0f) continue;
+            int film_w = 0, film_h = 0;
+            if (t == 0) {
+                if (!film_plane_pixel(P, sc.p, film_w, film_h)) continue;
+                if (film_w == W || film_h == H) continue;
+                if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) continue;
+            }
+            if (!visible(S, s + 1, t + 1, sc.p, tc.p, stk, st)) continue;
+            const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
+            if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) continue;
+            float3 cE, cL;
+            if (t == 0) {
+                const DevCamera &c = S.camera;
+                const float cs = dot3(tc.n, cwi);
+                const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
+                cE = c3(We / avg3(tc.pdf_fwd));
+            } else if (tc.onsurface) {
+                cE = vert_fr(S, tc, tc.n, cwi, t_wo) / (tc.pdf_fwd * tc.pdf_path);
+            } else {
+                cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
+            }
+            // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
+            // 350-351): a medium vertex takes the texture of the surface its segment was
+            // headed for, evaluated at the medium point; none without such a surface
+            if (t > 0 && S.prim_tex && tc.prim >= 0) cE = cE * tex_pattern(S, tc.prim, tc.p);
+            if (s == 0) {
+                cL = light_emission(light) / sc.pdf_fwd;
+            } else if (sc.onsurface) {
+                cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
+            } else {
+                cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
+            }
+            if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
+            if (t == 0) {
+                float3 lo = aE[t] * cE * G * cL * aL[s];
+                lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n, light);
+                float *dst = P.light_film + ((size_t)film_h * W + film_w) * 3;
+                atomicAdd(dst + 0, lo.z);
+                atomicAdd(dst + 1, lo.y);
+                atomicAdd(dst + 2, lo.x);
+            } else {
+                float3 lo = aE[t] * cE * G * cL * aL[s];
+                lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
+                L = L + lo;
             }
         }
-    }
-}
-
-// One thread renders one camera sample: both subpaths and every strategy.
-template <int MAXV>
-__global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
-    __shared__ int stack[BD_STACK * BD_THREADS];
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.n_paths) return;
-    TraceStats st{0, 0};
-    int *stk = stack + threadIdx.x;
-    BVert VE[MAXV], VL[MAXV];
-    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
-    int nE, nLv;
-    const BdLight bl = build_subpaths<MAXV>(P, j, VE, segE, aE, VL, segL, aL, nE, nLv, stk, st);
-    const float3 L = connect_strategies<MAXV>(P, j, VE, segE, aE, nE, VL, segL, aL, nLv, bl, stk, st);
-    P.L[j] = make_float4(L.x, L.y, L.z, 0.0f);
-}
-
-template <int MAXV>
-__global__ void __launch_bounds__(BD_THREADS) bdpt_subpaths(BdLaunch P, BdStore B) {
-    __shared__ int stack[BD_STACK * BD_THREADS];
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.n_paths) return;
-    TraceStats st{0, 0};
-    BVert VE[MAXV], VL[MAXV];
-    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
-    int nE, nLv;
-    const BdLight bl = build_subpaths<MAXV>(P, j, VE, segE, aE, VL, segL, aL, nE, nLv, stack + threadIdx.x, st);
-    const int n = B.n;
-    if (nE < 1 || nE > MAXV || nLv < 1 || nLv > MAXV || bl.li < 0 || bl.li >= P.s.n_lights || j >= n) {
-        bd_fail(B, 1, j);
-        B.counts[j] = make_int2(0, 0);
-        return;
-    }
-    for (int k = 0; k < nE; ++k) store_vertex<MAXV>(B.ev, n, j, k, VE[k], k + 1 < nE ? segE[k] : mk3(0, 0, 0));
-    for (int k = 0; k < nLv; ++k) store_vertex<MAXV>(B.lv, n, j, k, VL[k], k + 1 < nLv ? segL[k] : mk3(0, 0, 0));
-    // throughputs the subpath loops wrote: alpha[0 .. vertices], one more after an emitter hit
-    for (int k = 0; k <= nE && k < MAXV + 2; ++k) B.ea[(size_t)k * n + j] = make_float4(aE[k].x, aE[k].y, aE[k].z, 0.0f);
-    for (int k = 0; k < nLv; ++k) B.la[(size_t)k * n + j] = make_float4(aL[k].x, aL[k].y, aL[k].z, 0.0f);
-    B.counts[j] = make_int2(nE, nLv);
-    B.light[j] = make_float4(bl.n.x, bl.n.y, bl.n.z, __int_as_float(bl.li));
-}
-
-// Every lane of a warp stays to the end (the staged strategy loop votes with the whole
-// warp); lanes without a sample, or whose sample failed a check, take part without work.
-template <int MAXV>
-__global__ void __launch_bounds__(BD_THREADS) bdpt_connect(BdLaunch P, BdStore B) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    bool valid = j < P.n_paths;
-    const int n = B.n;
-    int nE = 1, nLv = 1;
-    if (valid) {
-        const int2 cnt = B.counts[j];
-        nE = cnt.x;
-        nLv = cnt.y;
-        if (nE < 1 || nE > MAXV || nLv < 1 || nLv > MAXV) {
-            bd_fail(B, 2, j);
-            valid = false;
-            nE = nLv = 1;
-        }
-    }
-    BVert VE[MAXV], VL[MAXV];
-    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
-    BdLight bl;
-    bl.li = 0;
-    bl.n = mk3(0, 0, 0);
-    if (valid) {
-        for (int k = 0; k < nE; ++k) load_vertex<MAXV>(B.ev, n, j, k, VE[k], segE[k]);
-        for (int k = 0; k < nLv; ++k) load_vertex<MAXV>(B.lv, n, j, k, VL[k], segL[k]);
-        // the one-thread form leaves the vertex after the last one cleared (its loop clears
-        // it before the segment that ends the subpath), and MISWeight's "locked" test reads
-        // VE[1] even when the eye subpath is the camera alone
-        for (int k = nE; k < MAXV; ++k) bvert_clear(VE[k]);
-        for (int k = nLv; k < MAXV; ++k) bvert_clear(VL[k]);
-        const int n_mat = P.s.n_materials;
-        for (int k = 1; k < nE; ++k)
-            if (VE[k].onsurface && (VE[k].mat < 0 || VE[k].mat >= n_mat)) valid = false;
-        for (int k = 1; k < nLv; ++k)
-            if (VL[k].onsurface && (VL[k].mat < 0 || VL[k].mat >= n_mat)) valid = false;
-        if (!valid) bd_fail(B, 4, j);
-        for (int k = 0; k <= nE && k < MAXV + 2; ++k) aE[k] = f4xyz(B.ea[(size_t)k * n + j]);
-        for (int k = 0; k < nLv; ++k) aL[k] = f4xyz(B.la[(size_t)k * n + j]);
-        const float4 l4 = B.light[j];
-        bl.n = f4xyz(l4);
-        bl.li = __float_as_int(l4.w);
-        if (valid && (bl.li < 0 || bl.li >= P.s.n_lights)) {
-            bd_fail(B, 3, j);
-            valid = false;
-        }
-    }
-    connect_strategies_staged<MAXV>(P, B, valid ? j : 0, valid, VE, segE, aE, nE, VL, segL, aL, nLv, bl);
-}
-
-// VisibilityTest for the queued strategies: blocked when something lies more than 1e-4
-// before the far vertex (bidirectionalpathtracer.cpp:1018-1050).
-__global__ void __launch_bounds__(128, 8) bdpt_shadow(BdLaunch P, BdStore B) {
-    __shared__ int stack[BD_STACK * 128];
-    TraceStats st{0, 0};
-    const int W = P.s.width;
-    auto fetch = [&](int i, float3 &o, float3 &d, float &tmax, bool &in_obj) {
-        const float4 a = B.q[3 * (size_t)i], b = B.q[3 * (size_t)i + 1];
-        o = f4xyz(a);
-        d = f4xyz(b);
-        tmax = b.w;
-        in_obj = false;
-    };
-    const int n_pix = P.s.width * P.s.height;
-    auto finish = [&](int i, const HitRec &h) {
-        if (i < 0 || i >= B.q_cap) {
-            bd_fail(B, 7, i);
-            return;
-        }
-        const float tmax = B.q[3 * (size_t)i + 1].w;
-        if (h.t > 0.0f && tmax - h.t > 1e-4f) return;
-        const int dest = __float_as_int(B.q[3 * (size_t)i].w);
-        const float4 c = B.q[3 * (size_t)i + 2];
-        if (dest >= 0) {
-            if (dest >= B.slots * B.n) {
-                bd_fail(B, 8, i);
-                return;
-            }
-            B.result[dest] = make_float4(c.x, c.y, c.z, 0.0f);
-        } else {
-            const int px = -1 - dest;
-            if (px >= n_pix) {
-                bd_fail(B, 9, i);
-                return;
-            }
-            float *dst = P.light_film + (size_t)px * 3;
-            (void)W;
-            atomicAdd(dst + 0, c.z);
-            atomicAdd(dst + 1, c.y);
-            atomicAdd(dst + 2, c.x);
-        }
-    };
-    const int n = *B.q_count < B.q_cap ? *B.q_count : B.q_cap;
-    traverse_queue_walk<true, BD_STACK, false>([&](int) { return &P.s; }, n, B.q_fetch, 8, stack + threadIdx.x, 128,
-                                               fetch, finish, st);
-}
-
-// The sample's radiance: its result slots summed in strategy order.
-__global__ void bdpt_resolve(BdLaunch P, BdStore B) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.n_paths) return;
-    float3 L = mk3(0, 0, 0);
-    for (int k = 0; k < B.slots; ++k) {
-        const float4 c = B.result[(size_t)k * B.n + j];
-        L.x += c.x;
-        L.y += c.y;
-        L.z += c.z;
     }
     P.L[j] = make_float4(L.x, L.y, L.z, 0.0f);
 }
@@ -1143,27 +808,14 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
     }
     const int W = S.width, H = S.height, spp = p->spp;
     const long long total_pix = (long long)W * H;
-    // trace_mode 1: the one-thread-per-sample kernel; otherwise the staged form
-    const bool staged = p->trace_mode != 1;
-    const int maxv = p->n_light <= 8 && p->n_eye <= 8 ? 8 : BD_MAXV;
-    const int slots = (p->n_eye + p->n_light - 1) * p->n_eye;
-    long long wave = p->wave_paths > 0 ? p->wave_paths : (staged ? (1 << 18) : (1 << 20));
+    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 20);
     long long pix_per_wave = wave / spp;
     if (pix_per_wave < 1) pix_per_wave = 1;
     if (pix_per_wave > total_pix) pix_per_wave = total_pix;
     const size_t npaths = (size_t)(pix_per_wave * spp);
-    const size_t q_cap = npaths * (size_t)p->n_eye * (size_t)p->n_light;
-    if (staged && q_cap > (size_t)0x7fffffff / 3) {
-        set_error("BDPT: wave_paths too large for the shadow queue");
-        return RUMI_ERR_INVALID_ARG;
-    }
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t film_bytes = sizeof(float) * 3 * (size_t)total_pix;
-    size_t bytes = al(npaths * sizeof(float4)) + al(film_bytes) + al(64);
-    if (staged)
-        bytes += 2 * al(6 * (size_t)maxv * npaths * sizeof(float4)) + 2 * al((size_t)(maxv + 2) * npaths * sizeof(float4)) +
-                 al(npaths * sizeof(int2)) + al(npaths * sizeof(float4)) + al((size_t)slots * npaths * sizeof(float4)) +
-                 al(3 * q_cap * sizeof(float4)) + al(64);
+    const size_t bytes = al(npaths * sizeof(float4)) + al(film_bytes) + al(64);
     rumi_status st = ensure_workspace(sc, bytes);
     if (st != RUMI_OK) return st;
     char *w = (char *)sc->ws;
@@ -1181,26 +833,6 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
     B.L = (float4 *)w; w += al(npaths * sizeof(float4));
     B.light_film = (float *)w; w += al(film_bytes);
     unsigned long long *nan_count = (unsigned long long *)w;
-    w += al(64);
-    BdStore Q;
-    memset(&Q, 0, sizeof(Q));
-    if (staged) {
-        Q.ev = (float4 *)w; w += al(6 * (size_t)maxv * npaths * sizeof(float4));
-        Q.lv = (float4 *)w; w += al(6 * (size_t)maxv * npaths * sizeof(float4));
-        Q.ea = (float4 *)w; w += al((size_t)(maxv + 2) * npaths * sizeof(float4));
-        Q.la = (float4 *)w; w += al((size_t)(maxv + 2) * npaths * sizeof(float4));
-        Q.counts = (int2 *)w; w += al(npaths * sizeof(int2));
-        Q.light = (float4 *)w; w += al(npaths * sizeof(float4));
-        Q.result = (float4 *)w; w += al((size_t)slots * npaths * sizeof(float4));
-        Q.q = (float4 *)w; w += al(3 * q_cap * sizeof(float4));
-        Q.q_count = (int *)w;
-        Q.q_fetch = Q.q_count + 1;
-        Q.overflow = Q.q_count + 2;
-        Q.err = Q.q_count + 3;
-        Q.slots = slots;
-        Q.q_cap = (int)q_cap;
-        cudaMemsetAsync(Q.overflow, 0, 3 * sizeof(int), stream);
-    }
     const DevCamera &c = S.camera;
     B.right = mk3(c.m[0] + c.m[3], c.m[4] + c.m[7], c.m[8] + c.m[11]);
     B.up = mk3(c.m[1] + c.m[3], c.m[5] + c.m[7], c.m[9] + c.m[11]);
@@ -1213,12 +845,6 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
         cudaEventCreate(&e1);
         cudaEventRecord(e0, stream);
     }
-    int shadow_grid = 0;
-    if (staged) {
-        int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bdpt_shadow, 128, 0);
-        shadow_grid = sc->num_sms * (occ > 0 ? occ : 1);
-    }
     long long launches = 0;
     for (long long pix0 = 0; pix0 < total_pix; pix0 += pix_per_wave) {
         const long long n_pix = pix0 + pix_per_wave <= total_pix ? pix_per_wave : total_pix - pix0;
@@ -1226,43 +852,19 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
         B.n_paths = (int)(n_pix * spp);
         B.path0 = pix0 * spp;
         const int blocks = (B.n_paths + BD_THREADS - 1) / BD_THREADS;
-        if (staged) {
-            Q.n = (int)npaths;
-            cudaMemsetAsync(Q.q_count, 0, 2 * sizeof(int), stream);
-            cudaMemsetAsync(Q.result, 0, (size_t)slots * npaths * sizeof(float4), stream);
-            if (maxv == 8) {
-                bdpt_subpaths<8><<<blocks, BD_THREADS, 0, stream>>>(B, Q);
-                bdpt_connect<8><<<blocks, BD_THREADS, 0, stream>>>(B, Q);
-            } else {
-                bdpt_subpaths<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B, Q);
-                bdpt_connect<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B, Q);
-            }
-            bdpt_shadow<<<shadow_grid, 128, 0, stream>>>(B, Q);
-            bdpt_resolve<<<(B.n_paths + 255) / 256, 256, 0, stream>>>(B, Q);
-            launches += 4;
-        } else {
-            if (maxv == 8)
-                bdpt_kernel<8><<<blocks, BD_THREADS, 0, stream>>>(B);
-            else
-                bdpt_kernel<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B);
-            launches += 1;
-        }
+        if (p->n_light <= 8 && p->n_eye <= 8)
+            bdpt_kernel<8><<<blocks, BD_THREADS, 0, stream>>>(B);
+        else
+            bdpt_kernel<BD_MAXV><<<blocks, BD_THREADS, 0, stream>>>(B);
         bdpt_write_film<<<(int)((n_pix + 255) / 256), 256, 0, stream>>>(B, (int)n_pix, film_dev, nan_count);
-        launches += 1;
+        launches += 2;
     }
     add_light_film<<<sc->num_sms * 4, 256, 0, stream>>>(film_dev, B.light_film, (size_t)total_pix * 3);
     if (timing) cudaEventRecord(e1, stream);
     unsigned long long h_nan = 0;
-    int h_chk[3] = {0, 0, 0};  // overflow, first failed check, its index
     cudaMemcpyAsync(&h_nan, nan_count, sizeof(h_nan), cudaMemcpyDeviceToHost, stream);
-    if (staged) cudaMemcpyAsync(h_chk, Q.overflow, sizeof(h_chk), cudaMemcpyDeviceToHost, stream);
     cudaError_t e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_status(e, "bdpt_render");
-    if (h_chk[0] || h_chk[1]) {  // neither can happen: the queue holds every strategy of every sample
-        set_error("bdpt_render: staged consistency check " + std::to_string(h_chk[1]) + " failed at " +
-                  std::to_string(h_chk[2]) + (h_chk[0] ? " (shadow queue overflow)" : ""));
-        return RUMI_ERR_INTERNAL;
-    }
     if (stats) {
         memset(stats, 0, sizeof(*stats));
         stats->paths = total_pix * spp;

@@ -572,24 +572,3 @@ def test_gpu_eight_wide_walk_hits_match_reference_on_the_1m_mesh():
     np.testing.assert_array_equal(a, b)
     assert sa["extend_prim_tests"] > 0 and sb["extend_prim_tests"] > 0
     assert sb["extend_node_fetches"] < sa["extend_node_fetches"]
-
-
-@pytest.mark.parametrize("builder", [
-    lambda: scenes.cornell_bdpt(40, 32, 9, 4, 5),
-    lambda: scenes.volumetric_caustic(40, 32, 9, 6, 7),
-    lambda: _bdpt45(scenes.cornell_two_lights_pt(40, 32, 9, 8)),
-])
-def test_gpu_staged_bdpt_equals_the_one_thread_form(builder):
-    """The staged BDPT (subpaths -> vertex store, strategies -> result slots and a shadow
-    queue through the persistent any-hit walk, per-sample sums in strategy order) and the
-    one-thread-per-sample kernel (trace_mode 1) compute the same strategies from the same
-    random numbers: the films agree up to the order of the light-tracing splats' float
-    atomics, at every wave size."""
-    sc = builder()
-    gs = rumi_b200.GpuScene(sc)
-    ref, st1 = gs.render(seed=21, trace_mode=1)
-    for wave in (0, 999):
-        film, st = gs.render(seed=21, wave_paths=wave)
-        assert st["nan_samples"] == st1["nan_samples"]
-        np.testing.assert_allclose(film, ref, rtol=1e-4, atol=1e-5 * float(ref.max()))
-    gs.close()
