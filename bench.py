@@ -691,7 +691,7 @@ def adjoint_arm(args):
     import rumi_b200
     from rumi_b200 import scenes
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from adjoint_torch import render, visible_triangles
+    from adjoint_torch import render, visible_triangles, footprint_albedo_rmse
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     size, spp, depth = 256, 64, 8
     gt = rumi_b200.GpuScene(scenes.inverse_rendering(size, size, spp, depth))
@@ -742,6 +742,9 @@ def adjoint_arm(args):
     # the triangles the camera sees (>= 1 pixel): only their albedo is observable
     vis = torch.from_numpy(visible_triangles(g, start, alb_all.shape[0] - n_mesh, n_mesh)).cuda()
     vis_rmse0 = float(((mesh.detach() - hidden_t)[vis] ** 2).mean().sqrt())
+    # what a 256x256 image observes of the albedo: its average over each pixel's footprint
+    first_mesh = alb_all.shape[0] - n_mesh
+    fp_rmse0 = footprint_albedo_rmse(g, start, first_mesh, n_mesh, mesh.detach(), hidden_t)
     for it in range(args.warmup):
         step(-1 - it)
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
@@ -759,6 +762,7 @@ def adjoint_arm(args):
     losses = [float(x) for x in losses]
     alb_rmse = float(((mesh.detach() - hidden_t) ** 2).mean().sqrt())
     vis_rmse = float(((mesh.detach() - hidden_t)[vis] ** 2).mean().sqrt())
+    fp_rmse = footprint_albedo_rmse(g, start, first_mesh, n_mesh, mesh.detach(), hidden_t)
     t = scenes.INVERSE_TARGET_MEDIUM
     line = dict(metric="adjoint grads/s", value=args.adam_steps / (ms / 1000.0), unit="gradient evaluations/s",
                 n_gpus=1, steps=args.adam_steps, warmup=args.warmup, ms_per_step=ms / args.adam_steps,
@@ -771,7 +775,8 @@ def adjoint_arm(args):
                 paths_per_step=size * size * spp, loss_first=losses[0], loss_last=losses[-1],
                 albedo_rmse_start=alb_rmse0, albedo_rmse_end=alb_rmse,
                 visible_triangles=int(vis.sum()), visible_albedo_rmse_start=vis_rmse0,
-                visible_albedo_rmse_end=vis_rmse,
+                visible_albedo_rmse_end=vis_rmse, footprint_albedo_rmse_start=fp_rmse0,
+                footprint_albedo_rmse_end=fp_rmse,
                 medium_end=[float(x) for x in med.detach().cpu()],
                 medium_target=list(t["sigma_s"]) + list(t["sigma_a"]) + [t["g"]],
                 gpu_launches=args.adam_steps * ((3 + 5 * depth) + 2 * (3 + 4 * depth)), clocks=clocks_info)

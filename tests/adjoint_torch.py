@@ -50,11 +50,9 @@ def render(albedo, medium, gscene, spp, seed, grad_seed=None):
                                 seed + 0x5BD1E995 if grad_seed is None else grad_seed)
 
 
-def visible_triangles(gscene, scene, first_mesh, n_mesh, sub=4, min_pixels=1.0):
-    """Mesh triangles the camera sees: closest hits of sub x sub rays per pixel through the
-    pinhole (Pinhole::CastViewRay's pixel grid, src/Camera/pinhole.cpp:97-136) counted per
-    triangle; a triangle covering at least `min_pixels` pixels is visible.  first_mesh:
-    canonical id of the mesh's first triangle.  Returns a boolean mask (n_mesh,)."""
+def _camera_hits(gscene, scene, sub):
+    """Closest-hit primitive of sub x sub rays per pixel through the pinhole
+    (Pinhole::CastViewRay's pixel grid, src/Camera/pinhole.cpp:97-136): (H*sub, W*sub)."""
     import numpy as np
     cam, img = scene.camera, scene.image
     W, H = img.width, img.height
@@ -73,6 +71,35 @@ def visible_triangles(gscene, scene, first_mesh, n_mesh, sub=4, min_pixels=1.0):
     rays[:, 3:6] = d
     rays[:, 6] = 3.4e38
     _, prim, _, _ = gscene.trace(rays)
+    return prim.reshape(H * sub, W * sub)
+
+
+def footprint_albedo_rmse(gscene, scene, first_mesh, n_mesh, albedo, hidden, sub=4):
+    """RMSE, over the pixels that see the mesh, of the albedo averaged over each pixel's
+    footprint (the mean over its sub x sub camera rays of the albedo of the triangle each
+    hits) -- the part of the per-triangle albedo an image of this resolution observes.
+    albedo, hidden: (n_mesh, 3) tensors.  Returns a float."""
+    import numpy as np
+    import torch
+    prim = _camera_hits(gscene, scene, sub) - first_mesh
+    H, W = prim.shape[0] // sub, prim.shape[1] // sub
+    on = (prim >= 0) & (prim < n_mesh)
+    ids = torch.from_numpy(np.where(on, prim, 0).astype(np.int64)).to(albedo.device)
+    mask = torch.from_numpy(on).to(albedo.device)
+    diff = (albedo - hidden)[ids] * mask[..., None]
+    cnt = mask.reshape(H, sub, W, sub).sum((1, 3))
+    fp = diff.reshape(H, sub, W, sub, 3).sum((1, 3)) / cnt.clamp(min=1)[..., None]
+    seen = cnt == sub * sub  # pixels wholly on the mesh
+    return float((fp[seen] ** 2).mean().sqrt())
+
+
+def visible_triangles(gscene, scene, first_mesh, n_mesh, sub=4, min_pixels=1.0):
+    """Mesh triangles the camera sees: closest hits of sub x sub rays per pixel through the
+    pinhole (Pinhole::CastViewRay's pixel grid, src/Camera/pinhole.cpp:97-136) counted per
+    triangle; a triangle covering at least `min_pixels` pixels is visible.  first_mesh:
+    canonical id of the mesh's first triangle.  Returns a boolean mask (n_mesh,)."""
+    import numpy as np
+    prim = _camera_hits(gscene, scene, sub).reshape(-1)
     k = prim - first_mesh
     k = k[(prim >= 0) & (k >= 0) & (k < n_mesh)]
     cover = np.bincount(k, minlength=n_mesh) / float(sub * sub)

@@ -193,10 +193,12 @@ def test_backward_rejects_what_it_cannot_differentiate():
 def test_inverse_rendering_reduces_loss_and_recovers_medium():
     """A short optimisation through the torch.autograd.Function wrapper: Adam on the mesh
     albedo and the medium from a wrong start.  The image loss, measured with a fixed-seed
-    256-spp render against a 256-spp target, must fall, and the medium coefficients must
-    move toward the hidden target."""
+    256-spp render against a 256-spp target, must fall; the medium coefficients must move
+    toward the hidden target; and the albedo must approach the hidden one where the image
+    observes it -- over the triangles that cover at least a pixel, and averaged over each
+    pixel's footprint (the 256 triangles here are a few pixels each)."""
     import torch
-    from adjoint_torch import render
+    from adjoint_torch import render, visible_triangles, footprint_albedo_rmse
     size, spp, depth, eval_spp = 48, 16, 6, 256
     gt = rumi_b200.GpuScene(scenes.inverse_rendering(size, size, eval_spp, depth, levels=3))
     target = torch.from_numpy(gt.forward(seed=1)[0] / eval_spp).cuda()
@@ -220,6 +222,12 @@ def test_inverse_rendering_reduces_loss_and_recovers_medium():
                 return float(((film - target) ** 2).mean())
 
         before = eval_loss()
+        hidden = torch.from_numpy(scenes.random_albedo(n_mesh, 23)).cuda()
+        first = alb_all.shape[0] - n_mesh
+        vis = torch.from_numpy(visible_triangles(g, start, first, n_mesh)).cuda()
+        assert int(vis.sum()) > 50
+        vis0 = float(((mesh.detach() - hidden)[vis] ** 2).mean().sqrt())
+        fp0 = footprint_albedo_rmse(g, start, first, n_mesh, mesh.detach(), hidden)
         opt = torch.optim.Adam([mesh, med], lr=2e-2)
         for it in range(60):
             film = render(torch.cat([walls, mesh]), med, g, spp, 100 + it) / spp
@@ -239,6 +247,9 @@ def test_inverse_rendering_reduces_loss_and_recovers_medium():
         # different; `after` fell to 0.6-0.85 of `before` over the runs observed.  The bound
         # 0.9 * before asks the removable part to shrink by a quarter.
         assert after < 0.9 * before, (before, after)
+        vis1 = float(((mesh.detach() - hidden)[vis] ** 2).mean().sqrt())
+        fp1 = footprint_albedo_rmse(g, start, first, n_mesh, mesh.detach(), hidden)
+        assert vis1 < vis0 and fp1 < fp0, (vis0, vis1, fp0, fp1)
         t = scenes.INVERSE_TARGET_MEDIUM
         tgt = np.array(list(t["sigma_s"]) + list(t["sigma_a"]) + [t["g"]])
         m_start = np.array(list(m0["sigma_s"]) + list(m0["sigma_a"]) + [m0["g"]])
