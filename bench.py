@@ -50,6 +50,11 @@ def parse():
                          "adjoint: inverse rendering with the path-replay adjoint")
     ap.add_argument("--adam-steps", type=int, default=200, help="adjoint workload: optimisation steps")
     ap.add_argument("--scenes", type=int, default=256, help="batched workload: number of scenes")
+    ap.add_argument("--breakdown", action="store_true",
+                    help="batched workload: also time every scene alone and report the per-size-class rates and "
+                         "the bound they put on any batching")
+    ap.add_argument("--trace-mode", type=int, default=0,
+                    help="bvh_bound workload: rumi_render_params.trace_mode (0 = library default)")
     return ap.parse_args()
 
 
@@ -419,13 +424,13 @@ def our_arm(args):
 
     # algorithmic bytes per closest-hit ray, from an instrumented (untimed) frame
     _, st0 = gs.render(seed=seed0 + 999, film_device_ptr=film.data_ptr(), stream=stream, count_stats=True,
-                       wave_paths=args.wave_paths)
+                       wave_paths=args.wave_paths, trace_mode=args.trace_mode)
     nodes_per_ray = st0["extend_node_fetches"] / st0["rays_extend"]
     prims_per_ray = st0["extend_prim_tests"] / st0["rays_extend"]
     bytes_per_ray = 32.0 * nodes_per_ray + 48.0 * prims_per_ray + 32.0 + 16.0
 
     for s in range(args.warmup):
-        gs.render(seed=seed0 + s, film_device_ptr=film.data_ptr(), stream=stream, wave_paths=args.wave_paths)
+        gs.render(seed=seed0 + s, film_device_ptr=film.data_ptr(), stream=stream, wave_paths=args.wave_paths, trace_mode=args.trace_mode)
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
@@ -437,7 +442,7 @@ def our_arm(args):
     # stream beside the next bounce's closest-hit rays, no per-kernel events
     for s in range(args.steps):
         _, st = gs.render(seed=seed0 + 100 + s, film_device_ptr=film.data_ptr(), stream=stream,
-                          wave_paths=args.wave_paths)
+                          wave_paths=args.wave_paths, trace_mode=args.trace_mode)
         rays_ext += st["rays_extend"]
         rays_sh += st["rays_shadow"]
         waves = st["extend_launches"] // w["max_depth"]
@@ -455,7 +460,7 @@ def our_arm(args):
     ext_ms, ext_launches, ext_rays, kern = 0.0, 0, 0, dict(extend_ms=0.0, shadow_ms=0.0, shade_ms=0.0, total_ms=0.0)
     for s in range(args.steps):
         _, st = gs.render(seed=seed0 + 100 + s, film_device_ptr=film.data_ptr(), stream=stream, timing=True,
-                          serial=True, wave_paths=args.wave_paths)
+                          serial=True, wave_paths=args.wave_paths, trace_mode=args.trace_mode)
         ext_ms += st["extend_ms"]
         ext_launches += st["extend_launches"]
         ext_rays += st["rays_extend"]
@@ -650,6 +655,9 @@ def batched_arm(args):
     ms_batch, l_batch = timed(batched)
     clocks_info = clocks.stop()
     equal = bool(torch.equal(films_plain, films_batch))
+    breakdown = None
+    if args.breakdown:
+        breakdown = scene_breakdown(gss, spp, stream)
     batch.close()
     for g in gss:
         g.close()
@@ -672,11 +680,48 @@ def batched_arm(args):
                     plain_loop=dict(value=plain_value, ms_per_step=ms_plain / args.steps, gpu_launches=l_plain),
                     speedup_vs_plain=value / plain_value, equal_images=equal, gpu_launches=l_batch,
                     clocks=clocks_info)
+        if breakdown:
+            line["per_scene_breakdown"] = breakdown
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0 if equal else 1
+
+
+def scene_breakdown(gss, spp, stream):
+    """Every scene rendered alone (CUDA events around three frames after two warm-up
+    frames), grouped by paths per frame: each class's share of the paths and of the loop's
+    time and its rate; and the bound on any batching of the frame -- the frame time if every
+    path ran at the rate the largest scenes reach alone, or at the best single scene's."""
+    import torch
+    rows = []
+    for g, s in zip(gss, spp):
+        film = torch.zeros((g.height, g.width, 3), device="cuda")
+        for w in range(2):
+            g.render(spp=s, seed=w, film_device_ptr=film.data_ptr(), stream=stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(3):
+            g.render(spp=s, seed=10 + k, film_device_ptr=film.data_ptr(), stream=stream)
+        e1.record()
+        torch.cuda.synchronize()
+        rows.append((g.width * g.height * s, e0.elapsed_time(e1) / 3))
+    tot_p = sum(p for p, _ in rows)
+    tot_ms = sum(m for _, m in rows)
+    classes = []
+    for lo, hi in [(0, 1e5), (1e5, 1e6), (1e6, 4e6), (4e6, 1e18)]:
+        sel = [(p, m) for p, m in rows if lo <= p < hi]
+        if sel:
+            p = sum(x for x, _ in sel)
+            m = sum(x for _, x in sel)
+            classes.append(dict(paths_from=lo, paths_to=hi, scenes=len(sel), path_share=p / tot_p,
+                                time_share=m / tot_ms, m_paths_per_s=p / m / 1e3))
+    big = [(p, m) for p, m in rows if p >= 4e6] or rows
+    rate_big = sum(p for p, _ in big) / sum(m for _, m in big)
+    best = max(p / m for p, m in rows)
+    return dict(loop_ms=tot_ms, classes=classes, bound_at_large_scene_rate=tot_ms / (tot_p / rate_big),
+                bound_at_best_scene_rate=tot_ms / (tot_p / best))
 
 
 def adjoint_arm(args):
