@@ -49,6 +49,9 @@ def parse():
                     help="batched: 256 seeded scenes as one frame vs the per-scene loop; "
                          "adjoint: inverse rendering with the path-replay adjoint")
     ap.add_argument("--adam-steps", type=int, default=200, help="adjoint workload: optimisation steps")
+    ap.add_argument("--adjoint-spp", type=int, default=0,
+                    help="adjoint workload: samples per pixel of the gradient pass (0 = the forward's 64)")
+    ap.add_argument("--adam-lr", type=float, default=1e-2, help="adjoint workload: Adam learning rate")
     ap.add_argument("--scenes", type=int, default=256, help="batched workload: number of scenes")
     ap.add_argument("--breakdown", action="store_true",
                     help="batched workload: also time every scene alone and report the per-size-class rates and "
@@ -753,11 +756,12 @@ def adjoint_arm(args):
     m0 = scenes.INVERSE_START_MEDIUM
     med = torch.nn.Parameter(torch.tensor(list(m0["sigma_s"]) + list(m0["sigma_a"]) + [m0["g"]],
                                           dtype=torch.float32, device="cuda"))
-    opt = torch.optim.Adam([mesh, med], lr=1e-2)
+    opt = torch.optim.Adam([mesh, med], lr=args.adam_lr)
+    grad_spp = args.adjoint_spp or spp
     hidden_t = torch.from_numpy(hidden).cuda()
 
     def step(it):
-        film = render(torch.cat([walls, mesh]), med, g, spp, 100 + it) / spp
+        film = render(torch.cat([walls, mesh]), med, g, spp, 100 + it, grad_spp=grad_spp) / spp
         loss = ((film - target) ** 2).mean()
         opt.zero_grad()
         loss.backward()
@@ -814,7 +818,8 @@ def adjoint_arm(args):
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
                 data="synthetic (seeded 65,536-triangle displaced sphere, hidden seeded albedo and medium)",
                 config=dict(workload="inverse rendering: 256x256, 64 spp, depth 8, 65,536 triangles in a medium",
-                            params=3 * n_mesh + 7, optimiser="Adam lr 1e-2", loss="L2 image"),
+                            params=3 * n_mesh + 7, optimiser=f"Adam lr {args.adam_lr:g}", loss="L2 image",
+                            gradient_spp=grad_spp),
                 forward_ms=fwd_ms, backward_ms=bwd_ms, backward_over_forward=bwd_ms / fwd_ms,
                 backward_after_kept_forward_ms=bwd_kept_ms,
                 paths_per_step=size * size * spp, loss_first=losses[0], loss_last=losses[-1],

@@ -206,7 +206,7 @@ typedef struct {
     int32_t blocks_per_sm; /* persistent traversal blocks (128 threads) per SM, capped by occupancy */
     int32_t refill_min;    /* idle lanes that trigger a refill (modes 2-5) */
     int32_t stack_depth;   /* traversal stack entries per thread kept in shared memory: 8, 16
-                              or 32 (0 = 32; modes 4 and 5 take all three, the others 32);
+                              or 32 (0 = 16; modes 4 and 5 take all three, the others 32);
                               deeper entries spill to local memory, and a smaller stack leaves
                               more of the SM's unified L1 / shared storage to L1 */
 } rumi_render_params;

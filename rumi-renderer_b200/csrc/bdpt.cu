@@ -603,23 +603,25 @@ RUMI_D bool volumetric_ok(const DevVolume &V, float3 sp, float3 tp, float xi) {
     return !(xi < 1.0f - expf(avg3(V.sigma_t) * -sm));
 }
 
+// The light a sample picked and its sampled point (Scene::LightsUniformSampling +
+// AreaLight::SolidAngleSampling's position).
+struct BdLight {
+    int li;
+    float3 n;
+};
+
+// Both subpaths of camera sample j (ConstructViewPath / ConstructLightPath with their
+// starts, bidirectionalpathtracer.cpp:121-180).  Returns the light; nE / nLv receive the
+// vertex counts.
 template <int MAXV>
-__global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
-    __shared__ int stack[BD_STACK * BD_THREADS];
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.n_paths) return;
+RUMI_D BdLight build_subpaths(const BdLaunch &P, int j, BVert *VE, float3 *segE, float3 *aE, BVert *VL, float3 *segL,
+                              float3 *aL, int &nE, int &nLv, int *stk, TraceStats &st) {
     const DevScene &S = P.s;
     const uint64_t path = (uint64_t)(P.path0 + j);
     const long long pixel = (long long)P.pix0 + j / P.spp;
     const int sidx = j % P.spp;
     const int W = S.width, H = S.height;
     const int pw_ = (int)(pixel % W), ph_ = (int)(pixel / W);
-    TraceStats st{0, 0};
-    int *stk = stack + threadIdx.x;
-
-    BVert VE[MAXV], VL[MAXV];
-    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
-    // Scene::LightsUniformSampling + AreaLight::SolidAngleSampling
     const Uniform4 UL = path_uniforms(path, 1000u, 0, P.k0, P.k1);
     const Uniform4 UD = path_uniforms(path, 1000u, 1, P.k0, P.k1);
     const int li = pick_light(S, UL.u[0]);
@@ -650,7 +652,7 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
         VE[0].pdf_dir = c.plane_dist * c.plane_dist / (l.z * l.z * l.z * c.film_area);
         VE[0].pdf_fwd = c3(1.0f);
     }
-    const int nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
+    nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
     // light subpath start: cosine-weighted emission from an area light
     // (AreaLight::SolidAngleSampling), uniform in the cone from a spot
     const bool spot = light.type == LIGHT_SPOT;
@@ -669,100 +671,182 @@ __global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
         VL[0].pdf_dir = emit.pdf;
         VL[0].cos_a = dot3(emit.wi, light_n);
     }
-    const int nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit_w, VL, segL, aL, light, light_n, stk, st);
+    nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit_w, VL, segL, aL, light, light_n, stk, st);
     // a delta position: the strategies in which the eye subpath reaches the light carry
     // no weight (the MIS sums skip a dirac first light vertex)
     if (spot) VL[0].dirac = true;
+    BdLight bl;
+    bl.li = li;
+    bl.n = light_n;
+    return bl;
+}
 
+// One strategy of Trace's double loop (bidirectionalpathtracer.cpp:182-390): eye subpath
+// vertex t and light subpath vertex s = len - (t + 1).  Returns
+//   STRAT_NONE   nothing to add (rejected, or a skipped combination);
+//   STRAT_ADD    `lo` is added to the sample as it is (the eye subpath reached a light);
+//   STRAT_SHADOW `lo` counts once the shadow ray (o, dir, tmax) is unoccluded; t == 0 splats
+//                it onto film pixel `px`.
+// *stop: Trace leaves the t loop of this length here (t past the eye subpath, or an eye
+// vertex on a light).  VisibilityTest is the caller's.
+enum { STRAT_NONE = 0, STRAT_ADD = 1, STRAT_SHADOW = 2 };
+
+struct StratOut {
+    float3 lo, o, dir;
+    float tmax;
+    int px;
+};
+
+template <int MAXV>
+RUMI_D int strategy(const BdLaunch &P, int j, int len, int t, const BVert *VE, const float3 *segE, const float3 *aE,
+                    int nE, const BVert *VL, const float3 *segL, const float3 *aL, int nLv, const DevLight &light,
+                    float3 light_n, bool &stop, StratOut &out) {
+    const DevScene &S = P.s;
+    const uint64_t path = (uint64_t)(P.path0 + j);
+    const int W = S.width, H = S.height;
+    const bool spot = light.type == LIGHT_SPOT;
+    if (t >= nE) {
+        stop = true;
+        return STRAT_NONE;
+    }
+    const BVert &tc = VE[t];
+    float3 t_wo = mk3(0, 0, 0);
+    if (t > 0) {
+        t_wo = -segE[t - 1];
+        if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
+            stop = true;
+            if (len == nE - 1) {
+                const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
+                out.lo = aE[t + 1] * w;
+                return STRAT_ADD;
+            }
+            return STRAT_NONE;
+        }
+        if (tc.dirac) return STRAT_NONE;
+    }
+    const int s = len - (t + 1);
+    if (s >= nLv || s <= -1) return STRAT_NONE;
+    const BVert &sc = VL[s];
+    float3 s_wi = mk3(0, 0, 0);
+    if (s > 0) {
+        s_wi = -segL[s - 1];
+        if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) return STRAT_NONE;
+        if (sc.dirac) return STRAT_NONE;
+    }
+    // the geometric rejections come before the two visibility tests: they read no random
+    // numbers and change nothing, so the order only saves traversals
+    const float3 cwi = normalize_ref(sc.p - tc.p);
+    const float3 cwo = normalize_ref(tc.p - sc.p);
+    const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
+    if (ci < 1e-4f) return STRAT_NONE;
+    float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
+    if (s == 0 && spot) {
+        if (dot3(cwo, light.direction) < light.cos_cone) return STRAT_NONE;  // outside the cone
+        co = 1.0f;                                                         // no cosine at a point
+    }
+    if (co < 1e-4f) return STRAT_NONE;
+    const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+    if (dist <= 0.0f) return STRAT_NONE;
+    const float G = ci * co / (dist * dist);
+    if (G <= 0.0f) return STRAT_NONE;
+    int film_w = 0, film_h = 0;
+    if (t == 0) {
+        if (!film_plane_pixel(P, sc.p, film_w, film_h)) return STRAT_NONE;
+        if (film_w == W || film_h == H) return STRAT_NONE;
+        if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) return STRAT_NONE;
+    }
+    // VolumetricTest reads its own uniform, so it may come before the visibility test
+    const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
+    if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) return STRAT_NONE;
+    float3 cE, cL;
+    if (t == 0) {
+        const DevCamera &c = S.camera;
+        const float cs = dot3(tc.n, cwi);
+        const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
+        cE = c3(We / avg3(tc.pdf_fwd));
+    } else if (tc.onsurface) {
+        cE = vert_fr(S, tc, tc.n, cwi, t_wo) / (tc.pdf_fwd * tc.pdf_path);
+    } else {
+        cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
+    }
+    // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
+    // 350-351): a medium vertex takes the texture of the surface its segment was headed
+    // for, evaluated at the medium point; none without such a surface
+    if (t > 0 && S.prim_tex && tc.prim >= 0) cE = cE * tex_pattern(S, tc.prim, tc.p);
+    if (s == 0) {
+        cL = light_emission(light) / sc.pdf_fwd;
+    } else if (sc.onsurface) {
+        cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
+    } else {
+        cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
+    }
+    if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
+    const float3 lo = aE[t] * cE * G * cL * aL[s];
+    out.lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
+    // the shadow ray of VisibilityTest (:1018-1050): from the eye vertex unless the eye
+    // vertex is the camera
+    if (t == 0) {
+        out.o = sc.p;
+        out.dir = normalize_ref(tc.p - sc.p);
+    } else {
+        out.o = tc.p;
+        out.dir = normalize_ref(sc.p - tc.p);
+    }
+    out.tmax = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+    out.px = t == 0 ? film_h * W + film_w : -1;
+    return STRAT_SHADOW;
+}
+
+// Every strategy of one sample in Trace's order, visibility traced by this thread; splats
+// go to the light film.  Returns the sample's radiance.
+template <int MAXV>
+RUMI_D float3 connect_strategies(const BdLaunch &P, int j, const BVert *VE, const float3 *segE, const float3 *aE,
+                                 int nE, const BVert *VL, const float3 *segL, const float3 *aL, int nLv,
+                                 const BdLight &bl, int *stk, TraceStats &st) {
+    const DevScene &S = P.s;
+    const DevLight light = S.lights[bl.li];
     float3 L = mk3(0, 0, 0);
     const int max_len = nE + nLv - 1;
     for (int len = 1; len <= max_len; ++len) {
         for (int t = 0; t <= len; ++t) {
-            if (t >= nE) break;
-            const BVert &tc = VE[t];
-            float3 t_wo = mk3(0, 0, 0);
-            if (t > 0) {
-                t_wo = -segE[t - 1];
-                if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
-                    if (len == nE - 1) {
-                        const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
-                        L = L + aE[t + 1] * w;
+            bool stop = false;
+            StratOut out;
+            const int r = strategy<MAXV>(P, j, len, t, VE, segE, aE, nE, VL, segL, aL, nLv, light, bl.n, stop, out);
+            if (r == STRAT_ADD) {
+                L = L + out.lo;
+            } else if (r == STRAT_SHADOW) {
+                const HitRec h = trace_ray<true, BD_STACK, false>(S, out.o, out.dir, out.tmax, false, stk, BD_THREADS, st);
+                if (!(h.t > 0.0f && out.tmax - h.t > 1e-4f)) {
+                    if (out.px >= 0) {
+                        float *dst = P.light_film + (size_t)out.px * 3;
+                        atomicAdd(dst + 0, out.lo.z);
+                        atomicAdd(dst + 1, out.lo.y);
+                        atomicAdd(dst + 2, out.lo.x);
+                    } else {
+                        L = L + out.lo;
                     }
-                    break;
                 }
-                if (tc.dirac) continue;
             }
-            const int s = len - (t + 1);
-            if (s >= nLv || s <= -1) continue;
-            const BVert &sc = VL[s];
-            float3 s_wi = mk3(0, 0, 0);
-            if (s > 0) {
-                s_wi = -segL[s - 1];
-                if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) continue;
-                if (sc.dirac) continue;
-            }
-            // the geometric rejections come before the two visibility tests: they read no
-            // random numbers and change nothing, so the order only saves traversals
-            const float3 cwi = normalize_ref(sc.p - tc.p);
-            const float3 cwo = normalize_ref(tc.p - sc.p);
-            const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
-            if (ci < 1e-4f) continue;
-            float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
-            if (s == 0 && spot) {
-                if (dot3(cwo, light.direction) < light.cos_cone) continue;  // outside the cone
-                co = 1.0f;                                                 // no cosine at a point
-            }
-            if (co < 1e-4f) continue;
-            const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
-            if (dist <= 0.0f) continue;
-            const float G = ci * co / (dist * dist);
-            if (G <= 0.0f) continue;
-            int film_w = 0, film_h = 0;
-            if (t == 0) {
-                if (!film_plane_pixel(P, sc.p, film_w, film_h)) continue;
-                if (film_w == W || film_h == H) continue;
-                if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) continue;
-            }
-            if (!visible(S, s + 1, t + 1, sc.p, tc.p, stk, st)) continue;
-            const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
-            if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) continue;
-            float3 cE, cL;
-            if (t == 0) {
-                const DevCamera &c = S.camera;
-                const float cs = dot3(tc.n, cwi);
-                const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
-                cE = c3(We / avg3(tc.pdf_fwd));
-            } else if (tc.onsurface) {
-                cE = vert_fr(S, tc, tc.n, cwi, t_wo) / (tc.pdf_fwd * tc.pdf_path);
-            } else {
-                cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
-            }
-            // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
-            // 350-351): a medium vertex takes the texture of the surface its segment was
-            // headed for, evaluated at the medium point; none without such a surface
-            if (t > 0 && S.prim_tex && tc.prim >= 0) cE = cE * tex_pattern(S, tc.prim, tc.p);
-            if (s == 0) {
-                cL = light_emission(light) / sc.pdf_fwd;
-            } else if (sc.onsurface) {
-                cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
-            } else {
-                cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
-            }
-            if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
-            if (t == 0) {
-                float3 lo = aE[t] * cE * G * cL * aL[s];
-                lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, 1, cwi, cwo, light_n, light);
-                float *dst = P.light_film + ((size_t)film_h * W + film_w) * 3;
-                atomicAdd(dst + 0, lo.z);
-                atomicAdd(dst + 1, lo.y);
-                atomicAdd(dst + 2, lo.x);
-            } else {
-                float3 lo = aE[t] * cE * G * cL * aL[s];
-                lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
-                L = L + lo;
-            }
+            if (stop) break;
         }
     }
+    return L;
+}
+
+
+// One thread renders one camera sample: both subpaths and every strategy.
+template <int MAXV>
+__global__ void __launch_bounds__(BD_THREADS) bdpt_kernel(BdLaunch P) {
+    __shared__ int stack[BD_STACK * BD_THREADS];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_paths) return;
+    TraceStats st{0, 0};
+    int *stk = stack + threadIdx.x;
+    BVert VE[MAXV], VL[MAXV];
+    float3 segE[MAXV], segL[MAXV], aE[MAXV + 2], aL[MAXV + 2];
+    int nE, nLv;
+    const BdLight bl = build_subpaths<MAXV>(P, j, VE, segE, aE, VL, segL, aL, nE, nLv, stk, st);
+    const float3 L = connect_strategies<MAXV>(P, j, VE, segE, aE, nE, VL, segL, aL, nLv, bl, stk, st);
     P.L[j] = make_float4(L.x, L.y, L.z, 0.0f);
 }
 

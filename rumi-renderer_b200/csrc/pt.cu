@@ -883,8 +883,11 @@ using ExtendKernel = void (*)(PtLaunch, int);
 using ShadowKernel = void (*)(PtLaunch);
 
 // Shared-memory stack depth from rumi_render_params.stack_depth: 8, 16 or 32 entries per
-// thread (0 = 32).  Only the while-while walks (schemes 3 and 4) come in all three depths.
-static inline int stack_entries(int stack_depth) { return stack_depth == 8 || stack_depth == 16 ? stack_depth : 32; }
+// thread (0 = 16).  Only the while-while walks (schemes 3 and 4) come in all three depths.
+// Measured on the 1024x1024x64 BVH-bound frame (binary walk, closest-hit ms): 8: 100.5,
+// 16: 100.3, 32 with the L1 carveout sized to it: 107.0 -- the 32-entry stack takes L1 that
+// node fetches use, and deeper entries are rare.
+static inline int stack_entries(int stack_depth) { return stack_depth == 8 || stack_depth == 32 ? stack_depth : 16; }
 
 template <bool STATS>
 static ExtendKernel extend_kernel(int mode, int smem) {

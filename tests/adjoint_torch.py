@@ -22,7 +22,7 @@ class PathTracedFilm(torch.autograd.Function):
     random numbers measure)."""
 
     @staticmethod
-    def forward(ctx, albedo, medium, gscene, spp, seed, grad_seed):
+    def forward(ctx, albedo, medium, gscene, spp, seed, grad_seed, grad_spp):
         albedo = albedo.detach().contiguous()
         m = medium.detach().cpu().tolist()
         torch.cuda.current_stream().synchronize()
@@ -30,7 +30,8 @@ class PathTracedFilm(torch.autograd.Function):
         gscene.set_volume(m[0:3], m[3:6], m[6])
         film = torch.empty((gscene.height, gscene.width, 3), dtype=torch.float32, device=albedo.device)
         gscene.forward(spp=spp, seed=seed, film_device_ptr=film.data_ptr())
-        ctx.gscene, ctx.spp, ctx.seed = gscene, spp, grad_seed
+        ctx.gscene, ctx.spp, ctx.seed = gscene, grad_spp or spp, grad_seed
+        ctx.scale = float(spp) / float(ctx.spp)
         ctx.shape_a = albedo.shape
         return film
 
@@ -41,13 +42,17 @@ class PathTracedFilm(torch.autograd.Function):
         gv = torch.empty(7, dtype=torch.float32, device=g.device)
         torch.cuda.current_stream().synchronize()
         ctx.gscene.backward_device(g.data_ptr(), ga.data_ptr(), gv.data_ptr(), spp=ctx.spp, seed=ctx.seed)
-        return ga, gv, None, None, None, None
+        if ctx.scale != 1.0:  # the film holds sums of spp samples; the adjoint traced grad_spp
+            ga *= ctx.scale
+            gv *= ctx.scale
+        return ga, gv, None, None, None, None, None
 
 
-def render(albedo, medium, gscene, spp, seed, grad_seed=None):
-    """Differentiable render; grad_seed defaults to a seed decorrelated from `seed`."""
+def render(albedo, medium, gscene, spp, seed, grad_seed=None, grad_spp=None):
+    """Differentiable render; grad_seed defaults to a seed decorrelated from `seed`;
+    grad_spp (default spp) is the number of samples per pixel the adjoint pass traces."""
     return PathTracedFilm.apply(albedo, medium, gscene, spp, seed,
-                                seed + 0x5BD1E995 if grad_seed is None else grad_seed)
+                                seed + 0x5BD1E995 if grad_seed is None else grad_seed, grad_spp)
 
 
 def _camera_hits(gscene, scene, sub):
