@@ -442,6 +442,12 @@ def main():
         image_fixture(os.path.join(HERE, "image_caustic_pt32.npz"), scene=sc)
         image_fixture(os.path.join(HERE, "image_sss_pt32.npz"), scene=scenes.subsurface_cornell(32, 32, 16, 12))
         return
+    if len(sys.argv) > 1 and sys.argv[1] == "bdpt67":
+        # the volumetric-caustic workload's subpath lengths (6 light, 7 eye vertices) on its
+        # area-light, isotropic-medium variant
+        image_fixture(os.path.join(HERE, "image_caustic_bdpt67_32.npz"),
+                      scene=scenes.volumetric_caustic(32, 32, 16, 6, 7, parity=True))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "bdpt":
         image_fixture(os.path.join(HERE, "image_cornell_bdpt32.npz"), scene=scenes.cornell_bdpt(32, 32, 16, 4, 5))
         image_fixture(os.path.join(HERE, "image_caustic_bdpt32.npz"),

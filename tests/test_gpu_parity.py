@@ -390,6 +390,9 @@ def test_gpu_pt_subsurface_matches_reference_3sigma(golden):
 @pytest.mark.parametrize("fixture,builder", [
     ("image_cornell_bdpt32.npz", lambda: scenes.cornell_bdpt(32, 32, 16, 4, 5)),
     ("image_caustic_bdpt32.npz", lambda: scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)),
+    # the volumetric-caustic workload's own subpath lengths (6 light, 7 eye vertices: the
+    # 8-vertex kernel instantiation, every strategy up to path length 12)
+    ("image_caustic_bdpt67_32.npz", lambda: scenes.volumetric_caustic(32, 32, 16, 6, 7, parity=True)),
 ])
 def test_gpu_bdpt_matches_reference_3sigma(golden, fixture, builder):
     """BDPT with MIS (all strategies incl. light tracing splats through the film plane)
