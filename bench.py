@@ -76,7 +76,7 @@ def bench_config(w, world):
     return dict(workload="bvh_bound_pt: Cornell box + displaced sphere", width=w["width"], height=w["height"],
                 spp=w["spp"], max_depth=w["max_depth"], triangles=4 * 4 ** w["levels"],
                 parallelism=f"replicas x{world} (spp shards)",
-                l2="inputs larger than L2 (scene ~170 MB + wave queues ~690 MB per GPU)")
+                l2="inputs larger than L2 (scene ~170 MB + wave queues ~5.9 GB per GPU)")
 
 
 def build_scene(w):
@@ -475,7 +475,9 @@ def our_arm(args):
     pk, pk_kind = peaks()
     traffic = extend_traffic()
     roofline = dict(bound="hbm", achieved=achieved, peak=pk["hbm_gbs"], unit="GB/s", frac=achieved / pk["hbm_gbs"],
-                    traffic=(traffic or {}).get("bytes_per_launch_full_workload"),
+                    # DRAM bytes per closest-hit ray from the committed ncu capture, times this
+                    # run's rays per launch (the capture's launches may hold another wave size)
+                    traffic=traffic["dram_bytes_per_ray"] * rays_per_launch if traffic else None,
                     kernel="pt_extend (closest-hit)", peak_kind=pk_kind,
                     algorithmic_bytes_per_ray=bytes_per_ray, nodes_per_ray=nodes_per_ray, prims_per_ray=prims_per_ray,
                     rays_per_launch=rays_per_launch, avg_launch_ms=avg_launch_ms,

@@ -193,7 +193,7 @@ typedef struct {
     int32_t n_eye;         /* BDPT nE (eye subpath vertices) */
     int32_t spp;           /* samples per pixel, rendered exactly */
     uint64_t seed;         /* Philox key: same seed -> same image */
-    int32_t wave_paths;    /* paths in flight per wave; 0 = library default */
+    int32_t wave_paths;    /* paths in flight per wave; 0 = library default (2^25) */
     int32_t flags;         /* RUMI_FLAG_* */
     void *stream;          /* cudaStream_t, NULL = the library's own stream */
     /* launch tuning (0 = library default; chosen by rumi_b200.autotune) */
@@ -279,7 +279,7 @@ typedef struct {
     int32_t max_depth;       /* path tracer depth shared by the batch */
     const int32_t *spp;      /* samples per pixel of each scene */
     const uint64_t *seeds;   /* Philox seed of each scene */
-    int32_t wave_paths;      /* paths in flight per wave (queue capacity); 0 = default */
+    int32_t wave_paths;      /* paths in flight per wave (queue capacity); 0 = default (2^25) */
     int32_t flags;           /* RUMI_FLAG_TIMING, RUMI_BATCH_GRAPH */
     int32_t blocks_per_sm;   /* persistent traversal blocks per SM; 0 = occupancy limit */
     void *stream;            /* cudaStream_t; NULL = the batch's own stream */

@@ -194,7 +194,7 @@ rumi_status rumi_render_batch(rumi_batch *b, const rumi_batch_params *p, float *
         keys[2 * i] = (uint32_t)p->seeds[i];
         keys[2 * i + 1] = (uint32_t)(p->seeds[i] >> 32) ^ 0x5851F42Du;  // rumi_render's key schedule
     }
-    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 22);
+    long long wave = p->wave_paths > 0 ? p->wave_paths : RUMI_DEFAULT_WAVE_PATHS;
     if (wave < max_spp) wave = max_spp;
     if (wave > path0.back()) wave = path0.back();
     if (wave < max_spp) wave = max_spp;

@@ -994,7 +994,7 @@ static rumi_status ensure_aux(rumi_scene *sc) {
 rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                       cudaStream_t stream, float4 *keep_L) {
     const long long total_pix = (long long)sc->dev.width * sc->dev.height;
-    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 22);
+    long long wave = p->wave_paths > 0 ? p->wave_paths : RUMI_DEFAULT_WAVE_PATHS;
     long long pix_per_wave = wave / p->spp;
     if (pix_per_wave < 1) pix_per_wave = 1;
     if (pix_per_wave > total_pix) pix_per_wave = total_pix;
@@ -1184,7 +1184,7 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
     const int W = sc->dev.width, H = sc->dev.height;
     const int spp = p->spp;
     const long long total_pix = (long long)W * H;
-    long long wave = p->wave_paths > 0 ? p->wave_paths : (1 << 22);
+    long long wave = p->wave_paths > 0 ? p->wave_paths : RUMI_DEFAULT_WAVE_PATHS;
     long long pix_per_wave = wave / spp;
     if (pix_per_wave < 1) pix_per_wave = 1;
     if (pix_per_wave > total_pix) pix_per_wave = total_pix;

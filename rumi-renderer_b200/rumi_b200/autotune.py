@@ -16,10 +16,11 @@ import time
 
 # What the library uses when a knob is 0 (include/rumi_b200.h, rumi_render_params): the
 # speculative while-while walk (trace_mode 4), the occupancy limit of traversal blocks, a
-# refill at 8 idle lanes and 4,194,304 paths per wave.  The search starts there.
-DEFAULTS = dict(trace_mode=4, blocks_per_sm=0, refill_min=8, wave_paths=1 << 22, stack_depth=16)
+# refill at 8 idle lanes, 2^25 paths per wave and 16 stack entries in shared memory.  The
+# search starts there.
+DEFAULTS = dict(trace_mode=4, blocks_per_sm=0, refill_min=8, wave_paths=1 << 25, stack_depth=16)
 SPACE = dict(trace_mode=[4, 5, 1, 2, 3], blocks_per_sm=[0, 4, 5, 6], refill_min=[4, 8, 16],
-             wave_paths=[1 << 21, 1 << 22, 1 << 23], stack_depth=[16, 32, 8])
+             wave_paths=[1 << 25, 1 << 22, 1 << 23, 1 << 24], stack_depth=[16, 32, 8])
 def default_cache_path() -> str:
     """$RUMI_TUNING_CACHE, else autotune_cache.json under the user's cache directory
     ($XDG_CACHE_HOME or ~/.cache)/rumi_b200 -- never inside the package tree."""
@@ -76,7 +77,7 @@ def tune(gs, spp: int, key: str, space: dict = None, repeats: int = 2, film_ptr=
     return result
 
 
-BATCH_WAVES = [1 << 21, 1 << 22, 1 << 23]
+BATCH_WAVES = [1 << 22, 1 << 23, 1 << 24, 1 << 25]
 
 
 def tune_batch(batch, spp, seeds, max_depth: int, key: str, waves=None, repeats: int = 2, log=None,

@@ -20,21 +20,21 @@ class FakeScene:
         ms += {1: 10.0, 2: 0.0, 3: 30.0, 4: 6.0, 5: 7.0}[t["trace_mode"]]
         ms += {0: 4.0, 4: 8.0, 5: 0.0, 6: 2.0}[t["blocks_per_sm"]]
         ms += {4: 0.0, 8: 1.0, 16: 3.0}[t["refill_min"]]
-        ms += {1 << 21: 5.0, 1 << 22: 2.0, 1 << 23: 0.0}[t["wave_paths"]]
+        ms += {1 << 22: 5.0, 1 << 23: 2.0, 1 << 24: 0.0, 1 << 25: 1.0}[t["wave_paths"]]
         ms += {32: 1.0, 16: 0.0, 8: 0.5}[t["stack_depth"]]
         return None, {"total_ms": ms}
 
 
 class FakeBatch:
     def render(self, spp, seeds, max_depth, graph=False, timing=False, wave_paths=0):
-        return None, {"total_ms": {1 << 21: 9.0, 1 << 22: 7.0, 1 << 23: 8.0}[wave_paths]}
+        return None, {"total_ms": {1 << 22: 9.0, 1 << 23: 7.0, 1 << 24: 8.0, 1 << 25: 10.0}[wave_paths]}
 
 
 def test_coordinate_descent_finds_the_optimum_and_caches(tmp_path):
     cache = str(tmp_path / "cache.json")
     g = FakeScene()
     res = autotune.tune(g, spp=4, key="fake", repeats=1, cache_path=cache)
-    assert res["params"] == dict(trace_mode=2, blocks_per_sm=5, refill_min=4, wave_paths=1 << 23, stack_depth=16)
+    assert res["params"] == dict(trace_mode=2, blocks_per_sm=5, refill_min=4, wave_paths=1 << 24, stack_depth=16)
     assert res["ms"] == 100.0
     # one baseline + every alternative value of every knob
     assert g.calls == 1 + sum(len(v) - 1 for v in autotune.SPACE.values())
@@ -45,7 +45,7 @@ def test_coordinate_descent_finds_the_optimum_and_caches(tmp_path):
 def test_batch_queue_capacity(tmp_path):
     cache = str(tmp_path / "cache.json")
     res = autotune.tune_batch(FakeBatch(), [4], [1], 8, key="batch", repeats=1, cache_path=cache)
-    assert res["params"] == dict(wave_paths=1 << 22)
+    assert res["params"] == dict(wave_paths=1 << 23)
     assert autotune.load("batch", cache_path=cache)["ms"] == 7.0
 
 
