@@ -82,7 +82,7 @@ def test_gpu_tune_on_a_small_scene_keeps_the_film(tmp_path):
     torch.cuda.set_device(0)
     gs = rumi_b200.GpuScene(scenes.bvh_bound_pt(64, 64, 4, 6, levels=5, seed=7))
     space = dict(trace_mode=[autotune.DEFAULTS["trace_mode"], 1], blocks_per_sm=[0, 4], refill_min=[8, 16],
-                 wave_paths=[1 << 22, 1 << 14], stack_depth=[16, 8])
+                 wave_paths=[autotune.DEFAULTS["wave_paths"], 1 << 14], stack_depth=[16, 8])
     res = autotune.tune(gs, spp=4, key="small", space=space, repeats=1, cache_path=str(tmp_path / "c.json"))
     assert len(res["history"]) == 1 + 5 and all(h["ms"] > 0 for h in res["history"])
     assert autotune.load("small", cache_path=str(tmp_path / "c.json"))["params"] == res["params"]
