@@ -58,6 +58,14 @@ rumi_status rumi_test_read_bandwidth(const void *buf_dev, int64_t bytes, int32_t
 rumi_status rumi_test_texture_pattern(rumi_scene *scene, int64_t n, const int32_t *prim, const float *pts,
                                       float *out);
 
+/* rumi_trace_rays (host arrays, n rays of 8 floats: o, in_object, d, tmax) through the
+ * traversal scheme trace_mode selects (as rumi_render_params.trace_mode: 1-4 the binary
+ * tree's walks, 5 the eight-wide tree's; 0 = the default), so every scheme's hits can be
+ * compared on the same rays.  t: n distances (0 = miss); prim: n canonical primitive ids
+ * (-1 = miss; any-hit: 1 = occluded, 0 = not). */
+rumi_status rumi_test_trace_scheme(rumi_scene *scene, int64_t n, const float *rays, int32_t anyhit,
+                                   int32_t trace_mode, float *t, int32_t *prim);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,6 +23,7 @@
 #include "shading.cuh"
 #include "camera.cuh"
 #include <vector>
+#include <type_traits>
 
 namespace rumi {
 
@@ -1411,7 +1412,7 @@ struct TraceLaunch {
 
 // Ray queries: the renderer's default traversal scheme (speculative while-while with
 // per-lane refill) over a caller's ray array, in chunks of at most 2^30 rays.
-template <bool ANYHIT, bool STATS>
+template <int MODE, bool ANYHIT, bool STATS>
 __global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) trace_batch_kernel(TraceLaunch T, long long first,
                                                                                          int n, int *fetch_counter) {
     __shared__ int stack[STACK_SMEM * TRACE_THREADS];
@@ -1429,18 +1430,18 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_TRACE_MIN_BLOCKS) trace_ba
         T.t[k] = h.t;
         T.prim[k] = ANYHIT ? (h.t > 0.0f ? 1 : 0) : (h.t > 0.0f ? h.id : -1);
     };
-    traverse_queue<DEFAULT_WALK_MODE, ANYHIT, STACK_SMEM, STATS>(T.s, n, fetch_counter, 8, stack + threadIdx.x,
-                                                                 TRACE_THREADS, fetch, finish, st);
+    traverse_queue<MODE, ANYHIT, STACK_SMEM, STATS>(T.s, n, fetch_counter, 8, stack + threadIdx.x, TRACE_THREADS,
+                                                    fetch, finish, st);
     if (STATS) {
         atomicAdd(&T.counters[1], (unsigned long long)st.nodes);
         atomicAdd(&T.counters[2], (unsigned long long)st.prims);
     }
 }
 
-template <bool ANYHIT, bool STATS>
+template <bool ANYHIT, bool STATS, int MODE = DEFAULT_WALK_MODE>
 static void launch_trace_batch(const TraceLaunch &T, int num_sms, cudaStream_t stream) {
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_batch_kernel<ANYHIT, STATS>, TRACE_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_batch_kernel<MODE, ANYHIT, STATS>, TRACE_THREADS, 0);
     if (occ < 1) occ = 1;
     const long long chunk = 1LL << 30;
     int k = 0;
@@ -1448,7 +1449,7 @@ static void launch_trace_batch(const TraceLaunch &T, int num_sms, cudaStream_t s
         const int n = (int)(T.n - first < chunk ? T.n - first : chunk);
         // one fetch counter per chunk (counters[3 + k]; chunk count is bounded by the caller's n)
         int *ctr = reinterpret_cast<int *>(T.counters + 3) + k;
-        trace_batch_kernel<ANYHIT, STATS><<<num_sms * occ, TRACE_THREADS, 0, stream>>>(T, first, n, ctr);
+        trace_batch_kernel<MODE, ANYHIT, STATS><<<num_sms * occ, TRACE_THREADS, 0, stream>>>(T, first, n, ctr);
     }
 }
 
@@ -1486,6 +1487,48 @@ rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int any
     if (e != cudaSuccess) return cuda_status(e, "trace_rays");
     if (node_visits) *node_visits = (int64_t)(h[1] / 2);  // 16-byte units -> 32-byte nodes
     if (prim_tests) *prim_tests = (int64_t)h[2];
+    return RUMI_OK;
+}
+
+// Ray queries through the traversal scheme trace_mode selects (1..5, as rumi_render_params;
+// 0 = the default), so a test can compare every scheme's hits on the same rays.
+rumi_status trace_rays_scheme(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, int trace_mode,
+                              float *t_dev, int32_t *prim_dev, cudaStream_t stream) {
+    if (n < 0 || n > (1LL << 30)) {
+        set_error("trace_rays_scheme: 0 <= n <= 2^30");
+        return RUMI_ERR_INVALID_ARG;
+    }
+    rumi_status st = ensure_workspace(sc, 256 + 3 * sizeof(unsigned long long) + 64 * sizeof(int));
+    if (st != RUMI_OK) return st;
+    TraceLaunch T;
+    T.s = sc->dev;
+    T.rays = (const float4 *)rays_dev;
+    T.t = t_dev;
+    T.prim = prim_dev;
+    T.n = n;
+    T.anyhit = anyhit;
+    T.counters = (unsigned long long *)sc->ws;
+    cudaMemsetAsync(T.counters, 0, 3 * sizeof(unsigned long long) + 64 * sizeof(int), stream);
+    if (n > 0) {
+        const int m = trace_scheme(trace_mode);
+        auto go = [&](auto mode_tag) {
+            constexpr int M = decltype(mode_tag)::value;
+            if (anyhit)
+                launch_trace_batch<true, false, M>(T, sc->num_sms, stream);
+            else
+                launch_trace_batch<false, false, M>(T, sc->num_sms, stream);
+        };
+        switch (m) {
+            case 0: go(std::integral_constant<int, 0>()); break;
+            case 1: go(std::integral_constant<int, 1>()); break;
+            case 2: go(std::integral_constant<int, 2>()); break;
+            case 3: go(std::integral_constant<int, 3>()); break;
+            default: go(std::integral_constant<int, 4>()); break;
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_status(e, "trace_rays_scheme");
     return RUMI_OK;
 }
 

@@ -106,6 +106,8 @@ rumi_status pt_render_in(rumi_scene *sc, const rumi_render_params *p, float *fil
                          float4 *keep_L = nullptr);
 rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, float *t_dev, int32_t *prim_dev,
                        int64_t *node_visits, int64_t *prim_tests, cudaStream_t stream);
+rumi_status trace_rays_scheme(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, int trace_mode,
+                              float *t_dev, int32_t *prim_dev, cudaStream_t stream);
 rumi_status ensure_workspace(rumi_scene *sc, size_t bytes);
 cudaError_t dalloc(void **p, size_t bytes, cudaStream_t s);
 void dfree(void *p, cudaStream_t s);

@@ -282,3 +282,20 @@ rumi_status rumi_test_texture_pattern(rumi_scene *scene, int64_t n, const int32_
     if (n) k_texture<<<blocks(n), 256>>>(scene->dev, n, (int32_t *)a.p, (float *)b.p, (float *)o.p);
     return from_dev(out, o, 3 * n);
 }
+
+rumi_status rumi_test_trace_scheme(rumi_scene *scene, int64_t n, const float *rays, int32_t anyhit,
+                                   int32_t trace_mode, float *t, int32_t *prim) {
+    if (!scene || n < 0 || (n > 0 && (!rays || !t || !prim)) || trace_mode < 0 || trace_mode > 5)
+        return set_error("rumi_test_trace_scheme: bad argument"), RUMI_ERR_INVALID_ARG;
+    DevBuf dr, dt, dp;
+    rumi_status st = to_dev(dr, rays, 8 * (size_t)n);
+    if (st == RUMI_OK) st = to_dev<float>(dt, nullptr, (size_t)n);
+    if (st == RUMI_OK) st = to_dev<int32_t>(dp, nullptr, (size_t)n);
+    if (st != RUMI_OK) return st;
+    st = trace_rays_scheme(scene, n, (const float *)dr.p, anyhit, trace_mode, (float *)dt.p, (int32_t *)dp.p,
+                           scene->stream);
+    if (st != RUMI_OK) return st;
+    st = from_dev(t, dt, (size_t)n);
+    if (st == RUMI_OK) st = from_dev(prim, dp, (size_t)n);
+    return st;
+}

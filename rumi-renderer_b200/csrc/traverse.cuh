@@ -938,7 +938,11 @@ RUMI_D Ray8 make_ray8(float3 o, float3 d) {
     Ray8 r;
     r.inv = safe_inv(d);
     r.oinv = mk3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
-    r.oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    // the sign bits of the reciprocal, which the slabs are computed with: a -0.0 component
+    // has a negative reciprocal (-2^80) although it does not compare below zero, and its
+    // near plane is the high one
+    r.oct = (__float_as_uint(r.inv.x) >> 31) | ((__float_as_uint(r.inv.y) >> 31) << 1) |
+            ((__float_as_uint(r.inv.z) >> 31) << 2);
     return r;
 }
 

@@ -97,7 +97,7 @@ EXPORTS = ["rumi_scene_create", "rumi_scene_destroy", "rumi_scene_bvh_info", "ru
            "rumi_last_error_string", "rumi_version",
            "rumi_test_philox", "rumi_test_material_sample", "rumi_test_material_fr", "rumi_test_distance_sample",
            "rumi_test_phase_sample", "rumi_test_camera_rays", "rumi_test_pixel_samples",
-           "rumi_test_read_bandwidth", "rumi_test_texture_pattern"]
+           "rumi_test_read_bandwidth", "rumi_test_texture_pattern", "rumi_test_trace_scheme"]
 
 _lib = None
 
@@ -159,6 +159,7 @@ def load(path: str = LIB_PATH):
     L.rumi_test_read_bandwidth.restype = C.c_int
     L.rumi_test_read_bandwidth.argtypes = [vp, C.c_int64, C.c_int32, vp, C.POINTER(C.c_double)]
     L.rumi_test_texture_pattern.argtypes = [vp, C.c_int64, vp, vp, vp]
+    L.rumi_test_trace_scheme.argtypes = [vp, C.c_int64, vp, C.c_int32, C.c_int32, vp, vp]
     L.rumi_last_error_string.restype = C.c_char_p
     L.rumi_version.restype = C.c_char_p
     _lib = L

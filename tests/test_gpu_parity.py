@@ -575,3 +575,59 @@ def test_gpu_eight_wide_walk_hits_match_reference_on_the_1m_mesh():
     np.testing.assert_array_equal(a, b)
     assert sa["extend_prim_tests"] > 0 and sb["extend_prim_tests"] > 0
     assert sb["extend_node_fetches"] < sa["extend_node_fetches"]
+
+
+def _trace_scheme(gs, rays, mode, anyhit=False):
+    """rumi_test_trace_scheme: ray queries (n, 7) through traversal scheme `mode`."""
+    r8 = np.zeros((rays.shape[0], 8), np.float32)
+    r8[:, 0:3], r8[:, 4:7], r8[:, 7] = rays[:, 0:3], rays[:, 3:6], rays[:, 6]
+    t = np.zeros(rays.shape[0], np.float32)
+    prim = np.zeros(rays.shape[0], np.int32)
+    _capi.check(_capi.load().rumi_test_trace_scheme(gs.h, rays.shape[0], r8.ctypes.data_as(C.c_void_p),
+                                                    1 if anyhit else 0, mode, t.ctypes.data_as(C.c_void_p),
+                                                    prim.ctypes.data_as(C.c_void_p)), "rumi_test_trace_scheme")
+    return t, prim
+
+
+def _signed_zero_rays(rng, n):
+    """Rays whose directions hold exact +0.0 and -0.0 components: axis-aligned ones (two
+    zero components) and ones in a coordinate plane (one), zero signs drawn at random,
+    origins inside the box."""
+    o = rng.uniform(0.05, 0.95, (2 * n, 3)).astype(np.float32)
+    d = np.zeros((2 * n, 3), np.float32)
+    axis = rng.integers(0, 3, 2 * n)
+    d[np.arange(n), axis[:n]] = rng.choice([-1.0, 1.0], n)
+    ab = rng.normal(size=(n, 2))
+    ab /= np.linalg.norm(ab, axis=1, keepdims=True)
+    for k in range(n):
+        a = axis[n + k]
+        d[n + k, (a + 1) % 3], d[n + k, (a + 2) % 3] = ab[k]
+    zero = d == 0.0
+    d[zero] = np.where(rng.random(zero.sum()) < 0.5, np.float32(-0.0), np.float32(0.0))
+    assert np.signbit(d[zero]).any() and (~np.signbit(d[zero])).any()
+    return np.concatenate([o, d, np.full((2 * n, 1), 3.4e38, np.float32)], 1).astype(np.float32)
+
+
+def test_gpu_every_traversal_scheme_finds_the_reference_hits_with_signed_zero_directions():
+    """Direction components of exactly -0.0 and +0.0 (axis-aligned and in-plane rays): a
+    -0.0 component has a negative reciprocal although it does not compare below zero, so a
+    walk that picked near and far planes by `d < 0` would cull every box the ray starts in.
+    Every scheme's closest hits and occlusion answers equal the reference's BVHAccel."""
+    sc = scenes.bvh_bound_pt(64, 64, 4, 10, levels=5, seed=7)
+    rng = np.random.default_rng(23)
+    rays = _signed_zero_rays(rng, 2048)
+    gs = rumi_b200.GpuScene(sc)
+    rs = refimpl.RefScene(sc, seed=1)
+    rt, rid = rs.trace(rays)
+    assert (rid >= 0).mean() > 0.9  # inside the closed box nearly every ray hits something
+    sh = rays.copy()
+    sh[:, 6] = np.where(rt > 0, rt * 0.5, 0.5)
+    _, rocc = rs.trace(sh, anyhit=True)
+    for mode in (1, 2, 3, 4, 5):
+        t, prim = _trace_scheme(gs, rays, mode)
+        ties = tie_mask(t, prim, rt, rid)
+        assert np.all((prim == rid) | ties), f"trace_mode {mode}: {np.sum((prim != rid) & ~ties)} rays differ"
+        np.testing.assert_array_equal(t, rt, err_msg=f"trace_mode {mode}")
+        _, occ = _trace_scheme(gs, sh, mode, anyhit=True)
+        np.testing.assert_array_equal(occ, rocc, err_msg=f"trace_mode {mode} (any-hit)")
+    gs.close()
