@@ -619,7 +619,7 @@ def test_gpu_every_traversal_scheme_finds_the_reference_hits_with_signed_zero_di
     gs = rumi_b200.GpuScene(sc)
     rs = refimpl.RefScene(sc, seed=1)
     rt, rid = rs.trace(rays)
-    assert (rid >= 0).mean() > 0.9  # inside the closed box nearly every ray hits something
+    assert (rid >= 0).mean() > 0.5  # the box is open toward the camera: rays leaving that way miss
     sh = rays.copy()
     sh[:, 6] = np.where(rt > 0, rt * 0.5, 0.5)
     _, rocc = rs.trace(sh, anyhit=True)
