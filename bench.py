@@ -849,6 +849,8 @@ def bdpt_arm(args):
     from rumi_b200 import scenes
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     W, H, spp, nL, nE = 512, 512, 32, 6, 7
+    if args.small:  # 128x128: one wave, for profiler captures
+        W = H = 128
     gs = rumi_b200.GpuScene(scenes.volumetric_caustic(W, H, spp, nL, nE))
     stream = torch.cuda.current_stream().cuda_stream
     film = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")

@@ -201,8 +201,10 @@ typedef struct {
                               completion; 2: per-lane ray refill; 3: per-lane refill with
                               leaves intersected warp-wide; 4: speculative while-while walk
                               with per-lane refill.  5: the same walk over the compressed
-                              eight-wide tree.  0: the library default.  Every scheme gives
-                              the same hits and films */
+                              eight-wide tree, collapsed from the binary tree by the scene's
+                              first call that asks for it (rumi_render_noalloc cannot: it
+                              rejects 5 until then).  0: the library default (4).  Every
+                              scheme gives the same hits and films */
     int32_t blocks_per_sm; /* persistent traversal blocks (128 threads) per SM, capped by occupancy */
     int32_t refill_min;    /* idle lanes that trigger a refill (modes 2-5) */
     int32_t stack_depth;   /* traversal stack entries per thread kept in shared memory: 8, 16

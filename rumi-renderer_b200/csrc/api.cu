@@ -106,6 +106,47 @@ rumi_status ensure_workspace(rumi_scene *sc, size_t bytes) {
     return RUMI_OK;
 }
 
+// The compressed eight-wide tree (trace_mode 5), collapsed from the binary tree the first
+// time a call asks for it: a worst-case array first, then an exact copy.  Synchronous on
+// the scene's stream; afterwards sc->dev carries it.
+rumi_status ensure_bvh8(rumi_scene *sc) {
+    if (sc->nodes8) return RUMI_OK;
+    cudaStream_t s = sc->stream;
+    const int N = sc->dev.n_prims;
+    const int cap8 = bvh8_node_capacity(N);
+    Bvh8Node *tmp8 = nullptr;
+    void *scratch8 = nullptr;
+    float4 *prims8 = nullptr;
+    cudaError_t e = dalloc((void **)&tmp8, sizeof(Bvh8Node) * (size_t)cap8, s);
+    if (e == cudaSuccess) e = dalloc((void **)&prims8, sizeof(float4) * 3 * (size_t)(N > 0 ? N : 1), s);
+    if (e == cudaSuccess) e = dalloc(&scratch8, bvh8_scratch_bytes(N), s);
+    int n8 = -1;
+    if (e == cudaSuccess) n8 = bvh8_collapse(sc->nodes, sc->n_nodes, sc->leaf_prims, N, tmp8, cap8, prims8, scratch8, s);
+    Bvh8Node *nodes8 = nullptr;
+    if (e == cudaSuccess && n8 > 0) e = dalloc((void **)&nodes8, sizeof(Bvh8Node) * (size_t)n8, s);
+    if (e == cudaSuccess && n8 > 0)
+        e = cudaMemcpyAsync(nodes8, tmp8, sizeof(Bvh8Node) * (size_t)n8, cudaMemcpyDeviceToDevice, s);
+    dfree(tmp8, s);
+    dfree(scratch8, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    // stack entries hold node << 8: fewer than 2^24 nodes
+    if (e != cudaSuccess || n8 <= 0 || n8 >= (1 << 24)) {
+        dfree(nodes8, s);
+        dfree(prims8, s);
+        cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "eight-wide BVH");
+        set_error("eight-wide BVH collapse failed");
+        return RUMI_ERR_INTERNAL;
+    }
+    sc->nodes8 = nodes8;
+    sc->prims8 = prims8;
+    sc->n_nodes8 = n8;
+    sc->dev.nodes8 = nodes8;
+    sc->dev.prims8 = prims8;
+    sc->dev.n_nodes8 = n8;
+    return RUMI_OK;
+}
+
 }  // namespace rumi
 
 using namespace rumi;
@@ -570,36 +611,6 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
         }
         sc->n_nodes4 = n4;
     }
-    {
-        // compressed eight-wide tree: collapse into a worst-case array, then keep an exact copy
-        const int cap8 = bvh8_node_capacity(N);
-        Bvh8Node *tmp8 = nullptr;
-        void *scratch8 = nullptr;
-        e = dalloc((void **)&tmp8, sizeof(Bvh8Node) * (size_t)cap8, s);
-        if (e == cudaSuccess) e = dalloc((void **)&sc->prims8, sizeof(float4) * 3 * (size_t)(N > 0 ? N : 1), s);
-        if (e == cudaSuccess) e = dalloc(&scratch8, bvh8_scratch_bytes(N), s);
-        int n8 = -1;
-        if (e == cudaSuccess)
-            n8 = bvh8_collapse(sc->nodes, sc->n_nodes, sc->leaf_prims, N, tmp8, cap8, sc->prims8, scratch8, s);
-        if (e == cudaSuccess && n8 > 0) e = dalloc((void **)&sc->nodes8, sizeof(Bvh8Node) * (size_t)n8, s);
-        if (e == cudaSuccess && n8 > 0)
-            e = cudaMemcpyAsync(sc->nodes8, tmp8, sizeof(Bvh8Node) * (size_t)n8, cudaMemcpyDeviceToDevice, s);
-        dfree(tmp8, s);
-        dfree(scratch8, s);
-        if (e != cudaSuccess) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            return fail(cuda_status(e, "eight-wide BVH"));
-        }
-        // stack entries hold node << 8: fewer than 2^24 nodes
-        if (n8 < 0 || n8 >= (1 << 24)) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            set_error("eight-wide BVH collapse failed");
-            return fail(RUMI_ERR_INTERNAL);
-        }
-        sc->n_nodes8 = n8;
-    }
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0.0f;
@@ -637,6 +648,10 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     ds.n_textures = sc->textures ? d->n_textures : 0;
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(cuda_status(e, "scene upload"));
+    if (uses_bvh8(0)) {  // the default walk is the eight-wide one: its tree is needed at once
+        const rumi_status st8 = ensure_bvh8(sc);
+        if (st8 != RUMI_OK) return fail(st8);
+    }
     *out = sc;
     return RUMI_OK;
 }

@@ -87,6 +87,11 @@ extern "C" rumi_status rumi_render_noalloc(rumi_scene *sc, const rumi_render_par
                   std::to_string(max_paths) + " paths the 16 MiB scratch holds");
         return RUMI_ERR_INVALID_ARG;
     }
+    if (uses_bvh8(p->trace_mode) && !sc->nodes8) {  // building it would allocate
+        set_error("rumi_render_noalloc: the eight-wide tree (trace_mode 5) is built by the scene's first "
+                  "rumi_render or rumi_trace_rays call that asks for it; none has yet");
+        return RUMI_ERR_INVALID_ARG;
+    }
     const long long total_pix = (long long)sc->dev.width * sc->dev.height;
     long long pix_per_wave = (p->wave_paths > 0 ? (long long)p->wave_paths : max_paths) / p->spp;
     if (pix_per_wave < 1) pix_per_wave = 1;

@@ -879,6 +879,7 @@ static constexpr int DEFAULT_WALK_MODE = RUMI_WALK8 ? 4 : 3;
 static inline int trace_scheme(int trace_mode) {
     return trace_mode >= 1 && trace_mode <= 5 ? trace_mode - 1 : DEFAULT_WALK_MODE;
 }
+bool uses_bvh8(int trace_mode) { return trace_scheme(trace_mode) == 4; }
 
 using ExtendKernel = void (*)(PtLaunch, int);
 using ShadowKernel = void (*)(PtLaunch);
@@ -1006,6 +1007,7 @@ rumi_status pt_render(rumi_scene *sc, const rumi_render_params *p, float *film_d
     }
     rumi_status st = ensure_workspace(sc, pt_workspace_bytes(n_paths_max));
     if (st != RUMI_OK) return st;
+    if (uses_bvh8(p->trace_mode) && (st = ensure_bvh8(sc)) != RUMI_OK) return st;
     if ((st = ensure_aux(sc)) != RUMI_OK) return st;
     return pt_render_in(sc, p, film_dev, stats, stream, sc->ws, pix_per_wave,
                         RUMI_PT_OVERLAP != 0 && !(p->flags & RUMI_FLAG_SERIAL), keep_L);
@@ -1196,6 +1198,7 @@ rumi_status pt_backward(rumi_scene *sc, const rumi_render_params *p, const float
     }
     rumi_status st = ensure_workspace(sc, pt_adjoint_workspace_bytes((long long)Wp));
     if (st != RUMI_OK) return st;
+    if (uses_bvh8(p->trace_mode) && (st = ensure_bvh8(sc)) != RUMI_OK) return st;
     const bool overlap = RUMI_PT_OVERLAP != 0 && !(p->flags & RUMI_FLAG_SERIAL);
     if (overlap && (st = ensure_aux(sc)) != RUMI_OK) return st;
     // the forward pass of this very frame kept its per-path radiance: pass 1 is not traced
@@ -1500,6 +1503,7 @@ rumi_status trace_rays_scheme(rumi_scene *sc, int64_t n, const float *rays_dev, 
     }
     rumi_status st = ensure_workspace(sc, 256 + 3 * sizeof(unsigned long long) + 64 * sizeof(int));
     if (st != RUMI_OK) return st;
+    if (uses_bvh8(trace_mode) && (st = ensure_bvh8(sc)) != RUMI_OK) return st;
     TraceLaunch T;
     T.s = sc->dev;
     T.rays = (const float4 *)rays_dev;

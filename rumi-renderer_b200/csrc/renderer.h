@@ -109,6 +109,10 @@ rumi_status trace_rays(rumi_scene *sc, int64_t n, const float *rays_dev, int any
 rumi_status trace_rays_scheme(rumi_scene *sc, int64_t n, const float *rays_dev, int anyhit, int trace_mode,
                               float *t_dev, int32_t *prim_dev, cudaStream_t stream);
 rumi_status ensure_workspace(rumi_scene *sc, size_t bytes);
+// builds the eight-wide tree on first use (trace_mode 5); a no-op once built
+rumi_status ensure_bvh8(rumi_scene *sc);
+// true when trace_mode selects the eight-wide walk
+bool uses_bvh8(int trace_mode);
 cudaError_t dalloc(void **p, size_t bytes, cudaStream_t s);
 void dfree(void *p, cudaStream_t s);
 void configure_pool(int device);
