@@ -138,3 +138,24 @@ def test_noalloc_pixel_at_the_array_capacity():
     np.testing.assert_allclose(film_dev.cpu().numpy(), want, rtol=1e-6, atol=0)
     assert st.paths == wst["paths"] == 2 * cap
     gs.close()
+
+
+def test_noalloc_eight_wide_walk_only_after_its_tree_is_built():
+    """trace_mode 5 needs the eight-wide tree, which the library collapses on first use;
+    the no-allocation entry point cannot build it, so it refuses 5 until a regular call
+    has, and afterwards renders the film rumi_render renders with 5."""
+    import torch
+    torch.cuda.set_device(0)
+    lib = _capi.load()
+    gs = rumi_b200.GpuScene(scenes.cornell_pt(48, 40, 4, 4))
+    film_dev = torch.zeros((40, 48, 3), dtype=torch.float32, device="cuda")
+    p = _params(4, 4, 5)
+    p.trace_mode = 5
+    st = _capi.rumi_render_stats()
+    assert lib.rumi_render_noalloc(gs.h, C.byref(p), C.c_void_p(film_dev.data_ptr()), C.byref(st)) != 0
+    assert b"eight-wide" in lib.rumi_last_error_string()
+    want, _ = gs.render(spp=4, seed=5, trace_mode=5)  # builds the tree
+    rc = lib.rumi_render_noalloc(gs.h, C.byref(p), C.c_void_p(film_dev.data_ptr()), C.byref(st))
+    assert rc == 0, lib.rumi_last_error_string()
+    np.testing.assert_allclose(film_dev.cpu().numpy(), want, rtol=1e-6, atol=0)
+    gs.close()
