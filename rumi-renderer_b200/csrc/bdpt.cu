@@ -158,13 +158,14 @@ RUMI_D float3 vert_fr(const DevScene &S, const BVert &v, float3 n, float3 wi, fl
     return material_fr(m, vert_albedo(S, v, m), n, wi, wo, v.in_obj, v.xi, v.pdf_path, v.t_in, v.vtau / v.vpdf);
 }
 
-// Subpath construction shared by both directions.  EYE: ConstructViewPath, else
+// Subpath construction shared by both directions.  eye: ConstructViewPath, else
 // ConstructLightPath.  V[0] is prepared by the caller; seg_d[k] receives the direction of
 // the segment from V[k] to V[k+1]; alpha[] the subpath throughputs.  Returns the vertex count.
-template <bool EYE>
-RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, uint32_t stream_base, float3 o,
-                             float3 d, BVert *V, float3 *seg_d, float3 *alpha, const DevLight &light, float3 light_n,
-                             int *stack, TraceStats &st) {
+// The direction is a run-time argument: the caller's one call site serves both subpaths,
+// so the kernel holds one copy of this code (the kernel is bound by instruction fetch).
+RUMI_D int construct_subpath(const BdLaunch &P, bool eye, int max_depth, uint64_t path, uint32_t stream_base,
+                             float3 o, float3 d, BVert *V, float3 *seg_d, float3 *alpha, const DevLight &light,
+                             float3 light_n, int *stack, TraceStats &st) {
     const DevScene &S = P.s;
     const DevVolume &vol = S.volume;
     bool le = true, in_object = false;
@@ -243,7 +244,7 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
         // cosine at the start vertex on its outgoing side
         float cos_s;
         if (start.onsurface) {
-            const bool use_stored = EYE ? (depth == 0 || !start.dirac) : !start.dirac;
+            const bool use_stored = eye ? (depth == 0 || !start.dirac) : !start.dirac;
             if (use_stored) {
                 cos_s = start.cos_a;
             } else {
@@ -270,7 +271,7 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
         float dwda = cos_e / (dist * dist);
         float fwd;
         if (start.onsurface) {
-            const bool plain = EYE ? (depth == 0 || !start.dirac) : !start.dirac;
+            const bool plain = eye ? (depth == 0 || !start.dirac) : !start.dirac;
             fwd = plain ? start.pdf_dir * dwda : start.pdf_dir * dwda * start.cos_a;
         } else {
             fwd = start.pdf_dir * dwda * start.cos_a;
@@ -280,6 +281,8 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
         // backward pdf of the start vertex
         dwda = cos_s / (dist * dist);
         const bool end_le = has_mat && m.type == MAT_EMISSIVE;
+        // the end surface's pdf of the reversed direction (both start kinds use it)
+        const float pw_end = end.onsurface && !end_le ? material_pdfw(m, end.xi, n, w, wrev) : 0.0f;
         float3 bwd;
         if (start.onsurface) {
             if (end.onsurface) {
@@ -292,7 +295,7 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
                     if (pw <= 0.0f) pw = 1e-4f;
                     bwd = c3(pw * dwda);
                 } else {
-                    pw = material_pdfw(m, end.xi, n, w, wrev);
+                    pw = pw_end;
                     bwd = end.dirac ? c3(pw * dwda * end.cos_b) : c3(pw * dwda);
                 }
                 if (vol.present && !end.in_obj) bwd = bwd * end.vpdf;
@@ -313,7 +316,7 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
                     if (pw <= 0.0f) pw = 1e-4f;
                     bwd = pdf_s * (pw * dwda);
                 } else {
-                    const float pw = material_pdfw(m, end.xi, n, w, wrev);
+                    const float pw = pw_end;
                     bwd = end.dirac ? pdf_s * (pw * dwda * end.cos_b) : pdf_s * (pw * dwda);
                 }
             } else {
@@ -326,7 +329,7 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
         float3 a = alpha[depth];
         if (start.onsurface) {
             if (depth == 0) {
-                if (EYE) {
+                if (eye) {
                     const DevCamera &c = S.camera;
                     const float cs = start.cos_a;
                     const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
@@ -335,18 +338,18 @@ RUMI_D int construct_subpath(const BdLaunch &P, int max_depth, uint64_t path, ui
                     a = a * (light_emission(light) / start.pdf_fwd * G);  // Light::L / pick pdf
                 }
             } else {
-                const float3 fr = EYE ? vert_fr(S, start, start.n, d, prev_w) : vert_fr(S, start, start.n, prev_w, d);
+                const float3 fr = vert_fr(S, start, start.n, eye ? d : prev_w, eye ? prev_w : d);
                 a = a * (fr / (start.pdf_fwd * start.pdf_path) * G);
                 // the surface's texture (bidirectionalpathtracer.cpp:660-661, 971-972)
                 if (S.prim_tex && start.prim >= 0) a = a * tex_pattern(S, start.prim, start.p);
             }
         } else {
-            const float fp = EYE ? phase_value(vol, d, prev_w) : phase_value(vol, prev_w, d);
+            const float fp = phase_value(vol, eye ? d : prev_w, eye ? prev_w : d);
             a = a * ((vol.sigma_s * fp) / (start.pdf_fwd * start.pdf_path) * G);
         }
         if (vol.present && !end.in_obj) a = a * end.vtau;
         alpha[depth + 1] = a;
-        if (EYE) {
+        if (eye) {
             if (end_le) {
                 const float3 fr = end.onsurface ? vert_fr(S, end, n, w, wrev) : mk3(0, 0, 0);
                 alpha[depth + 2] = a * (fr / (end.pdf_fwd * end.pdf_path));
@@ -410,123 +413,91 @@ RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, 
     if (s_connect && s_prev) sd = sqrtf(dot3(s_connect->p - s_prev->p, s_connect->p - s_prev->p));
     if (t_connect && t_prev) td = sqrtf(dot3(t_connect->p - t_prev->p, t_connect->p - t_prev->p));
 
-    // pdf of sampling `to` from `from` along direction dir (length len) in the
-    // reference's form: Tr (surface end) or PdfDistance (medium end) of the segment.
-    if (s_connect) {
+    // The two connection-side blocks of MISWeight mirror each other: side 0 gives the light
+    // vertex X = s_connect the pdf of being sampled from Y = t_connect (sb / sf) and its
+    // predecessor the pdf of being sampled from X; side 1 the same with the roles swapped
+    // (tb / tf).  One loop body serves both, so the kernel holds one copy of this code.
+    // pdf of sampling X from Y along the connection in the reference's form: Tr (surface
+    // end) or PdfDistance (medium end) of the segment, times the density of the direction
+    // at Y (a material, the camera or the light at a subpath's first vertex, or the phase
+    // function in the medium).
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const bool sl = side == 0;
+        const BVert *X = sl ? s_connect : t_connect, *Y = sl ? t_connect : s_connect;
+        const BVert *Xp = sl ? s_prev : t_prev;
+        if (!X || !Y) continue;                                       // ns == 0: side 1 below
+        const int nx = sl ? ns : nt, ny = sl ? nt : ns;
+        const float3 y_to_x = sl ? connect_wi : connect_wo, x_to_y = sl ? connect_wo : connect_wi;
+        const float3 y_in = sl ? t_wo : s_wi, x_in = sl ? s_wi : t_wo;  // toward Y's / X's predecessor
+        const float xd = sl ? sd : td;
+        float3 *xb = sl ? sb : tb, *xf = sl ? sf : tf;
         float3 pdf_s = c3(1.0f);
         float dwda;
-        if (s_connect->onsurface) {
+        if (X->onsurface) {
             if (vol.present) {
                 bool vh;
-                const float sm = vol_segment(vol, t_connect->p, connect_wi, connect_d, vh);
+                const float sm = vol_segment(vol, Y->p, y_to_x, connect_d, vh);
                 if (vh) pdf_s = vol_tr(vol, sm);
             }
-            dwda = dot3(s_connect->n, connect_wo) / (connect_d * connect_d);
+            dwda = dot3(X->n, x_to_y) / (connect_d * connect_d);
         } else {
             dwda = 1.0f / (connect_d * connect_d);
             bool vh;
-            const float sm = vol_segment(vol, t_connect->p, connect_wi, connect_d, vh);
+            const float sm = vol_segment(vol, Y->p, y_to_x, connect_d, vh);
             if (vh) pdf_s = vol_pdf_distance(vol, sm);
         }
         float pw;
-        if (t_connect->onsurface)
-            pw = nt > 1 ? material_pdfw(S.materials[t_connect->mat], t_connect->xi, t_connect->n, t_wo, connect_wi)
-                        : camera_pdfw(S.camera, connect_wi);
-        else
-            pw = phase_value(vol, t_wo, connect_wi);
-        sb[ns - 1] = pdf_s * (pw * dwda);
-        sf[ns - 1] = s_connect->pdf_fwd;
-        if (s_prev) {
-            if (s_prev->onsurface && s_prev->dirac) {
-                sb[ns - 2] = c3(1.0f);
-                sf[ns - 2] = c3(1.0f);
+        if (Y->onsurface) {
+            if (ny > 1)
+                pw = material_pdfw(S.materials[Y->mat], Y->xi, Y->n, y_in, y_to_x);
+            else if (sl)
+                pw = camera_pdfw(S.camera, connect_wi);
+            else
+                pw = light.type == LIGHT_SPOT ? spot_pdf_dir(light) : light_pdfw(connect_wo, light_n);
+        } else {
+            pw = phase_value(vol, y_in, y_to_x);
+        }
+        xb[nx - 1] = pdf_s * (pw * dwda);
+        xf[nx - 1] = X->pdf_fwd;
+        if (Xp) {
+            if (Xp->onsurface && Xp->dirac) {
+                xb[nx - 2] = c3(1.0f);
+                xf[nx - 2] = c3(1.0f);
             } else {
                 float3 ps = c3(1.0f);
                 float dw;
-                if (s_prev->onsurface) {
+                if (Xp->onsurface) {
                     if (vol.present) {
                         bool vh;
-                        const float sm = vol_segment(vol, s_connect->p, s_wi, sd, vh);
+                        const float sm = vol_segment(vol, X->p, x_in, xd, vh);
                         if (vh) ps = vol_tr(vol, sm);
                     }
-                    dw = -dot3(s_prev->n, s_wi) / (sd * sd);
+                    dw = -dot3(Xp->n, x_in) / (xd * xd);
                 } else {
-                    dw = 1.0f / (sd * sd);
+                    dw = 1.0f / (xd * xd);
                     bool vh;
-                    const float sm = vol_segment(vol, s_connect->p, s_wi, sd, vh);
+                    const float sm = vol_segment(vol, X->p, x_in, xd, vh);
                     if (vh) ps = vol_pdf_distance(vol, sm);
                 }
-                const float pw2 = s_connect->onsurface ? material_pdfw(S.materials[s_connect->mat], s_connect->xi,
-                                                                       s_connect->n, connect_wo, s_wi)
-                                                       : phase_value(vol, connect_wo, s_wi);
-                sb[ns - 2] = ps * (pw2 * dw);
-                sf[ns - 2] = s_prev->pdf_fwd;
+                const float pw2 = X->onsurface
+                                      ? material_pdfw(S.materials[X->mat], X->xi, X->n, x_to_y, x_in)
+                                      : phase_value(vol, x_to_y, x_in);
+                xb[nx - 2] = ps * (pw2 * dw);
+                xf[nx - 2] = Xp->pdf_fwd;
             }
         }
     }
-    if (t_connect) {
-        if (ns > 0) {
-            float3 pdf_s = c3(1.0f);
-            float dwda;
-            if (t_connect->onsurface) {
-                if (vol.present) {
-                    bool vh;
-                    const float sm = vol_segment(vol, s_connect->p, connect_wo, connect_d, vh);
-                    if (vh) pdf_s = vol_tr(vol, sm);
-                }
-                dwda = dot3(t_connect->n, connect_wi) / (connect_d * connect_d);
-            } else {
-                dwda = 1.0f / (connect_d * connect_d);
-                bool vh;
-                const float sm = vol_segment(vol, s_connect->p, connect_wo, connect_d, vh);
-                if (vh) pdf_s = vol_pdf_distance(vol, sm);
-            }
-            float pw;
-            if (s_connect->onsurface)
-                pw = ns > 1 ? material_pdfw(S.materials[s_connect->mat], s_connect->xi, s_connect->n, s_wi, connect_wo)
-                            : (light.type == LIGHT_SPOT ? spot_pdf_dir(light) : light_pdfw(connect_wo, light_n));
-            else
-                pw = phase_value(vol, s_wi, connect_wo);
-            tb[nt - 1] = pdf_s * (pw * dwda);
-            tf[nt - 1] = t_connect->pdf_fwd;
-            if (t_prev) {
-                if (t_prev->onsurface && t_prev->dirac) {
-                    tb[nt - 2] = c3(1.0f);
-                    tf[nt - 2] = c3(1.0f);
-                } else {
-                    float3 ps = c3(1.0f);
-                    float dw;
-                    if (t_prev->onsurface) {
-                        if (vol.present) {
-                            bool vh;
-                            const float sm = vol_segment(vol, t_connect->p, t_wo, td, vh);
-                            if (vh) ps = vol_tr(vol, sm);
-                        }
-                        dw = -dot3(t_prev->n, t_wo) / (td * td);
-                    } else {
-                        dw = 1.0f / (td * td);
-                        bool vh;
-                        const float sm = vol_segment(vol, t_connect->p, t_wo, td, vh);
-                        if (vh) ps = vol_pdf_distance(vol, sm);
-                    }
-                    const float pw2 = t_connect->onsurface ? material_pdfw(S.materials[t_connect->mat], t_connect->xi,
-                                                                           t_connect->n, connect_wi, t_wo)
-                                                           : phase_value(vol, connect_wi, t_wo);
-                    tb[nt - 2] = ps * (pw2 * dw);
-                    tf[nt - 2] = t_prev->pdf_fwd;
-                }
-            }
+    if (t_connect && ns == 0) {
+        // the eye subpath reached a light by itself ("kajiya" strategy)
+        tb[nt - 1] = VE[nt - 1].pdf_bwd;
+        tf[nt - 1] = VE[nt - 1].pdf_fwd;
+        if (t_prev->dirac) {
+            tb[nt - 2] = c3(1.0f);
+            tf[nt - 2] = c3(1.0f);
         } else {
-            // the eye subpath reached a light by itself ("kajiya" strategy)
-            tb[nt - 1] = VE[nt - 1].pdf_bwd;
-            tf[nt - 1] = VE[nt - 1].pdf_fwd;
-            if (t_prev->dirac) {
-                tb[nt - 2] = c3(1.0f);
-                tf[nt - 2] = c3(1.0f);
-            } else {
-                tb[nt - 2] = VE[nt - 2].pdf_bwd;
-                tf[nt - 2] = VE[nt - 2].pdf_fwd;
-            }
+            tb[nt - 2] = VE[nt - 2].pdf_bwd;
+            tf[nt - 2] = VE[nt - 2].pdf_fwd;
         }
     }
     for (int i = 0; i < ns - 2; ++i) {
@@ -652,7 +623,6 @@ RUMI_D BdLight build_subpaths(const BdLaunch &P, int j, BVert *VE, float3 *segE,
         VE[0].pdf_dir = c.plane_dist * c.plane_dist / (l.z * l.z * l.z * c.film_area);
         VE[0].pdf_fwd = c3(1.0f);
     }
-    nE = construct_subpath<true>(P, P.nE, path, 2000u, eo, ed, VE, segE, aE, light, light_n, stk, st);
     // light subpath start: cosine-weighted emission from an area light
     // (AreaLight::SolidAngleSampling), uniform in the cone from a spot
     const bool spot = light.type == LIGHT_SPOT;
@@ -671,7 +641,18 @@ RUMI_D BdLight build_subpaths(const BdLaunch &P, int j, BVert *VE, float3 *segE,
         VL[0].pdf_dir = emit.pdf;
         VL[0].cos_a = dot3(emit.wi, light_n);
     }
-    nLv = construct_subpath<false>(P, P.nL, path, 3000u, ls.P, emit_w, VL, segL, aL, light, light_n, stk, st);
+    // the eye subpath, then the light subpath, through one call site
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const bool eye = side == 0;
+        const int nv = construct_subpath(P, eye, eye ? P.nE : P.nL, path, eye ? 2000u : 3000u, eye ? eo : ls.P,
+                                         eye ? ed : emit_w, eye ? VE : VL, eye ? segE : segL, eye ? aE : aL, light,
+                                         light_n, stk, st);
+        if (eye)
+            nE = nv;
+        else
+            nLv = nv;
+    }
     // a delta position: the strategies in which the eye subpath reaches the light carry
     // no weight (the MIS sums skip a dirac first light vertex)
     if (spot) VL[0].dirac = true;
@@ -758,29 +739,37 @@ RUMI_D int strategy(const BdLaunch &P, int j, int len, int t, const BVert *VE, c
     // VolumetricTest reads its own uniform, so it may come before the visibility test
     const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
     if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) return STRAT_NONE;
-    float3 cE, cL;
-    if (t == 0) {
-        const DevCamera &c = S.camera;
-        const float cs = dot3(tc.n, cwi);
-        const float We = c.plane_dist * c.plane_dist / (c.film_area * cs * cs * cs * cs);
-        cE = c3(We / avg3(tc.pdf_fwd));
-    } else if (tc.onsurface) {
-        cE = vert_fr(S, tc, tc.n, cwi, t_wo) / (tc.pdf_fwd * tc.pdf_path);
-    } else {
-        cE = (S.volume.sigma_s * phase_value(S.volume, cwi, t_wo)) / (tc.pdf_fwd * tc.pdf_path);
+    // the eye end's and the light end's factors through one loop body (one copy of the
+    // material code in the kernel)
+    float3 cf[2];
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const bool ee = side == 0;
+        const BVert &v = ee ? tc : sc;
+        const int k = ee ? t : s;
+        const float3 wa = ee ? cwi : s_wi, wb = ee ? t_wo : cwo;
+        float3 c;
+        if (k == 0) {
+            if (ee) {
+                const DevCamera &cam = S.camera;
+                const float cs = dot3(tc.n, cwi);
+                const float We = cam.plane_dist * cam.plane_dist / (cam.film_area * cs * cs * cs * cs);
+                c = c3(We / avg3(tc.pdf_fwd));
+            } else {
+                c = light_emission(light) / sc.pdf_fwd;
+            }
+        } else if (v.onsurface) {
+            c = vert_fr(S, v, v.n, wa, wb) / (v.pdf_fwd * v.pdf_path);
+        } else {
+            c = (S.volume.sigma_s * phase_value(S.volume, wa, wb)) / (v.pdf_fwd * v.pdf_path);
+        }
+        // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
+        // 350-351): a medium vertex takes the texture of the surface its segment was
+        // headed for, evaluated at the medium point; none without such a surface
+        if (k > 0 && S.prim_tex && v.prim >= 0) c = c * tex_pattern(S, v.prim, v.p);
+        cf[side] = c;
     }
-    // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
-    // 350-351): a medium vertex takes the texture of the surface its segment was headed
-    // for, evaluated at the medium point; none without such a surface
-    if (t > 0 && S.prim_tex && tc.prim >= 0) cE = cE * tex_pattern(S, tc.prim, tc.p);
-    if (s == 0) {
-        cL = light_emission(light) / sc.pdf_fwd;
-    } else if (sc.onsurface) {
-        cL = vert_fr(S, sc, sc.n, s_wi, cwo) / (sc.pdf_fwd * sc.pdf_path);
-    } else {
-        cL = (S.volume.sigma_s * phase_value(S.volume, s_wi, cwo)) / (sc.pdf_fwd * sc.pdf_path);
-    }
-    if (s > 0 && S.prim_tex && sc.prim >= 0) cL = cL * tex_pattern(S, sc.prim, sc.p);
+    const float3 cE = cf[0], cL = cf[1];
     const float3 lo = aE[t] * cE * G * cL * aL[s];
     out.lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
     // the shadow ray of VisibilityTest (:1018-1050): from the eye vertex unless the eye
