@@ -6,7 +6,8 @@
 // entirely on the GPU and deterministically (same input -> same tree):
 //
 //  large phase (tasks with > SMALL_MAX primitives), one level per iteration:
-//    make_chunks   one block: chunk list (CHUNK primitives each) + bin reset per task
+//    make_chunks   one block: chunk list (CHUNK primitives each); reset_bins: empty bins
+//                  for every task
 //    bin           one block per chunk: 3 axes x 32 centroid bins in shared memory,
 //                  merged into the task's bins with global atomics (ordered-int floats)
 //    split         one warp per task, lane = bin: prefix/suffix scans, SAH argmin
@@ -237,8 +238,13 @@ __global__ void make_chunks_kernel(const BuildTask *tasks, const int *n_tasks_p,
         __syncthreads();
     }
     if (threadIdx.x == 0) *n_chunks = s_base;
-    // reset bins
-    for (int i = threadIdx.x; i < n_tasks * 3 * NBINS; i += blockDim.x) {
+}
+
+// Empty bins for every task of the level (count 0, bounds +inf / -inf as ordered ints),
+// grid-stride: a level can hold thousands of tasks.
+__global__ void reset_bins_kernel(const int *n_tasks_p, int *bins /*[task][3][NBINS][7]*/) {
+    const int n = *n_tasks_p * 3 * NBINS;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int *b = bins + 7 * (size_t)i;
         b[0] = 0;
         b[1] = b[2] = b[3] = f2o(INFINITY);
@@ -974,6 +980,7 @@ int bvh_build(const float *d_tri_v, int n_tris, const float4 *d_rects, const int
         int *nnext = counters + 1;
         const int max_ch = (int)(n / CHUNK) + h_n_tasks + 1;
         make_chunks_kernel<<<1, 1024, 0, stream>>>(tasks[cur], ncur, chunks, n_chunks, bins);
+        reset_bins_kernel<<<cdiv(h_n_tasks * 3 * NBINS, 256), 256, 0, stream>>>(ncur, bins);
         bin_kernel<<<max_ch, BIN_THREADS, 0, stream>>>(chunks, n_chunks, idx, aabb_lo, aabb_hi, cbs[cur], bins);
         split_kernel<<<cdiv(h_n_tasks * 32, 128), 128, 0, stream>>>(tasks[cur], ncur, bins, nodes, dec);
         count_kernel<<<max_ch, BIN_THREADS, 0, stream>>>(chunks, n_chunks, tasks[cur], dec, idx, aabb_lo, aabb_hi,
