@@ -691,111 +691,99 @@ RUMI_D int strategy(const BdLaunch &P, int j, int len, int t, const BVert *VE, c
         return STRAT_NONE;
     }
     const BVert &tc = VE[t];
-    // MISWeight's arguments and the unweighted contribution; one call site of MISWeight
-    // serves both kinds of strategy (one copy of it in the kernel)
-    int mw_ns = 0, mw_nt = t + 1;
-    float3 mw_wi = mk3(0, 0, 0), mw_wo = mk3(0, 0, 0), pre = mk3(0, 0, 0);
-    int result = STRAT_SHADOW;
-    if (t > 0 && tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
-        stop = true;
-        if (len != nE - 1) return STRAT_NONE;
-        result = STRAT_ADD;  // aE[t + 1] weighted by MISWeight(0, t + 1)
-        pre = aE[t + 1];
-    } else {
-        // false: the strategy is rejected
-        auto shadow_terms = [&]() -> bool {
-            float3 t_wo = mk3(0, 0, 0);
-            if (t > 0) {
-                t_wo = -segE[t - 1];
-                if (tc.dirac) return false;
+    float3 t_wo = mk3(0, 0, 0);
+    if (t > 0) {
+        t_wo = -segE[t - 1];
+        if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
+            stop = true;
+            if (len == nE - 1) {
+                const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
+                out.lo = aE[t + 1] * w;
+                return STRAT_ADD;
             }
-            const int s = len - (t + 1);
-            if (s >= nLv || s <= -1) return false;
-            const BVert &sc = VL[s];
-            float3 s_wi = mk3(0, 0, 0);
-            if (s > 0) {
-                s_wi = -segL[s - 1];
-                if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) return false;
-                if (sc.dirac) return false;
-            }
-            // the geometric rejections come before the two visibility tests: they read no random
-            // numbers and change nothing, so the order only saves traversals
-            const float3 cwi = normalize_ref(sc.p - tc.p);
-            const float3 cwo = normalize_ref(tc.p - sc.p);
-            const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
-            if (ci < 1e-4f) return false;
-            float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
-            if (s == 0 && spot) {
-                if (dot3(cwo, light.direction) < light.cos_cone) return false;  // outside the cone
-                co = 1.0f;                                                         // no cosine at a point
-            }
-            if (co < 1e-4f) return false;
-            const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
-            if (dist <= 0.0f) return false;
-            const float G = ci * co / (dist * dist);
-            if (G <= 0.0f) return false;
-            int film_w = 0, film_h = 0;
-            if (t == 0) {
-                if (!film_plane_pixel(P, sc.p, film_w, film_h)) return false;
-                if (film_w == W || film_h == H) return false;
-                if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) return false;
-            }
-            // VolumetricTest reads its own uniform, so it may come before the visibility test
-            const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
-            if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) return false;
-            // the eye end's and the light end's factors through one loop body (one copy of the
-            // material code in the kernel)
-            float3 cf[2];
-        #pragma unroll 1
-            for (int side = 0; side < 2; ++side) {
-                const bool ee = side == 0;
-                const BVert &v = ee ? tc : sc;
-                const int k = ee ? t : s;
-                const float3 wa = ee ? cwi : s_wi, wb = ee ? t_wo : cwo;
-                float3 c;
-                if (k == 0) {
-                    if (ee) {
-                        const DevCamera &cam = S.camera;
-                        const float cs = dot3(tc.n, cwi);
-                        const float We = cam.plane_dist * cam.plane_dist / (cam.film_area * cs * cs * cs * cs);
-                        c = c3(We / avg3(tc.pdf_fwd));
-                    } else {
-                        c = light_emission(light) / sc.pdf_fwd;
-                    }
-                } else if (v.onsurface) {
-                    c = vert_fr(S, v, v.n, wa, wb) / (v.pdf_fwd * v.pdf_path);
-                } else {
-                    c = (S.volume.sigma_s * phase_value(S.volume, wa, wb)) / (v.pdf_fwd * v.pdf_path);
-                }
-                // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
-                // 350-351): a medium vertex takes the texture of the surface its segment was
-                // headed for, evaluated at the medium point; none without such a surface
-                if (k > 0 && S.prim_tex && v.prim >= 0) c = c * tex_pattern(S, v.prim, v.p);
-                cf[side] = c;
-            }
-            const float3 cE = cf[0], cL = cf[1];
-            const float3 lo = aE[t] * cE * G * cL * aL[s];
-            pre = lo;
-            mw_ns = s + 1;
-            mw_wi = cwi;
-            mw_wo = cwo;
-            // the shadow ray of VisibilityTest (:1018-1050): from the eye vertex unless the eye
-            // vertex is the camera
-            if (t == 0) {
-                out.o = sc.p;
-                out.dir = normalize_ref(tc.p - sc.p);
-            } else {
-                out.o = tc.p;
-                out.dir = normalize_ref(sc.p - tc.p);
-            }
-            out.tmax = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
-            out.px = t == 0 ? film_h * W + film_w : -1;
-            return true;
-        };
-        if (!shadow_terms()) return STRAT_NONE;
+            return STRAT_NONE;
+        }
+        if (tc.dirac) return STRAT_NONE;
     }
-    out.lo = pre * mis_weight<MAXV>(P, VL, segL, VE, segE, mw_ns, mw_nt, mw_wi, mw_wo, light_n, light);
-    return result;
+    const int s = len - (t + 1);
+    if (s >= nLv || s <= -1) return STRAT_NONE;
+    const BVert &sc = VL[s];
+    float3 s_wi = mk3(0, 0, 0);
+    if (s > 0) {
+        s_wi = -segL[s - 1];
+        if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) return STRAT_NONE;
+        if (sc.dirac) return STRAT_NONE;
+    }
+    // the geometric rejections come before the two visibility tests: they read no random
+    // numbers and change nothing, so the order only saves traversals
+    const float3 cwi = normalize_ref(sc.p - tc.p);
+    const float3 cwo = normalize_ref(tc.p - sc.p);
+    const float ci = tc.onsurface ? dot3(cwi, tc.n) : 1.0f;
+    if (ci < 1e-4f) return STRAT_NONE;
+    float co = sc.onsurface ? dot3(cwo, sc.n) : 1.0f;
+    if (s == 0 && spot) {
+        if (dot3(cwo, light.direction) < light.cos_cone) return STRAT_NONE;  // outside the cone
+        co = 1.0f;                                                         // no cosine at a point
+    }
+    if (co < 1e-4f) return STRAT_NONE;
+    const float dist = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+    if (dist <= 0.0f) return STRAT_NONE;
+    const float G = ci * co / (dist * dist);
+    if (G <= 0.0f) return STRAT_NONE;
+    int film_w = 0, film_h = 0;
+    if (t == 0) {
+        if (!film_plane_pixel(P, sc.p, film_w, film_h)) return STRAT_NONE;
+        if (film_w == W || film_h == H) return STRAT_NONE;
+        if (film_w < 0 || film_h < 0 || film_w > W || film_h > H) return STRAT_NONE;
+    }
+    // VolumetricTest reads its own uniform, so it may come before the visibility test
+    const Uniform4 UC = path_uniforms(path, 4000u + (uint32_t)(s * 64 + t), 0, P.k0, P.k1);
+    if (!volumetric_ok(S.volume, sc.p, tc.p, UC.u[0])) return STRAT_NONE;
+    // the eye end's and the light end's factors through one loop body (one copy of the
+    // material code in the kernel)
+    float3 cf[2];
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const bool ee = side == 0;
+        const BVert &v = ee ? tc : sc;
+        const int k = ee ? t : s;
+        const float3 wa = ee ? cwi : s_wi, wb = ee ? t_wo : cwo;
+        float3 c;
+        if (k == 0) {
+            if (ee) {
+                const DevCamera &cam = S.camera;
+                const float cs = dot3(tc.n, cwi);
+                const float We = cam.plane_dist * cam.plane_dist / (cam.film_area * cs * cs * cs * cs);
+                c = c3(We / avg3(tc.pdf_fwd));
+            } else {
+                c = light_emission(light) / sc.pdf_fwd;
+            }
+        } else if (v.onsurface) {
+            c = vert_fr(S, v, v.n, wa, wb) / (v.pdf_fwd * v.pdf_path);
+        } else {
+            c = (S.volume.sigma_s * phase_value(S.volume, wa, wb)) / (v.pdf_fwd * v.pdf_path);
+        }
+        // Texture::Pattern of the connecting vertex's object (bidirectionalpathtracer.cpp:
+        // 350-351): a medium vertex takes the texture of the surface its segment was
+        // headed for, evaluated at the medium point; none without such a surface
+        if (k > 0 && S.prim_tex && v.prim >= 0) c = c * tex_pattern(S, v.prim, v.p);
+        cf[side] = c;
+    }
+    const float3 cE = cf[0], cL = cf[1];
+    const float3 lo = aE[t] * cE * G * cL * aL[s];
+    out.lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
+    // the shadow ray of VisibilityTest (:1018-1050): from the eye vertex unless the eye
+    // vertex is the camera
+    if (t == 0) {
+        out.o = sc.p;
+        out.dir = normalize_ref(tc.p - sc.p);
+    } else {
+        out.o = tc.p;
+        out.dir = normalize_ref(sc.p - tc.p);
+    }
+    out.tmax = sqrtf(dot3(tc.p - sc.p, tc.p - sc.p));
+    out.px = t == 0 ? film_h * W + film_w : -1;
+    return STRAT_SHADOW;
 }
 
 // Every strategy of one sample in Trace's order, visibility traced by this thread; splats
