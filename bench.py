@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--adjoint-spp", type=int, default=0,
                     help="adjoint workload: samples per pixel of the gradient pass (0 = the forward's 64)")
     ap.add_argument("--adam-lr", type=float, default=1e-2, help="adjoint workload: Adam learning rate")
+    ap.add_argument("--adam-lr-end", type=float, default=0.0,
+                    help="adjoint workload: learning rate at the last step, reached by exponential decay "
+                         "(0: constant --adam-lr)")
+    ap.add_argument("--adjoint-levels", type=int, default=7,
+                    help="adjoint workload: displaced-sphere subdivision levels (4 * 4**levels triangles)")
     ap.add_argument("--scenes", type=int, default=256, help="batched workload: number of scenes")
     ap.add_argument("--breakdown", action="store_true",
                     help="batched workload: also time every scene alone and report the per-size-class rates and "
@@ -743,14 +748,14 @@ def adjoint_arm(args):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from adjoint_torch import render, visible_triangles, footprint_albedo_rmse
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    size, spp, depth = 256, 64, 8
-    gt = rumi_b200.GpuScene(scenes.inverse_rendering(size, size, spp, depth))
+    size, spp, depth, levels = 256, 64, 8, args.adjoint_levels
+    gt = rumi_b200.GpuScene(scenes.inverse_rendering(size, size, spp, depth, levels=levels))
     target = torch.from_numpy(gt.forward(seed=1)[0] / spp).cuda()
     gt.close()
-    n_mesh = 4 * 4 ** 7
+    n_mesh = 4 * 4 ** levels
     hidden = scenes.random_albedo(n_mesh, 23)
-    start = scenes.inverse_rendering(size, size, spp, depth, albedo=np.full((n_mesh, 3), 0.5, np.float32),
-                                     medium=scenes.INVERSE_START_MEDIUM)
+    start = scenes.inverse_rendering(size, size, spp, depth, levels=levels,
+                                     albedo=np.full((n_mesh, 3), 0.5, np.float32), medium=scenes.INVERSE_START_MEDIUM)
     g = rumi_b200.GpuScene(start)
     alb_all = torch.from_numpy(start.flatten().tri_albedo.copy()).cuda()
     walls = alb_all[:-n_mesh].clone()
@@ -759,6 +764,8 @@ def adjoint_arm(args):
     med = torch.nn.Parameter(torch.tensor(list(m0["sigma_s"]) + list(m0["sigma_a"]) + [m0["g"]],
                                           dtype=torch.float32, device="cuda"))
     opt = torch.optim.Adam([mesh, med], lr=args.adam_lr)
+    decay = (args.adam_lr_end / args.adam_lr) ** (1.0 / max(args.adam_steps - 1, 1)) if args.adam_lr_end > 0 else 1.0
+    sched = torch.optim.lr_scheduler.ExponentialLR(opt, gamma=decay)
     grad_spp = args.adjoint_spp or spp
     hidden_t = torch.from_numpy(hidden).cuda()
 
@@ -789,6 +796,14 @@ def adjoint_arm(args):
         g.forward(seed=8 + i, keep=True)
         kept.append(g.backward(d, seed=8 + i, timing=True)[2]["total_ms"])
     bwd_kept_ms = statistics.median(kept)
+    def crn_loss():
+        """The image loss against the target rendered with the same seed as the target
+        (common random numbers): what remains is the parameters' difference, not noise."""
+        with torch.no_grad():
+            film = render(torch.cat([walls, mesh]), med, g, spp, 1) / spp
+            return float(((film - target) ** 2).mean())
+
+    crn0 = crn_loss()
     alb_rmse0 = float(((mesh.detach() - hidden_t) ** 2).mean().sqrt())
     # the triangles the camera sees (>= 1 pixel): only their albedo is observable
     vis = torch.from_numpy(visible_triangles(g, start, alb_all.shape[0] - n_mesh, n_mesh)).cuda()
@@ -806,31 +821,46 @@ def adjoint_arm(args):
     losses = []
     for it in range(args.adam_steps):
         losses.append(step(it))
+        sched.step()
     ev1.record()
     torch.cuda.synchronize()
     clocks_info = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     losses = [float(x) for x in losses]
+    crn1 = crn_loss()
     alb_rmse = float(((mesh.detach() - hidden_t) ** 2).mean().sqrt())
     vis_rmse = float(((mesh.detach() - hidden_t)[vis] ** 2).mean().sqrt())
     fp_rmse = footprint_albedo_rmse(g, start, first_mesh, n_mesh, mesh.detach(), hidden_t)
     t = scenes.INVERSE_TARGET_MEDIUM
+    m_tgt = np.array(list(t["sigma_s"]) + list(t["sigma_a"]) + [t["g"]])
+    m_start = np.array(list(m0["sigma_s"]) + list(m0["sigma_a"]) + [m0["g"]])
+    m_end = med.detach().cpu().numpy()
     line = dict(metric="adjoint grads/s", value=args.adam_steps / (ms / 1000.0), unit="gradient evaluations/s",
                 n_gpus=1, steps=args.adam_steps, warmup=args.warmup, ms_per_step=ms / args.adam_steps,
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
-                data="synthetic (seeded 65,536-triangle displaced sphere, hidden seeded albedo and medium)",
-                config=dict(workload="inverse rendering: 256x256, 64 spp, depth 8, 65,536 triangles in a medium",
-                            params=3 * n_mesh + 7, optimiser=f"Adam lr {args.adam_lr:g}", loss="L2 image",
+                data=f"synthetic (seeded {n_mesh:,}-triangle displaced sphere, hidden seeded albedo and medium)",
+                config=dict(workload=f"inverse rendering: 256x256, 64 spp, depth 8, {n_mesh:,} triangles in a medium",
+                            params=3 * n_mesh + 7,
+                            optimiser=f"Adam lr {args.adam_lr:g}" + (f" -> {args.adam_lr_end:g} (exponential)"
+                                                                    if args.adam_lr_end > 0 else ""),
+                            loss="L2 image",
                             gradient_spp=grad_spp),
                 forward_ms=fwd_ms, backward_ms=bwd_ms, backward_over_forward=bwd_ms / fwd_ms,
                 backward_after_kept_forward_ms=bwd_kept_ms,
                 paths_per_step=size * size * spp, loss_first=losses[0], loss_last=losses[-1],
+                loss_first20_mean=float(np.mean(losses[:20])), loss_last20_mean=float(np.mean(losses[-20:])),
+                loss_same_seed_as_target_start=crn0, loss_same_seed_as_target_end=crn1,
                 albedo_rmse_start=alb_rmse0, albedo_rmse_end=alb_rmse,
                 visible_triangles=int(vis.sum()), visible_albedo_rmse_start=vis_rmse0,
                 visible_albedo_rmse_end=vis_rmse, footprint_albedo_rmse_start=fp_rmse0,
                 footprint_albedo_rmse_end=fp_rmse,
                 medium_end=[float(x) for x in med.detach().cpu()],
                 medium_target=list(t["sigma_s"]) + list(t["sigma_a"]) + [t["g"]],
+                # sums of absolute errors: sigma_s RGB, sigma_a RGB, g
+                medium_error_start=[float(np.abs(m_start - m_tgt)[0:3].sum()), float(np.abs(m_start - m_tgt)[3:6].sum()),
+                                    float(abs(m_start[6] - m_tgt[6]))],
+                medium_error_end=[float(np.abs(m_end - m_tgt)[0:3].sum()), float(np.abs(m_end - m_tgt)[3:6].sum()),
+                                  float(abs(m_end[6] - m_tgt[6]))],
                 gpu_launches=args.adam_steps * ((3 + 5 * depth) + 2 * (3 + 4 * depth)), clocks=clocks_info)
     print(json.dumps(line), flush=True)
     g.close()
