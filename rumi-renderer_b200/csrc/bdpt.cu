@@ -545,24 +545,6 @@ RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, 
     return 1.0f / sum;
 }
 
-// VisibilityTest (:1018-1050): shadow ray between the two vertices, from the eye vertex
-// unless the eye vertex is the camera.
-RUMI_D bool visible(const DevScene &S, int ns, int nt, float3 sp, float3 tp, int *stack, TraceStats &st) {
-    float3 o, dir;
-    float tmax;
-    if (nt == 1) {
-        o = sp;
-        dir = normalize_ref(tp - sp);
-        tmax = sqrtf(dot3(tp - sp, tp - sp));
-    } else {
-        o = tp;
-        dir = normalize_ref(sp - tp);
-        tmax = sqrtf(dot3(sp - tp, sp - tp));
-    }
-    const HitRec h = trace_ray<true, BD_STACK, false>(S, o, dir, tmax, false, stack, BD_THREADS, st);
-    return !(h.t > 0.0f && tmax - h.t > 1e-4f);
-}
-
 // VolumetricTest (:1052-1094): binary transmittance between the vertices.
 RUMI_D bool volumetric_ok(const DevVolume &V, float3 sp, float3 tp, float xi) {
     if (!V.present) return true;
