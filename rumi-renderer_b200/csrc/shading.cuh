@@ -602,8 +602,9 @@ RUMI_D float volume_shadow_tr(const DevVolume &v, float3 o, float3 d, float tmax
     return 1.0f;
 }
 
-// Material::Pdfw (Matte: Lambertian::Pdfw; Glossy: the lobe recorded in xi; Dirac and
-// emissive materials: 1), src/Material/{matte,glossy,specular,dielectric}.cpp.
+// Material::Pdfw (Matte: Lambertian::Pdfw; Glossy: the lobe recorded in xi; Dirac,
+// emissive and subsurface materials: 1), src/Material/{matte,glossy,specular,dielectric,
+// material}.cpp.
 RUMI_D float material_pdfw(const DevMaterial &m, float xi, float3 n, float3 w, float3 w_pdf) {
     if (m.type == MAT_MATTE) return lambert_pdf(n, w_pdf);
     if (m.type == MAT_GLOSSY) {
@@ -613,8 +614,12 @@ RUMI_D float material_pdfw(const DevMaterial &m, float xi, float3 n, float3 w, f
     return 1.0f;
 }
 
+// Material::IsDirac: Specular and Dielectric always (specular.cpp:30-33,
+// dielectric.cpp:33-36), Glossy on its Phong lobe (glossy.cpp:35-41).  Subsurface derives
+// from Material and keeps its default (material.cpp:33-36): not dirac, so BDPT connects
+// through its vertices with its constant Fresnel Fr and the default Pdfw of 1.
 RUMI_D bool material_dirac(const DevMaterial &m, float xi) {
-    if (m.type == MAT_SPECULAR || m.type == MAT_DIELECTRIC || m.type == MAT_SUBSURFACE) return true;
+    if (m.type == MAT_SPECULAR || m.type == MAT_DIELECTRIC) return true;
     if (m.type == MAT_GLOSSY) return !(m.kd != 0.0f && xi <= m.kd_pdf);
     return false;
 }

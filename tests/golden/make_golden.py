@@ -442,6 +442,13 @@ def main():
         image_fixture(os.path.join(HERE, "image_caustic_pt32.npz"), scene=sc)
         image_fixture(os.path.join(HERE, "image_sss_pt32.npz"), scene=scenes.subsurface_cornell(32, 32, 16, 12))
         return
+    if len(sys.argv) > 1 and sys.argv[1] == "bdpt_sss":
+        # BDPT over the subsurface sphere and the glossy sphere (materials the reference's
+        # BDPT evaluates through BSDFSampling / Fr only)
+        sc = scenes.subsurface_cornell(32, 32, 16, 12)
+        sc.tracer = scenes.BidirectionalPathTracer(4, 5)
+        image_fixture(os.path.join(HERE, "image_sss_bdpt32.npz"), scene=sc)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "bdpt67":
         # the volumetric-caustic workload's subpath lengths (6 light, 7 eye vertices) on its
         # area-light, isotropic-medium variant

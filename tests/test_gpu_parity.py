@@ -393,6 +393,9 @@ def test_gpu_pt_subsurface_matches_reference_3sigma(golden):
     # the volumetric-caustic workload's own subpath lengths (6 light, 7 eye vertices: the
     # 8-vertex kernel instantiation, every strategy up to path length 12)
     ("image_caustic_bdpt67_32.npz", lambda: scenes.volumetric_caustic(32, 32, 16, 6, 7, parity=True)),
+    # a subsurface sphere (BSDF sampling and Fr of Subsurface, no random walk in BDPT) and a
+    # glossy sphere
+    ("image_sss_bdpt32.npz", lambda: _bdpt45(scenes.subsurface_cornell(32, 32, 16, 12))),
 ])
 def test_gpu_bdpt_matches_reference_3sigma(golden, fixture, builder):
     """BDPT with MIS (all strategies incl. light tracing splats through the film plane)
