@@ -442,6 +442,17 @@ def main():
         image_fixture(os.path.join(HERE, "image_caustic_pt32.npz"), scene=sc)
         image_fixture(os.path.join(HERE, "image_sss_pt32.npz"), scene=scenes.subsurface_cornell(32, 32, 16, 12))
         return
+    if len(sys.argv) > 1 and sys.argv[1] == "more":
+        # the thin-lens camera under BDPT (the reference's BDPT turns depth of field off),
+        # and the Whitted ray tracer over the subsurface + glossy scene and two lights
+        sc = scenes.cornell_dof_pt(32, 32, 16, 8)
+        sc.tracer = scenes.BidirectionalPathTracer(4, 5)
+        image_fixture(os.path.join(HERE, "image_dof_bdpt32.npz"), scene=sc)
+        image_fixture(os.path.join(HERE, "image_sss_whitted32.npz"),
+                      scene=scenes.whitted(scenes.subsurface_cornell(32, 32, 16, 12)))
+        image_fixture(os.path.join(HERE, "image_two_lights_whitted32.npz"),
+                      scene=scenes.whitted(scenes.cornell_two_lights_pt(32, 32, 16, 8)))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "bdpt_sss":
         # BDPT over the subsurface sphere and the glossy sphere (materials the reference's
         # BDPT evaluates through BSDFSampling / Fr only)
