@@ -12,7 +12,7 @@
 #include "Scene/scene.h"
 #include "rumi_gpu_integrators.h"
 
-// integrator 0: GpuPathTracer(scene, a); 1: GpuBDPT(scene, a, b).  `frames` calls of
+// integrator 0: GpuPathTracer(scene, a); 1: GpuBDPT(scene, a, b); 2: GpuRayTracer(scene, a).  `frames` calls of
 // Scene::Rendering in a row (each renders into a cleared film; the adapter advances its
 // seed per frame, starting at `seed`).  film_out (frames*H*W*3, B,G,R) receives each
 // frame's Film::_pixel_buffer.  Returns 0, or -1 with the adapter's error in err.
@@ -27,6 +27,10 @@ extern "C" int ref_gpu_rendering(void *scene_ptr, int integrator, int a, int b, 
     Integrator *gpu = nullptr;
     if (integrator == 0) {
         GpuPathTracer *t = new GpuPathTracer(sc, a);
+        state = &t->frame;
+        gpu = t;
+    } else if (integrator == 2) {
+        GpuRayTracer *t = new GpuRayTracer(sc, a);
         state = &t->frame;
         gpu = t;
     } else {

@@ -399,6 +399,17 @@ Color GpuPathTracer::Trace(const unsigned int &width_idx, const unsigned int &he
     return frame.Sample(_scene_ptr, p, width_idx, height_idx, image_ptr);
 }
 
+GpuRayTracer::GpuRayTracer(Scene *scene_ptr, int max_depth) : Integrator(scene_ptr), _max_depth(max_depth) {}
+GpuRayTracer::~GpuRayTracer() {}
+
+Color GpuRayTracer::Trace(const unsigned int &width_idx, const unsigned int &height_idx, Pinhole *, Film *image_ptr) {
+    rumi_render_params p;
+    memset(&p, 0, sizeof(p));
+    p.integrator = RUMI_RAY_TRACER;
+    p.max_depth = _max_depth;
+    return frame.Sample(_scene_ptr, p, width_idx, height_idx, image_ptr);
+}
+
 GpuBDPT::GpuBDPT(Scene *scene_ptr, int nL, int nE) : Integrator(scene_ptr), _nL(nL), _nE(nE) {
     if (scene_ptr && scene_ptr->_camera) scene_ptr->_camera->DepthOfField(0.0f, 0.0f);
 }

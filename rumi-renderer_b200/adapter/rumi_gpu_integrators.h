@@ -99,6 +99,21 @@ class GpuPathTracer : public Integrator {
     int _max_depth;
 };
 
+// Drop-in for RayTracer(Scene *scene_ptr, int max_depth) (src/Integrator/raytracer.h:14):
+// the Whitted integrator, trace depths 0..max_depth.
+class GpuRayTracer : public Integrator {
+  public:
+    GpuRayTracer(Scene *scene_ptr, int max_depth);
+    ~GpuRayTracer();
+    using Integrator::Trace;
+    Color Trace(const unsigned int &width_idx, const unsigned int &height_idx, Pinhole *camera_ptr,
+                Film *image_ptr);
+    RumiGpuFrame frame;
+
+  private:
+    int _max_depth;
+};
+
 // Drop-in for BidirectionalPathTracer(Scene *scene_ptr, int nL, int nE).  Like the
 // reference's constructor it turns the camera's thin lens off (BDPT renders through the
 // pinhole, src/Integrator/bidirectionalpathtracer.cpp:56).

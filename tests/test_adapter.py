@@ -112,6 +112,7 @@ def test_adapter_compiles_against_the_reference_headers():
     probe = ('#include "rumi_gpu_integrators.h"\n'
              'Integrator *make_pt(Scene *s) { return new GpuPathTracer(s, 15); }\n'
              'Integrator *make_bdpt(Scene *s) { return new GpuBDPT(s, 6, 7); }\n'
+             'Integrator *make_rt(Scene *s) { return new GpuRayTracer(s, 10); }\n'
              'static_assert(sizeof(GpuPathTracer) > sizeof(Integrator), "derived");\n')
     for src in (os.path.join(ADAPTER, "rumi_gpu_integrators.cpp"), "-"):
         r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Wno-unused-variable", "-include",
@@ -167,7 +168,8 @@ def test_adapter_flatten_matches_the_host_mirror(case):
 
 
 def _render_through_reference_loop(sc, integrator, a, b, frames, seed, tmp_path):
-    """Frames of Scene::Rendering with GpuPathTracer (integrator 0) or GpuBDPT (1)."""
+    """Frames of Scene::Rendering with GpuPathTracer (integrator 0), GpuBDPT (1) or
+    GpuRayTracer (2)."""
     import torch
     torch.cuda.set_device(0)
     rs = refimpl.RefScene(sc, seed=1)
@@ -206,4 +208,15 @@ def test_gpu_bdpt_adapter_in_the_reference_rendering_loop(golden, tmp_path):
     from test_oracle_golden import frames_vs_reference
     g = golden("image_cornell_bdpt32.npz")
     frames = _render_through_reference_loop(scenes.cornell_bdpt(32, 32, 16, 4, 5), 1, 4, 5, 32, 42000, tmp_path)
+    frames_vs_reference(frames, g)
+
+
+@pytest.mark.gpu
+@need_host
+def test_gpu_raytracer_adapter_in_the_reference_rendering_loop(golden, tmp_path):
+    """GpuRayTracer (the Whitted integrator) installed in place of RayTracer(scene, 10)."""
+    from test_oracle_golden import frames_vs_reference
+    g = golden("image_whitted_cornell32.npz")
+    sc = scenes.whitted(scenes.cornell_pt(32, 32, 16, 8))
+    frames = _render_through_reference_loop(sc, 2, sc.tracer.max_depth, 0, 32, 43000, tmp_path)
     frames_vs_reference(frames, g)
