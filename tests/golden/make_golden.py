@@ -452,6 +452,11 @@ def main():
                       scene=scenes.whitted(scenes.subsurface_cornell(32, 32, 16, 12)))
         image_fixture(os.path.join(HERE, "image_two_lights_whitted32.npz"),
                       scene=scenes.whitted(scenes.cornell_two_lights_pt(32, 32, 16, 8)))
+        # BDPT over a displaced-sphere mesh with per-triangle albedo (the workload's mesh
+        # kind, 256 triangles)
+        sc = scenes.bvh_bound_pt(32, 32, 16, 10, levels=3, seed=7)
+        sc.tracer = scenes.BidirectionalPathTracer(4, 5)
+        image_fixture(os.path.join(HERE, "image_mesh_bdpt32.npz"), scene=sc)
         return
     if len(sys.argv) > 1 and sys.argv[1] == "bdpt_sss":
         # BDPT over the subsurface sphere and the glossy sphere (materials the reference's

@@ -398,6 +398,8 @@ def test_gpu_pt_subsurface_matches_reference_3sigma(golden):
     ("image_sss_bdpt32.npz", lambda: _bdpt45(scenes.subsurface_cornell(32, 32, 16, 12))),
     # a thin-lens camera: the reference's BDPT turns depth of field off when constructed
     ("image_dof_bdpt32.npz", lambda: _bdpt45(scenes.cornell_dof_pt(32, 32, 16, 8))),
+    # a displaced-sphere mesh with per-triangle albedo (the workload's mesh kind)
+    ("image_mesh_bdpt32.npz", lambda: _bdpt45(scenes.bvh_bound_pt(32, 32, 16, 10, levels=3, seed=7))),
 ])
 def test_gpu_bdpt_matches_reference_3sigma(golden, fixture, builder):
     """BDPT with MIS (all strategies incl. light tracing splats through the film plane)
