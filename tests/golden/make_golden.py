@@ -458,6 +458,10 @@ def main():
         sc.tracer = scenes.BidirectionalPathTracer(4, 5)
         image_fixture(os.path.join(HERE, "image_mesh_bdpt32.npz"), scene=sc)
         return
+    if len(sys.argv) > 1 and sys.argv[1] == "dof_whitted":
+        image_fixture(os.path.join(HERE, "image_dof_whitted32.npz"),
+                      scene=scenes.whitted(scenes.cornell_dof_pt(32, 32, 16, 8)))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "bdpt_sss":
         # BDPT over the subsurface sphere and the glossy sphere (materials the reference's
         # BDPT evaluates through BSDFSampling / Fr only)

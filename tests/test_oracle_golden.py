@@ -230,6 +230,7 @@ WHITTED_CASES = [
     ("image_whitted_caustic32.npz", lambda: scenes.whitted(scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True))),
     ("image_sss_whitted32.npz", lambda: scenes.whitted(scenes.subsurface_cornell(32, 32, 16, 12))),
     ("image_two_lights_whitted32.npz", lambda: scenes.whitted(scenes.cornell_two_lights_pt(32, 32, 16, 8))),
+    ("image_dof_whitted32.npz", lambda: scenes.whitted(scenes.cornell_dof_pt(32, 32, 16, 8))),
 ]
 
 
