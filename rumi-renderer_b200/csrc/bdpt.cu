@@ -18,6 +18,32 @@
 
 namespace rumi {
 
+
+// Every index this file forms into a local subpath array or a scene array goes through
+// bd_index: none can leave its range by construction, and an index that did would be
+// recorded here (check code, index, bound, sample thread) and replaced by 0, and
+// bdpt_render would return RUMI_ERR_INTERNAL naming it, instead of the kernel reading or
+// writing out of range.  The kernel builds without these checks raised illegal-address
+// faults in some configurations (a scene with two area lights in a medium, among others)
+// without any index leaving its range in the checked build; the checked build runs them
+// all.  One word for the process: a check that fires during concurrent BDPT renders on
+// several streams is reported by whichever render reads it first.
+__device__ int g_bd_range[4];
+// Records the first out-of-range index; out of line, so each checked access costs a
+// compare and a branch.
+__device__ __noinline__ void bd_index_fail(int idx, int n, int code) {
+    if (atomicCAS(&g_bd_range[0], 0, code) == 0) {
+        g_bd_range[1] = idx;
+        g_bd_range[2] = n;
+        g_bd_range[3] = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    }
+}
+// idx when it lies in [0, n); otherwise the failure is recorded and 0 is used instead.
+RUMI_D int bd_index(int idx, int n, int code) {
+    if (__builtin_expect((unsigned)idx < (unsigned)n, 1)) return idx;
+    bd_index_fail(idx, n, code);
+    return 0;
+}
 static constexpr int BD_THREADS = 64;
 static constexpr int BD_STACK = 32;
 static constexpr int BD_MAXV = 16;  // vertices per subpath (nE, nL <= 16)
@@ -143,8 +169,8 @@ RUMI_D bool film_plane_pixel(const BdLaunch &P, float3 pos, int &wi, int &hi) {
 RUMI_D void record_hit(const DevScene &S, const HitRec &h, float3 o, float3 d, BVert &v) {
     v.p = rn_madd(o, d, h.t);
     v.prim = h.id;
-    v.mat = prim_material(S, h.id);
-    v.n = surface_normal(S, h.id, h.back != 0, h.u, h.v, o, v.p, S.materials[v.mat]);
+    v.mat = prim_material(S, bd_index(h.id, S.n_prims, 31));
+    v.n = surface_normal(S, h.id, h.back != 0, h.u, h.v, o, v.p, S.materials[bd_index(v.mat, S.n_materials, 1)]);
 }
 
 RUMI_D float3 vert_albedo(const DevScene &S, const BVert &v, const DevMaterial &m) {
@@ -154,7 +180,7 @@ RUMI_D float3 vert_albedo(const DevScene &S, const BVert &v, const DevMaterial &
 
 // Material::Fr with the vertex's arriving Intersection state.
 RUMI_D float3 vert_fr(const DevScene &S, const BVert &v, float3 n, float3 wi, float3 wo) {
-    const DevMaterial m = S.materials[v.mat];
+    const DevMaterial m = S.materials[bd_index(v.mat, S.n_materials, 2)];
     return material_fr(m, vert_albedo(S, v, m), n, wi, wo, v.in_obj, v.xi, v.pdf_path, v.t_in, v.vtau / v.vpdf);
 }
 
@@ -176,11 +202,11 @@ RUMI_D int construct_subpath(const BdLaunch &P, bool eye, int max_depth, uint64_
     const int max_seg = max_depth - 1;  // the reference's Path[max_depth - 1] array
     for (int depth = 0; depth < max_depth && depth < max_seg; ++depth) {
         BVert &start = V[depth];
-        BVert &end = V[depth + 1];
+        BVert &end = V[bd_index(depth + 1, max_depth, 28)];
         bvert_clear(end);
         end.in_obj = in_object;
         end.d_in = d;
-        seg_d[depth] = d;
+        seg_d[bd_index(depth, max_depth, 30)] = d;
         const Uniform4 U0 = path_uniforms(path, stream_base + depth, 0, P.k0, P.k1);
         const Uniform4 U1 = path_uniforms(path, stream_base + depth, 1, P.k0, P.k1);
         const HitRec h = trace_ray<false, BD_STACK, false>(S, o, d, FLT_MAX, in_object, stack, BD_THREADS, st);
@@ -212,7 +238,7 @@ RUMI_D int construct_subpath(const BdLaunch &P, bool eye, int max_depth, uint64_
         ++n_vertex;
         const bool has_mat = end.mat >= 0;
         DevMaterial m;
-        if (has_mat) m = S.materials[end.mat];
+        if (has_mat) m = S.materials[bd_index(end.mat, S.n_materials, 3)];
         const float3 wrev = -d;  // wo (eye) / wi (light)
         float3 w, n;
         float pdf_dir = 1.0f;
@@ -352,7 +378,7 @@ RUMI_D int construct_subpath(const BdLaunch &P, bool eye, int max_depth, uint64_
         if (eye) {
             if (end_le) {
                 const float3 fr = end.onsurface ? vert_fr(S, end, n, w, wrev) : mk3(0, 0, 0);
-                alpha[depth + 2] = a * (fr / (end.pdf_fwd * end.pdf_path));
+                alpha[bd_index(depth + 2, max_depth + 1, 29)] = a * (fr / (end.pdf_fwd * end.pdf_path));
                 end.pdf_bwd = c3(light.inv_area * (float)S.n_lights);  // Light::Pdf() * LightCount()
                 break;
             }
@@ -395,17 +421,17 @@ RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, 
     const BVert *s_connect = nullptr, *s_prev = nullptr, *t_connect = nullptr, *t_prev = nullptr;
     float3 s_wi = mk3(0, 0, 0), t_wo = mk3(0, 0, 0);
     if (ns > 0) {
-        s_connect = &VL[ns - 1];
+        s_connect = &VL[bd_index(ns - 1, MAXV, 17)];
         if (ns >= 2) {
-            s_prev = &VL[ns - 2];
-            s_wi = -segL[ns - 2];
+            s_prev = &VL[bd_index(ns - 2, MAXV, 17)];
+            s_wi = -segL[bd_index(ns - 2, MAXV, 19)];
         }
     }
     if (nt > 0) {
-        t_connect = &VE[nt - 1];
+        t_connect = &VE[bd_index(nt - 1, MAXV, 18)];
         if (nt >= 2) {
-            t_prev = &VE[nt - 2];
-            t_wo = -segE[nt - 2];
+            t_prev = &VE[bd_index(nt - 2, MAXV, 18)];
+            t_wo = -segE[bd_index(nt - 2, MAXV, 20)];
         }
     }
     float connect_d = 1.0f, sd = 1.0f, td = 1.0f;
@@ -450,7 +476,7 @@ RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, 
         float pw;
         if (Y->onsurface) {
             if (ny > 1)
-                pw = material_pdfw(S.materials[Y->mat], Y->xi, Y->n, y_in, y_to_x);
+                pw = material_pdfw(S.materials[bd_index(Y->mat, S.n_materials, 4)], Y->xi, Y->n, y_in, y_to_x);
             else if (sl)
                 pw = camera_pdfw(S.camera, connect_wi);
             else
@@ -458,8 +484,8 @@ RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, 
         } else {
             pw = phase_value(vol, y_in, y_to_x);
         }
-        xb[nx - 1] = pdf_s * (pw * dwda);
-        xf[nx - 1] = X->pdf_fwd;
+        xb[bd_index(nx - 1, MAXV, 11)] = pdf_s * (pw * dwda);
+        xf[bd_index(nx - 1, MAXV, 11)] = X->pdf_fwd;
         if (Xp) {
             if (Xp->onsurface && Xp->dirac) {
                 xb[nx - 2] = c3(1.0f);
@@ -481,22 +507,22 @@ RUMI_D float mis_weight(const BdLaunch &P, const BVert *VL, const float3 *segL, 
                     if (vh) ps = vol_pdf_distance(vol, sm);
                 }
                 const float pw2 = X->onsurface
-                                      ? material_pdfw(S.materials[X->mat], X->xi, X->n, x_to_y, x_in)
+                                      ? material_pdfw(S.materials[bd_index(X->mat, S.n_materials, 5)], X->xi, X->n, x_to_y, x_in)
                                       : phase_value(vol, x_to_y, x_in);
-                xb[nx - 2] = ps * (pw2 * dw);
-                xf[nx - 2] = Xp->pdf_fwd;
+                xb[bd_index(nx - 2, MAXV, 12)] = ps * (pw2 * dw);
+                xf[bd_index(nx - 2, MAXV, 12)] = Xp->pdf_fwd;
             }
         }
     }
     if (t_connect && ns == 0) {
         // the eye subpath reached a light by itself ("kajiya" strategy)
-        tb[nt - 1] = VE[nt - 1].pdf_bwd;
+        tb[bd_index(nt - 1, MAXV, 13)] = VE[nt - 1].pdf_bwd;
         tf[nt - 1] = VE[nt - 1].pdf_fwd;
         if (t_prev->dirac) {
             tb[nt - 2] = c3(1.0f);
             tf[nt - 2] = c3(1.0f);
         } else {
-            tb[nt - 2] = VE[nt - 2].pdf_bwd;
+            tb[bd_index(nt - 2, MAXV, 14)] = VE[nt - 2].pdf_bwd;
             tf[nt - 2] = VE[nt - 2].pdf_fwd;
         }
     }
@@ -578,7 +604,7 @@ RUMI_D BdLight build_subpaths(const BdLaunch &P, int j, BVert *VE, float3 *segE,
     const Uniform4 UL = path_uniforms(path, 1000u, 0, P.k0, P.k1);
     const Uniform4 UD = path_uniforms(path, 1000u, 1, P.k0, P.k1);
     const int li = pick_light(S, UL.u[0]);
-    const DevLight light = S.lights[li];
+    const DevLight light = S.lights[bd_index(li, S.n_lights, 6)];
     const LightSample ls = sample_light(S, UL.u[0], UL.u[1], UL.u[2]);
     const float3 light_n = ls.nL;
     // eye subpath start (Pinhole::CastViewRay, pinhole.cpp:97-136)
@@ -672,15 +698,15 @@ RUMI_D int strategy(const BdLaunch &P, int j, int len, int t, const BVert *VE, c
         stop = true;
         return STRAT_NONE;
     }
-    const BVert &tc = VE[t];
+    const BVert &tc = VE[bd_index(t, MAXV, 21)];
     float3 t_wo = mk3(0, 0, 0);
     if (t > 0) {
-        t_wo = -segE[t - 1];
-        if (tc.onsurface && tc.mat >= 0 && S.materials[tc.mat].type == MAT_EMISSIVE) {
+        t_wo = -segE[bd_index(t - 1, MAXV, 26)];
+        if (tc.onsurface && tc.mat >= 0 && S.materials[bd_index(tc.mat, S.n_materials, 8)].type == MAT_EMISSIVE) {
             stop = true;
             if (len == nE - 1) {
                 const float w = mis_weight<MAXV>(P, VL, segL, VE, segE, 0, t + 1, mk3(0, 0, 0), mk3(0, 0, 0), light_n, light);
-                out.lo = aE[t + 1] * w;
+                out.lo = aE[bd_index(t + 1, MAXV + 2, 23)] * w;
                 return STRAT_ADD;
             }
             return STRAT_NONE;
@@ -689,11 +715,11 @@ RUMI_D int strategy(const BdLaunch &P, int j, int len, int t, const BVert *VE, c
     }
     const int s = len - (t + 1);
     if (s >= nLv || s <= -1) return STRAT_NONE;
-    const BVert &sc = VL[s];
+    const BVert &sc = VL[bd_index(s, MAXV, 22)];
     float3 s_wi = mk3(0, 0, 0);
     if (s > 0) {
-        s_wi = -segL[s - 1];
-        if (sc.onsurface && sc.mat >= 0 && S.materials[sc.mat].type == MAT_EMISSIVE) return STRAT_NONE;
+        s_wi = -segL[bd_index(s - 1, MAXV, 27)];
+        if (sc.onsurface && sc.mat >= 0 && S.materials[bd_index(sc.mat, S.n_materials, 9)].type == MAT_EMISSIVE) return STRAT_NONE;
         if (sc.dirac) return STRAT_NONE;
     }
     // the geometric rejections come before the two visibility tests: they read no random
@@ -752,7 +778,7 @@ RUMI_D int strategy(const BdLaunch &P, int j, int len, int t, const BVert *VE, c
         cf[side] = c;
     }
     const float3 cE = cf[0], cL = cf[1];
-    const float3 lo = aE[t] * cE * G * cL * aL[s];
+    const float3 lo = aE[bd_index(t, MAXV + 2, 24)] * cE * G * cL * aL[bd_index(s, MAXV + 2, 25)];
     out.lo = lo * mis_weight<MAXV>(P, VL, segL, VE, segE, s + 1, t + 1, cwi, cwo, light_n, light);
     // the shadow ray of VisibilityTest (:1018-1050): from the eye vertex unless the eye
     // vertex is the camera
@@ -775,7 +801,7 @@ RUMI_D float3 connect_strategies(const BdLaunch &P, int j, const BVert *VE, cons
                                  int nE, const BVert *VL, const float3 *segL, const float3 *aL, int nLv,
                                  const BdLight &bl, int *stk, TraceStats &st) {
     const DevScene &S = P.s;
-    const DevLight light = S.lights[bl.li];
+    const DevLight light = S.lights[bd_index(bl.li, S.n_lights, 7)];
     float3 L = mk3(0, 0, 0);
     const int max_len = nE + nLv - 1;
     for (int len = 1; len <= max_len; ++len) {
@@ -789,7 +815,7 @@ RUMI_D float3 connect_strategies(const BdLaunch &P, int j, const BVert *VE, cons
                 const HitRec h = trace_ray<true, BD_STACK, false>(S, out.o, out.dir, out.tmax, false, stk, BD_THREADS, st);
                 if (!(h.t > 0.0f && out.tmax - h.t > 1e-4f)) {
                     if (out.px >= 0) {
-                        float *dst = P.light_film + (size_t)out.px * 3;
+                        float *dst = P.light_film + (size_t)bd_index(out.px, P.s.width * P.s.height, 10) * 3;
                         atomicAdd(dst + 0, out.lo.z);
                         atomicAdd(dst + 1, out.lo.y);
                         atomicAdd(dst + 2, out.lo.x);
@@ -891,6 +917,11 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
     const DevCamera &c = S.camera;
     B.right = mk3(c.m[0] + c.m[3], c.m[4] + c.m[7], c.m[8] + c.m[11]);
     B.up = mk3(c.m[1] + c.m[3], c.m[5] + c.m[7], c.m[9] + c.m[11]);
+    {
+        const int z[4] = {0, 0, 0, 0};
+        cudaStreamSynchronize(stream);
+        cudaMemcpyToSymbol(g_bd_range, z, sizeof(z));
+    }
     cudaMemsetAsync(B.light_film, 0, film_bytes, stream);
     cudaMemsetAsync(nan_count, 0, sizeof(unsigned long long), stream);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -920,6 +951,16 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
     cudaMemcpyAsync(&h_nan, nan_count, sizeof(h_nan), cudaMemcpyDeviceToHost, stream);
     cudaError_t e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_status(e, "bdpt_render");
+    {
+        int chk[4] = {0, 0, 0, 0};
+        cudaMemcpyFromSymbol(chk, g_bd_range, sizeof(chk));
+        if (chk[0]) {
+            set_error("bdpt_render: index check " + std::to_string(chk[0]) + " failed: index " +
+                      std::to_string(chk[1]) + " of " + std::to_string(chk[2]) + " (sample thread " +
+                      std::to_string(chk[3]) + ")");
+            return RUMI_ERR_INTERNAL;
+        }
+    }
     if (stats) {
         memset(stats, 0, sizeof(*stats));
         stats->paths = total_pix * spp;

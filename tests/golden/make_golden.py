@@ -458,6 +458,30 @@ def main():
         sc.tracer = scenes.BidirectionalPathTracer(4, 5)
         image_fixture(os.path.join(HERE, "image_mesh_bdpt32.npz"), scene=sc)
         return
+    if len(sys.argv) > 1 and sys.argv[1] == "sss_medium":
+        # a subsurface sphere (its own random walk inside) within a scene medium, path
+        # traced and under BDPT (4, 5)
+        for name, bdpt in (("image_sss_medium_pt32.npz", False), ("image_sss_medium_bdpt32.npz", True)):
+            sc = scenes.subsurface_cornell(32, 32, 16, 12)
+            sc.volume = scenes.HomogeneousVolume((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.3, 0.3, 0.3),
+                                                 (0.05, 0.05, 0.05), 0.0)
+            if bdpt:
+                sc.tracer = scenes.BidirectionalPathTracer(4, 5)
+            image_fixture(os.path.join(HERE, name), scene=sc)
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == "lights_medium":
+        # the spherical emitter inside the scene medium (path traced), and two area lights
+        # in it under BDPT (4, 5)
+        sc = scenes.cornell_sphere_light_pt(32, 32, 16, 8)
+        sc.volume = scenes.HomogeneousVolume((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.3, 0.3, 0.3),
+                                             (0.05, 0.05, 0.05), 0.0)
+        image_fixture(os.path.join(HERE, "image_sphere_light_medium_pt32.npz"), scene=sc)
+        sc = scenes.cornell_two_lights_pt(32, 32, 16, 8)
+        sc.volume = scenes.HomogeneousVolume((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.3, 0.3, 0.3),
+                                             (0.05, 0.05, 0.05), 0.0)
+        sc.tracer = scenes.BidirectionalPathTracer(4, 5)
+        image_fixture(os.path.join(HERE, "image_two_lights_medium_bdpt32.npz"), scene=sc)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "dof_whitted":
         image_fixture(os.path.join(HERE, "image_dof_whitted32.npz"),
                       scene=scenes.whitted(scenes.cornell_dof_pt(32, 32, 16, 8)))

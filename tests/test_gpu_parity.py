@@ -387,6 +387,23 @@ def test_gpu_pt_subsurface_matches_reference_3sigma(golden):
     frames_vs_reference(gpu_frames(scenes.subsurface_cornell(32, 32, 16, 12), 32, 12000), golden("image_sss_pt32.npz"))
 
 
+@pytest.mark.parametrize("fixture,bdpt", [("image_sss_medium_pt32.npz", False), ("image_sss_medium_bdpt32.npz", True)])
+def test_gpu_subsurface_in_a_medium_matches_reference_3sigma(golden, fixture, bdpt):
+    """A subsurface sphere inside the scene's medium: path traced (the sphere's walk
+    inside, the medium outside) and under BDPT."""
+    from test_oracle_golden import frames_vs_reference, sss_in_medium
+    frames_vs_reference(gpu_frames(sss_in_medium(bdpt), 32, 15000), golden(fixture))
+
+
+@pytest.mark.parametrize("fixture,kind", [("image_sphere_light_medium_pt32.npz", "sphere"),
+                                          ("image_two_lights_medium_bdpt32.npz", "two_bdpt")])
+def test_gpu_lights_in_a_medium_match_reference_3sigma(golden, fixture, kind):
+    """A spherical emitter inside the medium (path traced: NEE with the binary shadow
+    transmittance) and two area lights inside it under BDPT."""
+    from test_oracle_golden import frames_vs_reference, lights_in_medium
+    frames_vs_reference(gpu_frames(lights_in_medium(kind), 32, 16000), golden(fixture))
+
+
 @pytest.mark.parametrize("fixture,builder", [
     ("image_cornell_bdpt32.npz", lambda: scenes.cornell_bdpt(32, 32, 16, 4, 5)),
     ("image_caustic_bdpt32.npz", lambda: scenes.volumetric_caustic(32, 32, 16, 4, 5, parity=True)),

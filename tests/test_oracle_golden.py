@@ -276,6 +276,36 @@ def test_oracle_subsurface_matches_reference_3sigma(golden):
                         golden("image_sss_pt32.npz"))
 
 
+def sss_in_medium(bdpt=False):
+    """The subsurface + glossy Cornell scene inside a homogeneous medium filling the box
+    (sigma_s 0.3, sigma_a 0.05, isotropic): the sphere's own random walk inside, the scene's
+    medium outside."""
+    sc = scenes.subsurface_cornell(32, 32, 16, 12)
+    sc.volume = scenes.HomogeneousVolume((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.3, 0.3, 0.3), (0.05, 0.05, 0.05), 0.0)
+    if bdpt:
+        sc.tracer = scenes.BidirectionalPathTracer(4, 5)
+    return sc
+
+
+def lights_in_medium(kind):
+    """The spherical emitter (path traced) or the two area lights (BDPT (4, 5)) inside the
+    medium of sss_in_medium."""
+    sc = scenes.cornell_sphere_light_pt(32, 32, 16, 8) if kind == "sphere" else scenes.cornell_two_lights_pt(32, 32, 16, 8)
+    sc.volume = scenes.HomogeneousVolume((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.3, 0.3, 0.3), (0.05, 0.05, 0.05), 0.0)
+    if kind == "two_bdpt":
+        sc.tracer = scenes.BidirectionalPathTracer(4, 5)
+    return sc
+
+
+def test_oracle_sphere_light_in_a_medium_matches_reference_3sigma(golden):
+    frames_vs_reference(oracle_frames(lights_in_medium("sphere"), 8, 24, 1500),
+                        golden("image_sphere_light_medium_pt32.npz"))
+
+
+def test_oracle_subsurface_in_a_medium_matches_reference_3sigma(golden):
+    frames_vs_reference(oracle_frames(sss_in_medium(), 12, 24, 1400), golden("image_sss_medium_pt32.npz"))
+
+
 def test_oracle_rmse_at_matched_spp_within_5pct_of_reference(golden):
     """The oracle's 16-spp frames against the reference's 65,536-spp image: mean RMSE within
     5% of the reference's own 16-spp RMSE."""
