@@ -88,6 +88,32 @@ def cornell_pt(width: int = 256, height: int = 256, spp: int = 16, max_depth: in
     return sc
 
 
+def absorbing_glass_cornell(width: int = 32, height: int = 32, spp: int = 16, max_depth: int = 10) -> Scene:
+    """The Cornell box holding a coloured glass sphere (Dielectric(1.5, 1.0, rgb): Beer-Lambert
+    absorption exp(-rgb * length) on every segment travelled inside it,
+    src/Material/material.cpp:18-26) and the mirror sphere, path traced."""
+    sc = Scene()
+    add_cornell_box(sc)
+    sc.add(Sphere((0.35, 0.2, 0.55), 0.2), Dielectric(1.5, 1.0, (0.5, 1.5, 4.0)))
+    sc.add(Sphere((0.72, 0.12, 0.35), 0.12), Specular(1.0, (0.9, 0.9, 0.9)))
+    sc.camera = cornell_camera()
+    sc.image = Film(width, height, spp)
+    sc.tracer = PathTracer(max_depth)
+    return sc
+
+
+def with_medium(sc: Scene, sigma_s=(0.3, 0.3, 0.3), sigma_a=(0.05, 0.05, 0.05), g: float = 0.0) -> Scene:
+    """The scene with a homogeneous medium filling the unit box (the Cornell interior)."""
+    sc.volume = HomogeneousVolume((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), tuple(sigma_s), tuple(sigma_a), float(g))
+    return sc
+
+
+def with_bdpt(sc: Scene, nL: int = 4, nE: int = 5) -> Scene:
+    """The scene rendered by ``BidirectionalPathTracer(scene, nL, nE)``."""
+    sc.tracer = BidirectionalPathTracer(nL, nE)
+    return sc
+
+
 def cornell_sphere_light_pt(width: int = 32, height: int = 32, spp: int = 16, max_depth: int = 8) -> Scene:
     """The Cornell walls lit by a spherical emitter instead of the quad: an Emissive sphere
     of radius 0.06 under the ceiling with a 4096-point sample set and an AreaLight over it

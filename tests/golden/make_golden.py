@@ -482,6 +482,18 @@ def main():
         sc.tracer = scenes.BidirectionalPathTracer(4, 5)
         image_fixture(os.path.join(HERE, "image_two_lights_medium_bdpt32.npz"), scene=sc)
         return
+    if len(sys.argv) > 1 and sys.argv[1] == "combos":
+        # coloured (absorbing) glass under the three integrators; the sphere light and the two
+        # lights inside a medium under the integrators not covered yet
+        for name, sc in (("image_glass_pt32.npz", scenes.absorbing_glass_cornell()),
+                         ("image_glass_bdpt32.npz", scenes.with_bdpt(scenes.absorbing_glass_cornell())),
+                         ("image_glass_whitted32.npz", scenes.whitted(scenes.absorbing_glass_cornell())),
+                         ("image_sphere_light_medium_bdpt32.npz",
+                          scenes.with_bdpt(scenes.with_medium(scenes.cornell_sphere_light_pt(32, 32, 16, 8)))),
+                         ("image_two_lights_medium_pt32.npz",
+                          scenes.with_medium(scenes.cornell_two_lights_pt(32, 32, 16, 8)))):
+            image_fixture(os.path.join(HERE, name), scene=sc)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "dof_whitted":
         image_fixture(os.path.join(HERE, "image_dof_whitted32.npz"),
                       scene=scenes.whitted(scenes.cornell_dof_pt(32, 32, 16, 8)))

@@ -395,6 +395,20 @@ def test_gpu_subsurface_in_a_medium_matches_reference_3sigma(golden, fixture, bd
     frames_vs_reference(gpu_frames(sss_in_medium(bdpt), 32, 15000), golden(fixture))
 
 
+@pytest.mark.parametrize("fixture,builder", [
+    ("image_glass_pt32.npz", lambda: scenes.absorbing_glass_cornell()),
+    ("image_glass_bdpt32.npz", lambda: scenes.with_bdpt(scenes.absorbing_glass_cornell())),
+    ("image_two_lights_medium_pt32.npz", lambda: scenes.with_medium(scenes.cornell_two_lights_pt(32, 32, 16, 8))),
+    ("image_sphere_light_medium_bdpt32.npz",
+     lambda: scenes.with_bdpt(scenes.with_medium(scenes.cornell_sphere_light_pt(32, 32, 16, 8)))),
+])
+def test_gpu_glass_and_lights_in_a_medium_match_reference_3sigma(golden, fixture, builder):
+    """Coloured glass (Beer-Lambert absorption inside) path traced and under BDPT; two area
+    lights in a medium path traced; the spherical emitter in a medium under BDPT."""
+    from test_oracle_golden import frames_vs_reference
+    frames_vs_reference(gpu_frames(builder(), 32, 17000), golden(fixture))
+
+
 @pytest.mark.parametrize("fixture,kind", [("image_sphere_light_medium_pt32.npz", "sphere"),
                                           ("image_two_lights_medium_bdpt32.npz", "two_bdpt")])
 def test_gpu_lights_in_a_medium_match_reference_3sigma(golden, fixture, kind):

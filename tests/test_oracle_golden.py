@@ -231,6 +231,7 @@ WHITTED_CASES = [
     ("image_sss_whitted32.npz", lambda: scenes.whitted(scenes.subsurface_cornell(32, 32, 16, 12))),
     ("image_two_lights_whitted32.npz", lambda: scenes.whitted(scenes.cornell_two_lights_pt(32, 32, 16, 8))),
     ("image_dof_whitted32.npz", lambda: scenes.whitted(scenes.cornell_dof_pt(32, 32, 16, 8))),
+    ("image_glass_whitted32.npz", lambda: scenes.whitted(scenes.absorbing_glass_cornell())),
 ]
 
 
@@ -300,6 +301,17 @@ def lights_in_medium(kind):
 def test_oracle_sphere_light_in_a_medium_matches_reference_3sigma(golden):
     frames_vs_reference(oracle_frames(lights_in_medium("sphere"), 8, 24, 1500),
                         golden("image_sphere_light_medium_pt32.npz"))
+
+
+@pytest.mark.parametrize("fixture,builder", [
+    ("image_glass_pt32.npz", lambda: scenes.absorbing_glass_cornell()),
+    ("image_two_lights_medium_pt32.npz", lambda: scenes.with_medium(scenes.cornell_two_lights_pt(32, 32, 16, 8))),
+])
+def test_oracle_glass_and_two_lights_in_a_medium_match_reference_3sigma(golden, fixture, builder):
+    """Coloured glass (Beer-Lambert absorption inside) and two area lights in a medium,
+    path traced."""
+    sc = builder()
+    frames_vs_reference(oracle_frames(sc, sc.tracer.max_depth, 24, 1600), golden(fixture))
 
 
 def test_oracle_subsurface_in_a_medium_matches_reference_3sigma(golden):
