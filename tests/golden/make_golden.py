@@ -410,6 +410,17 @@ def main():
             for name, sc in TEXTURE_CASES(img, hdr):
                 image_fixture(os.path.join(HERE, name), scene=sc)
         return
+    if len(sys.argv) > 1 and sys.argv[1] == "tex_medium":
+        # the textured Cornell scene inside a medium, path traced and under BDPT
+        import tempfile
+        import texture_cases as TC
+        with tempfile.TemporaryDirectory() as d:
+            img, hdr = TC.case_files(d)
+            image_fixture(os.path.join(HERE, "image_tex_medium_pt32.npz"),
+                          scene=scenes.with_medium(TC.textured_cornell(32, 32, 16, 8, img)))
+            image_fixture(os.path.join(HERE, "image_tex_medium_bdpt32.npz"),
+                          scene=scenes.with_medium(TC.textured_bdpt(32, 32, 16, img)))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "whitted":
         image_fixture(os.path.join(HERE, "image_whitted_cornell32.npz"),
                       scene=scenes.whitted(scenes.cornell_pt(32, 32, 16, 8)))

@@ -210,3 +210,26 @@ def test_gpu_bdpt_rejects_image_based_lights(files):
     with pytest.raises(_capi.RumiError):
         gs.render(spp=1, tracer=BidirectionalPathTracer(3, 3))
     gs.close()
+
+
+def test_oracle_textured_scene_in_a_medium_matches_reference_3sigma(golden, files):
+    """The textured Cornell scene inside a homogeneous medium, path traced: a medium vertex
+    takes no texture, a surface vertex its own."""
+    sc = scenes.with_medium(TC.textured_cornell(32, 32, 16, 8, files[0]))
+    os_ = O.OracleScene(sc)
+    frames = []
+    for s in range(24):
+        film, nan = os_.render_pt(sc.tracer.max_depth, 16, seed=2100 + s)
+        assert nan == 0
+        frames.append(film / 16.0)
+    frames_vs_reference(frames, golden("image_tex_medium_pt32.npz"))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fixture,bdpt", [("image_tex_medium_pt32.npz", False), ("image_tex_medium_bdpt32.npz", True)])
+def test_gpu_textured_scene_in_a_medium_matches_reference_3sigma(golden, files, fixture, bdpt):
+    """The textured Cornell scene inside a medium, path traced and under BDPT (where a medium
+    connection vertex takes the texture of the surface its segment was headed for)."""
+    from test_gpu_parity import gpu_frames
+    sc = TC.textured_bdpt(32, 32, 16, files[0]) if bdpt else TC.textured_cornell(32, 32, 16, 8, files[0])
+    frames_vs_reference(gpu_frames(scenes.with_medium(sc), 32, 18000), golden(fixture))
