@@ -38,8 +38,9 @@
 extern "C" {
 #endif
 
-/* RUMI_ERR_INTERNAL: a device-side consistency check failed (the BVH builder's or the
- * four-wide collapse's range checks, which record the violation instead of writing).
+/* RUMI_ERR_INTERNAL: a device-side consistency check failed (the BVH builder's, the four-
+ * and eight-wide collapses' and the BDPT kernel's index range checks, which record the
+ * violation instead of reading or writing out of range; rumi_last_error_string names it).
  * RUMI_ERR_QUEUE_OVERFLOW and RUMI_ERR_TIMEOUT are reserved and returned by no entry
  * point: every ray queue is sized to its wave before launch, so no push can overflow,
  * and no kernel waits on another kernel or on a flag. */
