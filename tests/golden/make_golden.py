@@ -410,6 +410,20 @@ def main():
             for name, sc in TEXTURE_CASES(img, hdr):
                 image_fixture(os.path.join(HERE, name), scene=sc)
         return
+    if len(sys.argv) > 1 and sys.argv[1] == "combos2":
+        # an image-based light around a medium (PT), the Cornell spheres in a medium under
+        # BDPT, the spherical emitter under the Whitted ray tracer
+        import tempfile
+        import texture_cases as TC
+        with tempfile.TemporaryDirectory() as d:
+            img, hdr = TC.case_files(d)
+            image_fixture(os.path.join(HERE, "image_ibl_medium_pt32.npz"),
+                          scene=scenes.with_medium(TC.ibl_scene(32, 32, 16, 8, hdr)))
+        image_fixture(os.path.join(HERE, "image_cornell_medium_bdpt32.npz"),
+                      scene=scenes.with_medium(scenes.cornell_bdpt(32, 32, 16, 4, 5)))
+        image_fixture(os.path.join(HERE, "image_sphere_light_whitted32.npz"),
+                      scene=scenes.whitted(scenes.cornell_sphere_light_pt(32, 32, 16, 8)))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "tex_medium":
         # the textured Cornell scene inside a medium, path traced and under BDPT
         import tempfile

@@ -401,6 +401,7 @@ def test_gpu_subsurface_in_a_medium_matches_reference_3sigma(golden, fixture, bd
     ("image_two_lights_medium_pt32.npz", lambda: scenes.with_medium(scenes.cornell_two_lights_pt(32, 32, 16, 8))),
     ("image_sphere_light_medium_bdpt32.npz",
      lambda: scenes.with_bdpt(scenes.with_medium(scenes.cornell_sphere_light_pt(32, 32, 16, 8)))),
+    ("image_cornell_medium_bdpt32.npz", lambda: scenes.with_medium(scenes.cornell_bdpt(32, 32, 16, 4, 5))),
 ])
 def test_gpu_glass_and_lights_in_a_medium_match_reference_3sigma(golden, fixture, builder):
     """Coloured glass (Beer-Lambert absorption inside) path traced and under BDPT; two area

@@ -232,6 +232,7 @@ WHITTED_CASES = [
     ("image_two_lights_whitted32.npz", lambda: scenes.whitted(scenes.cornell_two_lights_pt(32, 32, 16, 8))),
     ("image_dof_whitted32.npz", lambda: scenes.whitted(scenes.cornell_dof_pt(32, 32, 16, 8))),
     ("image_glass_whitted32.npz", lambda: scenes.whitted(scenes.absorbing_glass_cornell())),
+    ("image_sphere_light_whitted32.npz", lambda: scenes.whitted(scenes.cornell_sphere_light_pt(32, 32, 16, 8))),
 ]
 
 

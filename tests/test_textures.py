@@ -233,3 +233,23 @@ def test_gpu_textured_scene_in_a_medium_matches_reference_3sigma(golden, files, 
     from test_gpu_parity import gpu_frames
     sc = TC.textured_bdpt(32, 32, 16, files[0]) if bdpt else TC.textured_cornell(32, 32, 16, 8, files[0])
     frames_vs_reference(gpu_frames(scenes.with_medium(sc), 32, 18000), golden(fixture))
+
+
+def test_oracle_image_based_light_around_a_medium_matches_reference_3sigma(golden, files):
+    """An image-based light (an emissive textured sphere around the scene) lighting the
+    Cornell scene through a medium, path traced."""
+    sc = scenes.with_medium(TC.ibl_scene(32, 32, 16, 8, files[1]))
+    os_ = O.OracleScene(sc)
+    frames = []
+    for s in range(24):
+        film, nan = os_.render_pt(sc.tracer.max_depth, 16, seed=2200 + s)
+        assert nan == 0
+        frames.append(film / 16.0)
+    frames_vs_reference(frames, golden("image_ibl_medium_pt32.npz"))
+
+
+@pytest.mark.gpu
+def test_gpu_image_based_light_around_a_medium_matches_reference_3sigma(golden, files):
+    from test_gpu_parity import gpu_frames
+    frames_vs_reference(gpu_frames(scenes.with_medium(TC.ibl_scene(32, 32, 16, 8, files[1])), 32, 19000),
+                        golden("image_ibl_medium_pt32.npz"))
