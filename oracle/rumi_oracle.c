@@ -813,6 +813,27 @@ static void lens_u(const orc_camera *c, uint64_t path, const uint32_t key[2], fl
  * L = sum_k beta_k direct_k, beta_{k+1} = beta_k vol_k fr_k cos_k / Average(pdf_wi_k pdf_path_k). */
 /* Debug record of one path's extension rays (orc_path_rays): o, in_object, d, tmax;
  * the closest hit's t and primitive. */
+/* The vertex normal a shape's Intersect writes at a hit: triangle.cpp:110-114
+ * (interpolated, flipped on a back hit of an opaque material), rect.cpp:118,
+ * sphere.cpp:117-128 (an emitter's normal faces the ray origin's side). */
+static V3 hit_normal(const orc_scene_desc *s, const Hit *h, V3 o, V3 p) {
+    const orc_material *m = prim_mat(s, h->id);
+    if (h->id < s->n_triangles) {
+        const float *q = s->tri_normals + 9 * (size_t)h->id;
+        V3 n = add(add(mul(fv(q), 1.0f - h->u - h->v), mul(fv(q + 3), h->u)), mul(fv(q + 6), h->v));
+        int opaque = m->type != DIELECTRIC && m->type != SUBSURFACE;
+        return h->back && opaque ? neg(n) : n;
+    }
+    if (h->id < s->n_triangles + s->n_rects) {
+        const float *q = s->rects + 9 * (size_t)(h->id - s->n_triangles);
+        return normalize(cross(fv(q + 3), fv(q + 6)));
+    }
+    const float *c = s->spheres + 4 * (size_t)(h->id - s->n_triangles - s->n_rects);
+    if (m->type == EMISSIVE)
+        return length(sub(o, fv(c))) > c[3] ? normalize(sub(p, fv(c))) : normalize(sub(fv(c), p));
+    return normalize(sub(p, fv(c)));
+}
+
 static float *g_dbg_rays, *g_dbg_t;
 static int32_t *g_dbg_prim;
 static int g_dbg_n;
@@ -857,7 +878,11 @@ static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, cons
                     V3 p = add(o, mul(d, tn < 0.0f ? sd : tn + sd));
                     V3 vol = vdiv(tau, pdf);
                     if (s->n_lights > 0) { /* HomogeneousVolume::DirectLighting */
-                        LSample ls = light_sample(s, U0[3], U1[0], U1[1], p, v3(0.0f, 1.0f, 0.0f));
+                        /* the vertex normal is the one of the surface the ray hit beyond the
+                         * scatter point (pathtracer.cpp:154-170 overwrites only _p), read by
+                         * an image-based light; (0,1,0) when the ray left the scene */
+                        V3 nb = hit ? hit_normal(s, &h, o, add(o, mul(d, h.t))) : v3(0.0f, 1.0f, 0.0f);
+                        LSample ls = light_sample(s, U0[3], U1[0], U1[1], p, nb);
                         V3 wi;
                         float dist, G;
                         if (nee_geom(&ls, p, &wi, &dist, &G)) {
@@ -893,23 +918,8 @@ static V3 trace_path(const orc_scene_desc *s, int max_depth, uint64_t path, cons
         }
         if (!done && hit) {
             const orc_material *m = prim_mat(s, h.id);
-            int opaque = m->type != DIELECTRIC && m->type != SUBSURFACE;
-            V3 p = add(o, mul(d, h.t)), n, albedo = fv(m->rgb);
-            if (h.id < s->n_triangles) {
-                const float *q = s->tri_normals + 9 * (size_t)h.id;
-                n = add(add(mul(fv(q), 1.0f - h.u - h.v), mul(fv(q + 3), h.u)), mul(fv(q + 6), h.v));
-                if (h.back && opaque) n = neg(n);
-                if (s->tri_albedo) albedo = fv(s->tri_albedo + 3 * (size_t)h.id);
-            } else if (h.id < s->n_triangles + s->n_rects) {
-                const float *q = s->rects + 9 * (size_t)(h.id - s->n_triangles);
-                n = normalize(cross(fv(q + 3), fv(q + 6)));
-            } else {
-                const float *c = s->spheres + 4 * (size_t)(h.id - s->n_triangles - s->n_rects);
-                if (m->type == EMISSIVE)
-                    n = length(sub(o, fv(c))) > c[3] ? normalize(sub(p, fv(c))) : normalize(sub(fv(c), p));
-                else
-                    n = normalize(sub(p, fv(c)));
-            }
+            V3 p = add(o, mul(d, h.t)), n = hit_normal(s, &h, o, p), albedo = fv(m->rgb);
+            if (h.id < s->n_triangles && s->tri_albedo) albedo = fv(s->tri_albedo + 3 * (size_t)h.id);
             if (m->type == EMISSIVE) {
                 if (le && !inobj && -dot(d, n) > 0.0f) L = add(L, vmul(vmul(beta, mat_le(m)), tex_pattern(s, h.id, p)));
             } else {
@@ -999,23 +1009,8 @@ static V3 whitted(const orc_scene_desc *s, int max_depth, uint64_t path, const u
     if (!(h.t > 0.0f)) return v3(0, 0, 0);
     *t_hit = h.t;
     const orc_material *m = prim_mat(s, h.id);
-    int opaque = m->type != DIELECTRIC && m->type != SUBSURFACE;
-    V3 p = add(o, mul(d, h.t)), n, albedo = fv(m->rgb);
-    if (h.id < s->n_triangles) {
-        const float *q = s->tri_normals + 9 * (size_t)h.id;
-        n = add(add(mul(fv(q), 1.0f - h.u - h.v), mul(fv(q + 3), h.u)), mul(fv(q + 6), h.v));
-        if (h.back && opaque) n = neg(n);
-        if (s->tri_albedo) albedo = fv(s->tri_albedo + 3 * (size_t)h.id);
-    } else if (h.id < s->n_triangles + s->n_rects) {
-        const float *q = s->rects + 9 * (size_t)(h.id - s->n_triangles);
-        n = normalize(cross(fv(q + 3), fv(q + 6)));
-    } else {
-        const float *c = s->spheres + 4 * (size_t)(h.id - s->n_triangles - s->n_rects);
-        if (m->type == EMISSIVE)
-            n = length(sub(o, fv(c))) > c[3] ? normalize(sub(p, fv(c))) : normalize(sub(fv(c), p));
-        else
-            n = normalize(sub(p, fv(c)));
-    }
+    V3 p = add(o, mul(d, h.t)), n = hit_normal(s, &h, o, p), albedo = fv(m->rgb);
+    if (h.id < s->n_triangles && s->tri_albedo) albedo = fv(s->tri_albedo + 3 * (size_t)h.id);
     float U0[4], U1[4], U2[4];
     path_u(path, depth, 0, key, U0);
     V3 wo = neg(d);

@@ -241,10 +241,6 @@ rumi_status validate(const rumi_scene_desc *d) {
             // ImageBasedLight reads its radiance from the sphere's texture
             if (!d->sphere_texture || d->sphere_texture[L.shape_index] < 0)
                 return set_error("the image-based light's sphere has no texture"), RUMI_ERR_INVALID_ARG;
-            // HomogeneousVolume::DirectLighting would sample it about the normal of the
-            // segment's surface hit; not supported
-            if (d->volume.present)
-                return set_error("image-based lights with a medium are not supported"), RUMI_ERR_INVALID_ARG;
         } else if (L.type != RUMI_LIGHT_SPOT) {
             return set_error("unknown light type"), RUMI_ERR_INVALID_ARG;
         }

@@ -489,7 +489,16 @@ __global__ void __launch_bounds__(SHADE_THREADS, ADJ ? 1 : RUMI_SHADE_MIN_BLOCKS
                     const float3 vol = ds.tau / ds.pdf;
                     // HomogeneousVolume::DirectLighting (homogeneousvolume.cpp:231-250)
                     if (S.n_lights > 0) {
-                        const LightSample ls = sample_light(S, U0.u[3], U1.u[0], U1.u[1]);
+                        // the vertex keeps the normal of the surface hit beyond the scatter
+                        // point (pathtracer.cpp:154-170 moves only _p); an image-based light
+                        // samples about it
+                        float3 nb = mk3(0.0f, 1.0f, 0.0f);
+                        if (hit && S.lights[pick_light(S, U0.u[3])].type == LIGHT_IBL) {
+                            const int hid = code & 0x7fffffff;
+                            nb = surface_normal(S, hid, code < 0, hv.z, hv.w, o, rn_madd(o, d, t),
+                                                S.materials[prim_material(S, hid)]);
+                        }
+                        const LightSample ls = sample_light(S, U0.u[3], U1.u[0], U1.u[1], p, nb);
                         float3 wi;
                         float dist, G;
                         if (nee_setup(ls, p, wi, dist, G)) {

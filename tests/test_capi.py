@@ -131,7 +131,6 @@ DESC_FAULTS = [
     ("triangle area light", lambda d, k: setattr(d.lights[0], "shape_type", 0), "rects or spheres"),
     ("image light on a rect", lambda d, k: (_ibl(d, k), setattr(d.lights[0], "shape_type", 1)), "sphere index"),
     ("image light without texture", lambda d, k: _ibl(d, k, with_texture=False), "has no texture"),
-    ("image light in a medium", lambda d, k: (_ibl(d, k), _set_volume(d)), "with a medium"),
     ("unknown light", lambda d, k: setattr(d.lights[0], "type", 7), "unknown light type"),
     ("no texture table", lambda d, k: setattr(d, "n_textures", 1), "textures missing"),
     ("unknown texture", lambda d, k: (k.append(_tex_table(5)), setattr(d, "n_textures", 1),
