@@ -164,8 +164,6 @@ rumi_status upload(T **dst, const void *src, size_t bytes, cudaStream_t s) {
     return RUMI_OK;
 }
 
-float f_len(const float *v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
-
 void free_scene(rumi_scene *sc) {
     if (!sc) return;
     cudaStream_t s = sc->stream;
@@ -331,32 +329,6 @@ static rumi_status upload_textures(rumi_scene *sc, const rumi_scene_desc *d, cud
     return RUMI_OK;
 }
 
-DevMaterial make_material(const rumi_material &m) {
-    DevMaterial d;
-    memset(&d, 0, sizeof(d));
-    d.type = m.type;
-    d.kd = m.kd;
-    d.ks = m.ks;
-    d.e = m.exponent;
-    d.rgb = make_float3(m.rgb[0], m.rgb[1], m.rgb[2]);
-    d.eta_in = m.eta_in;
-    d.eta_out = m.eta_out;
-    d.rgb2 = make_float3(m.rgb2[0], m.rgb2[1], m.rgb2[2]);
-    if (m.type == RUMI_MAT_GLOSSY) {
-        d.kd_pdf = m.kd / (m.kd + m.ks);
-        d.phong_norm = (float)((m.exponent + 1.0f) / (2.0f * 3.14159265358979323846));
-    }
-    if (m.type == RUMI_MAT_SUBSURFACE) {
-        const float st[3] = {m.rgb[0] + m.rgb2[0], m.rgb[1] + m.rgb2[1], m.rgb[2] + m.rgb2[2]};
-        d.sigma_t = make_float3(st[0], st[1], st[2]);
-        const float density = m.density > 0.0f ? m.density : 1.0f;
-        d.avg_sigma_t = (st[2] + st[1] + st[0]) / 3.0f * density;
-        d.absorb = ((m.rgb2[2] / st[2]) + (m.rgb2[1] / st[1]) + (m.rgb2[0] / st[0])) / 3.0f;
-    }
-    if (m.type == RUMI_MAT_EMISSIVE) d.le = make_float3(m.rgb[0] * m.kd, m.rgb[1] * m.kd, m.rgb[2] * m.kd);
-    return d;
-}
-
 // tri_shade[3i..3i+2] = (n0, material), (n1, 0), (n2, 0); without normals the face
 // normal Normalize(Cross(v1 - v0, v2 - v0)) as Model::LoadObjectFile computes it
 // (src/Shape/model.cpp:320-323), with correctly rounded operations.
@@ -388,39 +360,6 @@ __global__ void pack_albedo_kernel(const float *a, int n, float4 *out) {
 }  // namespace
 
 namespace rumi {
-
-// HomogeneousVolume's constructor (src/Volume/homogeneousvolume.cpp:24-44): the box, the
-// coefficients and the derived mean extinction and absorption probability.
-void fill_dev_volume(DevVolume &dv, const rumi_volume &v) {
-    dv.present = v.present ? 1 : 0;
-    dv.bmin = make_float3(v.pmin[0], v.pmin[1], v.pmin[2]);
-    dv.bmax = make_float3(v.pmax[0], v.pmax[1], v.pmax[2]);
-    dv.sigma_s = make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]);
-    dv.sigma_a = make_float3(v.sigma_a[0], v.sigma_a[1], v.sigma_a[2]);
-    dv.sigma_t = make_float3(v.sigma_a[0] + v.sigma_s[0], v.sigma_a[1] + v.sigma_s[1], v.sigma_a[2] + v.sigma_s[2]);
-    dv.avg_sigma_t = (dv.sigma_t.z + dv.sigma_t.y + dv.sigma_t.x) * 0.33333333333f;
-    const float3 r = make_float3(dv.sigma_a.x / dv.sigma_t.x, dv.sigma_a.y / dv.sigma_t.y, dv.sigma_a.z / dv.sigma_t.z);
-    dv.absorb = (r.z + r.y + r.x) * 0.33333333333f;
-    dv.g = v.g;
-}
-
-// Pinhole's constructor (src/Camera/pinhole.cpp:30-49) with _fov set, and DepthOfField.
-// _dir, _up and _right are Mat4x4 * Vector3, which adds the matrix's translation column.
-void fill_dev_camera(DevCamera &dc, const rumi_camera &c) {
-    memset(&dc, 0, sizeof(dc));
-    dc.p = make_float3(c.position[0], c.position[1], c.position[2]);
-    for (int k = 0; k < 12; ++k) dc.m[k] = c.basis[k];
-    const float fov = c.fov_deg > 0.0f ? c.fov_deg : 20.0f;
-    dc.tanfov = (float)std::tan(3.14159265358979323846 / 180.f * fov * 0.5f);
-    dc.plane_dist = 1.0f;
-    dc.y_ratio = c.y_ratio;
-    dc.film_area = (2.0f * dc.tanfov) * (2.0f * dc.tanfov * c.y_ratio);
-    dc.dir = make_float3(c.basis[2] + c.basis[3], c.basis[6] + c.basis[7], c.basis[10] + c.basis[11]);
-    dc.up = make_float3(c.basis[1] + c.basis[3], c.basis[5] + c.basis[7], c.basis[9] + c.basis[11]);
-    dc.right = make_float3(c.basis[0] + c.basis[3], c.basis[4] + c.basis[7], c.basis[8] + c.basis[11]);
-    dc.focal_distance = c.focal_distance;
-    dc.lens_radius = c.lens_radius;
-}
 
 void pack_albedo(const float *a_dev, int n, float4 *out, cudaStream_t s) {
     const int grid = n < 256 * 1184 ? (n + 255) / 256 : 1184;
@@ -477,34 +416,8 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     }
     std::vector<DevLight> lights(d->n_lights);
     for (int i = 0; i < d->n_lights; ++i) {
-        const rumi_light &L = d->lights[i];
-        DevLight &dl = lights[i];
-        memset(&dl, 0, sizeof(dl));
-        dl.type = L.type;
-        dl.shape_type = L.shape_type;
-        dl.shape_index = L.shape_index;
-        if (L.type == RUMI_LIGHT_IBL) {
-            sc->has_ibl = true;
-        } else if (L.type == RUMI_LIGHT_AREA) {
-            int mi;
-            if (L.shape_type == RUMI_SHAPE_RECT) {
-                const float *r = d->rects + 9 * (size_t)L.shape_index;
-                const float len = f_len(r + 3), wid = f_len(r + 6);
-                dl.inv_area = 1.0f / (len * wid);
-                mi = d->rect_material[L.shape_index];
-            } else {
-                const float rad = d->spheres[4 * L.shape_index + 3];
-                dl.inv_area = (float)(1.0f / (4.0f * 3.14159265358979323846 * rad * rad));
-                mi = d->sphere_material[L.shape_index];
-            }
-            dl.le = mats[mi].le;
-        } else {
-            dl.position = make_float3(L.position[0], L.position[1], L.position[2]);
-            dl.direction = make_float3(L.direction[0], L.direction[1], L.direction[2]);
-            dl.cos_cone = (float)std::cos(L.cone_deg * 3.14159265358979323846 / 180.0);
-            dl.intensity = make_float3(L.intensity[0], L.intensity[1], L.intensity[2]);
-            dl.inv_area = 1.0f;
-        }
+        lights[i] = make_light(*d, d->lights[i], mats.data());
+        if (d->lights[i].type == RUMI_LIGHT_IBL) sc->has_ibl = true;
     }
     DevScene &ds = sc->dev;
     memset(&ds, 0, sizeof(ds));

@@ -31,7 +31,7 @@ namespace rumi {
 __device__ int g_bd_range[4];
 // Records the first out-of-range index; out of line, so each checked access costs a
 // compare and a branch.
-__device__ __noinline__ void bd_index_fail(int idx, int n, int code) {
+__device__ RUMI_NOINLINE void bd_index_fail(int idx, int n, int code) {
     if (atomicCAS(&g_bd_range[0], 0, code) == 0) {
         g_bd_range[1] = idx;
         g_bd_range[2] = n;
@@ -872,6 +872,9 @@ __global__ void add_light_film(float *film, const float *light, size_t n) {
         film[i] += light[i];
 }
 
+// The launch sequence.  A host build of this file (RUMI_HOST_BUILD: the kernel body
+// compiled as plain C++ for address and undefined-behaviour checks on the CPU) leaves it out.
+#ifndef RUMI_HOST_BUILD
 rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film_dev, rumi_render_stats *stats,
                         cudaStream_t stream) {
     const DevScene &S = sc->dev;
@@ -976,5 +979,6 @@ rumi_status bdpt_render(rumi_scene *sc, const rumi_render_params *p, float *film
     if (e1) cudaEventDestroy(e1);
     return RUMI_OK;
 }
+#endif  // RUMI_HOST_BUILD
 
 }  // namespace rumi

@@ -7,6 +7,11 @@
 
 #define RUMI_HD __host__ __device__ __forceinline__
 #define RUMI_D __device__ __forceinline__
+#ifdef __CUDACC__
+#define RUMI_NOINLINE __noinline__
+#else  // a host compiler building device code as plain C++
+#define RUMI_NOINLINE __attribute__((noinline))
+#endif
 
 // The reference's epsilon for self-intersection and the light end of shadow rays
 // (src/Kernel/ray.cpp:4).

@@ -6,6 +6,7 @@
 #include "../../include/rumi_b200.h"
 #include "scene.cuh"
 #include "bvh_build.h"
+#include "scene_host.h"
 
 // Paths in flight per wave when the caller passes wave_paths = 0: 2^25 (5.9 GB of path
 // tracer wave state at 176 bytes per path; a frame with fewer paths takes one wave of
@@ -87,8 +88,6 @@ rumi_status pt_enqueue_batch(const BatchFrame &F, void *ws, float *films, cudaSt
 unsigned long long *pt_batch_stats_ptr(void *ws, long long wave_paths);
 
 void set_error(const std::string &msg);
-void fill_dev_volume(DevVolume &dv, const rumi_volume &v);
-void fill_dev_camera(DevCamera &dc, const rumi_camera &c);
 void pack_albedo(const float *a_dev, int n, float4 *out, cudaStream_t s);
 rumi_status cuda_status(cudaError_t e, const char *what);
 
