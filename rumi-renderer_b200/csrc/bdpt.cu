@@ -194,10 +194,9 @@ RUMI_D int construct_subpath(const BdLaunch &P, bool eye, int max_depth, uint64_
                              float3 light_n, int *stack, TraceStats &st) {
     const DevScene &S = P.s;
     const DevVolume &vol = S.volume;
-    bool le = true, in_object = false;
+    bool in_object = false;
     alpha[0] = c3(1.0f);
     int n_vertex = 1;
-    int prev_mat = -1;
     float3 prev_w = mk3(0, 0, 0);  // prev_wo (eye) / prev_wi (light)
     const int max_seg = max_depth - 1;  // the reference's Path[max_depth - 1] array
     for (int depth = 0; depth < max_depth && depth < max_seg; ++depth) {
@@ -246,7 +245,6 @@ RUMI_D int construct_subpath(const BdLaunch &P, bool eye, int max_depth, uint64_
             n = end.n;
             const BsdfSample b = material_sample(m, wrev, n, U0.u[0], U0.u[1], U0.u[2]);
             w = b.w;
-            le = b.le;
             in_object = b.go_in;
             end.xi = b.xi;
             end.pdf_path = b.pdf_path;
@@ -262,7 +260,6 @@ RUMI_D int construct_subpath(const BdLaunch &P, bool eye, int max_depth, uint64_
             } else {
                 w = hg_sample(d, vol.g, U0.u[1], U0.u[2], pdf_dir);
             }
-            le = false;
             in_object = false;
             end.pdf_dir = pdf_dir;
             end.dirac = false;
@@ -385,12 +382,10 @@ RUMI_D int construct_subpath(const BdLaunch &P, bool eye, int max_depth, uint64_
         } else {
             if (end.onsurface && end_le) break;
         }
-        prev_mat = end.mat;
         prev_w = wrev;
         o = end.p;
         d = w;
     }
-    (void)prev_mat;
     return n_vertex;
 }
 
