@@ -394,7 +394,10 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     std::vector<float4> rects((size_t)nR * 3);
     std::vector<int> rect_emissive((size_t)nR + nS);  // prim flags: rects, then spheres
     std::vector<DevMaterial> mats(d->n_materials);
-    for (int i = 0; i < d->n_materials; ++i) mats[i] = make_material(d->materials[i]);
+    for (int i = 0; i < d->n_materials; ++i) {
+        mats[i] = make_material(d->materials[i]);
+        if (mats[i].type == RUMI_MAT_SUBSURFACE) sc->has_subsurface = true;
+    }
     for (int i = 0; i < nR; ++i) {
         const float *r = d->rects + 9 * (size_t)i;
         int mi = d->rect_material[i];

@@ -25,6 +25,7 @@ struct rumi_batch {
     void *ws = nullptr;
     size_t ws_bytes = 0;
     float *d_films = nullptr;     // film staging for host-film calls
+    bool lean = true;             // every scene (as the table holds it) qualifies for lean shading
     // the captured frame and what it was captured for
     cudaGraphExec_t graph = nullptr;
     std::vector<int> graph_spp;
@@ -118,6 +119,7 @@ rumi_status rumi_batch_create(rumi_scene *const *scenes, int32_t n, rumi_batch *
     b->pix0.assign(n + 1, 0);
     for (int i = 0; i < n; ++i) {
         table[i] = scenes[i]->dev;
+        if (!shade_lean(scenes[i])) b->lean = false;
         b->pix0[i + 1] = b->pix0[i] + (long long)table[i].width * table[i].height;
     }
     e = dalloc((void **)&b->d_scenes, sizeof(DevScene) * n, b->stream);
@@ -200,6 +202,7 @@ rumi_status rumi_render_batch(rumi_batch *b, const rumi_batch_params *p, float *
     if (wave < max_spp) wave = max_spp;
     if (wave > 0x3fffffffLL) return set_error("wave_paths too large"), RUMI_ERR_INVALID_ARG;  // 30-bit slots
     BatchFrame F;
+    F.lean = b->lean;
     F.n_scenes = n;
     F.max_depth = p->max_depth;
     F.wave_paths = wave;

@@ -38,6 +38,7 @@ struct rumi_scene {
     float4 *sphere_frame = nullptr;
     std::vector<void *> tex_pixels;  // one device array per image texture
     bool has_ibl = false;
+    bool has_subsurface = false;  // a Subsurface material (its random walk runs in shading)
     // the any-hit launch of a bounce runs beside the next bounce's closest-hit launch
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -58,6 +59,12 @@ struct rumi_scene {
     size_t ws_bytes = 0;
 };
 
+// A scene without a medium, textures, image-based lights or subsurface materials: its
+// forward shading runs the instantiation with those branches compiled out.
+inline bool shade_lean(const rumi_scene *sc) {
+    return !sc->dev.volume.present && !sc->dev.prim_tex && !sc->has_ibl && !sc->has_subsurface;
+}
+
 namespace rumi {
 
 struct BatchWave {
@@ -66,6 +73,7 @@ struct BatchWave {
 
 // One frame of a multi-scene batch (device tables; `waves` on the host).
 struct BatchFrame {
+    bool lean = false;  // every scene qualifies for the lean shading instantiation (shade_lean)
     const DevScene *scenes;
     const long long *scene_path0, *scene_pix0;
     const uint32_t *scene_key;

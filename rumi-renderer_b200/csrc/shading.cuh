@@ -459,13 +459,15 @@ RUMI_D int pick_light(const DevScene &s, float u) {
 // Scene::VisibilityTest's light part: pick a light, sample a point on it
 // (AreaLight::Sampling -> Shape::ShapeSampling, uniform over the shape; an image-based
 // light samples a direction about the shading normal n at p instead).
+// IBL = false compiles the image-based branch out, for scenes without such a light.
+template <bool IBL = true>
 RUMI_D LightSample sample_light(const DevScene &s, float ul, float u1, float u2, float3 p = mk3(0.0f, 0.0f, 0.0f),
                                 float3 n = mk3(0.0f, 1.0f, 0.0f)) {
     LightSample ls;
     const DevLight L = s.lights[pick_light(s, ul)];
     ls.is_delta = false;
     ls.is_ibl = false;
-    if (L.type == LIGHT_IBL) {
+    if (IBL && L.type == LIGHT_IBL) {
         sample_ibl(s, L, p, n, u1, u2, ls);
         return ls;
     }
