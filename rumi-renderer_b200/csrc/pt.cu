@@ -42,13 +42,25 @@ static constexpr int TRACE_THREADS = 128;
 #ifndef RUMI_SHADOW_MIN_BLOCKS
 #define RUMI_SHADOW_MIN_BLOCKS RUMI_TRACE_MIN_BLOCKS
 #endif
+// The default walk (scheme 3, the speculative while-while walk over the binary tree) at 9
+// blocks: 56 registers with a 38-byte spill (closest-hit) and 55 without one (any-hit);
+// per 1024x1024x64 frame 83.3 / 44.5 ms of closest-hit / any-hit against 83.8 / 45.7 at 8.
+#ifndef RUMI_WW_MIN_BLOCKS
+#define RUMI_WW_MIN_BLOCKS 9
+#endif
+static constexpr int trace_min_blocks(int mode, bool extend) {
+    return mode == 3 ? RUMI_WW_MIN_BLOCKS : (extend ? RUMI_EXTEND_MIN_BLOCKS : RUMI_SHADOW_MIN_BLOCKS);
+}
 // 1: each bounce's any-hit launch runs on an auxiliary stream beside the next bounce's
 // closest-hit launch (pt_render_in); 0: one stream, launches in order.
 #ifndef RUMI_PT_OVERLAP
 #define RUMI_PT_OVERLAP 1
 #endif
 static constexpr int STACK_SMEM = 32;
-static constexpr int SHADE_THREADS = 256;
+#ifndef RUMI_SHADE_THREADS
+#define RUMI_SHADE_THREADS 256
+#endif
+static constexpr int SHADE_THREADS = RUMI_SHADE_THREADS;
 
 enum { PFL_LE = 1, PFL_IN = 2 };
 // A queued ray's o.w holds its path slot (bits 0-29) and its flags: bit 31 = in_object
@@ -236,7 +248,7 @@ __global__ void pt_reset_shade(PtLaunch P, int bounce) {
 // SMEM: traversal stack entries per thread kept in shared memory (deeper entries spill to
 // local memory); a smaller stack leaves more of the SM's unified L1/shared storage to L1.
 template <int MODE, bool STATS, int SMEM = STACK_SMEM>
-__global__ void __launch_bounds__(TRACE_THREADS, RUMI_EXTEND_MIN_BLOCKS) pt_extend(PtLaunch P, int bounce) {
+__global__ void __launch_bounds__(TRACE_THREADS, trace_min_blocks(MODE, true)) pt_extend(PtLaunch P, int bounce) {
     __shared__ int stack[SMEM * TRACE_THREADS];
     const int cur = bounce & 1;
     TraceStats st{0, 0};
@@ -261,7 +273,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, RUMI_EXTEND_MIN_BLOCKS) pt_exte
 }
 
 template <int MODE, bool ADJ = false, int SMEM = STACK_SMEM>
-__global__ void __launch_bounds__(TRACE_THREADS, RUMI_SHADOW_MIN_BLOCKS) pt_shadow(PtLaunch P) {
+__global__ void __launch_bounds__(TRACE_THREADS, trace_min_blocks(MODE, false)) pt_shadow(PtLaunch P) {
     __shared__ int stack[SMEM * TRACE_THREADS];
     TraceStats st{0, 0};
     float acc_sigma = 0.0f, acc_g = 0.0f;  // adjoint: score-weighted contributions
@@ -987,11 +999,11 @@ static void launch_shadow(int mode, int smem, int grid, cudaStream_t st, const P
     shadow_kernel<ADJ>(mode, smem)<<<grid, TRACE_THREADS, 0, st>>>(L);
 }
 
-// Asks for just the shared memory the resident blocks' stacks need (RUMI_TRACE_MIN_BLOCKS
-// blocks of smem entries per thread), so the rest of the unified L1 / shared storage stays L1.
+// Asks for just the shared memory the resident blocks' stacks need (`blocks` blocks of smem
+// entries per thread), so the rest of the unified L1 / shared storage stays L1.
 template <typename K>
-static void prefer_l1(K k, int smem) {
-    const int need = RUMI_TRACE_MIN_BLOCKS * smem * TRACE_THREADS * (int)sizeof(int);
+static void prefer_l1(K k, int smem, int blocks) {
+    const int need = blocks * smem * TRACE_THREADS * (int)sizeof(int);
     int pct = (need * 100 + 228 * 1024 - 1) / (228 * 1024);
     if (pct > 100) pct = 100;
     cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
@@ -1002,9 +1014,9 @@ static void trace_grids(int mode, int smem, int num_sms, int blocks_per_sm, bool
     int occ = 0, occ_sh = 0;
     const ExtendKernel ke = extend_kernel<false>(mode, smem);
     const ShadowKernel ks = adj ? shadow_kernel<true>(mode, smem) : shadow_kernel<false>(mode, smem);
-    prefer_l1(ke, smem);
-    prefer_l1(extend_kernel<true>(mode, smem), smem);
-    prefer_l1(ks, smem);
+    prefer_l1(ke, smem, trace_min_blocks(mode, true));
+    prefer_l1(extend_kernel<true>(mode, smem), smem, trace_min_blocks(mode, true));
+    prefer_l1(ks, smem, trace_min_blocks(mode, false));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ke, TRACE_THREADS, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, ks, TRACE_THREADS, 0);
     if (occ < 1) occ = 1;
