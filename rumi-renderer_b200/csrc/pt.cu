@@ -694,6 +694,10 @@ __global__ void __launch_bounds__(SHADE_THREADS, ADJ ? 1 : (LEAN ? RUMI_SHADE_LE
     // in queue order, so a warp then holds rays from a few neighbouring pixels' hit points
     // that head the same way (closest-hit 2% faster per frame on the 1M-triangle
     // workload).  A path's result does not depend on its queue position.
+#ifdef RUMI_HOST_BUILD
+    // host build (one emulated thread per block): the block's group is its one ray
+    const int kn = want_next ? atomicAdd(&P.cnt[nxt], 1) : -1;
+#else
     __shared__ int s_bins[32];
     if (threadIdx.x < 32) s_bins[threadIdx.x] = 0;
     __syncthreads();
@@ -721,6 +725,7 @@ __global__ void __launch_bounds__(SHADE_THREADS, ADJ ? 1 : (LEAN ? RUMI_SHADE_LE
     }
     __syncthreads();
     const int kn = want_next ? s_bins[dkey] + drank : -1;
+#endif
     const int ks = warp_push(&P.cnt[C_SHADOW], want_sh);
     if (want_next) {
         P.ray_o[nxt][kn] = make_float4(nx_o.x, nx_o.y, nx_o.z, pack_slot(slot, nx_flags));
@@ -954,6 +959,9 @@ using ShadowKernel = void (*)(PtLaunch);
 // node fetches use, and deeper entries are rare.
 static inline int stack_entries(int stack_depth) { return stack_depth == 8 || stack_depth == 32 ? stack_depth : 16; }
 
+// Kernel selection and launches.  A host build of this file (RUMI_HOST_BUILD: the kernels
+// compiled as plain C++ for the CPU tests) leaves them out; it keeps the wave layout below.
+#ifndef RUMI_HOST_BUILD
 template <bool STATS>
 static ExtendKernel extend_kernel(int mode, int smem) {
     switch (mode) {
@@ -1029,6 +1037,8 @@ static void trace_grids(int mode, int smem, int num_sms, int blocks_per_sm, bool
     grid_sh = num_sms * occ_sh;
 }
 
+#endif  // RUMI_HOST_BUILD
+
 // Carves the wave state for Wp paths out of ws (pt_workspace_bytes(Wp) bytes) and clears
 // every optional field; returns the first byte after it.
 static char *carve_wave(PtLaunch &L, void *ws, size_t Wp) {
@@ -1059,6 +1069,7 @@ size_t pt_workspace_bytes(long long paths) {
     return 11 * al(Wp * sizeof(float4)) + al(C_NUM * sizeof(int)) + al(S_NUM * sizeof(unsigned long long));
 }
 
+#ifndef RUMI_HOST_BUILD
 // The scene's second stream and its fork / join events, made on first use.
 static rumi_status ensure_aux(rumi_scene *sc) {
     if (sc->aux_stream) return RUMI_OK;
@@ -1612,5 +1623,7 @@ rumi_status trace_rays_scheme(rumi_scene *sc, int64_t n, const float *rays_dev, 
     if (e != cudaSuccess) return cuda_status(e, "trace_rays_scheme");
     return RUMI_OK;
 }
+
+#endif  // RUMI_HOST_BUILD
 
 }  // namespace rumi

@@ -1,7 +1,7 @@
 // Host-side conversions from the C-ABI scene description (include/rumi_b200.h) to the
 // device records of scene.cuh.  Pure host code: used by rumi_scene_create and by the
-// scene-parameter setters, and compiled with a host compiler alone by the host build of
-// the BDPT kernel that the CPU tests run under address and undefined-behaviour checks.
+// scene-parameter setters, and compiled with a host compiler alone by the host builds of
+// the kernels that the CPU tests run under address and undefined-behaviour checks.
 // Derived constants are computed the way the reference's constructors compute them, in
 // float (double where the reference mixes in its double PI):
 //   Rect              src/Shape/rect.cpp:12-38          Sphere  src/Shape/sphere.cpp:18-38

@@ -1256,6 +1256,21 @@ RUMI_D void traverse_queue_walk(SceneOf scene_of, int n, int *counter, int refil
 template <int MODE, bool ANYHIT, int STACK_SMEM, bool STATS, typename Fetch, typename Finish>
 RUMI_D void traverse_queue(const DevScene &s, int n, int *counter, int refill_min, int *smem_stack, int stride,
                            Fetch fetch, Finish finish, TraceStats &st) {
+#ifdef RUMI_HOST_BUILD
+    // Host build of the kernels (CPU tests under sanitizers): one emulated thread takes
+    // the queue's rays one after another through the per-ray walk; the warp-cooperative
+    // schemes above have no single-thread form.
+    (void)refill_min;
+    for (;;) {
+        const int i = atomicAdd(counter, 1);
+        if (i >= n) return;
+        float3 o, d;
+        float tmax;
+        bool in_obj;
+        fetch(i, o, d, tmax, in_obj);
+        finish(i, trace_ray<ANYHIT, STACK_SMEM, STATS>(s, o, d, tmax, in_obj, smem_stack, stride, st));
+    }
+#endif
     const int lane = threadIdx.x & 31;
     int spill[RUMI_MAX_BVH_DEPTH - STACK_SMEM > 0 ? RUMI_MAX_BVH_DEPTH - STACK_SMEM : 1];
     if (MODE == 3) {

@@ -93,6 +93,20 @@ template <typename T>
 inline T __shfl_sync(unsigned, T v, int, int = 32) {
     return v;
 }
+template <typename T>
+inline T __shfl_up_sync(unsigned, T v, unsigned, int = 32) {
+    return v;
+}
+template <typename T>
+inline T __shfl_xor_sync(unsigned, T v, int, int = 32) {
+    return v;
+}
+template <typename T>
+inline unsigned __match_any_sync(unsigned, T) {
+    return 1u;
+}
+inline int min(int a, int b) { return a < b ? a : b; }
+inline int max(int a, int b) { return a > b ? a : b; }
 inline void __syncthreads() {}
 inline void __syncwarp(unsigned = 0xffffffffu) {}
 
