@@ -281,46 +281,25 @@ rumi_status validate(const rumi_scene_desc *d) {
 // Textures: DevTexture table, pixel arrays, per-primitive texture index and sphere frames.
 // Nothing is allocated for a scene without textures.
 static rumi_status upload_textures(rumi_scene *sc, const rumi_scene_desc *d, cudaStream_t s) {
-    const int nT = d->n_triangles, nR = d->n_rects, nS = d->n_spheres;
-    const bool any = d->n_textures > 0 && (d->tri_texture || d->rect_texture || d->sphere_texture);
-    if (!any) return RUMI_OK;
+    if (!has_textures(*d)) return RUMI_OK;
     std::vector<DevTexture> tex(d->n_textures);
     for (int i = 0; i < d->n_textures; ++i) {
         const rumi_texture &t = d->textures[i];
-        DevTexture &dt = tex[i];
-        memset(&dt, 0, sizeof(dt));
-        dt.type = t.type;
-        dt.rep_u = t.repeat_u;
-        dt.rep_v = t.repeat_v;
-        dt.c1 = make_float3(t.color1[0], t.color1[1], t.color1[2]);
-        dt.c2 = make_float3(t.color2[0], t.color2[1], t.color2[2]);
-        dt.gamma = t.gamma;
-        dt.iw = t.img_width;
-        dt.ih = t.img_height;
-        dt.bpp = t.type == RUMI_TEX_HDR ? 3 : t.bytes_per_pixel;
+        tex[i] = make_texture(t);
         if (t.type == RUMI_TEX_CHECKER) continue;
-        const size_t bytes = t.type == RUMI_TEX_HDR ? sizeof(float) * 3 * (size_t)t.img_width * t.img_height
-                                                    : (size_t)t.img_width * t.img_height * t.bytes_per_pixel;
         void *p = nullptr;
-        rumi_status st = upload(&p, t.pixels, bytes, s);
+        rumi_status st = upload(&p, t.pixels, texture_pixel_bytes(t), s);
         if (p) sc->tex_pixels.push_back(p);
         if (st != RUMI_OK) return st;
         if (t.type == RUMI_TEX_HDR)
-            dt.hdr = (const float *)p;
+            tex[i].hdr = (const float *)p;
         else
-            dt.img = (const unsigned char *)p;
+            tex[i].img = (const unsigned char *)p;
     }
-    std::vector<int> prim_tex((size_t)nT + nR + nS, -1);
-    for (int i = 0; d->tri_texture && i < nT; ++i) prim_tex[i] = d->tri_texture[i];
-    for (int i = 0; d->rect_texture && i < nR; ++i) prim_tex[(size_t)nT + i] = d->rect_texture[i];
-    for (int i = 0; d->sphere_texture && i < nS; ++i) prim_tex[(size_t)nT + nR + i] = d->sphere_texture[i];
-    std::vector<float4> frame((size_t)nS * 3);
-    for (int i = 0; i < nS; ++i) {
-        const float *f = d->sphere_frame ? d->sphere_frame + 9 * (size_t)i : nullptr;
-        for (int r = 0; r < 3; ++r)
-            frame[3 * i + r] = f ? make_float4(f[3 * r], f[3 * r + 1], f[3 * r + 2], 0.0f)
-                                 : make_float4(r == 0, r == 1, r == 2, 0.0f);
-    }
+    std::vector<int> prim_tex;
+    std::vector<float4> frame;
+    texture_tables(*d, prim_tex, frame);
+    const int nS = d->n_spheres;
     rumi_status st;
     if ((st = upload(&sc->textures, tex.data(), sizeof(DevTexture) * tex.size(), s)) != RUMI_OK) return st;
     if ((st = upload(&sc->prim_tex, prim_tex.data(), sizeof(int) * prim_tex.size(), s)) != RUMI_OK) return st;
@@ -413,9 +392,7 @@ rumi_status rumi_scene_create(const rumi_scene_desc *d, rumi_scene **out) {
     std::vector<float4> spheres(nS);
     for (int i = 0; i < nS; ++i) {
         spheres[i] = make_float4(d->spheres[4 * i], d->spheres[4 * i + 1], d->spheres[4 * i + 2], d->spheres[4 * i + 3]);
-        // Sphere::Intersect's image-based-light branch: Material::IsLe() and a texture
-        rect_emissive[(size_t)nR + i] = mats[d->sphere_material[i]].type == RUMI_MAT_EMISSIVE &&
-                                        d->n_textures > 0 && d->sphere_texture && d->sphere_texture[i] >= 0;
+        rect_emissive[(size_t)nR + i] = sphere_is_ibl(*d, mats.data(), i);
     }
     std::vector<DevLight> lights(d->n_lights);
     for (int i = 0; i < d->n_lights; ++i) {

@@ -12,6 +12,7 @@
 #pragma once
 #include <cmath>
 #include <cstring>
+#include <vector>
 #include "../../include/rumi_b200.h"
 #include "scene.cuh"
 
@@ -106,6 +107,57 @@ inline void fill_dev_camera(DevCamera &dc, const rumi_camera &c) {
     dc.right = make_float3(c.basis[0] + c.basis[3], c.basis[4] + c.basis[7], c.basis[8] + c.basis[11]);
     dc.focal_distance = c.focal_distance;
     dc.lens_radius = c.lens_radius;
+}
+
+// One texture of the description without its pixels (the caller points img / hdr at them).
+inline DevTexture make_texture(const rumi_texture &t) {
+    DevTexture dt;
+    memset(&dt, 0, sizeof(dt));
+    dt.type = t.type;
+    dt.rep_u = t.repeat_u;
+    dt.rep_v = t.repeat_v;
+    dt.c1 = make_float3(t.color1[0], t.color1[1], t.color1[2]);
+    dt.c2 = make_float3(t.color2[0], t.color2[1], t.color2[2]);
+    dt.gamma = t.gamma;
+    dt.iw = t.img_width;
+    dt.ih = t.img_height;
+    dt.bpp = t.type == RUMI_TEX_HDR ? 3 : t.bytes_per_pixel;
+    return dt;
+}
+
+// Bytes of a texture's pixel array (0 for a checker).
+inline size_t texture_pixel_bytes(const rumi_texture &t) {
+    if (t.type == RUMI_TEX_CHECKER) return 0;
+    return t.type == RUMI_TEX_HDR ? sizeof(float) * 3 * (size_t)t.img_width * t.img_height
+                                  : (size_t)t.img_width * t.img_height * t.bytes_per_pixel;
+}
+
+// Whether the description binds any texture to a primitive.
+inline bool has_textures(const rumi_scene_desc &d) {
+    return d.n_textures > 0 && (d.tri_texture || d.rect_texture || d.sphere_texture);
+}
+
+// Per-primitive texture index in canonical order (-1 = none) and each sphere's frame rows
+// (identity when the description has none).
+inline void texture_tables(const rumi_scene_desc &d, std::vector<int> &prim_tex, std::vector<float4> &frame) {
+    const int nT = d.n_triangles, nR = d.n_rects, nS = d.n_spheres;
+    prim_tex.assign((size_t)nT + nR + nS, -1);
+    for (int i = 0; d.tri_texture && i < nT; ++i) prim_tex[i] = d.tri_texture[i];
+    for (int i = 0; d.rect_texture && i < nR; ++i) prim_tex[(size_t)nT + i] = d.rect_texture[i];
+    for (int i = 0; d.sphere_texture && i < nS; ++i) prim_tex[(size_t)nT + nR + i] = d.sphere_texture[i];
+    frame.resize((size_t)nS * 3);
+    for (int i = 0; i < nS; ++i) {
+        const float *f = d.sphere_frame ? d.sphere_frame + 9 * (size_t)i : nullptr;
+        for (int r = 0; r < 3; ++r)
+            frame[3 * i + r] = f ? make_float4(f[3 * r], f[3 * r + 1], f[3 * r + 2], 0.0f)
+                                 : make_float4(r == 0, r == 1, r == 2, 0.0f);
+    }
+}
+
+// Sphere::Intersect's image-based-light branch: an emissive sphere with a texture.
+inline bool sphere_is_ibl(const rumi_scene_desc &d, const DevMaterial *mats, int i) {
+    return mats[d.sphere_material[i]].type == RUMI_MAT_EMISSIVE && d.n_textures > 0 && d.sphere_texture &&
+           d.sphere_texture[i] >= 0;
 }
 
 }  // namespace rumi

@@ -28,7 +28,7 @@ int rumi_host_bdpt(const rumi_scene_desc *d, int n_light, int n_eye, int spp, ui
     if (n_light < 2 || n_eye < 2 || n_light > BD_MAXV || n_eye > BD_MAXV) return -2;
     if ((long long)pix0 + n_pix > (long long)d->width * d->height || d->n_lights <= 0) return -2;
     HostScene H;
-    if (build_scene(*d, H) != 0) return -1;
+    if (build_scene(*d, H) != 0 || H.has_ibl) return -1;  // bdpt_render rejects image-based lights
     BdLaunch B;
     memset(&B, 0, sizeof(B));
     B.s = H.dev;

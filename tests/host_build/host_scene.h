@@ -4,8 +4,8 @@
 // intersection records of the canonical primitives (prim_prepare_kernel in bvh_build.cu),
 // the shading normals (pack_tri_shade_kernel in api.cu) and a BVH of one leaf holding every
 // primitive in canonical order (every ray tests every primitive, which gives the closest hit
-// of any valid tree).  Include after the kernel source.  Scenes with textures or
-// image-based lights are not covered.
+// of any valid tree).  Texture pixels are read where the description holds them.  Include
+// after the kernel source.
 #pragma once
 #include <algorithm>
 #include <vector>
@@ -17,6 +17,10 @@ using namespace rumi;
 struct HostScene {
     std::vector<DevMaterial> mats;
     std::vector<DevLight> lights;
+    std::vector<DevTexture> tex;
+    std::vector<int> prim_tex;
+    std::vector<float4> frame;
+    bool has_ibl = false, has_subsurface = false;
     std::vector<float4> rects, spheres, tri_shade, tri_albedo, prims;
     std::vector<int> sphere_mat;
     BvhNode root;
@@ -30,14 +34,28 @@ void grow(float lo[3], float hi[3], float x, float y, float z) {
 
 // Returns 0, or -1 for a description this build does not cover.
 int build_scene(const rumi_scene_desc &d, HostScene &H) {
-    if (d.n_textures > 0 && (d.tri_texture || d.rect_texture || d.sphere_texture)) return -1;
     const int nT = d.n_triangles, nR = d.n_rects, nS = d.n_spheres, N = nT + nR + nS;
     H.mats.resize(d.n_materials);
-    for (int i = 0; i < d.n_materials; ++i) H.mats[i] = make_material(d.materials[i]);
+    for (int i = 0; i < d.n_materials; ++i) {
+        H.mats[i] = make_material(d.materials[i]);
+        H.has_subsurface |= H.mats[i].type == RUMI_MAT_SUBSURFACE;
+    }
     H.lights.resize(d.n_lights);
     for (int i = 0; i < d.n_lights; ++i) {
-        if (d.lights[i].type == RUMI_LIGHT_IBL) return -1;
+        H.has_ibl |= d.lights[i].type == RUMI_LIGHT_IBL;
         H.lights[i] = make_light(d, d.lights[i], H.mats.data());
+    }
+    if (has_textures(d)) {
+        H.tex.resize(d.n_textures);
+        for (int i = 0; i < d.n_textures; ++i) {
+            const rumi_texture &t = d.textures[i];
+            H.tex[i] = make_texture(t);
+            if (t.type == RUMI_TEX_HDR)
+                H.tex[i].hdr = static_cast<const float *>(t.pixels);
+            else if (t.type != RUMI_TEX_CHECKER)
+                H.tex[i].img = static_cast<const unsigned char *>(t.pixels);
+        }
+        texture_tables(d, H.prim_tex, H.frame);
     }
     float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     H.prims.resize(3 * (size_t)(N > 0 ? N : 1));
@@ -96,7 +114,8 @@ int build_scene(const rumi_scene_desc &d, HostScene &H) {
         grow(lo, hi, c[0] + c[3], c[1] + c[3], c[2] + c[3]);
         const int i = nT + nR + s;
         H.prims[3 * i + 0] = make_float4(c[0], c[1], c[2], __int_as_float(i));
-        H.prims[3 * i + 1] = make_float4(c[3], 0.0f, 0.0f, __int_as_float(PRIM_SPHERE));
+        H.prims[3 * i + 1] = make_float4(c[3], 0.0f, 0.0f,
+                                         __int_as_float(PRIM_SPHERE | (sphere_is_ibl(d, H.mats.data(), s) ? PRIM_FLAG_IBL : 0)));
         H.prims[3 * i + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     // the one leaf: its box padded by a little, so rays grazing the scene's bounds reach it
@@ -134,6 +153,12 @@ int build_scene(const rumi_scene_desc &d, HostScene &H) {
     fill_dev_camera(S.camera, d.camera);
     S.width = d.width;
     S.height = d.height;
+    if (!H.tex.empty()) {
+        S.textures = H.tex.data();
+        S.prim_tex = H.prim_tex.data();
+        S.sphere_frame = H.frame.empty() ? nullptr : H.frame.data();
+        S.n_textures = d.n_textures;
+    }
     return 0;
 }
 

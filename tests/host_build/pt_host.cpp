@@ -55,9 +55,8 @@ int rumi_host_pt(const rumi_scene_desc *d, int integrator, int max_depth, int sp
     if (!d || !film || spp < 1 || max_depth < 1) return -2;
     HostScene H;
     if (build_scene(*d, H) != 0) return -1;
-    bool subsurface = false;
-    for (int i = 0; i < d->n_materials; ++i) subsurface |= d->materials[i].type == RUMI_MAT_SUBSURFACE;
-    const bool can_lean = !H.dev.volume.present && !subsurface;  // no textures, no IBL here
+    // shade_lean's rule (renderer.h)
+    const bool can_lean = !H.dev.volume.present && !H.dev.prim_tex && !H.has_ibl && !H.has_subsurface;
     if (lean == 1 && !can_lean) return -2;
     const bool use_lean = lean < 0 ? can_lean : lean == 1;
     const long long n_pix = (long long)d->width * d->height;

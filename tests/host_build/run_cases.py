@@ -33,6 +33,30 @@ def _pt(sc, depth):
     return sc
 
 
+_FILES = []
+
+
+def _tex_files():
+    """(image BMP path, sky HDR path) of the textured cases, written once per process."""
+    if not _FILES:
+        import tempfile
+        import texture_cases as TC
+        _FILES.extend(TC.case_files(tempfile.mkdtemp(prefix="rumi_tex_")))
+    return _FILES
+
+
+def _textured(kind, medium=False):
+    import texture_cases as TC
+    img, hdr = _tex_files()
+    if kind == "tex":
+        sc = TC.textured_cornell(32, 32, 16, 8, img)
+    elif kind == "tex_bdpt":
+        sc = TC.textured_bdpt(32, 32, 16, img)
+    else:
+        sc = TC.ibl_scene(32, 32, 16, 8, hdr)
+    return scenes.with_medium(sc) if medium else sc
+
+
 def bdpt_cases():
     from test_oracle_golden import lights_in_medium, sss_in_medium
     S = scenes
@@ -59,6 +83,9 @@ def bdpt_cases():
         # subpaths of 6 and 7 vertices) and the 16-vertex kernel instantiation
         "workload": (lambda: S.volumetric_caustic(32, 32, 8, 6, 7), 8, None),
         "long": (lambda: S.cornell_bdpt(16, 16, 4, 12, 16), 4, None),
+        # textures (an image texture and checkers)
+        "textured": (lambda: _textured("tex_bdpt"), 16, "image_tex_bdpt32.npz"),
+        "textured_medium": (lambda: _textured("tex_bdpt", medium=True), 16, "image_tex_medium_bdpt32.npz"),
     }
 
 
@@ -85,6 +112,13 @@ def pt_cases():
                             "image_whitted_caustic32.npz"),
         "whitted_glass": (lambda: S.whitted(S.absorbing_glass_cornell()), 16, "image_glass_whitted32.npz"),
         "whitted_dof": (lambda: S.whitted(S.cornell_dof_pt(32, 32, 16, 8)), 16, "image_dof_whitted32.npz"),
+        # textures and an image-based light, alone and around a medium
+        "textured": (lambda: _textured("tex"), 16, "image_tex_pt32.npz"),
+        "textured_medium": (lambda: _textured("tex", medium=True), 16, "image_tex_medium_pt32.npz"),
+        "ibl": (lambda: _textured("ibl"), 16, "image_ibl_pt32.npz"),
+        "ibl_medium": (lambda: _textured("ibl", medium=True), 16, "image_ibl_medium_pt32.npz"),
+        "whitted_textured": (lambda: S.whitted(_textured("tex")), 16, "image_tex_whitted32.npz"),
+        "whitted_ibl": (lambda: S.whitted(_textured("ibl")), 16, "image_ibl_whitted32.npz"),
     }
 
 
