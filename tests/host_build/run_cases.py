@@ -6,6 +6,7 @@ instantiation.  Run as a separate process with the sanitizer runtime preloaded (
 interpreter itself is not built with it):
 
     LD_PRELOAD=$(g++ -print-file-name=libasan.so) python tests/host_build/run_cases.py bdpt|pt LIB [CASE ...]
+    LD_PRELOAD=... python tests/host_build/run_cases.py films LIB OUTDIR   (frames for the oracle)
 """
 import ctypes as C
 import hashlib
@@ -186,10 +187,42 @@ def run_pt(lib, names):
     return out
 
 
+def film_cases():
+    """Frames compared with the oracle pixel by pixel: (scene builder, integrator, depth,
+    samples per pixel, seed), the settings of the GPU's per-pixel tests."""
+    from test_oracle_golden import WHITTED_CASES
+    S = scenes
+    out = {"pt_cornell_d2": (lambda: S.cornell_pt(32, 32, 4, 2), 0, 2, 4, 21),
+           "pt_dof_d2": (lambda: S.cornell_dof_pt(32, 32, 4, 2), 0, 2, 4, 21)}
+    for fixture, builder in WHITTED_CASES:
+        out["whitted_" + fixture[len("image_"):-len(".npz")]] = (builder, 2, None, 4, 31)
+    return out
+
+
+def run_films(lib, outdir):
+    fn = lib.rumi_host_pt
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p]
+    out = {}
+    for name, (build, integrator, depth, spp, seed) in sorted(film_cases().items()):
+        sc = build()
+        fs = sc.flatten()
+        desc, keep = build_desc(fs)
+        film = np.zeros((fs.image.height, fs.image.width, 3), np.float32)
+        stats = np.zeros(16, np.uint64)
+        d = depth if depth is not None else sc.tracer.max_depth
+        rc = fn(C.addressof(desc), integrator, d, spp, seed, -1, film.ctypes.data, stats.ctypes.data)
+        np.save(os.path.join(outdir, name + ".npy"), film)
+        out[name] = {"rc": rc, "nan": int(stats[2])}
+    return out
+
+
 if __name__ == "__main__":
-    kind, lib_path, names = sys.argv[1], sys.argv[2], sys.argv[3:]
+    kind, lib_path, rest = sys.argv[1], sys.argv[2], sys.argv[3:]
     lib = C.CDLL(lib_path)
     if kind == "bdpt":
-        print(json.dumps(run_bdpt(lib, names or sorted(bdpt_cases()))))
+        print(json.dumps(run_bdpt(lib, rest or sorted(bdpt_cases()))))
+    elif kind == "films":
+        print(json.dumps(run_films(lib, rest[0])))
     else:
-        print(json.dumps(run_pt(lib, names or sorted(pt_cases()))))
+        print(json.dumps(run_pt(lib, rest or sorted(pt_cases()))))

@@ -26,6 +26,7 @@ import shutil
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -81,6 +82,13 @@ def host_runs(tmp_path_factory):
         assert r.returncode == 0, r.stderr[-6000:]
         assert "runtime error" not in r.stderr and "AddressSanitizer" not in r.stderr, r.stderr[-6000:]
         runs[(kind, init)] = json.loads(r.stdout.strip().splitlines()[-1])
+    films = out / "films"
+    films.mkdir()
+    r = subprocess.run([sys.executable, os.path.join(HOST_DIR, "run_cases.py"), "films", libs[("pt", "pattern")],
+                        str(films)], capture_output=True, text=True, env=env, timeout=1800)
+    assert r.returncode == 0, r.stderr[-6000:]
+    assert "runtime error" not in r.stderr and "AddressSanitizer" not in r.stderr, r.stderr[-6000:]
+    runs["films"] = (str(films), json.loads(r.stdout.strip().splitlines()[-1]))
     return runs
 
 
@@ -117,3 +125,26 @@ def test_path_tracer_kernels_stay_in_range_and_lean_shading_equals_general(host_
     if pat["lean_hash"] is not None:                # the lean instantiation applies
         assert pat["lean_hash"] == pat["general_hash"], case
     _mean_close(golden, pat)
+
+
+@pytest.mark.parametrize("case", sorted(run_cases.film_cases()))
+def test_path_tracer_kernels_match_the_oracle_per_pixel(host_runs, case):
+    """The kernels' source on the CPU against the oracle with the same Philox streams, with
+    the GPU per-pixel tests' settings: paths of two vertices, and the Whitted ray tracer (no
+    hemisphere sampling).  Both use the host's libm, so pixels agree to a few ulps (3.7e-5
+    relative at most here, most of them exactly); two pixels may differ more, for a lobe or
+    shadow decision that lands within an ulp of its threshold under another libm."""
+    import oraclelib as O
+    build, integrator, depth, spp, seed = run_cases.film_cases()[case]
+    folder, meta = host_runs["films"]
+    assert meta[case]["rc"] == 0, meta[case]
+    film = np.load(os.path.join(folder, case + ".npy"))
+    sc = build()
+    if integrator == 0:
+        ofilm, onan = O.OracleScene(sc).render_pt(depth, spp, seed)
+    else:
+        ofilm, onan = O.OracleScene(sc).render_whitted(sc.tracer.max_depth, spp, seed)
+    assert meta[case]["nan"] == onan == 0
+    rel = np.abs(film - ofilm) / np.maximum(np.abs(ofilm), 1e-3)
+    assert np.sum(rel.max(2) > 1e-4) <= 2, float(rel.max())
+    assert abs(film.sum() / ofilm.sum() - 1.0) < 1e-4
