@@ -193,7 +193,13 @@ def film_cases():
     from test_oracle_golden import WHITTED_CASES
     S = scenes
     out = {"pt_cornell_d2": (lambda: S.cornell_pt(32, 32, 4, 2), 0, 2, 4, 21),
-           "pt_dof_d2": (lambda: S.cornell_dof_pt(32, 32, 4, 2), 0, 2, 4, 21)}
+           "pt_dof_d2": (lambda: S.cornell_dof_pt(32, 32, 4, 2), 0, 2, 4, 21),
+           # full depth: paths part ways on some pixels once a float difference moves a
+           # scattering decision, without bias
+           "deep_cornell8": (lambda: S.cornell_pt(32, 32, 4, 8), 0, 8, 4, 21),
+           "deep_mesh10": (lambda: S.bvh_bound_pt(32, 32, 4, 10, levels=3, seed=7), 0, 10, 4, 21),
+           "deep_caustic8": (lambda: S.volumetric_caustic(32, 32, 4, 4, 5, parity=True), 0, 8, 4, 21),
+           "deep_sss12": (lambda: S.subsurface_cornell(32, 32, 4, 12), 0, 12, 4, 21)}
     for fixture, builder in WHITTED_CASES:
         out["whitted_" + fixture[len("image_"):-len(".npz")]] = (builder, 2, None, 4, 31)
     return out
