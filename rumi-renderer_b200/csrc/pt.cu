@@ -57,6 +57,9 @@ static constexpr int trace_min_blocks(int mode, bool extend) {
 #define RUMI_PT_OVERLAP 1
 #endif
 static constexpr int STACK_SMEM = 32;
+// Threads per block of the shading kernels; a block groups its next rays by direction, so
+// the block size is also the grouping's width (128: shading 0.5 ms faster per frame,
+// closest-hit 0.5 ms slower).
 #ifndef RUMI_SHADE_THREADS
 #define RUMI_SHADE_THREADS 256
 #endif
