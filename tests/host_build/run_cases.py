@@ -38,11 +38,15 @@ _FILES = []
 
 
 def _tex_files():
-    """(image BMP path, sky HDR path) of the textured cases, written once per process."""
+    """(image BMP path, sky HDR path) of the textured cases, written once per process into a
+    temporary folder that is removed when the process exits."""
     if not _FILES:
+        import atexit
         import tempfile
         import texture_cases as TC
-        _FILES.extend(TC.case_files(tempfile.mkdtemp(prefix="rumi_tex_")))
+        folder = tempfile.TemporaryDirectory(prefix="rumi_tex_")
+        atexit.register(folder.cleanup)
+        _FILES.extend(TC.case_files(folder.name))
     return _FILES
 
 
