@@ -97,6 +97,9 @@ template <typename T>
 inline T __shfl_up_sync(unsigned, T v, unsigned, int = 32) {
     return v;
 }
+// A butterfly exchange with no other lane: the lane's own value, which keeps min / max
+// reductions right; the warp sums of the adjoint kernels would come out scaled, and the host
+// builds do not run those kernels.
 template <typename T>
 inline T __shfl_xor_sync(unsigned, T v, int, int = 32) {
     return v;
